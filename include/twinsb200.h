@@ -1,0 +1,148 @@
+/* twins-b200: the C ABI of the B200 packet-level simulator (libtwinsb200.so).
+ *
+ * The reference (TwiNS) exposes its TCP model only through the `twins` program: command-line
+ * flags (src/main.cu:155-222), flow files (src/main.cu:110-137), topology files
+ * (src/main.cu:227-252), worlds files (src/main.cu:283-325), and fct.csv
+ * (src/main.cu:1143-1153); its device boundary is one Sim struct in constant memory and the
+ * slot kernel ns_slot (src/kernel.cuh:5) captured into CUDA graphs (src/main.cu:1017-1049).
+ * This header replaces that boundary with plain C entry points; the `twins` front-end
+ * (twins_b200/csrc/twins_cli.cpp) reproduces the reference's command line over them.
+ *
+ * Conventions: every call returns an int status (TB_OK, a negative error, or TB_WARN_INEXACT);
+ * tb_last_error() describes the last failure of the calling thread. The caller owns every host
+ * buffer; the library owns device memory. No call exits the process. One context per host
+ * thread.
+ */
+#ifndef TWINSB200_H
+#define TWINSB200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TB_OK 0
+#define TB_WARN_INEXACT 1    /* a capacity overflowed or a tie was guessed: results may differ */
+#define TB_ERR_ARG (-1)      /* a bad argument or input (bad flows, topology, world id) */
+#define TB_ERR_CUDA (-2)     /* a CUDA call failed (no device, launch error) */
+#define TB_ERR_MEMORY (-3)   /* the batch exceeds the context's HBM budget */
+#define TB_ERR_STATE (-4)    /* a call out of order (e.g. results before a run) */
+#define TB_ERR_TIMEOUT (-5)  /* a device-side wait ran out (the run was abandoned) */
+
+#define TB_TOPO_FATTREE 0
+#define TB_TOPO_LEAFSPINE 1
+#define TB_TOPO_GRAPH 2
+
+#define TB_TCP_NEWRENO 0
+#define TB_TCP_DCTCP 1
+#define TB_TCP_CUBIC 2
+
+typedef struct tb_ctx tb_ctx;
+
+/* A world's topology. Replaces --k / --topo=leafspine --leaves --spines --hpl /
+ * --topo=graph --topofile --fail (reference src/main.cu:155-222, 223-465).
+ * FatTree: k (a power of two, 4..32). Leaf-spine: leaves, spines, hpl (hosts per leaf).
+ * Graph: n_hosts, n_switches and n_links links in file order, endpoints host h -> h and switch
+ * j -> -1 - j (a host's one link has the host first); link failures at fail_t_ns[i] of the first
+ * link between switches fail_a[i] and fail_b[i], down or (fail_up[i]) up again. */
+typedef struct tb_topology
+{
+    int kind;
+    int k;
+    int leaves, spines, hpl;
+    int n_hosts, n_switches, n_links;
+    const int *link_a, *link_b;
+    int n_fails;
+    const long long *fail_t_ns;
+    const int *fail_a, *fail_b, *fail_up;
+} tb_topology;
+
+/* A TCP world's parameters: --tcp --ecnK --queue --fin --spray --RngSeed --RngRun
+ * (reference src/main.cu:155-222; per-world values as a worlds file gives them, :283-325). */
+typedef struct tb_tcp_params
+{
+    int tcp;       /* TB_TCP_* */
+    int ecn_k;     /* RED MinTh = MaxTh (packets), default 30 */
+    int queue;     /* RED queue limit (packets), default 200 */
+    int fin;       /* senders close after their last flow */
+    int spray;     /* per-packet ECMP (MRG32k3a), else per-flow ECMP */
+    unsigned rng_seed;
+    unsigned long long rng_run;
+} tb_tcp_params;
+
+/* Run statistics of the last tb_run. */
+typedef struct tb_stats
+{
+    long long slots;         /* the slot reached (simulated time in us) */
+    long long slots_run;     /* slots executed (idle slots are skipped exactly) */
+    long long launches;      /* persistent-kernel launches */
+    double kernel_ms;        /* device time of the slot loop (CUDA events) */
+    double upload_ms;        /* host-to-device time of the batch (tb_prepare) */
+    unsigned long long packet_events; /* frame arrivals handled at hosts and switch ports */
+    unsigned long long host_events, switch_events;
+    unsigned long long host_sender_events; /* host arrivals handled by a connection's sender */
+    unsigned long long host_frames;        /* frames hosts emitted */
+    unsigned long long bytes_h2d, bytes_d2h;
+    int grid, host_lanes, warps_per_block;
+} tb_stats;
+
+/* A context on CUDA device `device`, admitting batches up to hbm_budget_bytes of device memory
+ * (0: no limit). Replaces the reference's implicit device set-up (src/main.cu:51-58). Device -1
+ * gives a host-only context: worlds can be added and their ECMP hashes read (tb_hashes), but
+ * tb_prepare / tb_run fail with TB_ERR_STATE. */
+int tb_ctx_create(int device, unsigned long long hbm_budget_bytes, tb_ctx **out);
+int tb_ctx_destroy(tb_ctx *ctx);
+const char *tb_last_error(void);
+
+/* Adds one TCP world (one simulation) to the context's batch and returns its id in *world.
+ * Flows are rows of a flow file (reference src/main.cu:110-137, 531-648): src, dst, size
+ * (bytes), start_ns, and conn (NULL or -1: a connection of its own; rows with the same conn are
+ * messages of one persistent connection, same hosts, later starts). hash_data / hash_ack: NULL
+ * (the library computes ns-3's ECMP hashes, src/main.cu:674-723) or per-row hashes as
+ * --ecmp_from takes them from an ns-3 output (src/main.cu:724-768). Worlds of one batch may
+ * differ in topology and every parameter (the reference batches one topology only,
+ * src/main.cu:267-270). */
+int tb_world_add_tcp(tb_ctx *ctx, const tb_topology *topo, int n_flows, const int *src, const int *dst,
+                     const long long *size, const long long *start_ns, const long long *conn,
+                     const unsigned *hash_data, const unsigned *hash_ack, const tb_tcp_params *params, int *world);
+
+/* Builds the batch's device state (routes, connections, rings) and uploads it. Called by
+ * tb_run when needed; separate so that timing can exclude it. Replaces src/main.cu:807-1015. */
+int tb_prepare(tb_ctx *ctx);
+
+/* Restores every world of the prepared batch to its initial state (device-to-device). */
+int tb_reset(tb_ctx *ctx);
+
+/* Runs every world of the batch until all of its flows complete or max_slots slots (1 us each)
+ * have passed (0: the reference's default, 2,000,000). Replaces the graph loop of
+ * src/main.cu:1017-1049 and the slot kernel src/kernel.cuh:5-113. Returns TB_WARN_INEXACT if a
+ * capacity overflowed or an event-order tie was guessed (reference warnings, src/main.cu:1070-1075). */
+int tb_run(tb_ctx *ctx, long long max_slots);
+
+/* Per flow row (file order) of a world: established_ns and completed_ns (-1: not reached), the
+ * columns of fct.csv (src/main.cu:1143-1153). */
+int tb_results(tb_ctx *ctx, int world, long long *established_ns, long long *completed_ns);
+
+/* Counters of a world (n <= 16): drops, marks, retransmissions, RTOs, undecided ties, host
+ * packet-events, switch packet-events, overflow counts (active lists, timers, rings,
+ * out-of-order blocks, tx-cap), barrier timeouts, sender-side host packet-events, frames hosts
+ * emitted (reference counters, src/main.cu:1064-1075). */
+int tb_counters(tb_ctx *ctx, int world, unsigned long long *out, int n);
+
+/* Per flow row of a world: the ECMP hashes in use (reference --hash_check, src/main.cu:755-768). */
+int tb_hashes(tb_ctx *ctx, int world, unsigned *hash_data, unsigned *hash_ack);
+
+/* Statistics of the last run. */
+int tb_get_stats(tb_ctx *ctx, tb_stats *out);
+
+/* Launch shape: hosts per warp (1..32) and the grid (0: chosen from occupancy). */
+int tb_set_launch(tb_ctx *ctx, int host_lanes, int grid);
+
+/* sizeof(tb_topology), sizeof(tb_tcp_params), sizeof(tb_stats) in out[0..n-1], so that bindings
+ * in other languages can check their struct layouts (no counterpart in the reference). */
+int tb_abi_sizes(unsigned long long *out, int n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

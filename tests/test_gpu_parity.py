@@ -1,0 +1,122 @@
+"""Parity of the CUDA path (through the C ABI) on a B200.
+
+- every golden case: each flow's established / completed time bit-exact with sequential ns-3
+  (the stored outputs the reference and the oracle equal);
+- batching: many golden worlds of different topologies and TCPs in one launch, each equal to
+  its standalone result;
+- seeded synthetic workloads of the benchmark shapes (FatTree k=4 C1; a reduced k=8 C2 with
+  FIN, spraying and persistent connections, per TCP) against the CPU oracle, bit-exact;
+- run statistics: the packet-event count equals the oracle's.
+"""
+import csv
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, manifest
+from twins_b200 import api, workloads
+
+pytestmark = pytest.mark.gpu
+
+CASES = manifest()
+
+
+def ns3(case):
+    with open(GOLDEN / case["ns3"]) as f:
+        rows = list(csv.reader(f))[1:]
+    return np.array([int(r[4]) for r in rows]), np.array([int(r[5]) for r in rows])
+
+
+def world_of(case):
+    topo = api.Topology.from_args(case["args"], base=GOLDEN)
+    flows = api.Flows.load(GOLDEN / case["flows"], topo.hosts)
+    return topo, flows, api.TcpParams.from_args(case["args"], case["tcp"])
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: c["name"])
+def test_golden_case_bit_exact(native_lib, case):
+    topo, flows, params = world_of(case)
+    est, done, ctr, stats = api.run_world(topo, flows, params)
+    want_est, want_done = ns3(case)
+    bad = np.nonzero((est != want_est) | (done != want_done))[0]
+    assert len(bad) == 0, f"{len(bad)} of {len(flows)} flows differ, first row {bad[0]}"
+    assert ctr["ovf_active"] + ctr["ovf_due"] + ctr["ovf_ring"] + ctr["ovf_ooo"] + ctr["ovf_tx"] == 0
+    assert stats["packet_events"] > 0
+
+
+def test_batch_equals_standalone(native_lib):
+    """Worlds of different topologies (FatTree, leaf-spine, Jellyfish with failures, Dragonfly)
+    and TCPs in one batch: each equal to ns-3 (as standalone)."""
+    picks = [c for c in CASES if c["workload"] not in ("k8_a2a50s", "k16_a2a30")][::3]
+    with api.Simulator() as sim:
+        ids = [sim.add_world(*world_of(c)) for c in picks]
+        sim.run()
+        for c, w in zip(picks, ids):
+            est, done = sim.results(w)
+            want_est, want_done = ns3(c)
+            assert (est == want_est).all() and (done == want_done).all(), c["name"]
+
+
+def oracle_run(oracle_bin, tmp_path, w, extra=()):
+    path = tmp_path / f"{w.name}.csv"
+    w.flows.write_csv(path)
+    out = tmp_path / f"{w.name}.out.csv"
+    topo = [f"--k={w.topo.k}"] if w.topo.kind == api.TOPO_FATTREE else \
+        [f"--topo=leafspine", f"--leaves={w.topo.leaves}", f"--spines={w.topo.spines}", f"--hpl={w.topo.hpl}"]
+    p = w.params
+    cmd = [str(oracle_bin), *topo, f"--flows={path}", f"--out={out}", f"--tcp={p.tcp}", f"--ecnK={p.ecn_k}", f"--queue={p.queue}",
+           f"--fin={int(p.fin)}", f"--spray={int(p.spray)}", f"--RngSeed={p.rng_seed}", f"--RngRun={p.rng_run}", *extra]
+    r = subprocess.run(cmd, capture_output=True, text=True, check=True)
+    with open(out) as f:
+        rows = list(csv.reader(f))[1:]
+    events = int(r.stdout.split(" events ")[1].split()[0])
+    return np.array([int(x[4]) for x in rows]), np.array([int(x[5]) for x in rows]), events
+
+
+def test_c1_equals_oracle(native_lib, oracle_bin, tmp_path):
+    w = workloads.c1()[0]
+    want_est, want_done, events = oracle_run(oracle_bin, tmp_path, w)
+    est, done, ctr, stats = api.run_world(w.topo, w.flows, w.params)
+    assert (est == want_est).all() and (done == want_done).all()
+    assert (done >= 0).all()
+    assert stats["packet_events"] == events
+
+
+@pytest.mark.parametrize("tcp", ["newreno", "dctcp", "cubic"])
+def test_c2_reduced_equals_oracle(native_lib, oracle_bin, tmp_path, tcp):
+    """The C2 shape (k=8, web-search-like sizes, persistent connections, FIN, spraying) at 1,500
+    messages, per TCP."""
+    flows = workloads.c2_flows(seed=3, n_msgs=1500)
+    w = workloads.World(f"c2r_{tcp}", api.Topology.fattree(8), flows,
+                        api.TcpParams(tcp, 30, 200, fin=True, spray=True, rng_seed=1, rng_run=1))
+    want_est, want_done, events = oracle_run(oracle_bin, tmp_path, w)
+    est, done, ctr, stats = api.run_world(w.topo, w.flows, w.params)
+    assert (est == want_est).all() and (done == want_done).all()
+    assert stats["packet_events"] == events
+
+
+def test_repeated_runs_identical(native_lib):
+    """tb_reset restores the initial state: a second run gives the same results and counts."""
+    case = next(c for c in CASES if c["name"] == "k8_a2a30_cubic_spray")
+    with api.Simulator() as sim:
+        w = sim.add_world(*world_of(case))
+        sim.run()
+        a = sim.results(w)
+        ea = sim.stats()["packet_events"]
+        sim.run()
+        b = sim.results(w)
+        assert (a[0] == b[0]).all() and (a[1] == b[1]).all()
+        assert sim.stats()["packet_events"] == ea
+
+
+def test_max_slots_stops_early(native_lib):
+    """max_slots ends the run at that simulated time; unfinished flows read -1."""
+    w = workloads.c1()[0]
+    with api.Simulator() as sim:
+        i = sim.add_world(w.topo, w.flows, w.params)
+        sim.run(max_slots=300)
+        est, done = sim.results(i)
+        st = sim.stats()
+        assert st["slots"] <= 300
+        assert (done == -1).any()

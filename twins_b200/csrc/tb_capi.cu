@@ -1,0 +1,1153 @@
+// twins-b200: the C ABI (include/twinsb200.h): batches of worlds, their device state, the run.
+// World set-up restates the reference's driver (src/main.cu:223-1015): topologies and routes,
+// messages over connections, ns-3's ECMP hashes, the order of application events, link wiring.
+#include "tb_kernel.h"
+#include "tb_state.cuh"
+#include "../../include/twinsb200.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+using namespace tb;
+
+namespace
+{
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg)
+{
+    g_err = msg;
+    return code;
+}
+
+// ------------------------------------------------------------------ MRG32k3a stream seeding
+typedef unsigned __int128 u128;
+struct M3
+{
+    uint64_t a[3][3];
+};
+M3 mmul(const M3 &x, const M3 &y, uint64_t m)
+{
+    M3 r;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++)
+        {
+            u128 v = 0;
+            for (int t = 0; t < 3; t++)
+                v += (u128)x.a[i][t] * y.a[t][j] % m;
+            r.a[i][j] = (uint64_t)(v % m);
+        }
+    return r;
+}
+void mvec(const M3 &x, uint64_t v[3], uint64_t m)
+{
+    uint64_t r[3];
+    for (int i = 0; i < 3; i++)
+    {
+        u128 s = 0;
+        for (int t = 0; t < 3; t++)
+            s += (u128)x.a[i][t] * v[t] % m;
+        r[i] = (uint64_t)(s % m);
+    }
+    memcpy(v, r, sizeof r);
+}
+// the state of ns-3 stream SetStream(stream) under RngSeed seed and RngRun run: the seed vector
+// advanced by A^((2^63 + stream) 2^127 + run 2^76) (RngStream's AdvanceNthBy)
+struct RngPowers
+{
+    M3 p127[64], p76[64];
+    uint64_t m;
+    RngPowers(const M3 &a, uint64_t m_) : m(m_)
+    {
+        M3 x = a;
+        for (int i = 0; i < 76; i++)
+            x = mmul(x, x, m);
+        for (int b = 0; b < 64; b++)
+        {
+            p76[b] = x;
+            x = mmul(x, x, m);
+        }
+        x = a;
+        for (int i = 0; i < 127; i++)
+            x = mmul(x, x, m);
+        for (int b = 0; b < 64; b++)
+        {
+            p127[b] = x;
+            x = mmul(x, x, m);
+        }
+    }
+    void advance(uint64_t nth, bool by127, uint64_t v[3]) const
+    {
+        for (int b = 0; b < 64; b++)
+            if ((nth >> b) & 1)
+                mvec(by127 ? p127[b] : p76[b], v, m);
+    }
+};
+Rng stream_state(uint32_t seed, uint64_t stream, uint64_t run)
+{
+    const uint64_t m1 = 4294967087ull, m2 = 4294944443ull;
+    static const RngPowers P1({{{0, 1, 0}, {0, 0, 1}, {m1 - 810728, 1403580, 0}}}, m1);
+    static const RngPowers P2({{{0, 1, 0}, {0, 0, 1}, {m2 - 1370589, 0, 527612}}}, m2);
+    uint64_t v1[3] = {seed, seed, seed}, v2[3] = {seed, seed, seed};
+    uint64_t target = (1ull << 63) + stream;
+    P1.advance(target, true, v1);
+    P2.advance(target, true, v2);
+    P1.advance(run, false, v1);
+    P2.advance(run, false, v2);
+    Rng r;
+    for (int i = 0; i < 3; i++)
+    {
+        r.s[i] = (double)v1[i];
+        r.s[3 + i] = (double)v2[i];
+    }
+    return r;
+}
+
+// ------------------------------------------------------------------ a world on the host
+struct FlowRow
+{
+    int src, dst;
+    long long size, start_ns, conn;
+};
+
+struct HostWorld
+{
+    // inputs
+    tb_topology topo;
+    std::vector<int> link_a, link_b, fail_a, fail_b, fail_up;
+    std::vector<long long> fail_t;
+    std::vector<FlowRow> rows;
+    std::vector<uint32_t> given_hd, given_ha;
+    tb_tcp_params p;
+    // derived
+    int kind = 0, k = 0, hk = 0, H1 = 0, S1 = 0, ecmp_n = 1, leaves = 0, spines = 0, hpl = 0;
+    std::vector<int> host_sw, host_port;
+    std::vector<uint32_t> rt_off;
+    std::vector<uint8_t> rt_n, rt_ports, port_dn;
+    std::vector<int64_t> fail_ps;
+    std::vector<int> host_in_port;  // world-local: the port (switch*k + p) the host hangs off
+    std::vector<int> port_in;       // [S1*k]: the arriving link: host h (>= 0) or -2 - (switch*k + p), -1 unused
+    // connections and messages (world-local)
+    std::vector<std::vector<int>> conn_rows;
+    std::vector<int> row_conn, row_msg;
+    std::vector<uint32_t> hash_data, hash_ack; // per connection
+    std::vector<int> pend;                     // messages in each host's event order
+    std::vector<int> pend_first;               // [H1 + 1]
+    std::vector<int> msg_row;                  // message -> row
+    std::vector<uint64_t> conn_bytes;
+    // global offsets
+    int host0 = 0, sw0 = 0, port0 = 0, conn0 = 0, msg0 = 0;
+};
+
+bool build_topology(HostWorld &w, std::string &err)
+{
+    const tb_topology &T = w.topo;
+    w.kind = T.kind;
+    std::vector<std::vector<std::pair<int, int>>> adj;
+    if (T.kind == TB_TOPO_GRAPH)
+    {
+        w.H1 = T.n_hosts;
+        w.S1 = T.n_switches;
+        if (w.H1 < 1 || w.S1 < 1)
+        {
+            err = "a topology file needs hosts and switches";
+            return false;
+        }
+        std::vector<int> deg(w.S1, 0);
+        w.host_sw.assign(w.H1, -1);
+        w.host_port.assign(w.H1, 0);
+        adj.assign(w.S1, {});
+        for (size_t i = 0; i < w.link_a.size(); i++)
+        {
+            int a = w.link_a[i], b = w.link_b[i];
+            if (b >= 0 || (a >= 0 && (a >= w.H1 || w.host_sw[a] >= 0)) || -1 - b >= w.S1 || (a < 0 && -1 - a >= w.S1))
+            {
+                err = "hosts need exactly one link, as its first endpoint";
+                return false;
+            }
+            int sb = -1 - b, pb = deg[sb]++;
+            if (a >= 0)
+            {
+                w.host_sw[a] = sb;
+                w.host_port[a] = pb;
+            }
+            else
+            {
+                int sa = -1 - a, pa = deg[sa]++;
+                adj[sa].push_back({pa, sb});
+                adj[sb].push_back({pb, sa});
+            }
+        }
+        for (int h = 0; h < w.H1; h++)
+            if (w.host_sw[h] < 0)
+            {
+                err = "host " + std::to_string(h) + " has no link";
+                return false;
+            }
+        w.k = 0;
+        for (int d : deg)
+            w.k = std::max(w.k, d);
+        if (w.k > 32)
+        {
+            err = "a switch has more than 32 ports";
+            return false;
+        }
+        struct F
+        {
+            int64_t t;
+            int a, pa, b, pb;
+            bool up;
+        };
+        std::vector<F> fails;
+        for (size_t i = 0; i < w.fail_t.size(); i++)
+        {
+            F x{(int64_t)w.fail_t[i] * 1000, w.fail_a[i], -1, w.fail_b[i], -1, w.fail_up[i] != 0};
+            if (x.a < 0 || x.a >= w.S1 || x.b < 0 || x.b >= w.S1)
+            {
+                err = "--fail: no such switch";
+                return false;
+            }
+            for (auto &pn : adj[x.a])
+                if (pn.second == x.b && x.pa < 0)
+                    x.pa = pn.first;
+            for (auto &pn : adj[x.b])
+                if (pn.second == x.a && x.pb < 0)
+                    x.pb = pn.first;
+            if (x.pa < 0)
+            {
+                err = "--fail: no link between the switches";
+                return false;
+            }
+            fails.push_back(x);
+        }
+        std::stable_sort(fails.begin(), fails.end(), [](const F &x, const F &y) { return x.t < y.t; });
+        const int NE = (int)fails.size() + 1, S = w.S1, k = w.k;
+        for (auto &x : fails)
+            w.fail_ps.push_back(x.t);
+        w.rt_off.assign((size_t)NE * S * S, 0);
+        w.rt_n.assign((size_t)NE * S * S, 0);
+        w.port_dn.assign((size_t)NE * S * k, 0);
+        std::vector<uint8_t> dn((size_t)S * k, 0);
+        for (int ep = 0; ep < NE; ep++)
+        {
+            if (ep > 0)
+            {
+                const F &x = fails[ep - 1];
+                dn[(size_t)x.a * k + x.pa] = dn[(size_t)x.b * k + x.pb] = x.up ? 0 : 1;
+            }
+            std::copy(dn.begin(), dn.end(), w.port_dn.begin() + (size_t)ep * S * k);
+            // shortest paths (hops) to each switch; equal-cost ports towards a closer neighbour
+            // in interface order, as Ipv4GlobalRouting installs them (src/main.cu:420-456)
+            for (int e = 0; e < S; e++)
+            {
+                std::vector<int> dist(S, -1), todo{e};
+                dist[e] = 0;
+                for (size_t i = 0; i < todo.size(); i++)
+                    for (auto &pn : adj[todo[i]])
+                        if (!dn[(size_t)todo[i] * k + pn.first] && dist[pn.second] < 0)
+                        {
+                            dist[pn.second] = dist[todo[i]] + 1;
+                            todo.push_back(pn.second);
+                        }
+                for (int x = 0; x < S; x++)
+                {
+                    if (x == e)
+                        continue;
+                    if (dist[x] < 0)
+                    {
+                        err = "switch " + std::to_string(x) + " cannot reach switch " + std::to_string(e);
+                        return false;
+                    }
+                    std::vector<int> pts;
+                    for (auto &pn : adj[x])
+                        if (!dn[(size_t)x * k + pn.first] && dist[pn.second] == dist[x] - 1)
+                            pts.push_back(pn.first);
+                    std::sort(pts.begin(), pts.end());
+                    size_t r = ((size_t)ep * S + x) * S + e;
+                    w.rt_off[r] = (uint32_t)w.rt_ports.size();
+                    w.rt_n[r] = (uint8_t)pts.size();
+                    for (int q : pts)
+                        w.rt_ports.push_back((uint8_t)q);
+                }
+            }
+        }
+        w.ecmp_n = 1;
+    }
+    else if (T.kind == TB_TOPO_LEAFSPINE)
+    {
+        w.leaves = T.leaves, w.spines = T.spines, w.hpl = T.hpl;
+        if (w.leaves < 1 || w.spines < 1 || w.hpl < 1 || std::max(w.hpl + w.spines, w.leaves) > 32 || w.leaves * w.hpl > 65535)
+        {
+            err = "leaf-spine: max(hpl + spines, leaves) <= 32";
+            return false;
+        }
+        w.k = std::max(w.hpl + w.spines, w.leaves);
+        w.H1 = w.leaves * w.hpl;
+        w.S1 = w.leaves + w.spines;
+        w.ecmp_n = w.spines;
+    }
+    else if (T.kind == TB_TOPO_FATTREE)
+    {
+        int k = T.k;
+        if (k < 4 || k > 32 || (k & (k - 1)))
+        {
+            err = "FatTree k: a power of two, 4..32";
+            return false;
+        }
+        w.k = k;
+        w.H1 = k * k * k / 4;
+        w.S1 = k * k + k * k / 4;
+        w.ecmp_n = k / 2;
+    }
+    else
+    {
+        err = "unknown topology kind";
+        return false;
+    }
+    if (w.H1 > 65535)
+    {
+        err = "a world has more than 65535 hosts";
+        return false;
+    }
+    w.hk = w.k / 2;
+    // wiring (src/main.cu:870-945): which link arrives at each host and port
+    const int k = w.k, hk = w.hk;
+    w.host_in_port.assign(w.H1, -1);
+    w.port_in.assign((size_t)w.S1 * k, -1);
+    auto port_of = [&](int sw, int p) { return sw * k + p; };
+    auto from_port = [&](int sw, int p) { return -2 - port_of(sw, p); };
+    if (w.kind == TB_TOPO_GRAPH)
+    {
+        for (int h = 0; h < w.H1; h++)
+        {
+            w.host_in_port[h] = port_of(w.host_sw[h], w.host_port[h]);
+            w.port_in[port_of(w.host_sw[h], w.host_port[h])] = h;
+        }
+        for (int x = 0; x < w.S1; x++)
+            for (auto &pn : adj[x])
+            {
+                int y = pn.second, nth = 0;
+                for (auto &q : adj[x])
+                    if (q.second == y && q.first < pn.first)
+                        nth++;
+                for (auto &q : adj[y])
+                    if (q.second == x && nth-- == 0)
+                    {
+                        w.port_in[port_of(x, pn.first)] = from_port(y, q.first);
+                        break;
+                    }
+            }
+    }
+    else if (w.kind == TB_TOPO_LEAFSPINE)
+    {
+        for (int h = 0; h < w.H1; h++)
+        {
+            int l = h / w.hpl, q = h % w.hpl;
+            w.host_in_port[h] = port_of(l, q);
+            w.port_in[port_of(l, q)] = h;
+        }
+        for (int l = 0; l < w.leaves; l++)
+            for (int j = 0; j < w.spines; j++)
+            {
+                int sp = w.leaves + j;
+                w.port_in[port_of(l, w.hpl + j)] = from_port(sp, l);
+                w.port_in[port_of(sp, l)] = from_port(l, w.hpl + j);
+            }
+    }
+    else
+    {
+        const int E = k * hk;
+        for (int h = 0; h < w.H1; h++)
+        {
+            int e = h / hk, q = h % hk;
+            w.host_in_port[h] = port_of(e, q);
+            w.port_in[port_of(e, q)] = h;
+        }
+        for (int pod = 0; pod < k; pod++)
+            for (int j = 0; j < hk; j++)
+            {
+                int agg = E + pod * hk + j;
+                for (int x = 0; x < hk; x++)
+                {
+                    int e2 = pod * hk + x;
+                    w.port_in[port_of(agg, x)] = from_port(e2, j + hk);
+                    w.port_in[port_of(e2, j + hk)] = from_port(agg, x);
+                }
+            }
+        for (int i = 0; i < hk; i++)
+            for (int j = 0; j < hk; j++)
+            {
+                int core = k * k + i * hk + j;
+                for (int pod = 0; pod < k; pod++)
+                {
+                    int agg = E + pod * hk + i;
+                    w.port_in[port_of(core, pod)] = from_port(agg, j + hk);
+                    w.port_in[port_of(agg, j + hk)] = from_port(core, pod);
+                }
+            }
+    }
+    return true;
+}
+
+bool build_flows(HostWorld &w, std::string &err)
+{
+    const int M = (int)w.rows.size(), H = w.H1;
+    std::map<long long, int> by_id;
+    w.row_conn.assign(M, -1);
+    for (int i = 0; i < M; i++)
+    {
+        const FlowRow &r = w.rows[i];
+        if (r.src < 0 || r.src >= H || r.dst < 0 || r.dst >= H || r.src == r.dst || r.size < 0)
+        {
+            err = "flow row " + std::to_string(i) + ": hosts out of range";
+            return false;
+        }
+        int c;
+        if (r.conn < 0 || !by_id.count(r.conn))
+        {
+            c = (int)w.conn_rows.size();
+            w.conn_rows.push_back({});
+            if (r.conn >= 0)
+                by_id[r.conn] = c;
+        }
+        else
+        {
+            c = by_id[r.conn];
+            const FlowRow &first = w.rows[w.conn_rows[c][0]];
+            if (first.src != r.src || first.dst != r.dst || r.start_ns < w.rows[w.conn_rows[c].back()].start_ns)
+            {
+                err = "the flows of connection " + std::to_string(r.conn) + " need the same hosts and later starts";
+                return false;
+            }
+        }
+        w.conn_rows[c].push_back(i);
+        w.row_conn[i] = c;
+    }
+    const int F = (int)w.conn_rows.size();
+    w.row_msg.assign(M, -1);
+    w.msg_row.clear();
+    w.conn_bytes.assign(F, 0);
+    for (int c = 0; c < F; c++)
+        for (int i : w.conn_rows[c])
+        {
+            w.row_msg[i] = (int)w.msg_row.size();
+            w.msg_row.push_back(i);
+            w.conn_bytes[c] += (uint64_t)w.rows[i].size;
+            if (w.conn_bytes[c] >= 0xFFFFFFFFull)
+            {
+                err = "a connection carries 4 GB or more";
+                return false;
+            }
+        }
+    // application events per host in ns-3's order: message writes before starts at equal times
+    // (src/main.cu:590-612)
+    std::vector<int> byrow(M);
+    for (int i = 0; i < M; i++)
+        byrow[i] = i;
+    auto is_first = [&](int i) { return w.conn_rows[w.row_conn[i]][0] == i; };
+    std::stable_sort(byrow.begin(), byrow.end(), [&](int a, int b) {
+        const FlowRow &x = w.rows[a], &y = w.rows[b];
+        if (x.src != y.src)
+            return x.src < y.src;
+        if (x.start_ns != y.start_ns)
+            return x.start_ns < y.start_ns;
+        bool fa = is_first(a), fb = is_first(b);
+        if (fa != fb)
+            return !fa;
+        return fa ? w.row_conn[a] < w.row_conn[b] : a < b;
+    });
+    w.pend.resize(M);
+    w.pend_first.assign(H + 1, 0);
+    for (int i = 0; i < M; i++)
+        w.pend[i] = w.row_msg[byrow[i]];
+    {
+        int i = 0;
+        for (int h = 0; h < H; h++)
+        {
+            w.pend_first[h] = i;
+            while (i < M && w.rows[byrow[i]].src == h)
+                i++;
+        }
+        w.pend_first[H] = i;
+    }
+    // ECMP hashes (src/main.cu:674-723)
+    std::vector<int> hsub(H);
+    for (int h = 0; h < H; h++)
+        hsub[h] = h;
+    if (w.kind == TB_TOPO_GRAPH)
+        for (size_t i = 0; i < w.link_a.size(); i++)
+            if (w.link_a[i] >= 0)
+                hsub[w.link_a[i]] = (int)i;
+    auto ip = [&](int h) { return 0x0a000001u | (uint32_t)(hsub[h] & 0xFFFF) << 8; };
+    std::vector<int> byhost(F);
+    for (int c = 0; c < F; c++)
+        byhost[c] = c;
+    std::stable_sort(byhost.begin(), byhost.end(), [&](int a, int b) {
+        const FlowRow &x = w.rows[w.conn_rows[a][0]], &y = w.rows[w.conn_rows[b][0]];
+        return x.src != y.src ? x.src < y.src : x.start_ns < y.start_ns;
+    });
+    w.hash_data.assign(F, 0);
+    w.hash_ack.assign(F, 0);
+    const bool given = !w.given_hd.empty();
+    for (int i = 0, n = 0; i < F; i++, n++)
+    {
+        const int c = byhost[i];
+        const int src = w.rows[w.conn_rows[c][0]].src, dst = w.rows[w.conn_rows[c][0]].dst;
+        if (i > 0 && w.rows[w.conn_rows[byhost[i - 1]][0]].src != src)
+            n = 0;
+        if (n > 65535 - 49153 && !given)
+        {
+            err = "a host binds more than 16382 connections: give the hashes";
+            return false;
+        }
+        const uint16_t sport = (uint16_t)(49153 + n), dport = 1000;
+        w.hash_data[c] = flow_hash(ip(src), ip(dst), sport, dport);
+        w.hash_ack[c] = flow_hash(ip(dst), ip(src), dport, sport);
+    }
+    if (given)
+        for (int i = 0; i < M; i++)
+            if (is_first(i))
+            {
+                w.hash_data[w.row_conn[i]] = w.given_hd[i];
+                w.hash_ack[w.row_conn[i]] = w.given_ha[i];
+            }
+    return true;
+}
+
+template <typename T>
+struct DevBuf
+{
+    T *p = nullptr;
+    size_t n = 0;
+};
+
+} // namespace
+
+// ------------------------------------------------------------------ the context
+struct tb_ctx
+{
+    int device = 0;
+    unsigned long long budget = 0;
+    std::vector<HostWorld> worlds;
+    bool prepared = false, ran = false;
+    int host_lanes = 1, grid_req = 0, grid = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    Sim sim{};
+    std::vector<void *> allocs;
+    size_t dev_bytes = 0;
+    // pristine copies of the mutable state, for tb_reset
+    struct Snap
+    {
+        void *dst, *src;
+        size_t bytes;
+    };
+    std::vector<Snap> snaps;
+    std::vector<MsgRec> host_msgs;
+    std::vector<unsigned long long> ev_w;
+    tb_stats stats{};
+    int max_slots_per_launch = 4096;
+
+    ~tb_ctx() { release(); }
+    void release()
+    {
+        for (void *p : allocs)
+            cudaFree(p);
+        allocs.clear();
+        snaps.clear();
+        dev_bytes = 0;
+        prepared = false;
+    }
+    template <typename T>
+    int alloc(T **p, size_t n, bool snapshot)
+    {
+        size_t bytes = sizeof(T) * std::max<size_t>(n, 1);
+        if (budget && dev_bytes + bytes * (snapshot ? 2 : 1) > budget)
+            return fail(TB_ERR_MEMORY, "the batch needs more than the context's HBM budget");
+        void *d = nullptr;
+        if (cudaMalloc(&d, bytes) != cudaSuccess)
+            return fail(TB_ERR_CUDA, "cudaMalloc failed");
+        allocs.push_back(d);
+        dev_bytes += bytes;
+        cudaMemset(d, 0, bytes);
+        *p = (T *)d;
+        if (snapshot)
+        {
+            void *s = nullptr;
+            if (cudaMalloc(&s, bytes) != cudaSuccess)
+                return fail(TB_ERR_CUDA, "cudaMalloc failed");
+            allocs.push_back(s);
+            dev_bytes += bytes;
+            snaps.push_back({d, s, bytes});
+        }
+        return TB_OK;
+    }
+    template <typename T>
+    int upload(T **p, const std::vector<T> &v, bool snapshot)
+    {
+        int r = alloc(p, v.size(), snapshot);
+        if (r)
+            return r;
+        if (!v.empty() && cudaMemcpy(*p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+            return fail(TB_ERR_CUDA, "cudaMemcpy failed");
+        stats.bytes_h2d += sizeof(T) * v.size();
+        return TB_OK;
+    }
+};
+
+namespace
+{
+int prepare(tb_ctx *c)
+{
+    if (c->prepared)
+        return TB_OK;
+    if (c->worlds.empty())
+        return fail(TB_ERR_STATE, "no worlds");
+    if (c->device < 0)
+        return fail(TB_ERR_STATE, "a host-only context (device -1) cannot run");
+    if (cudaSetDevice(c->device) != cudaSuccess)
+        return fail(TB_ERR_CUDA, "cudaSetDevice failed");
+    auto t0 = std::chrono::steady_clock::now();
+    c->stats.bytes_h2d = 0;
+    const int W = (int)c->worlds.size();
+    int H = 0, S = 0, P = 0, C = 0, M = 0, kmax = 0, ring = 0;
+    for (HostWorld &w : c->worlds)
+    {
+        w.host0 = H;
+        w.sw0 = S;
+        w.port0 = P;
+        w.conn0 = C;
+        w.msg0 = M;
+        H += w.H1;
+        S += w.S1;
+        P += w.S1 * w.k;
+        C += (int)w.conn_rows.size();
+        M += (int)w.rows.size();
+        kmax = std::max(kmax, w.k);
+        ring = std::max(ring, w.p.queue + 2);
+    }
+    Sim &s = c->sim;
+    s = Sim{};
+    s.W = W;
+    s.H = H;
+    s.S = S;
+    s.P = P;
+    s.L = H + P;
+    s.C = C;
+    s.M = M;
+    s.ring = ring;
+    s.kmax = kmax;
+    // worlds (graph tables uploaded per world)
+    std::vector<WorldDesc> wd(W);
+    for (int i = 0; i < W; i++)
+    {
+        HostWorld &w = c->worlds[i];
+        WorldDesc &d = wd[i];
+        memset(&d, 0, sizeof d);
+        d.kind = w.kind;
+        d.k = w.k;
+        d.hk = w.hk;
+        d.leaves = w.leaves;
+        d.spines = w.spines;
+        d.hpl = w.hpl;
+        d.ecmp_n = w.ecmp_n;
+        d.H1 = w.H1;
+        d.S1 = w.S1;
+        d.host0 = w.host0;
+        d.sw0 = w.sw0;
+        d.conn0 = w.conn0;
+        d.msg0 = w.msg0;
+        d.n_msgs = (int)w.rows.size();
+        d.cc = (uint8_t)w.p.tcp;
+        d.fin = (uint8_t)(w.p.fin != 0);
+        d.spray = (uint8_t)(w.p.spray != 0);
+        d.red_k = w.p.ecn_k;
+        d.qcap = w.p.queue;
+        if (w.kind == TB_TOPO_GRAPH)
+        {
+            int *hsw;
+            uint8_t *hp, *rn, *rp, *pd;
+            uint32_t *ro;
+            int64_t *ft;
+            std::vector<uint8_t> hport(w.host_port.begin(), w.host_port.end());
+            int r;
+            if ((r = c->upload(&hsw, w.host_sw, false)) || (r = c->upload(&hp, hport, false)) || (r = c->upload(&ro, w.rt_off, false)) ||
+                (r = c->upload(&rn, w.rt_n, false)) || (r = c->upload(&rp, w.rt_ports, false)) || (r = c->upload(&pd, w.port_dn, false)) ||
+                (r = c->upload(&ft, w.fail_ps, false)))
+                return r;
+            d.host_sw = hsw;
+            d.host_port = hp;
+            d.rt_off = ro;
+            d.rt_n = rn;
+            d.rt_ports = rp;
+            d.port_dn = pd;
+            d.fail_t = ft;
+            d.n_fail = (int)w.fail_ps.size();
+        }
+    }
+    // hosts, switches, ports
+    std::vector<HostRec> hosts(H);
+    std::vector<SwRec> sws(S);
+    std::vector<PortRec> ports(P);
+    std::vector<int> pend(M);
+    int max_snd = 1, max_rcv = 1;
+    for (int i = 0; i < W; i++)
+    {
+        HostWorld &w = c->worlds[i];
+        std::vector<int> nsnd(w.H1, 0), nrcv(w.H1, 0);
+        for (auto &cr : w.conn_rows)
+        {
+            nsnd[w.rows[cr[0]].src]++;
+            nrcv[w.rows[cr[0]].dst]++;
+        }
+        for (int h = 0; h < w.H1; h++)
+        {
+            max_snd = std::max(max_snd, nsnd[h]);
+            max_rcv = std::max(max_rcv, nrcv[h]);
+            HostRec &hr = hosts[w.host0 + h];
+            memset(&hr, 0, sizeof hr);
+            hr.world = i;
+            hr.local = h;
+            hr.wake = 0; // every host runs the first slot
+            hr.pend_next = w.msg0 + w.pend_first[h];
+            hr.pend_end = w.msg0 + w.pend_first[h + 1];
+            hr.in_link = H + w.port0 + w.host_in_port[h];
+        }
+        for (int j = 0; j < M && j < (int)w.pend.size(); j++)
+            ;
+        for (size_t j = 0; j < w.pend.size(); j++)
+            pend[w.msg0 + j] = w.msg0 + w.pend[j];
+        for (int x = 0; x < w.S1; x++)
+        {
+            SwRec &sr = sws[w.sw0 + x];
+            sr.world = i;
+            sr.local = x;
+            sr.port0 = w.port0 + x * w.k;
+            sr.k = w.k;
+            for (int q = 0; q < w.k; q++)
+            {
+                PortRec &pr = ports[w.port0 + x * w.k + q];
+                memset(&pr, 0, sizeof pr);
+                pr.red_k = w.p.ecn_k;
+                pr.qcap = w.p.queue;
+                int src = w.port_in[(size_t)x * w.k + q];
+                pr.in_link = src >= 0 ? w.host0 + src : src == -1 ? -1 : H + w.port0 + (-2 - src);
+            }
+        }
+    }
+    s.act_cap = std::max(max_snd, max_rcv);
+    // connections and messages
+    std::vector<SndRec> snd(C);
+    std::vector<RcvRec> rcv(C);
+    std::vector<MsgRec> msgs(M);
+    uint64_t it_total = 0, oo_total = 0;
+    for (int i = 0; i < W; i++)
+    {
+        HostWorld &w = c->worlds[i];
+        const int F = (int)w.conn_rows.size();
+        for (int cc = 0; cc < F; cc++)
+        {
+            const auto &cr = w.conn_rows[cc];
+            const FlowRow &first = w.rows[cr[0]];
+            SndRec &S_ = snd[w.conn0 + cc];
+            RcvRec &R = rcv[w.conn0 + cc];
+            memset(&S_, 0, sizeof S_);
+            memset(&R, 0, sizeof R);
+            S_.world = R.world = i;
+            S_.src_local = R.src_local = first.src;
+            S_.dst_local = R.dst_local = first.dst;
+            S_.hash_data = w.hash_data[cc];
+            S_.hash_ack = R.hash_ack = w.hash_ack[cc];
+            S_.m_first = w.msg0 + w.row_msg[cr[0]];
+            S_.m_cnt = (int)cr.size();
+            S_.fin_on = R.fin_on = (uint8_t)(w.p.fin != 0);
+            uint64_t segs = (w.conn_bytes[cc] + MSS - 1) / MSS + cr.size() + 1;
+            S_.it_cap = (uint32_t)std::min<uint64_t>(segs, 65536);
+            S_.it_off = it_total;
+            it_total += S_.it_cap;
+            R.oo_cap = (uint32_t)std::min<uint64_t>(segs / 2 + 2, 4096);
+            R.oo_off = oo_total;
+            oo_total += R.oo_cap;
+            R.bytes = (uint32_t)w.conn_bytes[cc];
+            // initial values (reference src/model.h:124-277)
+            S_.cwnd = INIT_CWND;
+            S_.ssthresh = 0xFFFFFFFFu;
+            S_.first_partial = 1;
+            S_.cub_delaymin = S_.cub_epoch = S_.cub_roundstart = S_.cub_lastack = S_.cub_currrtt = INT64_MIN;
+            S_.ecn_echo_seq = S_.ecn_cwr_seq = -1;
+            S_.alpha = 1.0;
+            S_.srtt = -1;
+            S_.rto = MIN_RTO_PS;
+            S_.rto_at = -1;
+            S_.syn_at = -1;
+            R.fin_seq = R.synack_t = R.srtt = R.last_at = R.frx_at = R.syn_at = R.delack_at = R.ecn_ce_seq = -1;
+            for (int r : cr)
+            {
+                MsgRec &m = msgs[w.msg0 + w.row_msg[r]];
+                m.conn = w.conn0 + cc;
+                m.start = w.rows[r].start_ns * 1000;
+                m.est = m.done = -1;
+            }
+            uint64_t off = 0;
+            for (int r : cr)
+            {
+                off += (uint64_t)w.rows[r].size;
+                msgs[w.msg0 + w.row_msg[r]].end = (uint32_t)off;
+            }
+        }
+    }
+    c->host_msgs = msgs;
+    int r;
+    WorldDesc *dwd;
+    if ((r = c->upload(&dwd, wd, false)))
+        return r;
+    s.worlds = dwd;
+    if ((r = c->upload(&s.hosts, hosts, true)) || (r = c->upload(&s.sws, sws, false)) || (r = c->upload(&s.ports, ports, true)))
+        return r;
+    int *dpend;
+    if ((r = c->upload(&dpend, pend, false)))
+        return r;
+    s.pend_msg = dpend;
+    if ((r = c->upload(&s.snd, snd, true)) || (r = c->upload(&s.rcv, rcv, true)) || (r = c->upload(&s.msgs, msgs, true)))
+        return r;
+    // rings and scratch (zero; nothing in them matters before it is written)
+    if ((r = c->alloc(&s.host_ring, (size_t)H * ring, false)) || (r = c->alloc(&s.port_ring, (size_t)P * ring, false)) ||
+        (r = c->alloc(&s.act_snd, (size_t)H * s.act_cap, false)) || (r = c->alloc(&s.act_rcv, (size_t)H * s.act_cap, false)) ||
+        (r = c->alloc(&s.it_start, it_total, false)) || (r = c->alloc(&s.it_fl, it_total, false)) ||
+        (r = c->alloc(&s.h_seq, it_total, false)) || (r = c->alloc(&s.h_cnt, it_total, false)) || (r = c->alloc(&s.h_t, it_total, false)) ||
+        (r = c->alloc(&s.oo_s, oo_total, false)) || (r = c->alloc(&s.oo_e, oo_total, false)) ||
+        (r = c->alloc(&s.msg, (size_t)NB * s.L * MAX_TX, false)))
+        return r;
+    {
+        std::vector<int64_t> tags((size_t)NB * s.L, -(1ll << 16)); // no slot
+        if ((r = c->upload(&s.msg_tag, tags, true)))
+            return r;
+    }
+    size_t per_sw = (size_t)kmax * 2 * MAX_TX;
+    if ((r = c->alloc(&s.sw_ts, (size_t)S * per_sw, false)) || (r = c->alloc(&s.sw_ref, (size_t)S * per_sw, false)) ||
+        (r = c->alloc(&s.sw_up, (size_t)S * per_sw, false)))
+        return r;
+    {
+        std::vector<Rng> st(S);
+        for (int i = 0; i < W; i++)
+        {
+            HostWorld &w = c->worlds[i];
+            if (!w.p.spray)
+                continue;
+            // node i's Ipv4GlobalRouting draws from stream i; switches are nodes H1.. of the world
+            for (int x = 0; x < w.S1; x++)
+                st[w.sw0 + x] = stream_state(w.p.rng_seed, (uint64_t)(w.H1 + x), w.p.rng_run);
+        }
+        if ((r = c->upload(&s.sw_rng, st, true)))
+            return r;
+    }
+    {
+        // TcpCubic's K = pow(n / 0.4, 1/3) for window differences n, from the host libm (the
+        // function ns-3 calls), so that every K equals ns-3's
+        bool any_cubic = false;
+        for (auto &w : c->worlds)
+            any_cubic |= w.p.tcp == TB_TCP_CUBIC;
+        std::vector<double> tab(any_cubic ? 65536 : 1);
+        for (size_t n = 0; n < tab.size(); n++)
+            tab[n] = std::pow((double)n / 0.4, 1 / 3.);
+        double *dt;
+        if ((r = c->upload(&dt, tab, false)))
+            return r;
+        s.cub_k_tab = dt;
+        s.cub_k_n = (int)tab.size();
+    }
+    if ((r = c->alloc(&s.ev, EV_N, true)) || (r = c->alloc(&s.ev_w, (size_t)W * EV_N, true)))
+        return r;
+    {
+        std::vector<SlotCtl> ctl(1);
+        memset(&ctl[0], 0, sizeof(SlotCtl));
+        ctl[0].act_cur = 1; // no skip before the first slots have run
+        ctl[0].act_prev = 1;
+        ctl[0].next_wake = ~0ull;
+        ctl[0].finished = M == 0;
+        if ((r = c->upload(&s.ctl, ctl, true)))
+            return r;
+    }
+    // snapshots of the initial state
+    for (auto &sn : c->snaps)
+        if (cudaMemcpy(sn.src, sn.dst, sn.bytes, cudaMemcpyDeviceToDevice) != cudaSuccess)
+            return fail(TB_ERR_CUDA, "snapshot copy failed");
+    if (!c->stream && cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(TB_ERR_CUDA, "cudaStreamCreate failed");
+    if (!c->ev0)
+    {
+        cudaEventCreate(&c->ev0);
+        cudaEventCreate(&c->ev1);
+    }
+    // the grid: every unit a warp, at most what is co-resident
+    int dev_sms = 0;
+    cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->device);
+    int per_sm = tb::slot_kernel_blocks_per_sm();
+    if (per_sm <= 0 || dev_sms <= 0)
+        return fail(TB_ERR_CUDA, "the slot kernel does not fit on the device");
+    int units = (H + c->host_lanes - 1) / c->host_lanes + S;
+    int need = (units + TB_WARPS_PER_BLOCK - 1) / TB_WARPS_PER_BLOCK;
+    int most = dev_sms * per_sm;
+    c->grid = c->grid_req > 0 ? std::min(c->grid_req, most) : std::min(need, most);
+    c->prepared = true;
+    cudaDeviceSynchronize();
+    c->stats.upload_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return TB_OK;
+}
+} // namespace
+
+// ------------------------------------------------------------------ the C ABI
+extern "C" {
+
+const char *tb_last_error(void) { return g_err.c_str(); }
+
+int tb_ctx_create(int device, unsigned long long hbm_budget_bytes, tb_ctx **out)
+{
+    if (!out)
+        return fail(TB_ERR_ARG, "out is NULL");
+    int n = 0;
+    if (device >= 0 && (cudaGetDeviceCount(&n) != cudaSuccess || device >= n))
+        return fail(TB_ERR_CUDA, "no such CUDA device");
+    tb_ctx *c = new tb_ctx;
+    c->device = device;
+    c->budget = hbm_budget_bytes;
+    *out = c;
+    return TB_OK;
+}
+
+int tb_ctx_destroy(tb_ctx *ctx)
+{
+    if (!ctx)
+        return TB_OK;
+    if (ctx->device >= 0)
+        cudaSetDevice(ctx->device);
+    if (ctx->stream)
+        cudaStreamDestroy(ctx->stream);
+    if (ctx->ev0)
+    {
+        cudaEventDestroy(ctx->ev0);
+        cudaEventDestroy(ctx->ev1);
+    }
+    delete ctx;
+    return TB_OK;
+}
+
+int tb_world_add_tcp(tb_ctx *ctx, const tb_topology *topo, int n_flows, const int *src, const int *dst, const long long *size,
+                     const long long *start_ns, const long long *conn, const unsigned *hash_data, const unsigned *hash_ack,
+                     const tb_tcp_params *params, int *world)
+{
+    if (!ctx || !topo || !params || n_flows < 0 || (n_flows > 0 && (!src || !dst || !size || !start_ns)))
+        return fail(TB_ERR_ARG, "tb_world_add_tcp: missing argument");
+    if (ctx->prepared)
+        return fail(TB_ERR_STATE, "the batch is already prepared");
+    if (params->tcp < 0 || params->tcp > 2 || params->ecn_k < 0 || params->queue < 1 || params->queue > 65000)
+        return fail(TB_ERR_ARG, "bad TCP parameters");
+    HostWorld w;
+    w.topo = *topo;
+    w.p = *params;
+    if (topo->kind == TB_TOPO_GRAPH)
+    {
+        if (topo->n_links < 0 || (topo->n_links && (!topo->link_a || !topo->link_b)))
+            return fail(TB_ERR_ARG, "graph links missing");
+        w.link_a.assign(topo->link_a, topo->link_a + topo->n_links);
+        w.link_b.assign(topo->link_b, topo->link_b + topo->n_links);
+        for (int i = 0; i < topo->n_fails; i++)
+        {
+            w.fail_t.push_back(topo->fail_t_ns[i]);
+            w.fail_a.push_back(topo->fail_a[i]);
+            w.fail_b.push_back(topo->fail_b[i]);
+            w.fail_up.push_back(topo->fail_up ? topo->fail_up[i] : 0);
+        }
+    }
+    else if (topo->n_fails)
+        return fail(TB_ERR_ARG, "link failures need a topology file");
+    w.topo.link_a = w.topo.link_b = nullptr;
+    w.topo.fail_t_ns = nullptr;
+    w.topo.fail_a = w.topo.fail_b = w.topo.fail_up = nullptr;
+    w.rows.resize(n_flows);
+    for (int i = 0; i < n_flows; i++)
+        w.rows[i] = {src[i], dst[i], size[i], start_ns[i], conn ? conn[i] : -1};
+    if (hash_data && hash_ack)
+    {
+        w.given_hd.assign(hash_data, hash_data + n_flows);
+        w.given_ha.assign(hash_ack, hash_ack + n_flows);
+    }
+    std::string err;
+    if (!build_topology(w, err) || !build_flows(w, err))
+        return fail(TB_ERR_ARG, err);
+    int H = 0;
+    for (auto &x : ctx->worlds)
+        H += x.H1;
+    if ((long long)H + w.H1 > (1ll << 30))
+        return fail(TB_ERR_ARG, "too many hosts in the batch");
+    ctx->worlds.push_back(std::move(w));
+    if (world)
+        *world = (int)ctx->worlds.size() - 1;
+    return TB_OK;
+}
+
+int tb_prepare(tb_ctx *ctx)
+{
+    if (!ctx)
+        return fail(TB_ERR_ARG, "ctx is NULL");
+    return prepare(ctx);
+}
+
+int tb_reset(tb_ctx *ctx)
+{
+    if (!ctx || !ctx->prepared)
+        return fail(TB_ERR_STATE, "nothing prepared");
+    cudaSetDevice(ctx->device);
+    for (auto &sn : ctx->snaps)
+        if (cudaMemcpyAsync(sn.dst, sn.src, sn.bytes, cudaMemcpyDeviceToDevice, ctx->stream) != cudaSuccess)
+            return fail(TB_ERR_CUDA, "reset copy failed");
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+        return fail(TB_ERR_CUDA, "reset failed");
+    ctx->ran = false;
+    return TB_OK;
+}
+
+int tb_set_launch(tb_ctx *ctx, int host_lanes, int grid)
+{
+    if (!ctx || host_lanes < 1 || host_lanes > 32 || grid < 0)
+        return fail(TB_ERR_ARG, "host_lanes 1..32, grid >= 0");
+    if (ctx->prepared)
+        return fail(TB_ERR_STATE, "set the launch shape before tb_prepare");
+    ctx->host_lanes = host_lanes;
+    ctx->grid_req = grid;
+    return TB_OK;
+}
+
+int tb_run(tb_ctx *ctx, long long max_slots)
+{
+    if (!ctx)
+        return fail(TB_ERR_ARG, "ctx is NULL");
+    int r = prepare(ctx);
+    if (r)
+        return r;
+    if (ctx->ran && (r = tb_reset(ctx)))
+        return r;
+    cudaSetDevice(ctx->device);
+    Sim s = ctx->sim;
+    s.max_slots = max_slots > 0 ? max_slots : 2000000;
+    SlotCtl ctl{};
+    long long launches = 0;
+    cudaEventRecord(ctx->ev0, ctx->stream);
+    for (;;)
+    {
+        int e = tb::launch_slots(s, ctx->grid, ctx->max_slots_per_launch, ctx->host_lanes, ctx->stream);
+        if (e)
+            return fail(TB_ERR_CUDA, std::string("slot kernel launch: ") + cudaGetErrorString((cudaError_t)e));
+        launches++;
+        if (cudaMemcpyAsync(&ctl, s.ctl, sizeof ctl, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+            cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+            return fail(TB_ERR_CUDA, std::string("slot kernel: ") + cudaGetErrorString(cudaGetLastError()));
+        if (ctl.finished || ctl.error)
+            break;
+    }
+    cudaEventRecord(ctx->ev1, ctx->stream);
+    cudaEventSynchronize(ctx->ev1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    ctx->ran = true;
+    std::vector<unsigned long long> ev(EV_N);
+    ctx->ev_w.assign((size_t)s.W * EV_N, 0);
+    cudaMemcpy(ev.data(), s.ev, 8 * EV_N, cudaMemcpyDeviceToHost);
+    cudaMemcpy(ctx->ev_w.data(), s.ev_w, 8 * ctx->ev_w.size(), cudaMemcpyDeviceToHost);
+    tb_stats &st = ctx->stats;
+    st.slots = ctl.slot;
+    st.slots_run = ctl.slots_run;
+    st.launches = launches;
+    st.kernel_ms = ms;
+    st.host_events = ev[EV_HOST_PKT];
+    st.host_sender_events = ev[EV_HOST_SND];
+    st.host_frames = ev[EV_HOST_FRAMES];
+    st.switch_events = ev[EV_SW_PKT];
+    st.packet_events = st.host_events + st.switch_events;
+    st.grid = ctx->grid;
+    st.host_lanes = ctx->host_lanes;
+    st.warps_per_block = TB_WARPS_PER_BLOCK;
+    st.bytes_d2h = 0;
+    if (ctl.error)
+        return fail(TB_ERR_TIMEOUT, "a device-side barrier wait ran out; the run was abandoned");
+    if (ev[EV_OVF_ACT] || ev[EV_OVF_DUE] || ev[EV_OVF_RING] || ev[EV_OVF_OOO] || ev[EV_OVF_TX])
+    {
+        g_err = "a capacity overflowed; results may differ from the reference";
+        return TB_WARN_INEXACT;
+    }
+    return TB_OK;
+}
+
+int tb_results(tb_ctx *ctx, int world, long long *established_ns, long long *completed_ns)
+{
+    if (!ctx || world < 0 || world >= (int)ctx->worlds.size())
+        return fail(TB_ERR_ARG, "no such world");
+    if (!ctx->ran)
+        return fail(TB_ERR_STATE, "no run yet");
+    HostWorld &w = ctx->worlds[world];
+    const int M = (int)w.rows.size();
+    std::vector<MsgRec> m(M);
+    if (M && cudaMemcpy(m.data(), ctx->sim.msgs + w.msg0, sizeof(MsgRec) * M, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return fail(TB_ERR_CUDA, "cudaMemcpy failed");
+    ctx->stats.bytes_d2h += sizeof(MsgRec) * M;
+    for (int i = 0; i < M; i++)
+    {
+        const MsgRec &x = m[w.row_msg[i]];
+        if (established_ns)
+            established_ns[i] = x.est >= 0 ? x.est / 1000 : -1;
+        if (completed_ns)
+            completed_ns[i] = x.done >= 0 ? x.done / 1000 : -1;
+    }
+    return TB_OK;
+}
+
+int tb_counters(tb_ctx *ctx, int world, unsigned long long *out, int n)
+{
+    if (!ctx || !out || n < 0 || world < 0 || world >= (int)ctx->worlds.size())
+        return fail(TB_ERR_ARG, "bad arguments");
+    if (!ctx->ran)
+        return fail(TB_ERR_STATE, "no run yet");
+    for (int i = 0; i < n && i < EV_N; i++)
+        out[i] = ctx->ev_w[(size_t)world * EV_N + i];
+    return TB_OK;
+}
+
+int tb_hashes(tb_ctx *ctx, int world, unsigned *hash_data, unsigned *hash_ack)
+{
+    if (!ctx || world < 0 || world >= (int)ctx->worlds.size())
+        return fail(TB_ERR_ARG, "no such world");
+    HostWorld &w = ctx->worlds[world];
+    for (size_t i = 0; i < w.rows.size(); i++)
+    {
+        if (hash_data)
+            hash_data[i] = w.hash_data[w.row_conn[i]];
+        if (hash_ack)
+            hash_ack[i] = w.hash_ack[w.row_conn[i]];
+    }
+    return TB_OK;
+}
+
+int tb_abi_sizes(unsigned long long *out, int n)
+{
+    const unsigned long long v[3] = {sizeof(tb_topology), sizeof(tb_tcp_params), sizeof(tb_stats)};
+    for (int i = 0; i < n && i < 3; i++)
+        out[i] = v[i];
+    return TB_OK;
+}
+
+int tb_get_stats(tb_ctx *ctx, tb_stats *out)
+{
+    if (!ctx || !out)
+        return fail(TB_ERR_ARG, "bad arguments");
+    *out = ctx->stats;
+    return TB_OK;
+}
+
+} // extern "C"

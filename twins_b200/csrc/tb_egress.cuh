@@ -1,0 +1,182 @@
+// twins-b200: frame moves and the egress port (a point-to-point device: one-packet device queue
+// under a RED queue disc), used by hosts and switch ports.
+#pragma once
+#include "tb_state.cuh"
+
+namespace tb
+{
+
+// Frames that cross entities (link messages) move through L2 only: readers in later slots run
+// on other SMs, whose L1 would otherwise hold stale lines (the persistent kernel is never
+// relaunched between slots).
+TB_D void frame_copy(Frame *d, const Frame *s)
+{
+    const uint4 *a = reinterpret_cast<const uint4 *>(s);
+    uint4 *b = reinterpret_cast<uint4 *>(d);
+    uint4 v[FRAME_WORDS];
+#pragma unroll
+    for (int i = 0; i < FRAME_WORDS; i++)
+        v[i] = a[i];
+#pragma unroll
+    for (int i = 0; i < FRAME_WORDS; i++)
+        b[i] = v[i];
+}
+TB_D void frame_load_link(Frame &d, const Frame *s)
+{
+#if defined(__CUDA_ARCH__)
+    const uint4 *a = reinterpret_cast<const uint4 *>(s);
+    uint4 *b = reinterpret_cast<uint4 *>(&d);
+#pragma unroll
+    for (int i = 0; i < FRAME_WORDS; i++)
+        b[i] = __ldcg(a + i);
+#else
+    d = *s;
+#endif
+}
+TB_D void frame_store_link(Frame *d, const Frame &s)
+{
+#if defined(__CUDA_ARCH__)
+    const uint4 *a = reinterpret_cast<const uint4 *>(&s);
+    uint4 *b = reinterpret_cast<uint4 *>(d);
+#pragma unroll
+    for (int i = 0; i < FRAME_WORDS; i++)
+        __stcg(b + i, a[i]);
+#else
+    *d = s;
+#endif
+}
+TB_D int64_t ts_load_link(const Frame *s)
+{
+#if defined(__CUDA_ARCH__)
+    return __ldcg(&s->ts);
+#else
+    return s->ts;
+#endif
+}
+TB_D int64_t tag_load(const int64_t *p)
+{
+#if defined(__CUDA_ARCH__)
+    return __ldcg(p);
+#else
+    return *p;
+#endif
+}
+TB_D void tag_store(int64_t *p, int64_t v)
+{
+#if defined(__CUDA_ARCH__)
+    __stcg(p, v);
+#else
+    *p = v;
+#endif
+}
+
+TB_D void ev_add(const Sim &s, int world, int i, unsigned long long n)
+{
+    if (!n)
+        return;
+#if defined(__CUDA_ARCH__)
+    atomicAdd(&s.ev[i], n);
+    atomicAdd(&s.ev_w[(size_t)world * EV_N + i], n);
+#else
+    s.ev[i] += n;
+    s.ev_w[(size_t)world * EV_N + i] += n;
+#endif
+}
+
+// link messages: slot `slot` of link `link`
+TB_D size_t msg_index(const Sim &s, int64_t slot, int link) { return (size_t)(slot & (NB - 1)) * s.L + link; }
+TB_D int msg_count(const Sim &s, int64_t slot, int link)
+{
+    int64_t v = tag_load(&s.msg_tag[msg_index(s, slot, link)]);
+    return (v >> 16) == slot ? (int)(v & 0xFFFF) : 0;
+}
+TB_D const Frame *msg_frames(const Sim &s, int64_t slot, int link) { return s.msg + msg_index(s, slot, link) * MAX_TX; }
+
+// The egress port's working copy for one slot (reference: src/step.cuh:163-317, Fifo).
+struct Egress
+{
+    Frame *ring;
+    int cap, head, size;
+    int64_t link_free, last_start;
+    Chain *last; // persistent: the chain of the transmission in progress
+    int red_k, qcap;
+    int64_t woke, idle_start, slot_end;
+    Frame *out; // this slot's link message
+    int sent;
+    unsigned drops, marks, ovf, emitted;
+
+    // start every frame whose transmission begins by `until` and within this slot
+    TB_D void advance(int64_t until)
+    {
+        while (size > 0)
+        {
+            Frame *f = &ring[head];
+            int64_t start = f->ts > link_free ? f->ts : link_free;
+            if (start > until || start >= slot_end)
+                return;
+            if (sent >= MAX_TX)
+            {
+                ovf++;
+                return;
+            }
+            int64_t end = start + (int64_t)f->len * PS_PER_BYTE;
+            Frame o;
+            frame_copy(&o, f);
+            // its parent event: the previous frame's TransmitComplete, unless the link was idle
+            if (f->ts <= link_free && link_free > last_start)
+                chain_child(o.ch, *last, code_tc((int)((link_free - last_start) / PS_PER_BYTE)));
+            else
+                idle_start = start;
+            *last = o.ch;
+            last_start = start;
+            o.ts = end + PROP_PS;
+            frame_store_link(&out[sent], o);
+            sent++;
+            link_free = end;
+            head = head + 1 == cap ? 0 : head + 1;
+            size--;
+        }
+    }
+
+    // RED with MinTh = MaxTh = K and QW = 1 on the queue disc's length, which excludes the
+    // device queue's packet once ns-3's Wake (ScheduleNow) has refilled it; then the limit
+    TB_D bool enqueue(Frame &g, int64_t now)
+    {
+        emitted++;
+        advance(now);
+        bool refilled = last_start < now || (woke == now && idle_start == now);
+        int nq = (size > 0 && link_free > now && refilled) ? size - 1 : size;
+        g.ts = now;
+        if (nq >= red_k && nq > 1)
+        {
+            if (g.flags & F_ECT)
+            {
+                g.flags |= F_CE;
+                marks++;
+            }
+            else
+            {
+                drops++;
+                return false;
+            }
+        }
+        if (nq >= qcap)
+        {
+            drops++;
+            return false;
+        }
+        if (size >= cap)
+        {
+            ovf++;
+            return false;
+        }
+        int at = head + size;
+        if (at >= cap)
+            at -= cap;
+        frame_copy(&ring[at], &g);
+        size++;
+        return true;
+    }
+};
+
+} // namespace tb

@@ -1,0 +1,16 @@
+// twins-b200: launching the slot kernel (host side).
+#pragma once
+#include <cuda_runtime.h>
+
+#ifndef TB_WARPS_PER_BLOCK
+#define TB_WARPS_PER_BLOCK 4
+#endif
+
+namespace tb
+{
+struct Sim;
+// blocks of the slot kernel that fit on one SM at once (0 on error)
+int slot_kernel_blocks_per_sm();
+// one cooperative launch of up to max_slots_per_launch slots; 0 or a cudaError_t
+int launch_slots(const Sim &s, int grid, int max_slots_per_launch, int host_lanes, cudaStream_t stream);
+} // namespace tb

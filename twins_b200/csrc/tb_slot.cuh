@@ -1,0 +1,497 @@
+// twins-b200: one slot of a host and of a switch.
+//   host_step   (reference: src/step.cuh:2250-2528) one thread per host: every event of the host
+//               in [t us, t+1 us) in ns-3's order: arrivals, timers, application starts
+//   switch_step (reference: src/step.cuh:2530-2886) one warp per switch, one lane per port:
+//               ingress windows -> routes (per-flow ECMP or MRG32k3a spraying) -> counting sort to
+//               egress ports -> per-egress ordering by (time, ns-3 order) -> RED enqueue -> starts
+#pragma once
+#include "tb_tcp.cuh"
+
+namespace tb
+{
+
+// the chain of a timer (due_chain, step.cuh:2241-2247)
+TB_D const Chain &due_chain(const Sim &s, const Due &d)
+{
+    switch (d.kind)
+    {
+    case 1:
+    case 3:
+    case 4:
+        return s.rcv[d.flow].dchain;
+    case 5:
+        return s.rcv[d.flow].fchain;
+    case 2:
+        return s.snd[d.flow].st == S_EST ? s.snd[d.flow].schain : s.snd[d.flow].rchain;
+    default:
+        return s.snd[d.flow].rchain;
+    }
+}
+
+// a receiver that can arm no timer any more: all its timers idle and everything received (or,
+// with FIN, the connection closed)
+TB_D bool rcv_idle_for_good(const RcvRec &R)
+{
+    if (R.delack_at >= 0 || R.syn_at >= 0 || R.last_at >= 0 || R.frx_at >= 0)
+        return false;
+    if (R.fin_on)
+        return R.st == R_CLOSED;
+    return R.est && R.rcv_nxt >= R.bytes;
+}
+
+// One slot of host h. Returns true if it sent or holds frames; *wake: the next slot it must run.
+TB_D bool host_step(const Sim &s, int h, int64_t t, int64_t *wake, unsigned *ties_out, unsigned *done_out)
+{
+    const int64_t S0 = t * SLOT_PS, E0 = S0 + SLOT_PS;
+    HostRec &hr = s.hosts[h];
+    const int link = hr.in_link;
+    const Frame *m2 = nullptr, *m1 = nullptr;
+    int n2 = 0, n1 = 0, i2 = 0, i1 = 0;
+    if (t >= 2)
+    {
+        n2 = msg_count(s, t - 2, link);
+        m2 = msg_frames(s, t - 2, link);
+        while (i2 < n2 && ts_load_link(&m2[i2]) < S0)
+            i2++;
+    }
+    if (t >= 1)
+    {
+        n1 = msg_count(s, t - 1, link);
+        m1 = msg_frames(s, t - 1, link);
+    }
+    bool input = i2 < n2 || (n1 > 0 && ts_load_link(&m1[0]) < E0);
+    if (!input && t < hr.wake && hr.q_size == 0)
+    {
+        *wake = hr.wake;
+        return false;
+    }
+    const WorldDesc &wd = s.worlds[hr.world];
+    HostCtx c;
+    c.s = &s;
+    c.wd = &wd;
+    c.h = h;
+    c.dctcp = wd.cc == CC_DCTCP;
+    c.cubic = wd.cc == CC_CUBIC;
+    c.slot_end = E0;
+    c.retx = c.rtos = c.ovf = c.done = 0;
+    c.pkts = c.snd_pkts = 0;
+    Egress &nic = c.nic;
+    nic.ring = s.host_ring + (size_t)h * s.ring;
+    nic.cap = s.ring;
+    nic.head = hr.q_head;
+    nic.size = hr.q_size;
+    nic.link_free = hr.link_free;
+    nic.last_start = hr.last_start;
+    nic.last = &hr.last;
+    nic.red_k = wd.red_k;
+    nic.qcap = wd.qcap;
+    nic.woke = -1;
+    nic.idle_start = -1;
+    nic.slot_end = E0;
+    nic.out = s.msg + msg_index(s, t, h) * MAX_TX;
+    nic.sent = 0;
+    nic.drops = nic.marks = nic.ovf = nic.emitted = 0;
+    unsigned ties = 0;
+
+    // timers due in this slot (new timers lie >= 10 us ahead, except the 1 ps Send deferral,
+    // which due_insert adds), by time
+    int *act_snd = s.act_snd + (size_t)h * s.act_cap, *act_rcv = s.act_rcv + (size_t)h * s.act_cap;
+    const int ns = hr.n_snd, nr = hr.n_rcv;
+    c.nd = 0;
+    c.di = 0;
+    for (int i = 0; i < ns; i++)
+    {
+        int f = act_snd[i];
+        const SndRec &S = s.snd[f];
+        int64_t a = S.rto_at, b = S.syn_at;
+        if (a >= 0 && a < E0)
+        {
+            if (c.nd < DUE_CAP)
+                c.due[c.nd++] = {a, f, 0};
+            else
+                c.ovf++;
+        }
+        if (b >= 0 && b < E0)
+        {
+            if (c.nd < DUE_CAP)
+                c.due[c.nd++] = {b, f, 2};
+            else
+                c.ovf++;
+        }
+    }
+    for (int i = 0; i < nr; i++)
+    {
+        int f = act_rcv[i];
+        const RcvRec &R = s.rcv[f];
+        int64_t v[4] = {R.delack_at, R.syn_at, R.last_at, R.frx_at};
+        const int kinds[4] = {1, 3, 4, 5};
+        for (int j = 0; j < 4; j++)
+            if (v[j] >= 0 && v[j] < E0)
+            {
+                if (c.nd < DUE_CAP)
+                    c.due[c.nd++] = {v[j], f, kinds[j]};
+                else
+                    c.ovf++;
+            }
+    }
+    for (int i = 1; i < c.nd; i++)
+    {
+        Due x = c.due[i];
+        int j = i - 1;
+        while (j >= 0 && c.due[j].at > x.at)
+        {
+            c.due[j + 1] = c.due[j];
+            j--;
+        }
+        c.due[j + 1] = x;
+    }
+    int pn = hr.pend_next;
+    const int pe = hr.pend_end;
+    Frame p;
+    bool have_p = false; // p holds the next arrival
+    for (;;)
+    {
+        int64_t tr = INT64_MAX, td = INT64_MAX, tp = INT64_MAX;
+        if (!have_p)
+        {
+            if (i2 < n2)
+            {
+                frame_load_link(p, &m2[i2]);
+                have_p = true;
+            }
+            else if (i1 < n1 && ts_load_link(&m1[i1]) < E0)
+            {
+                frame_load_link(p, &m1[i1]);
+                have_p = true;
+            }
+        }
+        if (have_p)
+            tr = p.ts;
+        if (c.di < c.nd)
+            td = c.due[c.di].at;
+        int pm = -1;
+        if (pn < pe)
+        {
+            pm = s.pend_msg[pn];
+            int64_t st = s.msgs[pm].start;
+            if (st < E0)
+                tp = st;
+        }
+        int64_t now = tr < td ? tr : td;
+        now = now < tp ? now : tp;
+        if (now == INT64_MAX)
+            break;
+        if (now < S0)
+            now = S0;
+        nic.advance(now);
+        if (now == tp)
+        {
+            int f = s.msgs[pm].conn;
+            SndRec &S = s.snd[f];
+            pn++;
+            if (S.m_first != pm)
+            {
+                // a later message of a connection: FlowSender::SendMessage
+                chain_msg_root(c.ech, pm - wd.msg0);
+                S.m_due++;
+                if (S.st == S_EST)
+                    app_write(c, f, S, now);
+            }
+            else
+            {
+                // the connection's application starts: SYN (SendEmptyPacket)
+                chain_app_root(c.ech, hr.local, f - wd.conn0);
+                S.m_due = 1;
+                add_active(s, act_snd, hr.n_snd, f, c.ovf);
+                S.st = S_SYN_SENT;
+                if (c.cubic)
+                    cub_hystart_reset(S, now);
+                S.rto = CONN_TO_PS;
+                S.syn_at = now + CONN_TO_PS;
+                chain_child(S.rchain, c.ech, code_lead(CONN_TO_PS));
+                S.timing_time = now;
+                emit_snd(c, f, S, F_SYN, 0, 0, SYN_LEN, now);
+            }
+            continue;
+        }
+        bool timer = now == td;
+        if (timer && now == tr)
+        {
+            // a timer and an arrival at the same instant: the one scheduled first
+            Chain arr;
+            chain_child(arr, p.ch, code_arrival(p.len));
+            int r = chain_cmp(due_chain(s, c.due[c.di]), arr);
+            if (r == 0)
+                ties++;
+            timer = r <= 0; // (undecided: the timer)
+        }
+        if (timer)
+        {
+            Due d = c.due[c.di++];
+            c.ech = due_chain(s, d);
+            const int f = d.flow;
+            if (d.kind == 0 || d.kind == 2)
+            {
+                SndRec &S = s.snd[f];
+                if (d.kind == 0 && S.rto_at == d.at)
+                    on_rto(c, f, S, now);
+                else if (d.kind == 2 && S.syn_at == d.at && S.st == S_EST)
+                {
+                    S.syn_at = -1; // SendPendingData, deferred by Socket::Send
+                    send_pending(c, f, S, now);
+                }
+                else if (d.kind == 2 && S.syn_at == d.at && S.st == S_SYN_SENT)
+                {
+                    // SYN retransmission, backing off the connection timeout
+                    int tries = ++S.syn_tries;
+                    S.rto = CONN_TO_PS << tries;
+                    S.syn_at = now + S.rto;
+                    chain_child(S.rchain, c.ech, code_lead(S.rto));
+                    emit_snd(c, f, S, F_SYN, 0, 0, SYN_LEN, now);
+                }
+            }
+            else
+            {
+                RcvRec &R = s.rcv[f];
+                if (d.kind == 1 && R.delack_at == d.at)
+                    on_delack(c, f, R, now);
+                else if (d.kind == 4 && R.last_at == d.at && R.st == R_LAST_ACK)
+                {
+                    // LastAckTimeout: resend the FIN+ACK a limited number of times
+                    if (R.last_n == 0)
+                        rcv_closed(R);
+                    else
+                    {
+                        R.last_n--;
+                        send_fin_ack(c, f, R, now);
+                        int64_t lr = last_rto(R);
+                        R.last_at = now + lr;
+                        chain_child(R.dchain, c.ech, code_lead(lr));
+                    }
+                }
+                else if (d.kind == 5 && R.frx_at == d.at && R.st == R_LAST_ACK)
+                {
+                    R.frx_at = -1;
+                    send_fin_ack(c, f, R, now);
+                }
+                else if (d.kind == 3 && R.syn_at == d.at && !R.est)
+                {
+                    R.syn_at = -1;
+                    send_synack(c, f, R, now);
+                }
+            }
+            continue;
+        }
+        // the arrival
+        if (i2 < n2)
+            i2++;
+        else
+            i1++;
+        have_p = false;
+        c.pkts++;
+        c.snd_pkts += p.to_sender;
+        chain_child(c.ech, p.ch, code_arrival(p.len));
+        on_frame(c, hr, p, now);
+    }
+    nic.advance(E0 - 1);
+    tag_store(&s.msg_tag[msg_index(s, t, h)], (int64_t)t << 16 | nic.sent);
+    hr.q_head = nic.head;
+    hr.q_size = nic.size;
+    hr.link_free = nic.link_free;
+    hr.last_start = nic.last_start;
+    hr.pend_next = pn;
+
+    // drop finished connections from the active lists; the next wake-up
+    int64_t next = INT64_MAX;
+    {
+        int k = 0, n = hr.n_snd;
+        for (int i = 0; i < n; i++)
+        {
+            int f = act_snd[i];
+            const SndRec &S = s.snd[f];
+            if (S.st == S_DONE)
+                continue;
+            act_snd[k++] = f;
+            if (S.rto_at >= 0 && S.rto_at < next)
+                next = S.rto_at;
+            if (S.syn_at >= 0 && S.syn_at < next)
+                next = S.syn_at;
+        }
+        hr.n_snd = k;
+    }
+    {
+        int k = 0, n = hr.n_rcv;
+        for (int i = 0; i < n; i++)
+        {
+            int f = act_rcv[i];
+            const RcvRec &R = s.rcv[f];
+            if (rcv_idle_for_good(R))
+                continue;
+            act_rcv[k++] = f;
+            int64_t v[4] = {R.delack_at, R.syn_at, R.last_at, R.frx_at};
+            for (int j = 0; j < 4; j++)
+                if (v[j] >= 0 && v[j] < next)
+                    next = v[j];
+        }
+        hr.n_rcv = k;
+    }
+    if (pn < pe)
+    {
+        int64_t st = s.msgs[s.pend_msg[pn]].start;
+        if (st < next)
+            next = st;
+    }
+    hr.wake = nic.size > 0 ? t + 1 : (next == INT64_MAX ? INT64_MAX : next / SLOT_PS);
+    *wake = hr.wake;
+    // counters
+    ev_add(s, hr.world, EV_DROPS, nic.drops);
+    ev_add(s, hr.world, EV_MARKS, nic.marks);
+    ev_add(s, hr.world, EV_RETX, c.retx);
+    ev_add(s, hr.world, EV_RTO, c.rtos);
+    ev_add(s, hr.world, EV_HOST_PKT, c.pkts);
+    ev_add(s, hr.world, EV_HOST_SND, c.snd_pkts);
+    ev_add(s, hr.world, EV_HOST_FRAMES, nic.emitted);
+    ev_add(s, hr.world, EV_OVF_RING, c.ovf);
+    ev_add(s, hr.world, EV_OVF_TX, nic.ovf);
+    ev_add(s, hr.world, EV_TIES, ties);
+    *ties_out += ties;
+    *done_out += c.done;
+    return nic.sent > 0 || nic.size > 0;
+}
+
+// ------------------------------------------------------------------ switches
+TB_D int epoch_of(const WorldDesc &wd, int64_t ts)
+{
+    int e = 0;
+    while (e < wd.n_fail && ts >= wd.fail_t[e])
+        e++;
+    return e;
+}
+// the egress port at switch sw (world-local) towards host dst (world-local); `up` indexes the
+// equal-cost routes (reference: src/step.cuh:2554-2591)
+TB_D int route_up(const WorldDesc &wd, int sw, int dst, int up, int ep)
+{
+    if (wd.kind == TOPO_GRAPH)
+    {
+        int e = wd.host_sw[dst];
+        if (e == sw)
+            return wd.host_port[dst];
+        size_t r = ((size_t)ep * wd.S1 + sw) * wd.S1 + e;
+        return wd.rt_ports[wd.rt_off[r] + up];
+    }
+    if (wd.kind == TOPO_LEAFSPINE)
+    {
+        if (sw < wd.leaves)
+            return dst / wd.hpl == sw ? dst % wd.hpl : wd.hpl + up;
+        return dst / wd.hpl;
+    }
+    const int k = wd.k, hk = wd.hk, E = k * hk;
+    int dst_pod = dst / (hk * hk), dst_edge = (dst / hk) % hk;
+    if (sw < E)
+        return (dst_pod == sw / hk && dst_edge == sw % hk) ? dst % hk : hk + up;
+    if (sw < 2 * E)
+        return dst_pod == (sw - E) / hk ? dst_edge : hk + up;
+    return dst_pod;
+}
+TB_D int route(const Sim &s, const WorldDesc &wd, int sw, const Frame &p, int ep)
+{
+    if (wd.kind == TOPO_GRAPH)
+    {
+        int e = wd.host_sw[p.dst];
+        if (e == sw)
+            return wd.host_port[p.dst];
+        // the flow hash modulo the routes at this switch
+        const SndRec &S = s.snd[p.flow];
+        uint32_t hsh = p.to_sender ? S.hash_ack : S.hash_data;
+        return route_up(wd, sw, p.dst, (int)(hsh % wd.rt_n[((size_t)ep * wd.S1 + sw) * wd.S1 + e]), ep);
+    }
+    return route_up(wd, sw, p.dst, p.up, ep);
+}
+TB_D bool port_down(const WorldDesc &wd, int sw, int q, int ep)
+{
+    return wd.n_fail && wd.port_dn[((size_t)ep * wd.S1 + sw) * wd.k + q];
+}
+// equal-cost routes Ipv4GlobalRouting finds from sw towards dst (0: the host is attached)
+TB_D int routes_to(const WorldDesc &wd, int sw, int dst, int ep)
+{
+    if (wd.kind == TOPO_GRAPH)
+        return wd.host_sw[dst] == sw ? 0 : wd.rt_n[((size_t)ep * wd.S1 + sw) * wd.S1 + wd.host_sw[dst]];
+    if (wd.kind == TOPO_LEAFSPINE)
+        return sw < wd.leaves ? (dst / wd.hpl == sw ? 0 : wd.ecmp_n) : 1;
+    const int hk = wd.hk, E = wd.k * hk;
+    int dst_pod = dst / (hk * hk), dst_edge = (dst / hk) % hk;
+    if (sw < E)
+        return dst_pod == sw / hk && dst_edge == sw % hk ? 0 : wd.ecmp_n;
+    if (sw < 2 * E)
+        return dst_pod == (sw - E) / hk ? 1 : wd.ecmp_n;
+    return 1;
+}
+
+// simultaneous arrivals at a switch, as ns-3 orders their Receive events: the longer frame
+// started earlier upstream; else the chains of the upstream starts; else the lower connection id
+// (a guess, counted) (frame_before, step.cuh:2693-2705)
+TB_D bool frame_before(const Frame &a, const Frame &b, unsigned &ties)
+{
+    if (a.len != b.len)
+        return a.len > b.len;
+    int c = chain_cmp(a.ch, b.ch);
+    if (c == 0)
+        ties++;
+    return c != 0 ? c < 0 : a.flow < b.flow;
+}
+
+// per-warp shared scratch of a switch (k <= 32)
+struct SwShared
+{
+    int rows[32][33]; // [ingress][egress] counts, then offsets
+    int base[32], cnt[32];
+    int win[32][3];   // each ingress port's window: (i2, n2, n1)
+};
+
+// ingress window of port q: the tail of msg[t-2] from S0 on, the head of msg[t-1] before E0
+struct Input
+{
+    const Frame *m2, *m1;
+    int i2, n2, n1;
+    TB_D int count() const { return (n2 - i2) + n1; }
+    TB_D const Frame *at(int j) const { return j < n2 - i2 ? &m2[i2 + j] : &m1[j - (n2 - i2)]; }
+};
+
+TB_D Input input_window(const Sim &s, int link, int64_t t)
+{
+    const int64_t S0 = t * SLOT_PS, E0 = S0 + SLOT_PS;
+    Input in{nullptr, nullptr, 0, 0, 0};
+    if (link < 0)
+        return in;
+    if (t >= 2)
+    {
+        in.n2 = msg_count(s, t - 2, link);
+        in.m2 = msg_frames(s, t - 2, link);
+        while (in.i2 < in.n2 && ts_load_link(&in.m2[in.i2]) < S0)
+            in.i2++;
+    }
+    if (t >= 1)
+    {
+        int n = msg_count(s, t - 1, link);
+        in.m1 = msg_frames(s, t - 1, link);
+        while (in.n1 < n && ts_load_link(&in.m1[in.n1]) < E0)
+            in.n1++;
+    }
+    return in;
+}
+
+TB_D Input input_cached(const Sim &s, const SwShared &sh, const PortRec *ports, int q, int64_t t)
+{
+    int link = ports[q].in_link;
+    Input in;
+    in.i2 = sh.win[q][0];
+    in.n2 = sh.win[q][1];
+    in.n1 = sh.win[q][2];
+    if (link < 0)
+        link = 0;
+    in.m2 = t >= 2 ? msg_frames(s, t - 2, link) : nullptr;
+    in.m1 = t >= 1 ? msg_frames(s, t - 1, link) : nullptr;
+    return in;
+}
+
+} // namespace tb
