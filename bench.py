@@ -114,12 +114,7 @@ class Clocks:
 
 def load_worlds(name: str, rank: int):
     from twins_b200 import workloads
-    seed = 1 + rank
-    if name == "c1":
-        return workloads.c1(seed)
-    if name == "c4":
-        return workloads.c4(seed)
-    return workloads.c2(seed)
+    return workloads.WORKLOADS[name](1 + rank)
 
 
 def topo_flags(topo):
@@ -199,7 +194,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c4"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c2s", "c4"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--ref-slots", type=int, default=2500, help="reference arm: slots of each world per step")
     ap.add_argument("--cpu-slots", type=int, default=6000, help="cpu_baseline: slots of the sample world")
@@ -215,6 +210,7 @@ def main():
     worlds = load_worlds(args.workload, rank)
     config = {"workload": {"c1": "FatTree k=4, 240 flows, DCTCP (C1)",
                            "c2": "FatTree k=8, 10,000 flows x {NewReno, DCTCP, Cubic}, FIN, spraying (C2)",
+                           "c2s": "FatTree k=8, 1,500 flows x {NewReno, DCTCP, Cubic}, FIN, spraying (C2 shape, small)",
                            "c4": "256 leaf-spine worlds, 1k-20k flows each (C4)"}[args.workload],
               "worlds": len(worlds), "flows_per_step": int(sum(len(w.flows) for w in worlds)),
               "l2": "flushed between steps (256 MiB write); state restored device-to-device before each step",
@@ -306,7 +302,7 @@ def main():
         e2e_ms.append(1000 * (time.perf_counter() - t0))
         h2d = st2["bytes_h2d"]
         d2h = sum(len(w.flows) for w in worlds) * 32
-    e2e_step = statistics.mean(e2e_ms)
+    e2e_step = statistics.mean(e2e_ms) if e2e_ms else float("nan")
     if dist is not None:
         t = torch.tensor([e2e_step], dtype=torch.float64, device=f"cuda:{local_rank}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)

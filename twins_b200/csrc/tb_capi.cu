@@ -1057,6 +1057,18 @@ int tb_run(tb_ctx *ctx, long long max_slots)
     float ms = 0;
     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
     ctx->ran = true;
+#ifdef TB_PROFILE
+    if (ctl.slots_run > 1)
+    {
+        const double n = (double)ctl.slots_run;
+        fprintf(stderr, "profile: %lld slots; per slot: %.2f us, slowest host unit %.2f us, slowest switch unit %.2f us\n",
+                ctl.slots_run, ctl.prof_slot_sum / 1e3 / (n - 1), ctl.prof_host_sum / 1e3 / n, ctl.prof_sw_sum / 1e3 / n);
+        fprintf(stderr, "profile: per slot, summed over units (us): host setup %.2f timers %.2f events %.2f flush %.2f "
+                        "prune %.2f counters %.2f | switch ingress %.2f egress %.2f\n",
+                ctl.prof_phase[0] / 1e3 / n, ctl.prof_phase[1] / 1e3 / n, ctl.prof_phase[2] / 1e3 / n, ctl.prof_phase[3] / 1e3 / n,
+                ctl.prof_phase[4] / 1e3 / n, ctl.prof_phase[5] / 1e3 / n, ctl.prof_phase[6] / 1e3 / n, ctl.prof_phase[7] / 1e3 / n);
+    }
+#endif
     std::vector<unsigned long long> ev(EV_N);
     ctx->ev_w.assign((size_t)s.W * EV_N, 0);
     cudaMemcpy(ev.data(), s.ev, 8 * EV_N, cudaMemcpyDeviceToHost);

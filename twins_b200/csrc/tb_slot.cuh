@@ -40,26 +40,37 @@ TB_D bool rcv_idle_for_good(const RcvRec &R)
 }
 
 // One slot of host h. Returns true if it sent or holds frames; *wake: the next slot it must run.
-TB_D bool host_step(const Sim &s, int h, int64_t t, int64_t *wake, unsigned *ties_out, unsigned *done_out)
+// `stage`: the host's link messages of slots t-2 and t-1 copied to shared memory by its warp
+// (msg[t-2] then msg[t-1], as many frames as their tags count), or null to read them in place.
+TB_D bool host_step(const Sim &s, int h, int64_t t, int64_t *wake, unsigned *ties_out, unsigned *done_out,
+                    const Frame *stage = nullptr)
 {
     const int64_t S0 = t * SLOT_PS, E0 = S0 + SLOT_PS;
+    TB_PHASE_START
     HostRec &hr = s.hosts[h];
     const int link = hr.in_link;
     const Frame *m2 = nullptr, *m1 = nullptr;
     int n2 = 0, n1 = 0, i2 = 0, i1 = 0;
+    auto ts_at = [&](const Frame *m, int j) { return stage ? m[j].ts : ts_load_link(&m[j]); };
+    auto frame_at = [&](Frame &d, const Frame *m, int j) {
+        if (stage)
+            d = m[j];
+        else
+            frame_load_link(d, &m[j]);
+    };
     if (t >= 2)
     {
         n2 = msg_count(s, t - 2, link);
-        m2 = msg_frames(s, t - 2, link);
-        while (i2 < n2 && ts_load_link(&m2[i2]) < S0)
+        m2 = stage ? stage : msg_frames(s, t - 2, link);
+        while (i2 < n2 && ts_at(m2, i2) < S0)
             i2++;
     }
     if (t >= 1)
     {
         n1 = msg_count(s, t - 1, link);
-        m1 = msg_frames(s, t - 1, link);
+        m1 = stage ? stage + n2 : msg_frames(s, t - 1, link);
     }
-    bool input = i2 < n2 || (n1 > 0 && ts_load_link(&m1[0]) < E0);
+    bool input = i2 < n2 || (n1 > 0 && ts_at(m1, 0) < E0);
     if (!input && t < hr.wake && hr.q_size == 0)
     {
         *wake = hr.wake;
@@ -93,6 +104,7 @@ TB_D bool host_step(const Sim &s, int h, int64_t t, int64_t *wake, unsigned *tie
     nic.drops = nic.marks = nic.ovf = nic.emitted = 0;
     unsigned ties = 0;
 
+    TB_PHASE(0)
     // timers due in this slot (new timers lie >= 10 us ahead, except the 1 ps Send deferral,
     // which due_insert adds), by time
     int *act_snd = s.act_snd + (size_t)h * s.act_cap, *act_rcv = s.act_rcv + (size_t)h * s.act_cap;
@@ -145,6 +157,7 @@ TB_D bool host_step(const Sim &s, int h, int64_t t, int64_t *wake, unsigned *tie
         }
         c.due[j + 1] = x;
     }
+    TB_PHASE(1)
     int pn = hr.pend_next;
     const int pe = hr.pend_end;
     Frame p;
@@ -156,12 +169,12 @@ TB_D bool host_step(const Sim &s, int h, int64_t t, int64_t *wake, unsigned *tie
         {
             if (i2 < n2)
             {
-                frame_load_link(p, &m2[i2]);
+                frame_at(p, m2, i2);
                 have_p = true;
             }
-            else if (i1 < n1 && ts_load_link(&m1[i1]) < E0)
+            else if (i1 < n1 && ts_at(m1, i1) < E0)
             {
-                frame_load_link(p, &m1[i1]);
+                frame_at(p, m1, i1);
                 have_p = true;
             }
         }
@@ -293,6 +306,7 @@ TB_D bool host_step(const Sim &s, int h, int64_t t, int64_t *wake, unsigned *tie
         chain_child(c.ech, p.ch, code_arrival(p.len));
         on_frame(c, hr, p, now);
     }
+    TB_PHASE(2)
     nic.advance(E0 - 1);
     tag_store(&s.msg_tag[msg_index(s, t, h)], (int64_t)t << 16 | nic.sent);
     hr.q_head = nic.head;
@@ -301,6 +315,7 @@ TB_D bool host_step(const Sim &s, int h, int64_t t, int64_t *wake, unsigned *tie
     hr.last_start = nic.last_start;
     hr.pend_next = pn;
 
+    TB_PHASE(3)
     // drop finished connections from the active lists; the next wake-up
     int64_t next = INT64_MAX;
     {
@@ -343,6 +358,7 @@ TB_D bool host_step(const Sim &s, int h, int64_t t, int64_t *wake, unsigned *tie
     }
     hr.wake = nic.size > 0 ? t + 1 : (next == INT64_MAX ? INT64_MAX : next / SLOT_PS);
     *wake = hr.wake;
+    TB_PHASE(4)
     // counters
     ev_add(s, hr.world, EV_DROPS, nic.drops);
     ev_add(s, hr.world, EV_MARKS, nic.marks);
@@ -356,6 +372,7 @@ TB_D bool host_step(const Sim &s, int h, int64_t t, int64_t *wake, unsigned *tie
     ev_add(s, hr.world, EV_TIES, ties);
     *ties_out += ties;
     *done_out += c.done;
+    TB_PHASE(5)
     return nic.sent > 0 || nic.size > 0;
 }
 
@@ -438,60 +455,6 @@ TB_D bool frame_before(const Frame &a, const Frame &b, unsigned &ties)
     if (c == 0)
         ties++;
     return c != 0 ? c < 0 : a.flow < b.flow;
-}
-
-// per-warp shared scratch of a switch (k <= 32)
-struct SwShared
-{
-    int rows[32][33]; // [ingress][egress] counts, then offsets
-    int base[32], cnt[32];
-    int win[32][3];   // each ingress port's window: (i2, n2, n1)
-};
-
-// ingress window of port q: the tail of msg[t-2] from S0 on, the head of msg[t-1] before E0
-struct Input
-{
-    const Frame *m2, *m1;
-    int i2, n2, n1;
-    TB_D int count() const { return (n2 - i2) + n1; }
-    TB_D const Frame *at(int j) const { return j < n2 - i2 ? &m2[i2 + j] : &m1[j - (n2 - i2)]; }
-};
-
-TB_D Input input_window(const Sim &s, int link, int64_t t)
-{
-    const int64_t S0 = t * SLOT_PS, E0 = S0 + SLOT_PS;
-    Input in{nullptr, nullptr, 0, 0, 0};
-    if (link < 0)
-        return in;
-    if (t >= 2)
-    {
-        in.n2 = msg_count(s, t - 2, link);
-        in.m2 = msg_frames(s, t - 2, link);
-        while (in.i2 < in.n2 && ts_load_link(&in.m2[in.i2]) < S0)
-            in.i2++;
-    }
-    if (t >= 1)
-    {
-        int n = msg_count(s, t - 1, link);
-        in.m1 = msg_frames(s, t - 1, link);
-        while (in.n1 < n && ts_load_link(&in.m1[in.n1]) < E0)
-            in.n1++;
-    }
-    return in;
-}
-
-TB_D Input input_cached(const Sim &s, const SwShared &sh, const PortRec *ports, int q, int64_t t)
-{
-    int link = ports[q].in_link;
-    Input in;
-    in.i2 = sh.win[q][0];
-    in.n2 = sh.win[q][1];
-    in.n1 = sh.win[q][2];
-    if (link < 0)
-        link = 0;
-    in.m2 = t >= 2 ? msg_frames(s, t - 2, link) : nullptr;
-    in.m1 = t >= 1 ? msg_frames(s, t - 1, link) : nullptr;
-    return in;
 }
 
 } // namespace tb

@@ -158,7 +158,32 @@ struct SlotCtl
     int error;
     int pad;
     long long slots_run;
+    // TB_PROFILE builds: per-slot maxima of a host unit's and a switch unit's time, summed over
+    // slots, the slots' own time, and host / switch phase times (ns, the GPU's global timer)
+    unsigned long long prof_host_max, prof_sw_max, prof_host_sum, prof_sw_sum, prof_slot_sum, prof_release;
+    unsigned long long prof_phase[8];
 };
+
+#if defined(TB_PROFILE) && defined(__CUDACC__)
+__device__ __forceinline__ unsigned long long prof_now()
+{
+    unsigned long long t = 0;
+#if defined(__CUDA_ARCH__)
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+#endif
+    return t;
+}
+#define TB_PHASE_START unsigned long long prof_t0 = prof_now();
+#define TB_PHASE(i)                                                   \
+    {                                                                 \
+        unsigned long long prof_t1 = prof_now();                      \
+        atomicAdd(&s.ctl->prof_phase[i], prof_t1 - prof_t0);          \
+        prof_t0 = prof_t1;                                            \
+    }
+#else
+#define TB_PHASE_START
+#define TB_PHASE(i)
+#endif
 
 struct Sim
 {

@@ -1,51 +1,184 @@
-// twins-b200: one slot of one switch as phases of its warp, one lane per port (k <= 32).
-// The phases are separated by warp barriers on the device (switch_step in tb_kernel.cu).
+// twins-b200: one slot of one switch as phases of its warp (k <= 32 ports).
 // Reference: src/step.cuh:2748-2886 (switch_step), :2709-2745 (spray_draws).
+//
+// The warp first copies every frame of the slot's ingress link messages into shared memory in
+// one cooperative pass (all lanes, 16-byte loads from L2), so that the serial parts (the merged
+// arrival order of per-packet spraying, each egress port's ordering and enqueues) read shared
+// memory instead of making one dependent L2 round trip per frame. A slot whose messages exceed
+// the staging area reads them in place (the same phases, through L2).
 #pragma once
 #include "tb_slot.cuh"
 
 namespace tb
 {
 
+#ifndef TB_SW_STAGE
+#define TB_SW_STAGE 192 // frames staged per switch (or host) and slot
+#endif
+constexpr int SW_STAGE = TB_SW_STAGE;
+
+// per-warp shared scratch of a switch (also a host unit's staging area)
+struct SwShared
+{
+    int rows[32][33];       // [ingress][egress] counts, then offsets
+    int base[32], cnt[32];
+    int win[32][3];         // each ingress port's window in its messages: (i2, n2, n1)
+    int raw2[32], raw1[32]; // frames in the port's msg[t-2] / msg[t-1]
+    int off2[32], off1[32]; // where they start in `fr` (staged)
+    int staged, total;
+    Frame fr[SW_STAGE];
+    int64_t ets[SW_STAGE];  // staged slots: each egress region's arrival times and sources
+    uint32_t eref[SW_STAGE];
+};
+
+// ingress window of a port: the tail of msg[t-2] from S0 on, the head of msg[t-1] before E0;
+// frames in shared memory (staged) or in the link messages
+struct Input
+{
+    const Frame *m2, *m1;
+    int i2, n2, n1;
+    bool smem;
+    TB_D int count() const { return (n2 - i2) + n1; }
+    TB_D const Frame *at(int j) const { return j < n2 - i2 ? &m2[i2 + j] : &m1[j - (n2 - i2)]; }
+    TB_D void load(Frame &f, int j) const
+    {
+        if (smem)
+            f = *at(j);
+        else
+            frame_load_link(f, at(j));
+    }
+    TB_D int64_t ts(int j) const { return smem ? at(j)->ts : ts_load_link(at(j)); }
+};
+
 struct SwCtx
 {
     const Sim *s;
     const WorldDesc *wd;
     const SwRec *sr;
-    int sw;        // global switch id
-    PortRec *ports; // the switch's ports
-    size_t scratch; // its region in sw_ts / sw_ref / sw_up
+    int sw;          // global switch id
+    PortRec *ports;  // the switch's ports
+    size_t scratch;  // its region in sw_ts / sw_ref / sw_up
     int64_t t;
     bool spray;
 };
 
-TB_D int sw_egress_of(const SwCtx &x, const SwShared &sh, int q, int j, const Frame *p)
+TB_D Input input_of(const SwCtx &x, const SwShared &sh, int q)
+{
+    Input in;
+    in.i2 = sh.win[q][0];
+    in.n2 = sh.win[q][1];
+    in.n1 = sh.win[q][2];
+    in.smem = sh.staged != 0;
+    if (in.smem)
+    {
+        in.m2 = &sh.fr[sh.off2[q]];
+        in.m1 = &sh.fr[sh.off1[q]];
+        return in;
+    }
+    int link = x.ports[q].in_link;
+    if (link < 0)
+        link = 0; // (an unused port's window is empty; any link gives valid pointers)
+    in.m2 = x.t >= 2 ? msg_frames(*x.s, x.t - 2, link) : nullptr;
+    in.m1 = x.t >= 1 ? msg_frames(*x.s, x.t - 1, link) : nullptr;
+    return in;
+}
+
+// phase 1a (lane q < k): the port's message sizes; clear its row
+TB_D void sw_phase_sizes(const SwCtx &x, SwShared &sh, int q)
+{
+    const Sim &s = *x.s;
+    int link = x.ports[q].in_link;
+    sh.raw2[q] = link >= 0 && x.t >= 2 ? msg_count(s, x.t - 2, link) : 0;
+    sh.raw1[q] = link >= 0 && x.t >= 1 ? msg_count(s, x.t - 1, link) : 0;
+    for (int i = 0; i <= x.sr->k; i++)
+        sh.rows[q][i] = 0;
+}
+
+// phase 1b (lane 0): staging offsets
+TB_D void sw_phase_layout(const SwCtx &x, SwShared &sh)
+{
+    int off = 0;
+    for (int q = 0; q < x.sr->k; q++)
+    {
+        sh.off2[q] = off;
+        off += sh.raw2[q];
+        sh.off1[q] = off;
+        off += sh.raw1[q];
+    }
+    sh.staged = off <= SW_STAGE;
+    sh.total = off;
+}
+
+// phase 1c (every lane of the warp): copy the messages into shared memory
+TB_D void sw_phase_copy(const SwCtx &x, SwShared &sh, int lane, int lanes)
+{
+    if (!sh.staged)
+        return;
+    const Sim &s = *x.s;
+    const int total = sh.total, k = x.sr->k;
+    for (int i = lane; i < total; i += lanes)
+    {
+        // the port and message holding staged frame i (ports without frames are skipped)
+        int q = 0;
+        while (q + 1 < k && sh.off2[q + 1] <= i)
+            q++;
+        int link = x.ports[q].in_link;
+        const Frame *src = i < sh.off1[q] ? msg_frames(s, x.t - 2, link) + (i - sh.off2[q])
+                                          : msg_frames(s, x.t - 1, link) + (i - sh.off1[q]);
+        frame_load_link(sh.fr[i], src);
+    }
+}
+
+// phase 1d (lane q): the window (frames of msg[t-2] from S0 on, of msg[t-1] before E0)
+TB_D int sw_phase_window(const SwCtx &x, SwShared &sh, int q)
+{
+    const int64_t S0 = x.t * SLOT_PS, E0 = S0 + SLOT_PS;
+    const int r2 = sh.raw2[q], r1 = sh.raw1[q];
+    // index msg[t-2] (window i2 = 0, n2 = r2, n1 = 0), then msg[t-1] (n2 = 0)
+    sh.win[q][0] = 0;
+    sh.win[q][1] = r2;
+    sh.win[q][2] = 0;
+    Input all = input_of(x, sh, q);
+    int i2 = 0;
+    while (i2 < r2 && all.ts(i2) < S0)
+        i2++;
+    all.n2 = 0;
+    int n1 = 0;
+    while (n1 < r1 && all.ts(n1) < E0)
+        n1++;
+    sh.win[q][0] = i2;
+    sh.win[q][2] = n1;
+    return (r2 - i2) + n1;
+}
+
+// the egress port of an arrival (-1: dropped on arrival at a down interface); reads the frame's
+// routing fields only
+TB_D int sw_egress_for(const SwCtx &x, const Frame &f, int q, int j)
 {
     const WorldDesc &wd = *x.wd;
-    int ep = wd.n_fail ? epoch_of(wd, ts_load_link(p)) : 0;
+    int ep = wd.n_fail ? epoch_of(wd, f.ts) : 0;
     if (port_down(wd, x.sr->local, q, ep))
-        return -1; // dropped on arrival at a down interface
-    Frame f;
-    frame_load_link(f, p);
+        return -1;
     if (x.spray)
         return route_up(wd, x.sr->local, f.dst, x.s->sw_up[x.scratch + (size_t)q * 2 * MAX_TX + j], ep);
     return route(*x.s, wd, x.sr->local, f, ep);
 }
-
-// phase 1 (lane q): the ingress window; clear the row
-TB_D int sw_phase_window(const SwCtx &x, SwShared &sh, int q)
+TB_D int sw_egress_of(const SwCtx &x, const Input &in, int q, int j)
 {
-    Input in = input_window(*x.s, x.ports[q].in_link, x.t);
-    sh.win[q][0] = in.i2;
-    sh.win[q][1] = in.n2;
-    sh.win[q][2] = in.n1;
-    for (int i = 0; i <= x.sr->k; i++)
-        sh.rows[q][i] = 0;
-    return in.count();
+    if (in.smem)
+        return sw_egress_for(x, *in.at(j), q, j); // (read in place)
+    Frame f;
+    frame_load_link(f, in.at(j));
+    return sw_egress_for(x, f, q, j);
 }
+// the region of egress arrivals (times, sources): shared memory when staged
+TB_D int64_t *sw_ts_of(const SwCtx &x, SwShared &sh) { return sh.staged ? sh.ets : x.s->sw_ts + x.scratch; }
+TB_D uint32_t *sw_ref_of(const SwCtx &x, SwShared &sh) { return sh.staged ? sh.eref : x.s->sw_ref + x.scratch; }
 
 // phase 2 (one lane): per-packet ECMP draws, one per forwarded packet in the order the packets
-// arrive at the node (all ports merged), from the switch's MRG32k3a stream
+// arrive at the node (all ports merged), from the switch's MRG32k3a stream. (With staged frames
+// the warp does this with a warp-wide argmin, sw_phase_spray_warp in tb_kernel.cu, in the same
+// order.)
 TB_D void sw_phase_spray(const SwCtx &x, const SwShared &sh, unsigned &ties)
 {
     const int k = x.sr->k;
@@ -60,10 +193,10 @@ TB_D void sw_phase_spray(const SwCtx &x, const SwShared &sh, unsigned &ties)
         Frame bf, f;
         for (int q = 0; q < k; q++)
         {
-            Input in = input_cached(*x.s, sh, x.ports, q, x.t);
+            Input in = input_of(x, sh, q);
             if (pos[q] >= in.count())
                 continue;
-            frame_load_link(f, in.at(pos[q]));
+            in.load(f, pos[q]);
             if (best < 0 || f.ts < bf.ts || (f.ts == bf.ts && frame_before(f, bf, ties)))
             {
                 best = q;
@@ -86,12 +219,12 @@ TB_D void sw_phase_spray(const SwCtx &x, const SwShared &sh, unsigned &ties)
 // phase 3 (lane q): count arrivals per egress port; returns the drops at a down interface
 TB_D unsigned sw_phase_count(const SwCtx &x, SwShared &sh, int q)
 {
-    Input in = input_cached(*x.s, sh, x.ports, q, x.t);
+    Input in = input_of(x, sh, q);
     unsigned dropped = 0;
     int n = in.count();
     for (int j = 0; j < n; j++)
     {
-        int e = sw_egress_of(x, sh, q, j, in.at(j));
+        int e = sw_egress_of(x, in, q, j);
         if (e >= 0)
             sh.rows[q][e]++;
         else
@@ -113,7 +246,7 @@ TB_D void sw_phase_offsets(const SwCtx &x, SwShared &sh, int e)
     sh.cnt[e] = off;
 }
 
-// phase 5 (lane e): egress e's region in the scratch
+// phase 5 (lane e): egress e's region
 TB_D void sw_phase_base(const SwCtx &x, SwShared &sh, int e)
 {
     int b = 0;
@@ -125,34 +258,32 @@ TB_D void sw_phase_base(const SwCtx &x, SwShared &sh, int e)
 // phase 6 (lane q): scatter (time, source) of each arrival to its egress region
 TB_D void sw_phase_scatter(const SwCtx &x, SwShared &sh, int q)
 {
-    Input in = input_cached(*x.s, sh, x.ports, q, x.t);
+    Input in = input_of(x, sh, q);
+    int64_t *ts = sw_ts_of(x, sh);
+    uint32_t *ref = sw_ref_of(x, sh);
     int n = in.count();
     for (int j = 0; j < n; j++)
     {
-        const Frame *p = in.at(j);
-        int e = sw_egress_of(x, sh, q, j, p);
+        int e = sw_egress_of(x, in, q, j);
         if (e < 0)
             continue;
         int at = sh.base[e] + sh.rows[q][e]++;
-        x.s->sw_ts[x.scratch + at] = ts_load_link(p);
-        x.s->sw_ref[x.scratch + at] = (uint32_t)(q << 16 | j);
+        ts[at] = in.ts(j);
+        ref[at] = (uint32_t)(q << 16 | j);
     }
 }
 
 // phase 7 (lane e): egress e's arrivals in time order (ties: ns-3's order, insertion sort in
 // ingress order), each enqueued (RED) with its arrival event's chain; then the starts of the
 // slot. Returns true if the port sent or holds frames.
-TB_D bool sw_phase_egress(const SwCtx &x, const SwShared &sh, int e, unsigned &ties, unsigned &drops, unsigned &marks,
+TB_D bool sw_phase_egress(const SwCtx &x, SwShared &sh, int e, unsigned &ties, unsigned &drops, unsigned &marks,
                           unsigned &ovf)
 {
     const Sim &s = *x.s;
     const int n = sh.cnt[e];
-    int64_t *ts = s.sw_ts + x.scratch + sh.base[e];
-    uint32_t *ref = s.sw_ref + x.scratch + sh.base[e];
-    auto frame_at = [&](uint32_t r) -> const Frame * {
-        Input src = input_cached(s, sh, x.ports, (int)(r >> 16), x.t);
-        return src.at((int)(r & 0xFFFF));
-    };
+    int64_t *ts = sw_ts_of(x, sh) + sh.base[e];
+    uint32_t *ref = sw_ref_of(x, sh) + sh.base[e];
+    auto load_ref = [&](Frame &f, uint32_t r) { input_of(x, sh, (int)(r >> 16)).load(f, (int)(r & 0xFFFF)); };
     for (int i = 1; i < n; i++)
     {
         int64_t tx = ts[i];
@@ -164,10 +295,18 @@ TB_D bool sw_phase_egress(const SwCtx &x, const SwShared &sh, int e, unsigned &t
                 break;
             if (ts[j] == tx)
             {
-                Frame a, b;
-                frame_load_link(a, frame_at(r));
-                frame_load_link(b, frame_at(ref[j]));
-                if (!frame_before(a, b, ties))
+                bool before;
+                if (sh.staged)
+                    before = frame_before(*input_of(x, sh, (int)(r >> 16)).at((int)(r & 0xFFFF)),
+                                          *input_of(x, sh, (int)(ref[j] >> 16)).at((int)(ref[j] & 0xFFFF)), ties);
+                else
+                {
+                    Frame a, b;
+                    load_ref(a, r);
+                    load_ref(b, ref[j]);
+                    before = frame_before(a, b, ties);
+                }
+                if (!before)
                     break;
             }
             ts[j + 1] = ts[j];
@@ -199,7 +338,7 @@ TB_D bool sw_phase_egress(const SwCtx &x, const SwShared &sh, int e, unsigned &t
     for (int i = 0; i < n; i++)
     {
         Frame p;
-        frame_load_link(p, frame_at(ref[i]));
+        load_ref(p, ref[i]);
         chain_child(p.ch, p.ch, code_arrival(p.len)); // queued: the arrival event's chain
         eg.enqueue(p, p.ts);
     }

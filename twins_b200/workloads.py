@@ -131,4 +131,11 @@ def c4(seed: int = 1, n_worlds: int = 256, min_flows: int = 1000, max_flows: int
     return worlds
 
 
-WORKLOADS = {"c1": c1, "c2": c2, "c4": c4}
+def c2_small(seed: int = 1, tcps=("newreno", "dctcp", "cubic")) -> list[World]:
+    """The C2 shape at 1,500 messages (profiling and quick checks)."""
+    topo = Topology.fattree(8)
+    flows = c2_flows(seed, n_msgs=1500)
+    return [World(f"c2s_k8_{t}", topo, flows, TcpParams(t, 30, 200, fin=True, spray=True, rng_seed=1, rng_run=1)) for t in tcps]
+
+
+WORKLOADS = {"c1": c1, "c2": c2, "c2s": c2_small, "c4": c4}
