@@ -141,6 +141,23 @@ int tb_set_launch(tb_ctx *ctx, int host_lanes, int grid);
  * in other languages can check their struct layouts (no counterpart in the reference). */
 int tb_abi_sizes(unsigned long long *out, int n);
 
+/* One TCP world run to completion without allocating device memory (no counterpart in the
+ * reference). For callers that cannot call cudaMalloc: a process whose device memory belongs to
+ * a framework's caching pool, code that must not allocate while it runs, or a process under a
+ * hard memory cap. The world's whole device state is carved from a fixed 48 MiB area that every
+ * process loading the library holds on each device it uses until it exits; a world that needs
+ * more (e.g. a FatTree k=8) is rejected with TB_ERR_MEMORY before anything runs. Arguments are
+ * tb_world_add_tcp's and tb_run's (ECMP hashes computed), results as tb_results gives them into
+ * the caller's host arrays. The first call on a device sets the area up there (it looks up its
+ * device address with that device current), so make that first call before any stream
+ * capture. Every call on a device shares the area, which keeps the last call's contents; each
+ * call clears what must start at zero. Calls that overlapped on the GPU would race on the area,
+ * so the library makes the calls of one process take turns (a lock held for the whole call). */
+int tb_run_static(int device, const tb_topology *topo, int n_flows, const int *src, const int *dst,
+                  const long long *size, const long long *start_ns, const long long *conn,
+                  const tb_tcp_params *params, long long max_slots, long long *established_ns,
+                  long long *completed_ns);
+
 #ifdef __cplusplus
 }
 #endif

@@ -76,6 +76,9 @@ ENTRY_POINTS = [
     ("tb_get_stats", ctypes.c_int, [ctypes.c_void_p, _P(_Stats)]),
     ("tb_set_launch", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     ("tb_abi_sizes", ctypes.c_int, [_P(ctypes.c_ulonglong), ctypes.c_int]),
+    ("tb_run_static", ctypes.c_int, [ctypes.c_int, _P(_Topology), ctypes.c_int, _P(ctypes.c_int), _P(ctypes.c_int),
+                                     _P(ctypes.c_longlong), _P(ctypes.c_longlong), _P(ctypes.c_longlong),
+                                     _P(_TcpParams), ctypes.c_longlong, _P(ctypes.c_longlong), _P(ctypes.c_longlong)]),
 ]
 
 _lib = None
@@ -356,3 +359,23 @@ def run_world(topo: Topology, flows: Flows, params: TcpParams, max_slots: int = 
         sim.run(max_slots)
         est, done = sim.results(w)
         return est, done, sim.counters(w), sim.stats()
+
+
+def run_world_static(topo: Topology, flows: Flows, params: TcpParams, max_slots: int = 0, device: int = 0):
+    """One world through tb_run_static, which allocates no device memory (for callers that may
+    not allocate: the world's device state lives in the library's fixed area). Returns
+    (established_ns, completed_ns, status)."""
+    lib = load_library()
+    t, keep = topo._c()
+    p = params._c()
+    n = len(flows)
+    est = np.empty(n, dtype=np.int64)
+    done = np.empty(n, dtype=np.int64)
+    r = lib.tb_run_static(device, ctypes.byref(t), n, _ptr(flows.src, ctypes.c_int), _ptr(flows.dst, ctypes.c_int),
+                          _ptr(flows.size, ctypes.c_longlong), _ptr(flows.start_ns, ctypes.c_longlong),
+                          _ptr(flows.conn, ctypes.c_longlong), ctypes.byref(p), max_slots,
+                          _ptr(est, ctypes.c_longlong), _ptr(done, ctypes.c_longlong))
+    del keep
+    if r < 0:
+        raise TwinsError(r, lib.tb_last_error().decode())
+    return est, done, r

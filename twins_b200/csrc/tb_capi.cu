@@ -12,6 +12,7 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <mutex>
 #include <vector>
 
 using namespace tb;
@@ -554,6 +555,9 @@ struct tb_ctx
     std::vector<unsigned long long> ev_w;
     tb_stats stats{};
     int max_slots_per_launch = 4096;
+    // tb_run_static: device state carved from a fixed area instead of allocated
+    unsigned char *arena = nullptr;
+    size_t arena_cap = 0, arena_used = 0;
 
     ~tb_ctx() { release(); }
     void release()
@@ -569,6 +573,20 @@ struct tb_ctx
     int alloc(T **p, size_t n, bool snapshot)
     {
         size_t bytes = sizeof(T) * std::max<size_t>(n, 1);
+        if (arena)
+        {
+            // a piece of the fixed area, 256-byte aligned and zeroed (no snapshot: no tb_reset)
+            size_t at = (arena_used + 255) & ~(size_t)255;
+            if (at + bytes > arena_cap)
+                return fail(TB_ERR_MEMORY, "the world needs more device memory than tb_run_static's fixed area (" +
+                                               std::to_string(arena_cap >> 20) + " MiB) holds");
+            if (cudaMemset(arena + at, 0, bytes) != cudaSuccess)
+                return fail(TB_ERR_CUDA, "cudaMemset failed");
+            arena_used = at + bytes;
+            dev_bytes = arena_used;
+            *p = (T *)(arena + at);
+            return TB_OK;
+        }
         if (budget && dev_bytes + bytes * (snapshot ? 2 : 1) > budget)
             return fail(TB_ERR_MEMORY, "the batch needs more than the context's HBM budget");
         void *d = nullptr;
@@ -879,9 +897,9 @@ int prepare(tb_ctx *c)
     for (auto &sn : c->snaps)
         if (cudaMemcpy(sn.src, sn.dst, sn.bytes, cudaMemcpyDeviceToDevice) != cudaSuccess)
             return fail(TB_ERR_CUDA, "snapshot copy failed");
-    if (!c->stream && cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+    if (!c->arena && !c->stream && cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
         return fail(TB_ERR_CUDA, "cudaStreamCreate failed");
-    if (!c->ev0)
+    if (!c->arena && !c->ev0)
     {
         cudaEventCreate(&c->ev0);
         cudaEventCreate(&c->ev1);
@@ -1163,3 +1181,89 @@ int tb_get_stats(tb_ctx *ctx, tb_stats *out)
 }
 
 } // extern "C"
+
+// ------------------------------------------------------------------ a run that allocates nothing
+// Some callers may not allocate device memory: a host program whose memory is managed by a
+// framework's pool (the caching allocator of a training or serving process, which owns the
+// device's free memory), code running where cudaMalloc is not allowed at that moment, or a
+// process under a hard memory cap. tb_run_static serves them: one world's whole device state
+// lives in this fixed area, which every process that loads the library holds on each device it
+// uses until it exits.
+#define TB_STATIC_AREA_BYTES (48ull << 20)
+static __device__ __align__(256) unsigned char tb_static_area[TB_STATIC_AREA_BYTES];
+
+namespace
+{
+std::mutex g_static_mu;       // calls of this process take turns
+void *g_static_area[64] = {}; // per device: the area's device address (null: not set up yet)
+} // namespace
+
+extern "C" int tb_run_static(int device, const tb_topology *topo, int n_flows, const int *src, const int *dst,
+                             const long long *size, const long long *start_ns, const long long *conn,
+                             const tb_tcp_params *params, long long max_slots, long long *established_ns,
+                             long long *completed_ns)
+{
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    int n = 0;
+    if (device < 0 || device >= 64 || cudaGetDeviceCount(&n) != cudaSuccess || device >= n)
+        return fail(TB_ERR_CUDA, "no such CUDA device");
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (cudaSetDevice(device) != cudaSuccess)
+        return fail(TB_ERR_CUDA, "cudaSetDevice failed");
+    struct Restore
+    {
+        int d;
+        ~Restore()
+        {
+            if (d >= 0)
+                cudaSetDevice(d);
+        }
+    } restore{prev};
+    if (!g_static_area[device])
+    {
+        // once per device, with that device current: the host-side name of the area is not a
+        // device address; the runtime gives the address
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, tb_static_area);
+        if (e != cudaSuccess || !p)
+            return fail(TB_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        g_static_area[device] = p;
+    }
+    tb_ctx c;
+    c.device = device;
+    c.arena = (unsigned char *)g_static_area[device];
+    c.arena_cap = TB_STATIC_AREA_BYTES;
+    int r = tb_world_add_tcp(&c, topo, n_flows, src, dst, size, start_ns, conn, nullptr, nullptr, params, nullptr);
+    if (r)
+        return r;
+    if ((r = prepare(&c)))
+        return r;
+    Sim s = c.sim;
+    s.max_slots = max_slots > 0 ? max_slots : 2000000;
+    SlotCtl ctl{};
+    for (;;)
+    {
+        int e = tb::launch_slots(s, c.grid, c.max_slots_per_launch, c.host_lanes, 0);
+        if (e)
+            return fail(TB_ERR_CUDA, std::string("slot kernel launch: ") + cudaGetErrorString((cudaError_t)e));
+        if (cudaMemcpy(&ctl, s.ctl, sizeof ctl, cudaMemcpyDeviceToHost) != cudaSuccess)
+            return fail(TB_ERR_CUDA, std::string("slot kernel: ") + cudaGetErrorString(cudaGetLastError()));
+        if (ctl.finished || ctl.error)
+            break;
+    }
+    if (ctl.error)
+        return fail(TB_ERR_TIMEOUT, "a device-side barrier wait ran out; the run was abandoned");
+    c.ran = true;
+    c.ev_w.assign(EV_N, 0);
+    if (cudaMemcpy(c.ev_w.data(), s.ev_w, 8 * EV_N, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return fail(TB_ERR_CUDA, "cudaMemcpy failed");
+    if ((r = tb_results(&c, 0, established_ns, completed_ns)))
+        return r;
+    if (c.ev_w[EV_OVF_ACT] || c.ev_w[EV_OVF_DUE] || c.ev_w[EV_OVF_RING] || c.ev_w[EV_OVF_OOO] || c.ev_w[EV_OVF_TX])
+    {
+        g_err = "a capacity overflowed; results may differ from the reference";
+        return TB_WARN_INEXACT;
+    }
+    return TB_OK;
+}
