@@ -276,15 +276,8 @@ def main():
         if (done < 0).any():
             print(f"warning: world {worlds[w].name}: {(done < 0).sum()} flows unfinished", file=sys.stderr)
     ms = statistics.mean(kernel_ms)
-    if dist is not None:
-        t = torch.tensor([ms, float(events)], dtype=torch.float64, device=f"cuda:{local_rank}")
-        mx = t.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        tot = t.clone()
-        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
-        ms_max, events_all = float(mx[0]), float(tot[1])
-    else:
-        ms_max, events_all = ms, float(events)
+    from twins_b200 import shard
+    ms_max, events_all = shard.aggregate(ms, float(events), dist, device=f"cuda:{local_rank}")
     value = events_all / (ms_max / 1000.0)
 
     # end to end through the C ABI from host buffers
