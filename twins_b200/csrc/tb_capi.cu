@@ -1085,6 +1085,8 @@ int tb_run(tb_ctx *ctx, long long max_slots)
                         "prune %.2f counters %.2f | switch ingress %.2f egress %.2f\n",
                 ctl.prof_phase[0] / 1e3 / n, ctl.prof_phase[1] / 1e3 / n, ctl.prof_phase[2] / 1e3 / n, ctl.prof_phase[3] / 1e3 / n,
                 ctl.prof_phase[4] / 1e3 / n, ctl.prof_phase[5] / 1e3 / n, ctl.prof_phase[6] / 1e3 / n, ctl.prof_phase[7] / 1e3 / n);
+        fprintf(stderr, "profile: host events split (us per slot, summed): egress advance %.2f arrivals %.2f timers+starts %.2f\n",
+                ctl.prof_phase[8] / 1e3 / n, ctl.prof_phase[9] / 1e3 / n, ctl.prof_phase[10] / 1e3 / n);
     }
 #endif
     std::vector<unsigned long long> ev(EV_N);

@@ -215,22 +215,29 @@ struct Rng
     double s[6];
 };
 // RngStream::RandU01: every intermediate is an integer below 2^53, exact in doubles
+// RngStream reduces each component as p - trunc(p / m) m, plus m if negative; with the
+// division correctly rounded that is always the exact residue p mod m in [0, m). This computes
+// the same residue without a division: the quotient from the reciprocal may be off by one either
+// way, and the two corrections bring the (exact, integer-valued) remainder into [0, m).
+TB_HD double mod_exact(double p, double m, double inv_m)
+{
+    double k = (double)(int64_t)(p * inv_m);
+    double r = p - k * m;
+    if (r < 0.0)
+        r += m;
+    if (r >= m)
+        r -= m;
+    return r;
+}
 TB_HDI double rand_u01(Rng &r)
 {
     const double m1 = 4294967087.0, m2 = 4294944443.0, norm = 1.0 / (4294967087.0 + 1.0);
-    double p1 = 1403580.0 * r.s[1] - 810728.0 * r.s[0];
-    int32_t k = (int32_t)(p1 / m1);
-    p1 -= k * m1;
-    if (p1 < 0.0)
-        p1 += m1;
+    const double inv1 = 1.0 / 4294967087.0, inv2 = 1.0 / 4294944443.0;
+    double p1 = mod_exact(1403580.0 * r.s[1] - 810728.0 * r.s[0], m1, inv1);
     r.s[0] = r.s[1];
     r.s[1] = r.s[2];
     r.s[2] = p1;
-    double p2 = 527612.0 * r.s[5] - 1370589.0 * r.s[3];
-    k = (int32_t)(p2 / m2);
-    p2 -= k * m2;
-    if (p2 < 0.0)
-        p2 += m2;
+    double p2 = mod_exact(527612.0 * r.s[5] - 1370589.0 * r.s[3], m2, inv2);
     r.s[3] = r.s[4];
     r.s[4] = r.s[5];
     r.s[5] = p2;

@@ -196,7 +196,9 @@ TB_D bool host_step(const Sim &s, int h, int64_t t, int64_t *wake, unsigned *tie
             break;
         if (now < S0)
             now = S0;
+        TB_PHASE(2)
         nic.advance(now);
+        TB_PHASE(8)
         if (now == tp)
         {
             int f = s.msgs[pm].conn;
@@ -225,6 +227,7 @@ TB_D bool host_step(const Sim &s, int h, int64_t t, int64_t *wake, unsigned *tie
                 S.timing_time = now;
                 emit_snd(c, f, S, F_SYN, 0, 0, SYN_LEN, now);
             }
+            TB_PHASE(10)
             continue;
         }
         bool timer = now == td;
@@ -293,6 +296,7 @@ TB_D bool host_step(const Sim &s, int h, int64_t t, int64_t *wake, unsigned *tie
                     send_synack(c, f, R, now);
                 }
             }
+            TB_PHASE(10)
             continue;
         }
         // the arrival
@@ -305,6 +309,7 @@ TB_D bool host_step(const Sim &s, int h, int64_t t, int64_t *wake, unsigned *tie
         c.snd_pkts += p.to_sender;
         chain_child(c.ech, p.ch, code_arrival(p.len));
         on_frame(c, hr, p, now);
+        TB_PHASE(9)
     }
     TB_PHASE(2)
     nic.advance(E0 - 1);
