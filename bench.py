@@ -189,21 +189,119 @@ def reference_gpu(worlds, d: Path):
     return {"seconds_per_step": total, "binary": "oracle/_ref/twins (reference src/main.cu, nvcc sm_100a)"}
 
 
+def plain_sample(worlds, n, device, batched_wps):
+    """The plain path: worlds run one at a time on the same GPU (each its own context and run),
+    on every (len / n)-th world; worlds/s = sample size / summed device time of the sample."""
+    from twins_b200 import api
+    step = max(1, len(worlds) // max(1, n))
+    idx = list(range(0, len(worlds), step))[:n]
+    ms, events = [], 0
+    for i in idx:
+        w = worlds[i]
+        with api.Simulator(device=device) as sim:
+            sim.add_world(w.topo, w.flows, w.params)
+            sim.run()
+            st = sim.stats()
+        ms.append(st["kernel_ms"])
+        events += st["packet_events"]
+    wps = len(idx) / (sum(ms) / 1000.0)
+    return {"worlds_per_s": wps, "events_per_s": events / (sum(ms) / 1000.0), "sample_worlds": idx,
+            "sample": f"{len(idx)} of {len(worlds)} worlds (every {step}th), each alone, device time summed",
+            "batched_over_plain_worlds_per_s": batched_wps / wps}
+
+
+def serve_bench(args):
+    """C5: a seeded Poisson stream of simulation requests served by continuous batching (requests
+    join the running batch between launches), against the same requests run one at a time.
+    Latency = completion - submission on the server's clock; worlds/s = requests / (last
+    completion - first submission). One GPU (each rank would serve its own stream)."""
+    import torch
+    from twins_b200 import api, workloads
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local_rank)
+    reqs = workloads.served_stream(seed=1, n=args.requests + 3, rate_per_s=args.rate)
+    warm, reqs = reqs[:3], reqs[3:]
+    caps = dict(worlds=48, hosts=24000, switches=8000, ports=80000, connections=120000, messages=120000,
+                sent_list_entries=1 << 28, ooo_blocks=1 << 26, slots_per_launch=128, hbm_budget_bytes=160 * 10 ** 9)
+    with api.Server(device=local_rank, **caps) as srv:
+        srv.start()
+        for r in warm:  # warm-up requests (untimed)
+            srv.wait(srv.submit(r.topo, r.flows, r.params), timeout_s=600)
+        st0 = srv.stats()
+        ids = []
+        with Clocks(local_rank) as clocks:
+            t0 = time.perf_counter()
+            for r in reqs:
+                delay = r.arrival_s - reqs[0].arrival_s - (time.perf_counter() - t0)
+                if delay > 0:
+                    time.sleep(delay)
+                ids.append(srv.submit(r.topo, r.flows, r.params))
+            for i in ids:
+                srv.wait(i, timeout_s=900)
+        infos = [srv.info(i) for i in ids]
+        st = srv.stats()
+    lat = np.array([x["t_done"] - x["t_submit"] for x in infos])
+    span = max(x["t_done"] for x in infos) - min(x["t_submit"] for x in infos)
+    served_wps = len(ids) / span
+    events = st["packet_events"] - st0["packet_events"]
+    # the plain path: every request alone, one after the other (device time)
+    plain_ms, plain_events = 0.0, 0
+    for r in reqs:
+        with api.Simulator(device=local_rank) as sim:
+            sim.add_world(r.topo, r.flows, r.params)
+            sim.run()
+            x = sim.stats()
+        plain_ms += x["kernel_ms"]
+        plain_events += x["packet_events"]
+    plain_wps = len(reqs) / (plain_ms / 1000.0)
+    mix = {}
+    for r in reqs:
+        k = r.name.split("_")[2]
+        mix[k] = mix.get(k, 0) + 1
+    print(json.dumps({
+        "metric": "worlds/s (served)", "value": served_wps, "unit": "worlds/s", "n_gpus": 1, "steps": 1, "warmup": len(warm),
+        "ms_per_step": 1000 * span, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+        "data": "synthetic",
+        "config": {"workload": "served stream (C5 shape, TCP requests): Poisson arrivals, 40% FatTree k=4, 30% k=8, 10% k=16, "
+                               "10% Jellyfish 64x8 (4 hosts/switch), 10% Dragonfly 9x4; a tenth with a link failure",
+                   "requests": len(reqs), "rate_per_s": args.rate, "mix": mix, "flows": int(sum(len(r.flows) for r in reqs)),
+                   "capacities": caps},
+        "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)), "max": float(lat.max())},
+        "packet_events_per_s": events / span,
+        "device_busy_frac": (st["kernel_ms"] - st0["kernel_ms"]) / 1000.0 / span,
+        "plain": {"worlds_per_s": plain_wps, "events_per_s": plain_events / (plain_ms / 1000.0),
+                  "sample": "every request alone, one after the other, device time summed"},
+        "served_over_plain_worlds_per_s": served_wps / plain_wps,
+        "server": {k: st[k] for k in ("launches", "slots_run", "admitted", "retired", "hbm_bytes", "host_lanes", "stage_frames", "grid")},
+        "clocks": clocks.summary(),
+    }))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c2s", "c4"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c2s", "c4", "c5"])
+    ap.add_argument("--requests", type=int, default=200, help="C5: requests in the served stream")
+    ap.add_argument("--rate", type=float, default=100.0, help="C5: request arrivals per second (Poisson)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--ref-slots", type=int, default=2500, help="reference arm: slots of each world per step")
     ap.add_argument("--cpu-slots", type=int, default=6000, help="cpu_baseline: slots of the sample world")
     ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--host-lanes", type=int, default=1)
+    ap.add_argument("--host-lanes", type=int, default=None, help="fixed hosts per warp (default: autotuned launch shapes)")
     ap.add_argument("--no-ref-gpu", action="store_true")
+    ap.add_argument("--warmup-slots", type=int, default=None,
+                    help="slots of each warm-up run (default: whole runs; C4: 400)")
+    ap.add_argument("--plain-sample", type=int, default=16,
+                    help="C4: worlds of the plain path (one world at a time) timed, every (256 / n)-th world")
     args = ap.parse_args()
+    if args.warmup_slots is None:
+        args.warmup_slots = 400 if args.workload == "c4" else 0
     args.warmup = max(args.warmup, 3)
 
+    if args.workload == "c5":
+        return serve_bench(args)
     rank = int(os.environ.get("RANK", 0))
     world_size = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
@@ -257,7 +355,7 @@ def main():
     sim.prepare()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local_rank}")
     for _ in range(args.warmup):
-        sim.run()
+        sim.run(args.warmup_slots)
     kernel_ms, launches, stats = [], 0, None
     with Clocks(local_rank) as clocks:
         for _ in range(args.steps):
@@ -322,15 +420,24 @@ def main():
     sample_world = next((w for w in worlds if w.params.tcp == "dctcp"), worlds[0])
     ev_cpu, wall_cpu, res = cpu_sample([sample_world], args.cpu_slots, 1)
     cpu_value = ev_cpu / res[0][1]
+    plain = None
+    if args.workload == "c4":
+        plain = plain_sample(worlds, args.plain_sample, local_rank, len(worlds) / (ms_max / 1000.0))
     ref_gpu = None
     if not args.no_ref_gpu and rank == 0:
         d = Path("/tmp") / "twins_bench_ref"
         d.mkdir(exist_ok=True)
         try:
-            ref_gpu = reference_gpu(worlds, d)
+            # (C4: the plain path's sample of worlds, one at a time as the reference runs them)
+            ref_worlds = [worlds[i] for i in plain["sample_worlds"]] if plain else worlds
+            ref_gpu = reference_gpu(ref_worlds, d)
             if ref_gpu and "seconds_per_step" in ref_gpu:
-                ref_gpu["value"] = events / ref_gpu["seconds_per_step"]
-                ref_gpu["unit"] = "events/s"
+                if plain:
+                    ref_gpu["worlds_per_s"] = len(ref_worlds) / ref_gpu["seconds_per_step"]
+                    ref_gpu["sample_worlds"] = plain["sample_worlds"]
+                else:
+                    ref_gpu["value"] = events / ref_gpu["seconds_per_step"]
+                    ref_gpu["unit"] = "events/s"
         except Exception as e:
             ref_gpu = {"error": str(e)[:200]}
     out = {
@@ -348,10 +455,13 @@ def main():
                          "sample": f"oracle on the first {args.cpu_slots} slots of {sample_world.name}"},
         "clocks": clocks.summary(),
         "gpu_launches": launches,
-        "launch": {"grid": stats["grid"], "host_lanes": stats["host_lanes"], "warps_per_block": stats["warps_per_block"]},
+        "launch": {"grid": stats["grid"], "host_lanes": stats["host_lanes"], "warps_per_block": stats["warps_per_block"],
+                   "stage_frames": stats["stage_frames"], "autotuned": bool(stats["autotuned"])},
     }
     if ref_gpu is not None:
         out["reference_gpu"] = ref_gpu
+    if plain:
+        out["plain"] = plain
     print(json.dumps(out))
     sim.close()
     if dist is not None:

@@ -82,7 +82,9 @@ typedef struct tb_stats
     unsigned long long host_sender_events; /* host arrivals handled by a connection's sender */
     unsigned long long host_frames;        /* frames hosts emitted */
     unsigned long long bytes_h2d, bytes_d2h;
-    int grid, host_lanes, warps_per_block;
+    int grid, host_lanes, warps_per_block; /* the launch shape that ran the most slots */
+    int stage_frames;        /* frames a warp stages in shared memory in that shape */
+    int autotuned;           /* 1: the shape was picked per launch by measured throughput */
 } tb_stats;
 
 /* A context on CUDA device `device`, admitting batches up to hbm_budget_bytes of device memory
@@ -134,11 +136,20 @@ int tb_hashes(tb_ctx *ctx, int world, unsigned *hash_data, unsigned *hash_ack);
 /* Statistics of the last run. */
 int tb_get_stats(tb_ctx *ctx, tb_stats *out);
 
-/* Launch shape: hosts per warp (1..32) and the grid (0: chosen from occupancy). */
+/* Launch shape: hosts per warp (1..32) and the grid (0: chosen from occupancy); turns autotuning
+ * off. Replaces the reference's --host_lanes (src/main.cu:183-184, 523-526). */
 int tb_set_launch(tb_ctx *ctx, int host_lanes, int grid);
+/* The same with the frames a warp stages in shared memory per slot (1..192; fewer leave room for
+ * more resident blocks per SM). */
+int tb_set_launch_shape(tb_ctx *ctx, int host_lanes, int stage_frames, int grid);
+/* Autotuning (on by default): tb_run picks each launch's shape (hosts per warp, staging size)
+ * among a fixed set by the packet-events per ms that short probe launches of each achieve. The
+ * results never depend on the shape (no counterpart in the reference). */
+int tb_set_autotune(tb_ctx *ctx, int on);
 
-/* sizeof(tb_topology), sizeof(tb_tcp_params), sizeof(tb_stats) in out[0..n-1], so that bindings
- * in other languages can check their struct layouts (no counterpart in the reference). */
+/* sizeof(tb_topology), sizeof(tb_tcp_params), sizeof(tb_stats), sizeof(tb_serve_caps),
+ * sizeof(tb_request_info), sizeof(tb_serve_stats) in out[0..n-1], so that bindings in other
+ * languages can check their struct layouts (no counterpart in the reference). */
 int tb_abi_sizes(unsigned long long *out, int n);
 
 /* One TCP world run to completion without allocating device memory (no counterpart in the
@@ -157,6 +168,65 @@ int tb_run_static(int device, const tb_topology *topo, int n_flows, const int *s
                   const long long *size, const long long *start_ns, const long long *conn,
                   const tb_tcp_params *params, long long max_slots, long long *established_ns,
                   long long *completed_ns);
+
+/* ---- serving: requests join a running batch (no counterpart in the reference, which runs one
+ * batch fixed at start, src/main.cu:283-325). A server holds device arrays sized by its
+ * capacities and runs the slot kernel over them in launches of slots_per_launch slots; between
+ * launches it retires finished worlds and admits queued requests into free room, each starting
+ * its own time at the launch slot it joins, so its results equal a standalone run's. */
+typedef struct tb_server tb_server;
+
+typedef struct tb_serve_caps
+{
+    int worlds;                           /* requests in the batch at once */
+    int hosts, switches, ports;           /* entities over all requests in the batch */
+    int connections, messages;
+    unsigned long long sent_list_entries; /* per-connection sent-list / RTT-history ring entries */
+    unsigned long long ooo_blocks;        /* receivers' out-of-order block entries */
+    int active_per_host;                  /* connections one host holds on one side */
+    int max_queue;                        /* the largest RED queue limit a request may set */
+    int max_ports;                        /* ports per switch, <= 32 */
+    int slots_per_launch;                 /* admission granularity (slots of 1 us) */
+    unsigned long long hbm_budget_bytes;  /* 0: no limit */
+} tb_serve_caps;
+
+typedef struct tb_request_info
+{
+    int state;            /* 0 queued, 1 running, 2 done, 3 failed */
+    int n_flows;
+    double t_submit, t_admit, t_done; /* seconds, the server's steady clock */
+    long long slot0, slots;          /* the launch slot it joined, the slots it took */
+} tb_request_info;
+
+typedef struct tb_serve_stats
+{
+    long long launches, slots_run, admitted, retired, queued, running;
+    double kernel_ms;                 /* device time of all launches */
+    unsigned long long packet_events, hbm_bytes;
+    int host_lanes, stage_frames, grid;
+} tb_serve_stats;
+
+int tb_server_create(int device, const tb_serve_caps *caps, tb_server **out);
+int tb_server_destroy(tb_server *srv);
+/* Queues a TCP world (the arguments of tb_world_add_tcp without given hashes); thread-safe.
+ * Fails with TB_ERR_MEMORY if the request could never fit the server's capacities. */
+int tb_server_submit_tcp(tb_server *srv, const tb_topology *topo, int n_flows, const int *src, const int *dst,
+                         const long long *size, const long long *start_ns, const long long *conn,
+                         const tb_tcp_params *params, long long *request);
+/* One round on the calling thread: admit, run one launch, retire. *running: requests in the
+ * batch afterwards. Not with tb_server_start. */
+int tb_server_step(tb_server *srv, int *running);
+/* Runs the rounds on a thread of the server's own while requests are queued or running. */
+int tb_server_start(tb_server *srv);
+/* Blocks until the request is done (timeout_s <= 0: no limit). */
+int tb_server_wait(tb_server *srv, long long request, double timeout_s);
+/* A done request's results (as tb_results / tb_counters, rows in submission order) and its
+ * timeline; any output may be NULL (info alone also works before it is done). */
+int tb_server_results(tb_server *srv, long long request, long long *established_ns, long long *completed_ns,
+                      unsigned long long *counters, int n_counters, tb_request_info *info);
+/* Forgets a queued or done request. */
+int tb_server_release(tb_server *srv, long long request);
+int tb_server_stats(tb_server *srv, tb_serve_stats *out);
 
 #ifdef __cplusplus
 }

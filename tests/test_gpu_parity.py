@@ -120,3 +120,40 @@ def test_max_slots_stops_early(native_lib):
         st = sim.stats()
         assert st["slots"] <= 300
         assert (done == -1).any()
+
+
+@pytest.mark.parametrize("name", ["k8_a2a30_dctcp_spray", "k8_r30_cubic_sprayfin", "jf32f_a2a50_newreno_spray"])
+def test_launch_shapes_identical(native_lib, name):
+    """Every launch shape (hosts per warp, frames staged per warp: 8 leaves most slots unstaged)
+    gives the same results and event counts as ns-3 and as each other."""
+    case = next(c for c in CASES if c["name"] == name)
+    want_est, want_done = ns3(case)
+    events = set()
+    for lanes, stage in [(1, 192), (1, 8), (1, 96), (4, 96), (32, 192), (7, 64)]:
+        est, done, ctr, stats = api.run_world(*world_of(case), host_lanes=lanes, stage_frames=stage)
+        assert (est == want_est).all() and (done == want_done).all(), (lanes, stage)
+        assert stats["host_lanes"] == lanes and stats["stage_frames"] == stage and not stats["autotuned"]
+        events.add(stats["packet_events"])
+    assert len(events) == 1
+
+
+def test_batch_worlds_finish_apart(native_lib):
+    """Leaf-spine worlds of different sizes, TCPs and lengths in one batch (the batched-sweep
+    shape, small): each world stops when its last message is done, so its results and all its
+    counters equal its standalone run."""
+    rng = np.random.default_rng(7)
+    worlds = []
+    for i, (leaves, tcp, n) in enumerate([(4, "dctcp", 300), (6, "cubic", 60), (4, "newreno", 900), (8, "dctcp", 150)]):
+        topo = api.Topology.leafspine(leaves, leaves // 2, 16)
+        flows = workloads.leafspine_flows(rng, topo.hosts, n, 0.4)
+        flows.size = np.minimum(flows.size, 300_000)
+        worlds.append((topo, flows, api.TcpParams(tcp, [10, 20, 40, 80][i], [100, 200, 400, 100][i])))
+    alone = [api.run_world(*w) for w in worlds]
+    with api.Simulator() as sim:
+        ids = [sim.add_world(*w) for w in worlds]
+        sim.run()
+        for (est, done, ctr, _), i in zip(alone, ids):
+            e2, d2 = sim.results(i)
+            assert (est == e2).all() and (done == d2).all()
+            assert (done >= 0).all()
+            assert sim.counters(i) == ctr

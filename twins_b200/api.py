@@ -55,7 +55,27 @@ class _Stats(ctypes.Structure):
                 ("host_events", ctypes.c_ulonglong), ("switch_events", ctypes.c_ulonglong),
                 ("host_sender_events", ctypes.c_ulonglong), ("host_frames", ctypes.c_ulonglong),
                 ("bytes_h2d", ctypes.c_ulonglong), ("bytes_d2h", ctypes.c_ulonglong),
-                ("grid", ctypes.c_int), ("host_lanes", ctypes.c_int), ("warps_per_block", ctypes.c_int)]
+                ("grid", ctypes.c_int), ("host_lanes", ctypes.c_int), ("warps_per_block", ctypes.c_int),
+                ("stage_frames", ctypes.c_int), ("autotuned", ctypes.c_int)]
+
+
+class _ServeCaps(ctypes.Structure):
+    _fields_ = [("worlds", ctypes.c_int), ("hosts", ctypes.c_int), ("switches", ctypes.c_int), ("ports", ctypes.c_int),
+                ("connections", ctypes.c_int), ("messages", ctypes.c_int), ("sent_list_entries", ctypes.c_ulonglong),
+                ("ooo_blocks", ctypes.c_ulonglong), ("active_per_host", ctypes.c_int), ("max_queue", ctypes.c_int),
+                ("max_ports", ctypes.c_int), ("slots_per_launch", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_ulonglong)]
+
+
+class _RequestInfo(ctypes.Structure):
+    _fields_ = [("state", ctypes.c_int), ("n_flows", ctypes.c_int), ("t_submit", ctypes.c_double), ("t_admit", ctypes.c_double),
+                ("t_done", ctypes.c_double), ("slot0", ctypes.c_longlong), ("slots", ctypes.c_longlong)]
+
+
+class _ServeStats(ctypes.Structure):
+    _fields_ = [("launches", ctypes.c_longlong), ("slots_run", ctypes.c_longlong), ("admitted", ctypes.c_longlong),
+                ("retired", ctypes.c_longlong), ("queued", ctypes.c_longlong), ("running", ctypes.c_longlong),
+                ("kernel_ms", ctypes.c_double), ("packet_events", ctypes.c_ulonglong), ("hbm_bytes", ctypes.c_ulonglong),
+                ("host_lanes", ctypes.c_int), ("stage_frames", ctypes.c_int), ("grid", ctypes.c_int)]
 
 
 # every entry point of include/twinsb200.h: (name, restype, argtypes)
@@ -75,7 +95,21 @@ ENTRY_POINTS = [
     ("tb_hashes", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _P(ctypes.c_uint), _P(ctypes.c_uint)]),
     ("tb_get_stats", ctypes.c_int, [ctypes.c_void_p, _P(_Stats)]),
     ("tb_set_launch", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    ("tb_set_launch_shape", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    ("tb_set_autotune", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("tb_abi_sizes", ctypes.c_int, [_P(ctypes.c_ulonglong), ctypes.c_int]),
+    ("tb_server_create", ctypes.c_int, [ctypes.c_int, _P(_ServeCaps), _P(ctypes.c_void_p)]),
+    ("tb_server_destroy", ctypes.c_int, [ctypes.c_void_p]),
+    ("tb_server_submit_tcp", ctypes.c_int, [ctypes.c_void_p, _P(_Topology), ctypes.c_int, _P(ctypes.c_int), _P(ctypes.c_int),
+                                            _P(ctypes.c_longlong), _P(ctypes.c_longlong), _P(ctypes.c_longlong), _P(_TcpParams),
+                                            _P(ctypes.c_longlong)]),
+    ("tb_server_step", ctypes.c_int, [ctypes.c_void_p, _P(ctypes.c_int)]),
+    ("tb_server_start", ctypes.c_int, [ctypes.c_void_p]),
+    ("tb_server_wait", ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_double]),
+    ("tb_server_results", ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, _P(ctypes.c_longlong), _P(ctypes.c_longlong),
+                                         _P(ctypes.c_ulonglong), ctypes.c_int, _P(_RequestInfo)]),
+    ("tb_server_release", ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
+    ("tb_server_stats", ctypes.c_int, [ctypes.c_void_p, _P(_ServeStats)]),
     ("tb_run_static", ctypes.c_int, [ctypes.c_int, _P(_Topology), ctypes.c_int, _P(ctypes.c_int), _P(ctypes.c_int),
                                      _P(ctypes.c_longlong), _P(ctypes.c_longlong), _P(ctypes.c_longlong),
                                      _P(_TcpParams), ctypes.c_longlong, _P(ctypes.c_longlong), _P(ctypes.c_longlong)]),
@@ -97,9 +131,10 @@ def load_library(path: Optional[os.PathLike] = None) -> ctypes.CDLL:
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    sizes = (ctypes.c_ulonglong * 3)()
-    lib.tb_abi_sizes(sizes, 3)
-    want = [ctypes.sizeof(_Topology), ctypes.sizeof(_TcpParams), ctypes.sizeof(_Stats)]
+    sizes = (ctypes.c_ulonglong * 6)()
+    lib.tb_abi_sizes(sizes, 6)
+    want = [ctypes.sizeof(_Topology), ctypes.sizeof(_TcpParams), ctypes.sizeof(_Stats), ctypes.sizeof(_ServeCaps),
+            ctypes.sizeof(_RequestInfo), ctypes.sizeof(_ServeStats)]
     if list(sizes) != want:
         raise RuntimeError(f"{p}: struct sizes {list(sizes)} differ from these bindings' {want}: rebuild")
     if path is None:
@@ -269,11 +304,14 @@ class TcpParams:
 class Simulator:
     """A batch of worlds on one GPU: add worlds, run, read results (tb_* of the C ABI)."""
 
-    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, host_lanes: int = 1, grid: int = 0):
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, host_lanes: Optional[int] = None, grid: int = 0,
+                 stage_frames: int = 192):
+        """host_lanes None: the launch shape is autotuned per launch; else that fixed shape."""
         self.lib = load_library()
         self.ctx = ctypes.c_void_p()
         self._check(self.lib.tb_ctx_create(device, hbm_budget_bytes, ctypes.byref(self.ctx)))
-        self._check(self.lib.tb_set_launch(self.ctx, host_lanes, grid))
+        if host_lanes is not None:
+            self._check(self.lib.tb_set_launch_shape(self.ctx, host_lanes, stage_frames, grid))
         self.sizes: list[int] = []
         self.last_status = TB_OK
 
@@ -379,3 +417,88 @@ def run_world_static(topo: Topology, flows: Flows, params: TcpParams, max_slots:
     if r < 0:
         raise TwinsError(r, lib.tb_last_error().decode())
     return est, done, r
+
+
+# ------------------------------------------------------------------ serving
+class Server:
+    """Continuous batching of simulation requests on one GPU (tb_server_* of the C ABI): requests
+    join the running batch between launches and each runs exactly as it would alone."""
+
+    def __init__(self, device: int = 0, worlds: int = 64, hosts: int = 8192, switches: int = 2048, ports: int = 32768,
+                 connections: int = 1 << 18, messages: int = 1 << 18, sent_list_entries: int = 1 << 27, ooo_blocks: int = 1 << 25,
+                 active_per_host: int = 256, max_queue: int = 400, max_ports: int = 32, slots_per_launch: int = 256,
+                 hbm_budget_bytes: int = 0):
+        self.lib = load_library()
+        caps = _ServeCaps(worlds, hosts, switches, ports, connections, messages, sent_list_entries, ooo_blocks, active_per_host,
+                          max_queue, max_ports, slots_per_launch, hbm_budget_bytes)
+        self.srv = ctypes.c_void_p()
+        self._check(self.lib.tb_server_create(device, ctypes.byref(caps), ctypes.byref(self.srv)))
+        self.sizes: dict[int, int] = {}
+
+    def _check(self, r: int) -> int:
+        if r < 0:
+            raise TwinsError(r, self.lib.tb_last_error().decode())
+        return r
+
+    def submit(self, topo: Topology, flows: Flows, params: TcpParams) -> int:
+        t, keep = topo._c()
+        p = params._c()
+        rid = ctypes.c_longlong()
+        self._check(self.lib.tb_server_submit_tcp(
+            self.srv, ctypes.byref(t), len(flows), _ptr(flows.src, ctypes.c_int), _ptr(flows.dst, ctypes.c_int),
+            _ptr(flows.size, ctypes.c_longlong), _ptr(flows.start_ns, ctypes.c_longlong), _ptr(flows.conn, ctypes.c_longlong),
+            ctypes.byref(p), ctypes.byref(rid)))
+        del keep
+        self.sizes[rid.value] = len(flows)
+        return rid.value
+
+    def step(self) -> int:
+        n = ctypes.c_int()
+        self._check(self.lib.tb_server_step(self.srv, ctypes.byref(n)))
+        return n.value
+
+    def start(self) -> None:
+        self._check(self.lib.tb_server_start(self.srv))
+
+    def wait(self, request: int, timeout_s: float = 0.0) -> None:
+        self._check(self.lib.tb_server_wait(self.srv, request, timeout_s))
+
+    def info(self, request: int) -> dict:
+        i = _RequestInfo()
+        self._check(self.lib.tb_server_results(self.srv, request, None, None, None, 0, ctypes.byref(i)))
+        return {name: getattr(i, name) for name, _ in _RequestInfo._fields_}
+
+    def results(self, request: int) -> tuple[np.ndarray, np.ndarray, dict]:
+        n = self.sizes[request]
+        est = np.empty(n, dtype=np.int64)
+        done = np.empty(n, dtype=np.int64)
+        ctr = np.zeros(16, dtype=np.uint64)
+        self._check(self.lib.tb_server_results(self.srv, request, _ptr(est, ctypes.c_longlong), _ptr(done, ctypes.c_longlong),
+                                               _ptr(ctr, ctypes.c_ulonglong), 16, None))
+        return est, done, {name: int(ctr[i]) for i, name in enumerate(COUNTERS)}
+
+    def release(self, request: int) -> None:
+        self._check(self.lib.tb_server_release(self.srv, request))
+        self.sizes.pop(request, None)
+
+    def stats(self) -> dict:
+        s = _ServeStats()
+        self._check(self.lib.tb_server_stats(self.srv, ctypes.byref(s)))
+        return {name: getattr(s, name) for name, _ in _ServeStats._fields_}
+
+    def close(self) -> None:
+        if self.srv:
+            self.lib.tb_server_destroy(self.srv)
+            self.srv = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

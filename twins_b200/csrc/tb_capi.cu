@@ -6,6 +6,7 @@
 #include "../../include/twinsb200.h"
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -539,8 +540,12 @@ struct tb_ctx
     std::vector<HostWorld> worlds;
     bool prepared = false, ran = false;
     int host_lanes = 1, grid_req = 0, grid = 0;
+    int stage_cap = SW_STAGE_MAX; // frames staged per warp
+    int *d_units = nullptr;       // the running units' list (tb_run)
+    bool autotune = true;         // pick the launch shape per launch by measured throughput
+    int dev_sms = 0;
     cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, la = nullptr, lb = nullptr;
     Sim sim{};
     std::vector<void *> allocs;
     size_t dev_bytes = 0;
@@ -622,6 +627,268 @@ struct tb_ctx
 
 namespace
 {
+// Where a world's entities sit in the device arrays (global ids), and where the ports' links
+// start: host h sends on link h, port p on link port_links + p.
+struct Place
+{
+    int world = 0, host0 = 0, sw0 = 0, port0 = 0, conn0 = 0, msg0 = 0;
+    uint64_t it0 = 0, oo0 = 0;
+    int port_links = 0;
+};
+
+// A world's initial device records for a place (reference src/model.h:124-277 for the initial
+// socket values, src/main.cu:327-1015 for the wiring and the per-host application order)
+struct WorldImage
+{
+    WorldDesc desc;
+    std::vector<HostRec> hosts;
+    std::vector<SwRec> sws;
+    std::vector<PortRec> ports;
+    std::vector<int> pend;
+    std::vector<SndRec> snd;
+    std::vector<RcvRec> rcv;
+    std::vector<MsgRec> msgs;
+    std::vector<Rng> rng;
+    uint64_t it_n = 0, oo_n = 0; // sent-list / RTT-history and out-of-order ring entries it uses
+    int active = 1;              // the most connections one host holds on one side
+};
+
+void build_image(const HostWorld &w, const Place &pl, WorldImage &img)
+{
+    WorldDesc &d = img.desc;
+    memset(&d, 0, sizeof d);
+    d.kind = w.kind;
+    d.k = w.k;
+    d.hk = w.hk;
+    d.leaves = w.leaves;
+    d.spines = w.spines;
+    d.hpl = w.hpl;
+    d.ecmp_n = w.ecmp_n;
+    d.H1 = w.H1;
+    d.S1 = w.S1;
+    d.host0 = pl.host0;
+    d.sw0 = pl.sw0;
+    d.conn0 = pl.conn0;
+    d.msg0 = pl.msg0;
+    d.n_msgs = (int)w.rows.size();
+    d.cc = (uint8_t)w.p.tcp;
+    d.fin = (uint8_t)(w.p.fin != 0);
+    d.spray = (uint8_t)(w.p.spray != 0);
+    d.red_k = w.p.ecn_k;
+    d.qcap = w.p.queue;
+    // hosts, switches, ports
+    img.hosts.assign(w.H1, HostRec{});
+    img.sws.assign(w.S1, SwRec{});
+    img.ports.assign((size_t)w.S1 * w.k, PortRec{});
+    img.pend.assign(w.rows.size(), 0);
+    std::vector<int> nsnd(w.H1, 0), nrcv(w.H1, 0);
+    for (auto &cr : w.conn_rows)
+    {
+        nsnd[w.rows[cr[0]].src]++;
+        nrcv[w.rows[cr[0]].dst]++;
+    }
+    for (int h = 0; h < w.H1; h++)
+    {
+        img.active = std::max(img.active, std::max(nsnd[h], nrcv[h]));
+        HostRec &hr = img.hosts[h];
+        memset(&hr, 0, sizeof hr);
+        hr.world = pl.world;
+        hr.local = h;
+        hr.wake = 0; // every host runs the first slot
+        hr.pend_next = pl.msg0 + w.pend_first[h];
+        hr.pend_end = pl.msg0 + w.pend_first[h + 1];
+        hr.in_link = pl.port_links + pl.port0 + w.host_in_port[h];
+    }
+    for (size_t j = 0; j < w.pend.size(); j++)
+        img.pend[j] = pl.msg0 + w.pend[j];
+    for (int x = 0; x < w.S1; x++)
+    {
+        SwRec &sr = img.sws[x];
+        sr.world = pl.world;
+        sr.local = x;
+        sr.port0 = pl.port0 + x * w.k;
+        sr.k = w.k;
+        for (int q = 0; q < w.k; q++)
+        {
+            PortRec &pr = img.ports[(size_t)x * w.k + q];
+            memset(&pr, 0, sizeof pr);
+            pr.red_k = w.p.ecn_k;
+            pr.qcap = w.p.queue;
+            int src = w.port_in[(size_t)x * w.k + q];
+            pr.in_link = src >= 0 ? pl.host0 + src : src == -1 ? -1 : pl.port_links + pl.port0 + (-2 - src);
+        }
+    }
+    // connections and messages
+    const int F = (int)w.conn_rows.size();
+    img.snd.assign(F, SndRec{});
+    img.rcv.assign(F, RcvRec{});
+    img.msgs.assign(w.rows.size(), MsgRec{});
+    uint64_t it_n = 0, oo_n = 0;
+    for (int cc = 0; cc < F; cc++)
+    {
+        const auto &cr = w.conn_rows[cc];
+        const FlowRow &first = w.rows[cr[0]];
+        SndRec &S_ = img.snd[cc];
+        RcvRec &R = img.rcv[cc];
+        memset(&S_, 0, sizeof S_);
+        memset(&R, 0, sizeof R);
+        S_.world = R.world = pl.world;
+        S_.src_local = R.src_local = first.src;
+        S_.dst_local = R.dst_local = first.dst;
+        S_.hash_data = w.hash_data[cc];
+        S_.hash_ack = R.hash_ack = w.hash_ack[cc];
+        S_.m_first = pl.msg0 + w.row_msg[cr[0]];
+        S_.m_cnt = (int)cr.size();
+        S_.fin_on = R.fin_on = (uint8_t)(w.p.fin != 0);
+        uint64_t segs = (w.conn_bytes[cc] + MSS - 1) / MSS + cr.size() + 1;
+        S_.it_cap = (uint32_t)std::min<uint64_t>(segs, 65536);
+        S_.it_off = pl.it0 + it_n;
+        it_n += S_.it_cap;
+        R.oo_cap = (uint32_t)std::min<uint64_t>(segs / 2 + 2, 4096);
+        R.oo_off = pl.oo0 + oo_n;
+        oo_n += R.oo_cap;
+        R.bytes = (uint32_t)w.conn_bytes[cc];
+        // initial values (reference src/model.h:124-277)
+        S_.cwnd = INIT_CWND;
+        S_.ssthresh = 0xFFFFFFFFu;
+        S_.first_partial = 1;
+        S_.cub_delaymin = S_.cub_epoch = S_.cub_roundstart = S_.cub_lastack = S_.cub_currrtt = INT64_MIN;
+        S_.ecn_echo_seq = S_.ecn_cwr_seq = -1;
+        S_.alpha = 1.0;
+        S_.srtt = -1;
+        S_.rto = MIN_RTO_PS;
+        S_.rto_at = -1;
+        S_.syn_at = -1;
+        R.fin_seq = R.synack_t = R.srtt = R.last_at = R.frx_at = R.syn_at = R.delack_at = R.ecn_ce_seq = -1;
+        for (int r : cr)
+        {
+            MsgRec &m = img.msgs[w.row_msg[r]];
+            m.conn = pl.conn0 + cc;
+            m.start = w.rows[r].start_ns * 1000;
+            m.est = m.done = -1;
+        }
+        uint64_t off = 0;
+        for (int r : cr)
+        {
+            off += (uint64_t)w.rows[r].size;
+            img.msgs[w.row_msg[r]].end = (uint32_t)off;
+        }
+    }
+    img.it_n = it_n;
+    img.oo_n = oo_n;
+    // per-packet spraying: node i's Ipv4GlobalRouting draws from stream i; switches are nodes
+    // H1.. of the world
+    img.rng.assign(w.S1, Rng{});
+    if (w.p.spray)
+        for (int x = 0; x < w.S1; x++)
+            img.rng[x] = stream_state(w.p.rng_seed, (uint64_t)(w.H1 + x), w.p.rng_run);
+}
+
+// a graph world's routing tables, uploaded into the context (pointers into d)
+int upload_graph(tb_ctx *c, const HostWorld &w, WorldDesc &d)
+{
+    if (w.kind != TB_TOPO_GRAPH)
+        return TB_OK;
+    int *hsw;
+    uint8_t *hp, *rn, *rp, *pd;
+    uint32_t *ro;
+    int64_t *ft;
+    std::vector<uint8_t> hport(w.host_port.begin(), w.host_port.end());
+    int r;
+    if ((r = c->upload(&hsw, w.host_sw, false)) || (r = c->upload(&hp, hport, false)) || (r = c->upload(&ro, w.rt_off, false)) ||
+        (r = c->upload(&rn, w.rt_n, false)) || (r = c->upload(&rp, w.rt_ports, false)) || (r = c->upload(&pd, w.port_dn, false)) ||
+        (r = c->upload(&ft, w.fail_ps, false)))
+        return r;
+    d.host_sw = hsw;
+    d.host_port = hp;
+    d.rt_off = ro;
+    d.rt_n = rn;
+    d.rt_ports = rp;
+    d.port_dn = pd;
+    d.fail_t = ft;
+    d.n_fail = (int)w.fail_ps.size();
+    return TB_OK;
+}
+
+// A world from the caller's arrays: topology, flow rows (reference src/main.cu:110-137,
+// 531-648), parameters; validated, wired and hashed.
+int make_world(const tb_topology *topo, int n_flows, const int *src, const int *dst, const long long *size, const long long *start_ns,
+               const long long *conn, const unsigned *hash_data, const unsigned *hash_ack, const tb_tcp_params *params, HostWorld &w)
+{
+    if (!topo || !params || n_flows < 0 || (n_flows > 0 && (!src || !dst || !size || !start_ns)))
+        return fail(TB_ERR_ARG, "tb_world_add_tcp: missing argument");
+    if (params->tcp < 0 || params->tcp > 2 || params->ecn_k < 0 || params->queue < 1 || params->queue > 65000)
+        return fail(TB_ERR_ARG, "bad TCP parameters");
+    w.topo = *topo;
+    w.p = *params;
+    if (topo->kind == TB_TOPO_GRAPH)
+    {
+        if (topo->n_links < 0 || (topo->n_links && (!topo->link_a || !topo->link_b)))
+            return fail(TB_ERR_ARG, "graph links missing");
+        w.link_a.assign(topo->link_a, topo->link_a + topo->n_links);
+        w.link_b.assign(topo->link_b, topo->link_b + topo->n_links);
+        for (int i = 0; i < topo->n_fails; i++)
+        {
+            w.fail_t.push_back(topo->fail_t_ns[i]);
+            w.fail_a.push_back(topo->fail_a[i]);
+            w.fail_b.push_back(topo->fail_b[i]);
+            w.fail_up.push_back(topo->fail_up ? topo->fail_up[i] : 0);
+        }
+    }
+    else if (topo->n_fails)
+        return fail(TB_ERR_ARG, "link failures need a topology file");
+    w.topo.link_a = w.topo.link_b = nullptr;
+    w.topo.fail_t_ns = nullptr;
+    w.topo.fail_a = w.topo.fail_b = w.topo.fail_up = nullptr;
+    w.rows.resize(n_flows);
+    for (int i = 0; i < n_flows; i++)
+        w.rows[i] = {src[i], dst[i], size[i], start_ns[i], conn ? conn[i] : -1};
+    if (hash_data && hash_ack)
+    {
+        w.given_hd.assign(hash_data, hash_data + n_flows);
+        w.given_ha.assign(hash_ack, hash_ack + n_flows);
+    }
+    std::string err;
+    if (!build_topology(w, err) || !build_flows(w, err))
+        return fail(TB_ERR_ARG, err);
+    return TB_OK;
+}
+
+// The units of the worlds still running (WorldCtl::next != INT64_MAX), hosts grouped `lanes` to
+// a unit: host units in order, then host_units + switch. `worlds`: (host0, hosts, sw0, switches)
+// of each world slot.
+void running_units(const std::vector<WorldCtl> &wc, const std::vector<std::array<int, 4>> &worlds, int lanes, int H,
+                   std::vector<int> &out)
+{
+    out.clear();
+    const int host_units = (H + lanes - 1) / lanes;
+    for (size_t w = 0; w < worlds.size(); w++)
+    {
+        if (wc[w].next == INT64_MAX || worlds[w][1] == 0)
+            continue;
+        for (int u = worlds[w][0] / lanes; u <= (worlds[w][0] + worlds[w][1] - 1) / lanes; u++)
+            if (out.empty() || out.back() < u)
+                out.push_back(u);
+    }
+    for (size_t w = 0; w < worlds.size(); w++)
+        if (wc[w].next != INT64_MAX)
+            for (int x = 0; x < worlds[w][3]; x++)
+                out.push_back(host_units + worlds[w][2] + x);
+}
+
+// the grid of a launch shape: a warp per unit, at most what is co-resident (0: does not fit)
+int grid_for(const tb_ctx *c, int host_lanes, int stage, int units = -1)
+{
+    int per_sm = tb::slot_kernel_blocks_per_sm(stage);
+    if (per_sm <= 0 || c->dev_sms <= 0)
+        return 0;
+    if (units < 0)
+        units = (c->sim.H + host_lanes - 1) / host_lanes + c->sim.S;
+    int need = std::max(1, (units + TB_WARPS_PER_BLOCK - 1) / TB_WARPS_PER_BLOCK);
+    int most = c->dev_sms * per_sm;
+    return c->grid_req > 0 ? std::min(c->grid_req, most) : std::min(need, most);
+}
+
 int prepare(tb_ctx *c)
 {
     if (c->prepared)
@@ -662,165 +929,50 @@ int prepare(tb_ctx *c)
     s.M = M;
     s.ring = ring;
     s.kmax = kmax;
-    // worlds (graph tables uploaded per world)
+    // worlds: each one's records for its place in the batch (graph tables uploaded per world)
     std::vector<WorldDesc> wd(W);
-    for (int i = 0; i < W; i++)
-    {
-        HostWorld &w = c->worlds[i];
-        WorldDesc &d = wd[i];
-        memset(&d, 0, sizeof d);
-        d.kind = w.kind;
-        d.k = w.k;
-        d.hk = w.hk;
-        d.leaves = w.leaves;
-        d.spines = w.spines;
-        d.hpl = w.hpl;
-        d.ecmp_n = w.ecmp_n;
-        d.H1 = w.H1;
-        d.S1 = w.S1;
-        d.host0 = w.host0;
-        d.sw0 = w.sw0;
-        d.conn0 = w.conn0;
-        d.msg0 = w.msg0;
-        d.n_msgs = (int)w.rows.size();
-        d.cc = (uint8_t)w.p.tcp;
-        d.fin = (uint8_t)(w.p.fin != 0);
-        d.spray = (uint8_t)(w.p.spray != 0);
-        d.red_k = w.p.ecn_k;
-        d.qcap = w.p.queue;
-        if (w.kind == TB_TOPO_GRAPH)
-        {
-            int *hsw;
-            uint8_t *hp, *rn, *rp, *pd;
-            uint32_t *ro;
-            int64_t *ft;
-            std::vector<uint8_t> hport(w.host_port.begin(), w.host_port.end());
-            int r;
-            if ((r = c->upload(&hsw, w.host_sw, false)) || (r = c->upload(&hp, hport, false)) || (r = c->upload(&ro, w.rt_off, false)) ||
-                (r = c->upload(&rn, w.rt_n, false)) || (r = c->upload(&rp, w.rt_ports, false)) || (r = c->upload(&pd, w.port_dn, false)) ||
-                (r = c->upload(&ft, w.fail_ps, false)))
-                return r;
-            d.host_sw = hsw;
-            d.host_port = hp;
-            d.rt_off = ro;
-            d.rt_n = rn;
-            d.rt_ports = rp;
-            d.port_dn = pd;
-            d.fail_t = ft;
-            d.n_fail = (int)w.fail_ps.size();
-        }
-    }
-    // hosts, switches, ports
     std::vector<HostRec> hosts(H);
     std::vector<SwRec> sws(S);
     std::vector<PortRec> ports(P);
     std::vector<int> pend(M);
-    int max_snd = 1, max_rcv = 1;
-    for (int i = 0; i < W; i++)
-    {
-        HostWorld &w = c->worlds[i];
-        std::vector<int> nsnd(w.H1, 0), nrcv(w.H1, 0);
-        for (auto &cr : w.conn_rows)
-        {
-            nsnd[w.rows[cr[0]].src]++;
-            nrcv[w.rows[cr[0]].dst]++;
-        }
-        for (int h = 0; h < w.H1; h++)
-        {
-            max_snd = std::max(max_snd, nsnd[h]);
-            max_rcv = std::max(max_rcv, nrcv[h]);
-            HostRec &hr = hosts[w.host0 + h];
-            memset(&hr, 0, sizeof hr);
-            hr.world = i;
-            hr.local = h;
-            hr.wake = 0; // every host runs the first slot
-            hr.pend_next = w.msg0 + w.pend_first[h];
-            hr.pend_end = w.msg0 + w.pend_first[h + 1];
-            hr.in_link = H + w.port0 + w.host_in_port[h];
-        }
-        for (int j = 0; j < M && j < (int)w.pend.size(); j++)
-            ;
-        for (size_t j = 0; j < w.pend.size(); j++)
-            pend[w.msg0 + j] = w.msg0 + w.pend[j];
-        for (int x = 0; x < w.S1; x++)
-        {
-            SwRec &sr = sws[w.sw0 + x];
-            sr.world = i;
-            sr.local = x;
-            sr.port0 = w.port0 + x * w.k;
-            sr.k = w.k;
-            for (int q = 0; q < w.k; q++)
-            {
-                PortRec &pr = ports[w.port0 + x * w.k + q];
-                memset(&pr, 0, sizeof pr);
-                pr.red_k = w.p.ecn_k;
-                pr.qcap = w.p.queue;
-                int src = w.port_in[(size_t)x * w.k + q];
-                pr.in_link = src >= 0 ? w.host0 + src : src == -1 ? -1 : H + w.port0 + (-2 - src);
-            }
-        }
-    }
-    s.act_cap = std::max(max_snd, max_rcv);
-    // connections and messages
     std::vector<SndRec> snd(C);
     std::vector<RcvRec> rcv(C);
     std::vector<MsgRec> msgs(M);
+    std::vector<Rng> rng(S);
     uint64_t it_total = 0, oo_total = 0;
+    int active = 1;
     for (int i = 0; i < W; i++)
     {
         HostWorld &w = c->worlds[i];
-        const int F = (int)w.conn_rows.size();
-        for (int cc = 0; cc < F; cc++)
-        {
-            const auto &cr = w.conn_rows[cc];
-            const FlowRow &first = w.rows[cr[0]];
-            SndRec &S_ = snd[w.conn0 + cc];
-            RcvRec &R = rcv[w.conn0 + cc];
-            memset(&S_, 0, sizeof S_);
-            memset(&R, 0, sizeof R);
-            S_.world = R.world = i;
-            S_.src_local = R.src_local = first.src;
-            S_.dst_local = R.dst_local = first.dst;
-            S_.hash_data = w.hash_data[cc];
-            S_.hash_ack = R.hash_ack = w.hash_ack[cc];
-            S_.m_first = w.msg0 + w.row_msg[cr[0]];
-            S_.m_cnt = (int)cr.size();
-            S_.fin_on = R.fin_on = (uint8_t)(w.p.fin != 0);
-            uint64_t segs = (w.conn_bytes[cc] + MSS - 1) / MSS + cr.size() + 1;
-            S_.it_cap = (uint32_t)std::min<uint64_t>(segs, 65536);
-            S_.it_off = it_total;
-            it_total += S_.it_cap;
-            R.oo_cap = (uint32_t)std::min<uint64_t>(segs / 2 + 2, 4096);
-            R.oo_off = oo_total;
-            oo_total += R.oo_cap;
-            R.bytes = (uint32_t)w.conn_bytes[cc];
-            // initial values (reference src/model.h:124-277)
-            S_.cwnd = INIT_CWND;
-            S_.ssthresh = 0xFFFFFFFFu;
-            S_.first_partial = 1;
-            S_.cub_delaymin = S_.cub_epoch = S_.cub_roundstart = S_.cub_lastack = S_.cub_currrtt = INT64_MIN;
-            S_.ecn_echo_seq = S_.ecn_cwr_seq = -1;
-            S_.alpha = 1.0;
-            S_.srtt = -1;
-            S_.rto = MIN_RTO_PS;
-            S_.rto_at = -1;
-            S_.syn_at = -1;
-            R.fin_seq = R.synack_t = R.srtt = R.last_at = R.frx_at = R.syn_at = R.delack_at = R.ecn_ce_seq = -1;
-            for (int r : cr)
-            {
-                MsgRec &m = msgs[w.msg0 + w.row_msg[r]];
-                m.conn = w.conn0 + cc;
-                m.start = w.rows[r].start_ns * 1000;
-                m.est = m.done = -1;
-            }
-            uint64_t off = 0;
-            for (int r : cr)
-            {
-                off += (uint64_t)w.rows[r].size;
-                msgs[w.msg0 + w.row_msg[r]].end = (uint32_t)off;
-            }
-        }
+        Place pl;
+        pl.world = i;
+        pl.host0 = w.host0;
+        pl.sw0 = w.sw0;
+        pl.port0 = w.port0;
+        pl.conn0 = w.conn0;
+        pl.msg0 = w.msg0;
+        pl.it0 = it_total;
+        pl.oo0 = oo_total;
+        pl.port_links = H;
+        WorldImage img;
+        build_image(w, pl, img);
+        int r;
+        if ((r = upload_graph(c, w, img.desc)))
+            return r;
+        wd[i] = img.desc;
+        std::copy(img.hosts.begin(), img.hosts.end(), hosts.begin() + w.host0);
+        std::copy(img.sws.begin(), img.sws.end(), sws.begin() + w.sw0);
+        std::copy(img.ports.begin(), img.ports.end(), ports.begin() + w.port0);
+        std::copy(img.pend.begin(), img.pend.end(), pend.begin() + w.msg0);
+        std::copy(img.snd.begin(), img.snd.end(), snd.begin() + w.conn0);
+        std::copy(img.rcv.begin(), img.rcv.end(), rcv.begin() + w.conn0);
+        std::copy(img.msgs.begin(), img.msgs.end(), msgs.begin() + w.msg0);
+        std::copy(img.rng.begin(), img.rng.end(), rng.begin() + w.sw0);
+        it_total += img.it_n;
+        oo_total += img.oo_n;
+        active = std::max(active, img.active);
     }
+    s.act_cap = active;
     c->host_msgs = msgs;
     int r;
     WorldDesc *dwd;
@@ -852,20 +1004,8 @@ int prepare(tb_ctx *c)
     if ((r = c->alloc(&s.sw_ts, (size_t)S * per_sw, false)) || (r = c->alloc(&s.sw_ref, (size_t)S * per_sw, false)) ||
         (r = c->alloc(&s.sw_up, (size_t)S * per_sw, false)))
         return r;
-    {
-        std::vector<Rng> st(S);
-        for (int i = 0; i < W; i++)
-        {
-            HostWorld &w = c->worlds[i];
-            if (!w.p.spray)
-                continue;
-            // node i's Ipv4GlobalRouting draws from stream i; switches are nodes H1.. of the world
-            for (int x = 0; x < w.S1; x++)
-                st[w.sw0 + x] = stream_state(w.p.rng_seed, (uint64_t)(w.H1 + x), w.p.rng_run);
-        }
-        if ((r = c->upload(&s.sw_rng, st, true)))
-            return r;
-    }
+    if ((r = c->upload(&s.sw_rng, rng, true)))
+        return r;
     {
         // TcpCubic's K = pow(n / 0.4, 1/3) for window differences n, from the host libm (the
         // function ns-3 calls), so that every K equals ns-3's
@@ -892,7 +1032,19 @@ int prepare(tb_ctx *c)
         ctl[0].finished = M == 0;
         if ((r = c->upload(&s.ctl, ctl, true)))
             return r;
+        std::vector<WorldCtl> wctl(W);
+        for (auto &x : wctl)
+        {
+            memset(&x, 0, sizeof x);
+            x.next = 0;
+            x.wake = (unsigned long long)INT64_MAX;
+            x.act = x.prev = 1; // (as the ticket block's: no skip before the first slots have run)
+        }
+        if ((r = c->upload(&s.wctl, wctl, true)))
+            return r;
     }
+    if (!c->arena && (r = c->alloc(&c->d_units, (size_t)H + S, false)))
+        return r;
     // snapshots of the initial state
     for (auto &sn : c->snaps)
         if (cudaMemcpy(sn.src, sn.dst, sn.bytes, cudaMemcpyDeviceToDevice) != cudaSuccess)
@@ -903,17 +1055,12 @@ int prepare(tb_ctx *c)
     {
         cudaEventCreate(&c->ev0);
         cudaEventCreate(&c->ev1);
+        cudaEventCreate(&c->la);
+        cudaEventCreate(&c->lb);
     }
-    // the grid: every unit a warp, at most what is co-resident
-    int dev_sms = 0;
-    cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->device);
-    int per_sm = tb::slot_kernel_blocks_per_sm();
-    if (per_sm <= 0 || dev_sms <= 0)
+    cudaDeviceGetAttribute(&c->dev_sms, cudaDevAttrMultiProcessorCount, c->device);
+    if ((c->grid = grid_for(c, c->host_lanes, c->stage_cap)) <= 0)
         return fail(TB_ERR_CUDA, "the slot kernel does not fit on the device");
-    int units = (H + c->host_lanes - 1) / c->host_lanes + S;
-    int need = (units + TB_WARPS_PER_BLOCK - 1) / TB_WARPS_PER_BLOCK;
-    int most = dev_sms * per_sm;
-    c->grid = c->grid_req > 0 ? std::min(c->grid_req, most) : std::min(need, most);
     c->prepared = true;
     cudaDeviceSynchronize();
     c->stats.upload_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -952,6 +1099,8 @@ int tb_ctx_destroy(tb_ctx *ctx)
     {
         cudaEventDestroy(ctx->ev0);
         cudaEventDestroy(ctx->ev1);
+        cudaEventDestroy(ctx->la);
+        cudaEventDestroy(ctx->lb);
     }
     delete ctx;
     return TB_OK;
@@ -961,45 +1110,14 @@ int tb_world_add_tcp(tb_ctx *ctx, const tb_topology *topo, int n_flows, const in
                      const long long *start_ns, const long long *conn, const unsigned *hash_data, const unsigned *hash_ack,
                      const tb_tcp_params *params, int *world)
 {
-    if (!ctx || !topo || !params || n_flows < 0 || (n_flows > 0 && (!src || !dst || !size || !start_ns)))
+    if (!ctx)
         return fail(TB_ERR_ARG, "tb_world_add_tcp: missing argument");
     if (ctx->prepared)
         return fail(TB_ERR_STATE, "the batch is already prepared");
-    if (params->tcp < 0 || params->tcp > 2 || params->ecn_k < 0 || params->queue < 1 || params->queue > 65000)
-        return fail(TB_ERR_ARG, "bad TCP parameters");
     HostWorld w;
-    w.topo = *topo;
-    w.p = *params;
-    if (topo->kind == TB_TOPO_GRAPH)
-    {
-        if (topo->n_links < 0 || (topo->n_links && (!topo->link_a || !topo->link_b)))
-            return fail(TB_ERR_ARG, "graph links missing");
-        w.link_a.assign(topo->link_a, topo->link_a + topo->n_links);
-        w.link_b.assign(topo->link_b, topo->link_b + topo->n_links);
-        for (int i = 0; i < topo->n_fails; i++)
-        {
-            w.fail_t.push_back(topo->fail_t_ns[i]);
-            w.fail_a.push_back(topo->fail_a[i]);
-            w.fail_b.push_back(topo->fail_b[i]);
-            w.fail_up.push_back(topo->fail_up ? topo->fail_up[i] : 0);
-        }
-    }
-    else if (topo->n_fails)
-        return fail(TB_ERR_ARG, "link failures need a topology file");
-    w.topo.link_a = w.topo.link_b = nullptr;
-    w.topo.fail_t_ns = nullptr;
-    w.topo.fail_a = w.topo.fail_b = w.topo.fail_up = nullptr;
-    w.rows.resize(n_flows);
-    for (int i = 0; i < n_flows; i++)
-        w.rows[i] = {src[i], dst[i], size[i], start_ns[i], conn ? conn[i] : -1};
-    if (hash_data && hash_ack)
-    {
-        w.given_hd.assign(hash_data, hash_data + n_flows);
-        w.given_ha.assign(hash_ack, hash_ack + n_flows);
-    }
-    std::string err;
-    if (!build_topology(w, err) || !build_flows(w, err))
-        return fail(TB_ERR_ARG, err);
+    int r = make_world(topo, n_flows, src, dst, size, start_ns, conn, hash_data, hash_ack, params, w);
+    if (r)
+        return r;
     int H = 0;
     for (auto &x : ctx->worlds)
         H += x.H1;
@@ -1032,14 +1150,26 @@ int tb_reset(tb_ctx *ctx)
     return TB_OK;
 }
 
-int tb_set_launch(tb_ctx *ctx, int host_lanes, int grid)
+int tb_set_launch_shape(tb_ctx *ctx, int host_lanes, int stage_frames, int grid)
 {
-    if (!ctx || host_lanes < 1 || host_lanes > 32 || grid < 0)
-        return fail(TB_ERR_ARG, "host_lanes 1..32, grid >= 0");
-    if (ctx->prepared)
-        return fail(TB_ERR_STATE, "set the launch shape before tb_prepare");
+    if (!ctx || host_lanes < 1 || host_lanes > 32 || grid < 0 || stage_frames < 1 || stage_frames > SW_STAGE_MAX)
+        return fail(TB_ERR_ARG, "host_lanes 1..32, stage_frames 1.." + std::to_string(SW_STAGE_MAX) + ", grid >= 0");
     ctx->host_lanes = host_lanes;
+    ctx->stage_cap = stage_frames;
     ctx->grid_req = grid;
+    ctx->autotune = false;
+    if (ctx->prepared && (ctx->grid = grid_for(ctx, host_lanes, stage_frames)) <= 0)
+        return fail(TB_ERR_CUDA, "the slot kernel does not fit on the device with this shape");
+    return TB_OK;
+}
+
+int tb_set_launch(tb_ctx *ctx, int host_lanes, int grid) { return tb_set_launch_shape(ctx, host_lanes, SW_STAGE_MAX, grid); }
+
+int tb_set_autotune(tb_ctx *ctx, int on)
+{
+    if (!ctx)
+        return fail(TB_ERR_ARG, "ctx is NULL");
+    ctx->autotune = on != 0;
     return TB_OK;
 }
 
@@ -1056,17 +1186,113 @@ int tb_run(tb_ctx *ctx, long long max_slots)
     Sim s = ctx->sim;
     s.max_slots = max_slots > 0 ? max_slots : 2000000;
     SlotCtl ctl{};
-    long long launches = 0;
+    // Launch shapes: hosts per warp and frames staged per warp (a smaller staging area leaves room
+    // for more resident blocks). The results do not depend on the shape. Autotuning starts from
+    // one host per warp while the hosts fit the resident warps about once (latency-bound: each
+    // host's serial events are the slot's critical path), else 32 hosts per warp (throughput-
+    // bound: the lanes' memory accesses overlap). Every `period` launches, each shape runs a
+    // probe of `probe` slots, and a shape whose device time per slot beats the current one's by
+    // more than 5% takes over.
+    struct Shape
+    {
+        int lanes, stage, grid;
+        long long slots;
+    };
+    std::vector<Shape> shapes;
+    size_t best = 0;
+    if (ctx->autotune)
+    {
+        const int cand[][2] = {{1, SW_STAGE_MAX}, {4, SW_STAGE_MAX}, {32, SW_STAGE_MAX}, {1, 96}, {32, 96}};
+        for (auto &c : cand)
+        {
+            int g = grid_for(ctx, c[0], c[1]);
+            if (g > 0)
+                shapes.push_back({c[0], c[1], g, 0});
+        }
+        const long long resident = (long long)ctx->dev_sms * std::max(1, tb::slot_kernel_blocks_per_sm(SW_STAGE_MAX)) * TB_WARPS_PER_BLOCK;
+        const int lanes0 = s.H + s.S <= 2 * resident ? 1 : 32;
+        for (size_t k = 0; k < shapes.size(); k++)
+            if (shapes[k].lanes == lanes0 && shapes[k].stage == SW_STAGE_MAX)
+                best = k;
+    }
+    if (shapes.empty())
+        shapes.push_back({ctx->host_lanes, ctx->stage_cap, ctx->grid, 0});
+    const int probe = 64, period = 6;
+    const int run_slots = shapes.size() > 1 ? std::min(ctx->max_slots_per_launch, 1024) : ctx->max_slots_per_launch;
+    long long launches = 0, since = 0;
+    // the running worlds' units: rebuilt when a world finishes (or the shape changes), so that a
+    // finished world's entities cost a launch nothing and the grid shrinks with the work
+    std::vector<std::array<int, 4>> wr(s.W);
+    for (int i = 0; i < s.W; i++)
+        wr[i] = {ctx->worlds[i].host0, ctx->worlds[i].H1, ctx->worlds[i].sw0, ctx->worlds[i].S1};
+    std::vector<WorldCtl> wc(s.W);
+    std::vector<int> ulist;
+    int alive = s.W, list_alive = s.W, list_lanes = 0;
+    s.unit_list = nullptr;
+    s.n_list = 0;
     cudaEventRecord(ctx->ev0, ctx->stream);
     for (;;)
     {
-        int e = tb::launch_slots(s, ctx->grid, ctx->max_slots_per_launch, ctx->host_lanes, ctx->stream);
-        if (e)
-            return fail(TB_ERR_CUDA, std::string("slot kernel launch: ") + cudaGetErrorString((cudaError_t)e));
-        launches++;
-        if (cudaMemcpyAsync(&ctl, s.ctl, sizeof ctl, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
-            cudaStreamSynchronize(ctx->stream) != cudaSuccess)
-            return fail(TB_ERR_CUDA, std::string("slot kernel: ") + cudaGetErrorString(cudaGetLastError()));
+        const bool explore = shapes.size() > 1 && since >= period;
+        std::vector<double> per_slot(shapes.size(), -1);
+        for (size_t k = 0; k < shapes.size(); k++)
+        {
+            if (!explore && k != best)
+                continue;
+            Shape &sh = shapes[k];
+            int grid = sh.grid;
+            if (ctx->d_units && alive < s.W)
+            {
+                if (alive != list_alive || sh.lanes != list_lanes)
+                {
+                    running_units(wc, wr, sh.lanes, s.H, ulist);
+                    if (!ulist.empty() &&
+                        cudaMemcpyAsync(ctx->d_units, ulist.data(), sizeof(int) * ulist.size(), cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
+                        return fail(TB_ERR_CUDA, "cudaMemcpyAsync failed");
+                    list_alive = alive;
+                    list_lanes = sh.lanes;
+                }
+                s.unit_list = ctx->d_units;
+                s.n_list = (int)ulist.size();
+                grid = grid_for(ctx, sh.lanes, sh.stage, s.n_list);
+            }
+            const long long slots_before = ctl.slots_run;
+            cudaEventRecord(ctx->la, ctx->stream);
+            int e = tb::launch_slots(s, grid, explore ? probe : run_slots, sh.lanes, sh.stage, ctx->stream);
+            if (e)
+                return fail(TB_ERR_CUDA, std::string("slot kernel launch: ") + cudaGetErrorString((cudaError_t)e));
+            cudaEventRecord(ctx->lb, ctx->stream);
+            launches++;
+            if (cudaMemcpyAsync(&ctl, s.ctl, sizeof ctl, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+                (s.W > 1 && cudaMemcpyAsync(wc.data(), s.wctl, sizeof(WorldCtl) * s.W, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess) ||
+                cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+                return fail(TB_ERR_CUDA, std::string("slot kernel: ") + cudaGetErrorString(cudaGetLastError()));
+            if (s.W > 1)
+            {
+                alive = 0;
+                for (const WorldCtl &x : wc)
+                    alive += x.next != INT64_MAX;
+            }
+            const long long ran = ctl.slots_run - slots_before;
+            sh.slots += ran;
+            float lms = 0;
+            cudaEventElapsedTime(&lms, ctx->la, ctx->lb);
+            if (ran >= probe / 2)
+                per_slot[k] = lms / (double)ran;
+            if (ctl.finished || ctl.error)
+                break;
+        }
+        if (explore)
+        {
+            size_t b = best;
+            for (size_t k = 0; k < shapes.size(); k++)
+                if (per_slot[k] > 0 && (per_slot[b] <= 0 || per_slot[k] < 0.95 * per_slot[b]))
+                    b = k;
+            best = b;
+            since = 0;
+        }
+        else
+            since++;
         if (ctl.finished || ctl.error)
             break;
     }
@@ -1075,6 +1301,11 @@ int tb_run(tb_ctx *ctx, long long max_slots)
     float ms = 0;
     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
     ctx->ran = true;
+    // the shape that ran the most slots
+    size_t most = 0;
+    for (size_t k = 1; k < shapes.size(); k++)
+        if (shapes[k].slots > shapes[most].slots)
+            most = k;
 #ifdef TB_PROFILE
     if (ctl.slots_run > 1)
     {
@@ -1103,9 +1334,11 @@ int tb_run(tb_ctx *ctx, long long max_slots)
     st.host_frames = ev[EV_HOST_FRAMES];
     st.switch_events = ev[EV_SW_PKT];
     st.packet_events = st.host_events + st.switch_events;
-    st.grid = ctx->grid;
-    st.host_lanes = ctx->host_lanes;
+    st.grid = shapes[most].grid;
+    st.host_lanes = shapes[most].lanes;
     st.warps_per_block = TB_WARPS_PER_BLOCK;
+    st.stage_frames = shapes[most].stage;
+    st.autotuned = shapes.size() > 1;
     st.bytes_d2h = 0;
     if (ctl.error)
         return fail(TB_ERR_TIMEOUT, "a device-side barrier wait ran out; the run was abandoned");
@@ -1168,8 +1401,9 @@ int tb_hashes(tb_ctx *ctx, int world, unsigned *hash_data, unsigned *hash_ack)
 
 int tb_abi_sizes(unsigned long long *out, int n)
 {
-    const unsigned long long v[3] = {sizeof(tb_topology), sizeof(tb_tcp_params), sizeof(tb_stats)};
-    for (int i = 0; i < n && i < 3; i++)
+    const unsigned long long v[6] = {sizeof(tb_topology),   sizeof(tb_tcp_params),   sizeof(tb_stats),
+                                     sizeof(tb_serve_caps), sizeof(tb_request_info), sizeof(tb_serve_stats)};
+    for (int i = 0; i < n && i < 6; i++)
         out[i] = v[i];
     return TB_OK;
 }
@@ -1246,7 +1480,7 @@ extern "C" int tb_run_static(int device, const tb_topology *topo, int n_flows, c
     SlotCtl ctl{};
     for (;;)
     {
-        int e = tb::launch_slots(s, c.grid, c.max_slots_per_launch, c.host_lanes, 0);
+        int e = tb::launch_slots(s, c.grid, c.max_slots_per_launch, c.host_lanes, c.stage_cap, 0);
         if (e)
             return fail(TB_ERR_CUDA, std::string("slot kernel launch: ") + cudaGetErrorString((cudaError_t)e));
         if (cudaMemcpy(&ctl, s.ctl, sizeof ctl, cudaMemcpyDeviceToHost) != cudaSuccess)
@@ -1269,3 +1503,6 @@ extern "C" int tb_run_static(int device, const tb_topology *topo, int n_flows, c
     }
     return TB_OK;
 }
+
+// ------------------------------------------------------------------ serving
+#include "tb_serve.cuh"

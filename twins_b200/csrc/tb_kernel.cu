@@ -19,6 +19,9 @@ namespace tb
 {
 
 constexpr int WARPS_PER_BLOCK = TB_WARPS_PER_BLOCK;
+#ifndef TB_MIN_BLOCKS
+#define TB_MIN_BLOCKS 4 // resident blocks per SM the register budget allows (with the smaller staging areas)
+#endif
 constexpr long long BARRIER_SPIN_LIMIT = 1ll << 22; // polls of >= 64 ns: several seconds
 
 __device__ __forceinline__ unsigned long long globaltimer()
@@ -118,68 +121,133 @@ __device__ void sw_phase_spray_warp(const SwCtx &x, const SwShared &sh, int lane
         x.s->sw_rng[x.sw] = st;
 }
 
-// A host unit with one host per warp: the warp copies the host's incoming link messages to shared
-// memory (one cooperative pass) and prefetches into L1 what the host's events will read: the
-// records of the frames' connections with the heads of their sent lists and RTT histories, the
-// head frames of the host's egress queue, and the timers of its active connections. Lane 0 then
-// runs the host's slot (host_step) on the staged frames. Returns the staging area, or null when
-// the messages do not fit it (host_step then reads them in place).
-__device__ const Frame *host_prepare(const Sim &s, int h, int64_t t, int lane, SwShared &sh)
+// The world's rule for this slot (reference src/kernel.cuh:79-112, per world): the next launch
+// slot its entities run, and its time origin; both read through L2 (the controller of another SM
+// writes them)
+__device__ __forceinline__ int64_t world_next(const Sim &s, int w) { return __ldcg(&s.wctl[w].next); }
+__device__ __forceinline__ int64_t world_t0(const Sim &s, int w) { return __ldcg(&s.wctl[w].t0); }
+
+// a host's slot results into its world's record (wake: a world-local slot)
+__device__ __forceinline__ void host_report(const Sim &s, int w, int64_t t0, bool act, int64_t wake, unsigned done)
 {
-    const HostRec &hr = s.hosts[h];
-    const int link = hr.in_link;
-    const int n2 = t >= 2 ? msg_count(s, t - 2, link) : 0, n1 = t >= 1 ? msg_count(s, t - 1, link) : 0, n = n2 + n1;
-    if (n == 0 && t < hr.wake && hr.q_size == 0)
-        return nullptr; // (nothing to do this slot: host_step returns at once)
-    const bool staged = n <= SW_STAGE;
-    if (staged)
-        for (int i = lane; i < n; i += 32)
-            frame_load_link(sh.fr[i], i < n2 ? msg_frames(s, t - 2, link) + i : msg_frames(s, t - 1, link) + (i - n2));
-    __syncwarp();
-    if (staged)
-        for (int i = lane; i < n; i += 32)
-        {
-            const Frame &f = sh.fr[i];
-            if (f.to_sender)
-            {
-                const SndRec *S = &s.snd[f.flow];
-                for (int b = 0; b < (int)sizeof(SndRec); b += 128)
-                    prefetch_l1((const char *)S + b);
-                const uint64_t off = S->it_off;
-                prefetch_l1(&s.it_start[off + S->it_head]);
-                prefetch_l1(&s.it_fl[off + S->it_head]);
-                const uint32_t hh = S->h_head;
-                prefetch_l1(&s.h_seq[off + hh]);
-                prefetch_l1(&s.h_cnt[off + hh]);
-                prefetch_l1(&s.h_t[off + hh]);
-            }
-            else
-            {
-                const RcvRec *R = &s.rcv[f.flow];
-                for (int b = 0; b < (int)sizeof(RcvRec); b += 128)
-                    prefetch_l1((const char *)R + b);
-            }
-        }
-    if (lane < 8 && lane < hr.q_size)
-    {
-        int at = hr.q_head + lane;
-        if (at >= s.ring)
-            at -= s.ring;
-        prefetch_l1(&s.host_ring[(size_t)h * s.ring + at]);
-    }
-    const int *as = s.act_snd + (size_t)h * s.act_cap, *ar = s.act_rcv + (size_t)h * s.act_cap;
-    for (int i = lane; i < hr.n_snd; i += 32)
-        prefetch_l1(&s.snd[as[i]].rto_at);
-    for (int i = lane; i < hr.n_rcv; i += 32)
-        prefetch_l1(&s.rcv[ar[i]].delack_at);
-    __syncwarp();
-    return staged ? sh.fr : nullptr;
+    WorldCtl *wc = &s.wctl[w];
+    if (act)
+        atomicOr(&wc->act, 1u);
+    if (wake != INT64_MAX)
+        atomicMin(&wc->wake, (unsigned long long)(wake + t0));
+    if (done)
+        atomicAdd(&wc->fdone, done);
 }
 
-// one switch, one slot, by its warp (lanes >= k idle but take part in the warp barriers)
-__device__ bool switch_step(const Sim &s, int sw, int64_t t, int lane, SwShared &sh, unsigned &ties)
+// A host unit at launch slot t: one host per warp (host_lanes 1) or one per lane. With one host
+// per warp, the warp reads the host's link-message tags (by launch slot) together with its world's
+// rule; a host whose world does not run this slot, or that has no frame arriving, no timer due and
+// an empty queue, only reports its wake-up. Otherwise the warp copies the host's incoming link
+// messages to shared memory (one cooperative pass) and prefetches into L1 what the host's events
+// will read: the records of the frames' connections with the heads of their sent lists and RTT
+// histories, the head frames of the host's egress queue, and the timers of its active
+// connections; then lane 0 runs the host's slot (host_step) on the staged frames, or in place
+// when they do not fit. With several hosts per warp each lane runs its own host in place.
+__device__ __forceinline__ void host_unit(const Sim &s, int u, int host_lanes, int64_t t, int lane, SwShared &sh, unsigned &ties,
+                                          unsigned &blk_done)
+{
+    int h, w = 0, n2 = -1, n1 = -1;
+    int64_t t0 = 0;
+    bool run = false;
+    const Frame *stage = nullptr;
+    if (host_lanes == 1)
+    {
+        h = u;
+        const HostRec &hr = s.hosts[h];
+        w = hr.world;
+        const int link = hr.in_link;
+        n2 = t >= 2 ? msg_count(s, t - 2, link) : 0;
+        n1 = t >= 1 ? msg_count(s, t - 1, link) : 0;
+        const int n = n2 + n1;
+        const int64_t next = world_next(s, w);
+        t0 = world_t0(s, w);
+        if (t < next)
+            return;
+        if (n == 0 && t - t0 < hr.wake && hr.q_size == 0)
+        {
+            if (lane == 0 && hr.wake != INT64_MAX)
+                atomicMin(&s.wctl[w].wake, (unsigned long long)(hr.wake + t0));
+            return;
+        }
+        const bool staged = n <= sh.cap;
+        if (staged)
+            for (int i = lane; i < n; i += 32)
+                frame_load_link(sh.fr()[i], i < n2 ? msg_frames(s, t - 2, link) + i : msg_frames(s, t - 1, link) + (i - n2));
+        __syncwarp();
+        if (staged)
+            for (int i = lane; i < n; i += 32)
+            {
+                const Frame &f = sh.fr()[i];
+                if (f.to_sender)
+                {
+                    const SndRec *S = &s.snd[f.flow];
+                    for (int b = 0; b < (int)sizeof(SndRec); b += 128)
+                        prefetch_l1((const char *)S + b);
+                    const uint64_t off = S->it_off;
+                    prefetch_l1(&s.it_start[off + S->it_head]);
+                    prefetch_l1(&s.it_fl[off + S->it_head]);
+                    const uint32_t hh = S->h_head;
+                    prefetch_l1(&s.h_seq[off + hh]);
+                    prefetch_l1(&s.h_cnt[off + hh]);
+                    prefetch_l1(&s.h_t[off + hh]);
+                }
+                else
+                {
+                    const RcvRec *R = &s.rcv[f.flow];
+                    for (int b = 0; b < (int)sizeof(RcvRec); b += 128)
+                        prefetch_l1((const char *)R + b);
+                }
+            }
+        if (lane < 8 && lane < hr.q_size)
+        {
+            int at = hr.q_head + lane;
+            if (at >= s.ring)
+                at -= s.ring;
+            prefetch_l1(&s.host_ring[(size_t)h * s.ring + at]);
+        }
+        const int *as = s.act_snd + (size_t)h * s.act_cap, *ar = s.act_rcv + (size_t)h * s.act_cap;
+        for (int i = lane; i < hr.n_snd; i += 32)
+            prefetch_l1(&s.snd[as[i]].rto_at);
+        for (int i = lane; i < hr.n_rcv; i += 32)
+            prefetch_l1(&s.rcv[ar[i]].delack_at);
+        __syncwarp();
+        stage = staged ? sh.fr() : nullptr;
+        run = lane == 0;
+    }
+    else
+    {
+        h = u * host_lanes + lane;
+        if (lane < host_lanes && h < s.H)
+        {
+            w = s.hosts[h].world;
+            t0 = world_t0(s, w);
+            run = t >= world_next(s, w);
+        }
+    }
+    if (run)
+    {
+        int64_t wake = INT64_MAX;
+        unsigned done = 0;
+        const bool act = host_step(s, h, t - t0, t, &wake, &ties, &done, stage, n2, n1);
+        host_report(s, w, t0, act, wake, done);
+        if (done)
+            atomicAdd(&blk_done, done);
+    }
+    __syncwarp(); // (the staging area is reused by the warp's next unit)
+}
+
+// one switch, one slot (launch slot gt), by its warp (lanes >= k idle but take part in the warp
+// barriers); nothing when its world does not run this slot
+__device__ bool switch_step(const Sim &s, int sw, int64_t gt, int lane, SwShared &sh, unsigned &ties)
 {
     const SwRec &sr = s.sws[sw];
+    const int64_t next = world_next(s, sr.world), t0 = world_t0(s, sr.world);
+    const int64_t t = gt - t0;
     SwCtx x;
     x.s = &s;
     x.wd = &s.worlds[sr.world];
@@ -188,6 +256,7 @@ __device__ bool switch_step(const Sim &s, int sw, int64_t t, int lane, SwShared 
     x.ports = s.ports + sr.port0;
     x.scratch = (size_t)sw * s.kmax * 2 * MAX_TX;
     x.t = t;
+    x.gt = gt;
     x.spray = x.wd->spray != 0;
     const int k = sr.k;
     const bool on = lane < k;
@@ -197,6 +266,10 @@ __device__ bool switch_step(const Sim &s, int sw, int64_t t, int lane, SwShared 
 #endif
     if (on)
         sw_phase_sizes(x, sh, lane);
+    // its world does not run this slot; or no frame arriving and every queue empty: nothing to do
+    // (its link messages of this slot stay unwritten, and a stale tag reads as an empty message)
+    if (gt < next || !__any_sync(0xffffffffu, on && (sh.raw2[lane] | sh.raw1[lane] | x.ports[lane].q_size) != 0))
+        return false;
     __syncwarp();
     if (lane == 0)
         sw_phase_layout(x, sh);
@@ -261,94 +334,106 @@ __device__ bool switch_step(const Sim &s, int sw, int64_t t, int lane, SwShared 
     return any;
 }
 
-__global__ void __launch_bounds__(WARPS_PER_BLOCK * 32) slot_kernel(Sim s, int max_slots_per_launch, int host_lanes)
+__global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, TB_MIN_BLOCKS) slot_kernel(Sim s, int max_slots_per_launch, int host_lanes, int stage_cap)
 {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
-    SwShared *sw_sh = reinterpret_cast<SwShared *>(dyn_smem); // one per warp
-    __shared__ unsigned blk_act, blk_done;
-    __shared__ unsigned long long blk_wake;
+    __shared__ unsigned blk_done;
+    __shared__ int blk_last;
+    __shared__ unsigned long long blk_next;
+    __shared__ unsigned blk_alive;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int gwarp = blockIdx.x * WARPS_PER_BLOCK + warp, nwarps = gridDim.x * WARPS_PER_BLOCK;
     const int host_units = (s.H + host_lanes - 1) / host_lanes;
     const int units = host_units + s.S;
+    SwShared &sh = *sw_shared_at(dyn_smem + (size_t)warp * sw_shared_bytes(stage_cap), stage_cap); // the warp's scratch
+    __syncwarp();
     SlotCtl *ctl = s.ctl;
     volatile SlotCtl *vc = ctl;
     for (int it = 0; it < max_slots_per_launch; it++)
     {
         if (threadIdx.x == 0)
-        {
-            blk_act = 0;
             blk_done = 0;
-            blk_wake = ~0ull;
-        }
         __syncthreads();
         // (written by the last block of the previous barrier, before it released the others)
         if (vc->finished)
             return;
         const int64_t t = vc->slot;
         unsigned ties = 0;
-        for (int u = gwarp; u < units; u += nwarps)
+        const int n_iter = s.unit_list ? s.n_list : units;
+        for (int i = gwarp; i < n_iter; i += nwarps)
         {
+            const int u = s.unit_list ? __ldg(&s.unit_list[i]) : i;
 #ifdef TB_PROFILE
             unsigned long long p0 = globaltimer();
 #endif
             if (u < host_units)
+                host_unit(s, u, host_lanes, t, lane, sh, ties, blk_done);
+            else
             {
-                int h = u * host_lanes + lane;
-                const Frame *stage = nullptr;
-                if (host_lanes == 1)
-                {
-                    h = u;
-                    stage = host_prepare(s, h, t, lane, sw_sh[warp]);
-                }
-                if (lane < host_lanes && h < s.H)
-                {
-                    int64_t w = INT64_MAX;
-                    unsigned done = 0;
-                    if (host_step(s, h, t, &w, &ties, &done, stage))
-                        atomicOr(&blk_act, 1u);
-                    if (done)
-                        atomicAdd(&blk_done, done);
-                    atomicMin(&blk_wake, (unsigned long long)w);
-                }
-                __syncwarp(); // (the staging area is reused by the warp's next unit)
+                const int sw = u - host_units;
+                if (switch_step(s, sw, t, lane, sh, ties) && lane == 0)
+                    atomicOr(&s.wctl[s.sws[sw].world].act, 1u);
             }
-            else if (switch_step(s, u - host_units, t, lane, sw_sh[warp], ties) && lane == 0)
-                atomicOr(&blk_act, 1u);
 #ifdef TB_PROFILE
             if (lane == 0)
                 atomicMax(u < host_units ? &ctl->prof_host_max : &ctl->prof_sw_max, globaltimer() - p0);
 #endif
         }
         __syncthreads();
+        unsigned g = 0; // (thread 0: the barrier generation before it arrives)
         if (threadIdx.x == 0)
         {
-            if (blk_act)
-                atomicOr(&ctl->act_cur, 1u);
-            if (blk_wake != ~0ull)
-                atomicMin(&ctl->next_wake, blk_wake);
             if (blk_done)
                 atomicAdd(&ctl->flows_done, blk_done);
+            blk_next = ~0ull;
+            blk_alive = 0;
             // grid barrier: the last block to arrive ends the slot and releases the others
-            unsigned g = ld_gen(&ctl->gen);
+            g = ld_gen(&ctl->gen);
             __threadfence();
             unsigned arrived = atomicAdd(&ctl->arrive, 1u) + 1;
-            if (arrived == gridDim.x)
+            blk_last = arrived == gridDim.x;
+        }
+        __syncthreads();
+        if (blk_last)
+        {
+            __threadfence();
+            // every world's next slot: finished worlds stop; a world where nothing was sent in
+            // this or the previous slot skips to its earliest wake-up
+            for (int w = threadIdx.x; w < s.W; w += blockDim.x)
             {
-                __threadfence();
+                WorldCtl *wc = &s.wctl[w];
+                volatile WorldCtl *vw = wc;
+                int64_t nx = vw->next;
+                if (nx == INT64_MAX)
+                    continue;
+                const unsigned cur = atomicExch(&wc->act, 0u), prev = vw->prev;
+                const unsigned long long wake = atomicExch(&wc->wake, (unsigned long long)INT64_MAX);
+                vw->prev = cur;
+                if (t >= nx)
+                {
+                    if (atomicAdd(&wc->fdone, 0u) >= (unsigned)s.worlds[w].n_msgs)
+                    {
+                        vw->next = INT64_MAX;
+                        continue;
+                    }
+                    nx = (cur == 0 && prev == 0 && (int64_t)wake > t + 1) ? (int64_t)wake : t + 1;
+                    vw->next = nx;
+                }
+                atomicMin(&blk_next, (unsigned long long)nx);
+                atomicAdd(&blk_alive, 1u);
+            }
+            __syncthreads();
+            if (threadIdx.x == 0)
+            {
                 vc->arrive = 0;
-                unsigned fd = atomicAdd(&ctl->flows_done, 0u);
-                if (fd >= (unsigned)s.M || t + 1 >= s.max_slots)
+                int64_t next = (int64_t)blk_next;
+                if (next > s.max_slots)
+                    next = s.max_slots;
+                if (blk_alive == 0)
+                    next = t + 1; // (finished: nothing left to skip to)
+                if (blk_alive == 0 || t + 1 >= s.max_slots)
                     vc->finished = 1;
-                unsigned cur = atomicAdd(&ctl->act_cur, 0u), prev = vc->act_prev;
-                unsigned long long nw = atomicAdd(&ctl->next_wake, 0ull);
-                int64_t next = t + 1;
-                if (cur == 0 && prev == 0 && nw != ~0ull && (int64_t)nw > next)
-                    next = (int64_t)nw < s.max_slots ? (int64_t)nw : s.max_slots;
-                vc->act_prev = cur;
-                vc->act_cur = 0;
-                vc->next_wake = ~0ull;
-                vc->slot = next;
+                vc->slot = next > t + 1 ? next : t + 1;
                 vc->slots_run = vc->slots_run + 1;
 #ifdef TB_PROFILE
                 unsigned long long now = globaltimer();
@@ -363,50 +448,52 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32) slot_kernel(Sim s, int m
                 __threadfence();
                 atomicAdd(&ctl->gen, 1u);
             }
-            else
-            {
-                long long spins = 0;
-                while (ld_gen(&ctl->gen) == g)
-                {
-                    if (++spins > BARRIER_SPIN_LIMIT)
-                    {
-                        atomicExch(&ctl->error, 1);
-                        atomicExch(&ctl->finished, 1);
-                        atomicAdd(&s.ev[EV_BARRIER_TIMEOUT], 1ull);
-                        break;
-                    }
-                    __nanosleep(64);
-                }
-            }
-            __threadfence();
         }
+        else if (threadIdx.x == 0)
+        {
+            long long spins = 0;
+            while (ld_gen(&ctl->gen) == g)
+            {
+                if (++spins > BARRIER_SPIN_LIMIT)
+                {
+                    atomicExch(&ctl->error, 1);
+                    atomicExch(&ctl->finished, 1);
+                    atomicAdd(&s.ev[EV_BARRIER_TIMEOUT], 1ull);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        if (threadIdx.x == 0)
+            __threadfence();
         __syncthreads();
     }
 }
 
 // dynamic shared memory of a block: one switch scratch (with its staging area) per warp
-constexpr size_t SMEM_BYTES = sizeof(SwShared) * WARPS_PER_BLOCK;
+static size_t smem_bytes(int stage_cap) { return sw_shared_bytes(stage_cap) * WARPS_PER_BLOCK; }
 
 static bool smem_attr()
 {
-    static bool ok = cudaFuncSetAttribute(slot_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES) == cudaSuccess;
+    static bool ok = cudaFuncSetAttribute(slot_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes(SW_STAGE_MAX)) == cudaSuccess;
     return ok;
 }
 
-int slot_kernel_blocks_per_sm()
+int slot_kernel_blocks_per_sm(int stage_cap)
 {
     int n = 0;
-    if (!smem_attr() || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, slot_kernel, WARPS_PER_BLOCK * 32, SMEM_BYTES) != cudaSuccess)
+    if (stage_cap < 1 || stage_cap > SW_STAGE_MAX || !smem_attr() ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, slot_kernel, WARPS_PER_BLOCK * 32, smem_bytes(stage_cap)) != cudaSuccess)
         return 0;
     return n;
 }
 
-int launch_slots(const Sim &s, int grid, int max_slots_per_launch, int host_lanes, cudaStream_t stream)
+int launch_slots(const Sim &s, int grid, int max_slots_per_launch, int host_lanes, int stage_cap, cudaStream_t stream)
 {
-    if (!smem_attr())
+    if (!smem_attr() || stage_cap < 1 || stage_cap > SW_STAGE_MAX)
         return (int)cudaErrorInvalidValue;
-    void *args[] = {(void *)&s, (void *)&max_slots_per_launch, (void *)&host_lanes};
-    cudaError_t e = cudaLaunchCooperativeKernel((const void *)slot_kernel, dim3(grid), dim3(WARPS_PER_BLOCK * 32), args, SMEM_BYTES, stream);
+    void *args[] = {(void *)&s, (void *)&max_slots_per_launch, (void *)&host_lanes, (void *)&stage_cap};
+    cudaError_t e = cudaLaunchCooperativeKernel((const void *)slot_kernel, dim3(grid), dim3(WARPS_PER_BLOCK * 32), args, smem_bytes(stage_cap), stream);
     return e == cudaSuccess ? 0 : (int)e;
 }
 

@@ -40,17 +40,20 @@ TB_D bool rcv_idle_for_good(const RcvRec &R)
 }
 
 // One slot of host h. Returns true if it sent or holds frames; *wake: the next slot it must run.
-// `stage`: the host's link messages of slots t-2 and t-1 copied to shared memory by its warp
-// (msg[t-2] then msg[t-1], as many frames as their tags count), or null to read them in place.
-TB_D bool host_step(const Sim &s, int h, int64_t t, int64_t *wake, unsigned *ties_out, unsigned *done_out,
-                    const Frame *stage = nullptr)
+// t: the world's own slot (time); gt: the launch's slot, which indexes the link messages (equal
+// in a batch; a world that joins a running launch starts its own time at a later launch slot).
+// `stage`: the host's link messages of slots gt-2 and gt-1 copied to shared memory by its warp
+// (msg[gt-2] then msg[gt-1], n2 and n1 frames as their tags count), or null to read them in place
+// (n2, n1 < 0: read the tags).
+TB_D bool host_step(const Sim &s, int h, int64_t t, int64_t gt, int64_t *wake, unsigned *ties_out, unsigned *done_out,
+                    const Frame *stage = nullptr, int n2 = -1, int n1 = -1)
 {
     const int64_t S0 = t * SLOT_PS, E0 = S0 + SLOT_PS;
     TB_PHASE_START
     HostRec &hr = s.hosts[h];
     const int link = hr.in_link;
     const Frame *m2 = nullptr, *m1 = nullptr;
-    int n2 = 0, n1 = 0, i2 = 0, i1 = 0;
+    int i2 = 0, i1 = 0;
     auto ts_at = [&](const Frame *m, int j) { return stage ? m[j].ts : ts_load_link(&m[j]); };
     auto frame_at = [&](Frame &d, const Frame *m, int j) {
         if (stage)
@@ -58,18 +61,18 @@ TB_D bool host_step(const Sim &s, int h, int64_t t, int64_t *wake, unsigned *tie
         else
             frame_load_link(d, &m[j]);
     };
-    if (t >= 2)
+    if (n2 < 0)
+        n2 = gt >= 2 ? msg_count(s, gt - 2, link) : 0;
+    if (n1 < 0)
+        n1 = gt >= 1 ? msg_count(s, gt - 1, link) : 0;
+    if (n2 > 0)
     {
-        n2 = msg_count(s, t - 2, link);
-        m2 = stage ? stage : msg_frames(s, t - 2, link);
+        m2 = stage ? stage : msg_frames(s, gt - 2, link);
         while (i2 < n2 && ts_at(m2, i2) < S0)
             i2++;
     }
-    if (t >= 1)
-    {
-        n1 = msg_count(s, t - 1, link);
-        m1 = stage ? stage + n2 : msg_frames(s, t - 1, link);
-    }
+    if (n1 > 0)
+        m1 = stage ? stage + n2 : msg_frames(s, gt - 1, link);
     bool input = i2 < n2 || (n1 > 0 && ts_at(m1, 0) < E0);
     if (!input && t < hr.wake && hr.q_size == 0)
     {
@@ -99,7 +102,7 @@ TB_D bool host_step(const Sim &s, int h, int64_t t, int64_t *wake, unsigned *tie
     nic.woke = -1;
     nic.idle_start = -1;
     nic.slot_end = E0;
-    nic.out = s.msg + msg_index(s, t, h) * MAX_TX;
+    nic.out = s.msg + msg_index(s, gt, h) * MAX_TX;
     nic.sent = 0;
     nic.drops = nic.marks = nic.ovf = nic.emitted = 0;
     unsigned ties = 0;
@@ -313,7 +316,7 @@ TB_D bool host_step(const Sim &s, int h, int64_t t, int64_t *wake, unsigned *tie
     }
     TB_PHASE(2)
     nic.advance(E0 - 1);
-    tag_store(&s.msg_tag[msg_index(s, t, h)], (int64_t)t << 16 | nic.sent);
+    tag_store(&s.msg_tag[msg_index(s, gt, h)], (int64_t)gt << 16 | nic.sent);
     hr.q_head = nic.head;
     hr.q_size = nic.size;
     hr.link_free = nic.link_free;

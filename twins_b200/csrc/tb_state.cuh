@@ -14,6 +14,10 @@
 namespace tb
 {
 
+// frames a warp stages in shared memory per switch (or host) and slot: the largest staging area;
+// a launch may use a smaller one (more resident warps per SM, fewer slots staged)
+constexpr int SW_STAGE_MAX = 192;
+
 // a world's topology and parameters (read-only on the device)
 struct WorldDesc
 {
@@ -164,6 +168,24 @@ struct SlotCtl
     unsigned long long prof_phase[12];
 };
 
+// Per world: the slot rule of the reference's ticket block (src/kernel.cuh:79-112) applied to each
+// world of a batch on its own, so that a world that is finished, or quiet until a timer, costs
+// its entities nothing. Slots here are the launch's (global) slots; a world's own time starts at
+// global slot `t0` (0 in a batch; the admission slot of a world that joins a running launch), and
+// its entities run in world-local slots t - t0. `next` is the next global slot the world's
+// entities run (INT64_MAX: all its messages are done); `act` / `prev` whether any of its entities
+// sent or held frames in this and the previous slot; `wake` the earliest global wake-up its hosts
+// reported in this slot.
+struct WorldCtl
+{
+    int64_t next;
+    unsigned long long wake;
+    unsigned act, prev;
+    unsigned fdone; // messages done
+    unsigned pad;
+    int64_t t0;
+};
+
 #if defined(TB_PROFILE) && defined(__CUDACC__)
 __device__ __forceinline__ unsigned long long prof_now()
 {
@@ -218,6 +240,11 @@ struct Sim
     unsigned long long *ev;  // [EV_N]
     unsigned long long *ev_w; // [W][EV_N]
     SlotCtl *ctl;
+    WorldCtl *wctl;           // [W]
+    // the units a launch runs (null: all): host units (host_lanes hosts each) of the worlds still
+    // running, then host_units + switch; rebuilt between launches
+    const int *unit_list;
+    int n_list;
 };
 
 } // namespace tb

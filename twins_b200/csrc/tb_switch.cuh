@@ -12,12 +12,9 @@
 namespace tb
 {
 
-#ifndef TB_SW_STAGE
-#define TB_SW_STAGE 192 // frames staged per switch (or host) and slot
-#endif
-constexpr int SW_STAGE = TB_SW_STAGE;
-
-// per-warp shared scratch of a switch (also a host unit's staging area)
+// per-warp shared scratch of a switch (also a host unit's staging area). The staging arrays
+// follow the header in the warp's part of the block's dynamic shared memory; their capacity
+// (`cap` frames) is chosen per launch.
 struct SwShared
 {
     int rows[32][33];       // [ingress][egress] counts, then offsets
@@ -26,10 +23,30 @@ struct SwShared
     int raw2[32], raw1[32]; // frames in the port's msg[t-2] / msg[t-1]
     int off2[32], off1[32]; // where they start in `fr` (staged)
     int staged, total;
-    Frame fr[SW_STAGE];
-    int64_t ets[SW_STAGE];  // staged slots: each egress region's arrival times and sources
-    uint32_t eref[SW_STAGE];
+    int cap;
+    // the staging arrays, addressed from the scratch itself (so that the compiler keeps them in
+    // the shared address space): frames [cap], then each egress region's arrival times [cap] and
+    // sources [cap] (staged slots)
+    TB_D Frame *fr() { return reinterpret_cast<Frame *>(reinterpret_cast<unsigned char *>(this) + header()); }
+    TB_D const Frame *fr() const { return reinterpret_cast<const Frame *>(reinterpret_cast<const unsigned char *>(this) + header()); }
+    TB_D int64_t *ets() { return reinterpret_cast<int64_t *>(reinterpret_cast<unsigned char *>(this) + header() + (size_t)cap * sizeof(Frame)); }
+    TB_D uint32_t *eref()
+    {
+        return reinterpret_cast<uint32_t *>(reinterpret_cast<unsigned char *>(this) + header() + (size_t)cap * (sizeof(Frame) + 8));
+    }
+    static TB_HDI size_t header();
 };
+
+TB_HDI size_t SwShared::header() { return (sizeof(SwShared) + 15) & ~(size_t)15; }
+// bytes of one warp's scratch with `cap` staged frames (16-byte multiple)
+TB_HDI size_t sw_shared_bytes(int cap) { return (SwShared::header() + (size_t)cap * (sizeof(Frame) + 8 + 4) + 15) & ~(size_t)15; }
+// a warp's scratch at `p` (every lane may call it: the same value is written)
+TB_D SwShared *sw_shared_at(unsigned char *p, int cap)
+{
+    SwShared *sh = reinterpret_cast<SwShared *>(p);
+    sh->cap = cap;
+    return sh;
+}
 
 // ingress window of a port: the tail of msg[t-2] from S0 on, the head of msg[t-1] before E0;
 // frames in shared memory (staged) or in the link messages
@@ -58,7 +75,8 @@ struct SwCtx
     int sw;          // global switch id
     PortRec *ports;  // the switch's ports
     size_t scratch;  // its region in sw_ts / sw_ref / sw_up
-    int64_t t;
+    int64_t t;       // the world's own slot (time)
+    int64_t gt;      // the launch's slot (indexes the link messages)
     bool spray;
 };
 
@@ -71,15 +89,15 @@ TB_D Input input_of(const SwCtx &x, const SwShared &sh, int q)
     in.smem = sh.staged != 0;
     if (in.smem)
     {
-        in.m2 = &sh.fr[sh.off2[q]];
-        in.m1 = &sh.fr[sh.off1[q]];
+        in.m2 = &sh.fr()[sh.off2[q]];
+        in.m1 = &sh.fr()[sh.off1[q]];
         return in;
     }
     int link = x.ports[q].in_link;
     if (link < 0)
         link = 0; // (an unused port's window is empty; any link gives valid pointers)
-    in.m2 = x.t >= 2 ? msg_frames(*x.s, x.t - 2, link) : nullptr;
-    in.m1 = x.t >= 1 ? msg_frames(*x.s, x.t - 1, link) : nullptr;
+    in.m2 = x.gt >= 2 ? msg_frames(*x.s, x.gt - 2, link) : nullptr;
+    in.m1 = x.gt >= 1 ? msg_frames(*x.s, x.gt - 1, link) : nullptr;
     return in;
 }
 
@@ -88,8 +106,8 @@ TB_D void sw_phase_sizes(const SwCtx &x, SwShared &sh, int q)
 {
     const Sim &s = *x.s;
     int link = x.ports[q].in_link;
-    sh.raw2[q] = link >= 0 && x.t >= 2 ? msg_count(s, x.t - 2, link) : 0;
-    sh.raw1[q] = link >= 0 && x.t >= 1 ? msg_count(s, x.t - 1, link) : 0;
+    sh.raw2[q] = link >= 0 && x.gt >= 2 ? msg_count(s, x.gt - 2, link) : 0;
+    sh.raw1[q] = link >= 0 && x.gt >= 1 ? msg_count(s, x.gt - 1, link) : 0;
     for (int i = 0; i <= x.sr->k; i++)
         sh.rows[q][i] = 0;
 }
@@ -105,7 +123,7 @@ TB_D void sw_phase_layout(const SwCtx &x, SwShared &sh)
         sh.off1[q] = off;
         off += sh.raw1[q];
     }
-    sh.staged = off <= SW_STAGE;
+    sh.staged = off <= sh.cap;
     sh.total = off;
 }
 
@@ -123,9 +141,9 @@ TB_D void sw_phase_copy(const SwCtx &x, SwShared &sh, int lane, int lanes)
         while (q + 1 < k && sh.off2[q + 1] <= i)
             q++;
         int link = x.ports[q].in_link;
-        const Frame *src = i < sh.off1[q] ? msg_frames(s, x.t - 2, link) + (i - sh.off2[q])
-                                          : msg_frames(s, x.t - 1, link) + (i - sh.off1[q]);
-        frame_load_link(sh.fr[i], src);
+        const Frame *src = i < sh.off1[q] ? msg_frames(s, x.gt - 2, link) + (i - sh.off2[q])
+                                          : msg_frames(s, x.gt - 1, link) + (i - sh.off1[q]);
+        frame_load_link(sh.fr()[i], src);
     }
 }
 
@@ -172,8 +190,8 @@ TB_D int sw_egress_of(const SwCtx &x, const Input &in, int q, int j)
     return sw_egress_for(x, f, q, j);
 }
 // the region of egress arrivals (times, sources): shared memory when staged
-TB_D int64_t *sw_ts_of(const SwCtx &x, SwShared &sh) { return sh.staged ? sh.ets : x.s->sw_ts + x.scratch; }
-TB_D uint32_t *sw_ref_of(const SwCtx &x, SwShared &sh) { return sh.staged ? sh.eref : x.s->sw_ref + x.scratch; }
+TB_D int64_t *sw_ts_of(const SwCtx &x, SwShared &sh) { return sh.staged ? sh.ets() : x.s->sw_ts + x.scratch; }
+TB_D uint32_t *sw_ref_of(const SwCtx &x, SwShared &sh) { return sh.staged ? sh.eref() : x.s->sw_ref + x.scratch; }
 
 // phase 2 (one lane): per-packet ECMP draws, one per forwarded packet in the order the packets
 // arrive at the node (all ports merged), from the switch's MRG32k3a stream. (With staged frames
@@ -332,7 +350,7 @@ TB_D bool sw_phase_egress(const SwCtx &x, SwShared &sh, int e, unsigned &ties, u
     eg.idle_start = -1;
     eg.slot_end = (x.t + 1) * SLOT_PS;
     const int out_link = s.H + port;
-    eg.out = s.msg + msg_index(s, x.t, out_link) * MAX_TX;
+    eg.out = s.msg + msg_index(s, x.gt, out_link) * MAX_TX;
     eg.sent = 0;
     eg.drops = eg.marks = eg.ovf = eg.emitted = 0;
     for (int i = 0; i < n; i++)
@@ -343,7 +361,7 @@ TB_D bool sw_phase_egress(const SwCtx &x, SwShared &sh, int e, unsigned &ties, u
         eg.enqueue(p, p.ts);
     }
     eg.advance(eg.slot_end - 1);
-    tag_store(&s.msg_tag[msg_index(s, x.t, out_link)], (int64_t)x.t << 16 | eg.sent);
+    tag_store(&s.msg_tag[msg_index(s, x.gt, out_link)], (int64_t)x.gt << 16 | eg.sent);
     pr.q_head = eg.head;
     pr.q_size = eg.size;
     pr.link_free = eg.link_free;

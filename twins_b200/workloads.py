@@ -20,7 +20,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from .api import Flows, TcpParams, Topology
+from .api import TOPO_GRAPH, Flows, TcpParams, Topology
 
 LINK_BYTES_PER_NS = 12.5  # 100 Gbps
 
@@ -139,3 +139,108 @@ def c2_small(seed: int = 1, tcps=("newreno", "dctcp", "cubic")) -> list[World]:
 
 
 WORKLOADS = {"c1": c1, "c2": c2, "c2s": c2_small, "c4": c4}
+
+
+# ------------------------------------------------------------------ served stream (C5 shape)
+def jellyfish(n_sw: int = 64, degree: int = 8, hosts_per_sw: int = 4, seed: int = 1) -> Topology:
+    """A seeded random regular graph of switches (each with `degree` switch links) and
+    `hosts_per_sw` hosts on every switch, as a topology file's links (host h: h, switch j: -1-j).
+    Jellyfish's construction: link random pairs of switches that have free ports and no link yet;
+    when only switches that are already linked keep free ports, a switch with two free ports
+    takes the place of a random link (x, y) it is not next to: (x, y) becomes (s, x) and (s, y)."""
+    rng = np.random.default_rng(seed)
+    free = [degree] * n_sw
+    adj = set()
+    while True:
+        cand = [i for i in range(n_sw) if free[i] > 0]
+        pairs = [(a, b) for ia, a in enumerate(cand) for b in cand[ia + 1:] if (a, b) not in adj]
+        if pairs:
+            a, b = pairs[int(rng.integers(len(pairs)))]
+            adj.add((a, b))
+            free[a] -= 1
+            free[b] -= 1
+            continue
+        stuck = [i for i in cand if free[i] >= 2]
+        if not stuck:
+            break
+        s_ = stuck[0]
+        near = lambda x: (min(s_, x), max(s_, x)) in adj
+        options = sorted((x, y) for x, y in adj if s_ not in (x, y) and not near(x) and not near(y))
+        x, y = options[int(rng.integers(len(options)))]
+        adj.discard((x, y))
+        adj.add((min(s_, x), max(s_, x)))
+        adj.add((min(s_, y), max(s_, y)))
+        free[s_] -= 2
+    links = [(h, -1 - h // hosts_per_sw) for h in range(n_sw * hosts_per_sw)]
+    links += [(-1 - a, -1 - b) for a, b in sorted(adj)]
+    return Topology(kind=TOPO_GRAPH, n_hosts=n_sw * hosts_per_sw, n_switches=n_sw, links=links)
+
+
+def dragonfly(groups: int = 9, a: int = 4, h: int = 2, p: int = 4) -> Topology:
+    """Dragonfly: `groups` groups of `a` switches, each group a full mesh, every switch with `h`
+    global links and `p` hosts; with groups = a*h + 1 every pair of groups has one global link
+    (switch j's global links go to groups g + 1 + j*h + i, i < h, in the consecutive arrangement)."""
+    if groups != a * h + 1:
+        raise ValueError("groups must be a*h + 1")
+    n_sw = groups * a
+    links = [(x, -1 - x // p) for x in range(n_sw * p)]
+    for g in range(groups):
+        for i in range(a):
+            for j in range(i + 1, a):
+                links.append((-1 - (g * a + i), -1 - (g * a + j)))
+    seen = set()
+    for g in range(groups):
+        for j in range(a):
+            for i in range(h):
+                d = (g + 1 + j * h + i) % groups
+                # the switch of group d that holds the link back to g
+                off = (g - d - 1) % groups
+                k = off // h
+                e = (min(g * a + j, d * a + k), max(g * a + j, d * a + k))
+                if e not in seen:
+                    seen.add(e)
+                    links.append((-1 - e[0], -1 - e[1]))
+    return Topology(kind=TOPO_GRAPH, n_hosts=n_sw * p, n_switches=n_sw, links=links)
+
+
+@dataclass
+class Request:
+    name: str
+    arrival_s: float
+    topo: Topology
+    flows: Flows
+    params: TcpParams
+
+
+def served_stream(seed: int = 1, n: int = 200, rate_per_s: float = 40.0, size_cap: int = 1_000_000) -> list[Request]:
+    """Seeded Poisson arrivals of TCP simulation requests: 40% FatTree k=4, 30% k=8, 10% k=16,
+    10% Jellyfish (64 switches, degree 8, 4 hosts per switch), 10% Dragonfly (9 groups of 4
+    switches, 2 global links and 4 hosts per switch). Each request draws its TCP, ecnK and queue
+    from the sweep grid, flows from the web-search-like CDF (capped at `size_cap` bytes) at 30-60%
+    load over about 0.5 ms of arrivals. A tenth of the graph requests carry one switch-switch link
+    failure between 100 and 500 us, recovered 400 us later."""
+    rng = np.random.default_rng(seed)
+    jf = jellyfish(seed=seed)
+    df = dragonfly()
+    t = 0.0
+    out = []
+    for i in range(n):
+        t += rng.exponential(1.0 / rate_per_s)
+        kind = rng.choice(["k4", "k8", "k16", "jf", "df"], p=[0.4, 0.3, 0.1, 0.1, 0.1])
+        topo = {"k4": Topology.fattree(4), "k8": Topology.fattree(8), "k16": Topology.fattree(16), "jf": jf, "df": df}[kind]
+        if kind in ("jf", "df") and rng.random() < 0.5:  # (a tenth of all requests: half of the graph ones)
+            sw = [(a, b) for a, b in topo.links if a < 0 and b < 0]
+            a, b = sw[int(rng.integers(len(sw)))]
+            tf = int(rng.integers(100_000, 500_001))
+            topo = Topology(kind=topo.kind, n_hosts=topo.n_hosts, n_switches=topo.n_switches, links=topo.links,
+                            fails=[(tf, -1 - a, -1 - b, 0), (tf + 400_000, -1 - a, -1 - b, 1)])
+        H = topo.hosts
+        load = float(rng.uniform(0.3, 0.6))
+        n_flows = int(max(8, round(load * H * LINK_BYTES_PER_NS * 500_000 / min(web_mean(), size_cap / 2))))
+        n_flows = min(n_flows, 4000)
+        flows = leafspine_flows(rng, H, n_flows, load)
+        flows.size = np.minimum(flows.size, size_cap)
+        params = TcpParams(str(rng.choice(["newreno", "dctcp", "cubic"])), int(rng.choice([10, 20, 40, 80])),
+                           int(rng.choice([100, 200, 400])), spray=bool(kind in ("jf", "df")))
+        out.append(Request(f"c5_{i:04d}_{kind}", t, topo, flows, params))
+    return out
