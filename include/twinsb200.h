@@ -139,8 +139,9 @@ int tb_get_stats(tb_ctx *ctx, tb_stats *out);
 /* Launch shape: hosts per warp (1..32) and the grid (0: chosen from occupancy); turns autotuning
  * off. Replaces the reference's --host_lanes (src/main.cu:183-184, 523-526). */
 int tb_set_launch(tb_ctx *ctx, int host_lanes, int grid);
-/* The same with the frames a warp stages in shared memory per slot (1..192; fewer leave room for
- * more resident blocks per SM). */
+/* The same with the frames a warp stages in shared memory per slot (1..384, 1..256 in the 25-run
+ * build; default 192; fewer leave room for more resident blocks per SM, more stage the slots of
+ * big switches). */
 int tb_set_launch_shape(tb_ctx *ctx, int host_lanes, int stage_frames, int grid);
 /* Autotuning (on by default): tb_run picks each launch's shape (hosts per warp, staging size)
  * among a fixed set by the packet-events per ms that short probe launches of each achieve. The

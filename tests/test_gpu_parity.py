@@ -129,7 +129,7 @@ def test_launch_shapes_identical(native_lib, name):
     case = next(c for c in CASES if c["name"] == name)
     want_est, want_done = ns3(case)
     events = set()
-    for lanes, stage in [(1, 192), (1, 8), (1, 96), (4, 96), (32, 192), (7, 64)]:
+    for lanes, stage in [(1, 192), (1, 8), (1, 96), (1, 384), (4, 96), (32, 192), (7, 64)]:
         est, done, ctr, stats = api.run_world(*world_of(case), host_lanes=lanes, stage_frames=stage)
         assert (est == want_est).all() and (done == want_done).all(), (lanes, stage)
         assert stats["host_lanes"] == lanes and stats["stage_frames"] == stage and not stats["autotuned"]
@@ -157,3 +157,14 @@ def test_batch_worlds_finish_apart(native_lib):
             assert (est == e2).all() and (done == d2).all()
             assert (done >= 0).all()
             assert sim.counters(i) == ctr
+
+
+@pytest.mark.parametrize("name", ["k8_a2a30_cubic_spray", "k8_r30_dctcp_sprayfin", "df4x9_a2a30_newreno_spray"])
+def test_chain_runs_25(native_lib, name):
+    """The 25-run event-chain build (the reference's twins128, 128-byte frames) gives the same
+    results as ns-3 and decides every tie."""
+    case = next(c for c in CASES if c["name"] == name)
+    est, done, ctr, stats = api.run_world(*world_of(case), chain_runs=25)
+    want_est, want_done = ns3(case)
+    assert (est == want_est).all() and (done == want_done).all()
+    assert ctr["undecided_ties"] == 0

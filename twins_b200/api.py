@@ -19,6 +19,8 @@ from typing import Optional, Sequence
 import numpy as np
 
 LIB_PATH = Path(__file__).resolve().parent / "lib" / "libtwinsb200.so"
+# the 25-run event-chain build (the reference's twins128)
+LIB25_PATH = Path(__file__).resolve().parent / "lib" / "libtwinsb200_runs25.so"
 
 TB_OK, TB_WARN_INEXACT = 0, 1
 TB_ERR = {-1: "bad argument", -2: "CUDA error", -3: "HBM budget exceeded", -4: "call out of order",
@@ -305,9 +307,12 @@ class Simulator:
     """A batch of worlds on one GPU: add worlds, run, read results (tb_* of the C ABI)."""
 
     def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, host_lanes: Optional[int] = None, grid: int = 0,
-                 stage_frames: int = 192):
-        """host_lanes None: the launch shape is autotuned per launch; else that fixed shape."""
-        self.lib = load_library()
+                 stage_frames: int = 192, chain_runs: int = 9):
+        """host_lanes None: the launch shape is autotuned per launch; else that fixed shape.
+        chain_runs 25: the 25-run event-chain build (the reference's twins128)."""
+        if chain_runs not in (9, 25):
+            raise ValueError("chain_runs is 9 or 25")
+        self.lib = load_library(LIB25_PATH if chain_runs == 25 else None)
         self.ctx = ctypes.c_void_p()
         self._check(self.lib.tb_ctx_create(device, hbm_budget_bytes, ctypes.byref(self.ctx)))
         if host_lanes is not None:

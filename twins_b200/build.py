@@ -1,11 +1,13 @@
 """Builds the twins-b200 native code in-tree for sm_100a.
 
-    python -m twins_b200.build            # libtwinsb200.so and the twins front-end
+    python -m twins_b200.build            # the libraries and the twins / twins128 front-ends
     python -m twins_b200.build --force
 
 Outputs (git-ignored, they travel with the repository to the GPU machine):
-    twins_b200/lib/libtwinsb200.so    the C ABI of include/twinsb200.h
-    twins_b200/lib/twins              the reference's command line over it
+    twins_b200/lib/libtwinsb200.so        the C ABI of include/twinsb200.h (9-run event chains)
+    twins_b200/lib/twins                  the reference's command line over it
+    twins_b200/lib/libtwinsb200_runs25.so the same with 25-run chains (128-byte frames), as the
+    twins_b200/lib/twins128               reference's twins128 build (-DTWINS_CHAIN_RUNS=25)
 """
 from __future__ import annotations
 
@@ -20,6 +22,10 @@ CSRC = PKG / "csrc"
 LIB = PKG / "lib"
 SO = LIB / "libtwinsb200.so"
 CLI = LIB / "twins"
+SO25 = LIB / "libtwinsb200_runs25.so"
+CLI25 = LIB / "twins128"
+# (library, front-end, extra flags) per event-chain length
+VARIANTS = [(SO, CLI, []), (SO25, CLI25, ["-DTB_CHAIN_RUNS=25"])]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # exactness: no floating-point contraction (fma() is written where ns-3 fuses), IEEE division
@@ -47,23 +53,24 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     deps = list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + \
         [ROOT / "include" / "twinsb200.h", Path(__file__)]
     nvcc = _nvcc()
-    if force or _stale(SO, deps):
-        objs = []
-        for src in SOURCES:
-            obj = LIB / (Path(src).stem + ".o")
-            cmd = [nvcc, *NVFLAGS, "-c", str(CSRC / src), "-o", str(obj)]
-            if verbose:
-                print(" ".join(cmd))
+    for so, cli, extra in VARIANTS:
+        if force or _stale(so, deps):
+            objs = []
+            for src in SOURCES:
+                obj = LIB / (Path(src).stem + so.stem + ".o")
+                cmd = [nvcc, *NVFLAGS, *extra, "-c", str(CSRC / src), "-o", str(obj)]
+                if verbose:
+                    print(" ".join(cmd))
+                subprocess.run(cmd, check=True)
+                objs.append(str(obj))
+            cmd = [nvcc, *ARCH, "-shared", "-o", str(so), *objs, "-lcudart"]
             subprocess.run(cmd, check=True)
-            objs.append(str(obj))
-        cmd = [nvcc, *ARCH, "-shared", "-o", str(SO), *objs, "-lcudart"]
-        subprocess.run(cmd, check=True)
-        for o in objs:
-            Path(o).unlink(missing_ok=True)
-    if force or _stale(CLI, deps + [SO]):
-        cmd = ["g++", "-std=c++17", "-O2", "-o", str(CLI), str(CSRC / "twins_cli.cpp"),
-               f"-L{LIB}", "-ltwinsb200", f"-Wl,-rpath,$ORIGIN"]
-        subprocess.run(cmd, check=True)
+            for o in objs:
+                Path(o).unlink(missing_ok=True)
+        if force or _stale(cli, deps + [so]):
+            cmd = ["g++", "-std=c++17", "-O2", "-o", str(cli), str(CSRC / "twins_cli.cpp"),
+                   f"-L{LIB}", f"-l{so.stem[3:]}", f"-Wl,-rpath,$ORIGIN"]
+            subprocess.run(cmd, check=True)
     return SO
 
 

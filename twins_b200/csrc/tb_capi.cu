@@ -540,7 +540,7 @@ struct tb_ctx
     std::vector<HostWorld> worlds;
     bool prepared = false, ran = false;
     int host_lanes = 1, grid_req = 0, grid = 0;
-    int stage_cap = SW_STAGE_MAX; // frames staged per warp
+    int stage_cap = SW_STAGE;     // frames staged per warp
     int *d_units = nullptr;       // the running units' list (tb_run)
     bool autotune = true;         // pick the launch shape per launch by measured throughput
     int dev_sms = 0;
@@ -1163,7 +1163,7 @@ int tb_set_launch_shape(tb_ctx *ctx, int host_lanes, int stage_frames, int grid)
     return TB_OK;
 }
 
-int tb_set_launch(tb_ctx *ctx, int host_lanes, int grid) { return tb_set_launch_shape(ctx, host_lanes, SW_STAGE_MAX, grid); }
+int tb_set_launch(tb_ctx *ctx, int host_lanes, int grid) { return tb_set_launch_shape(ctx, host_lanes, SW_STAGE, grid); }
 
 int tb_set_autotune(tb_ctx *ctx, int on)
 {
@@ -1197,27 +1197,28 @@ int tb_run(tb_ctx *ctx, long long max_slots)
     {
         int lanes, stage, grid;
         long long slots;
+        int strikes; // probes it lost by more than 30% (it is not probed again after two)
     };
     std::vector<Shape> shapes;
     size_t best = 0;
     if (ctx->autotune)
     {
-        const int cand[][2] = {{1, SW_STAGE_MAX}, {4, SW_STAGE_MAX}, {32, SW_STAGE_MAX}, {1, 96}, {32, 96}};
+        const int cand[][2] = {{1, SW_STAGE}, {4, SW_STAGE}, {32, SW_STAGE}, {1, SW_STAGE_SMALL}, {32, SW_STAGE_SMALL}, {1, SW_STAGE_MAX}};
         for (auto &c : cand)
         {
             int g = grid_for(ctx, c[0], c[1]);
             if (g > 0)
-                shapes.push_back({c[0], c[1], g, 0});
+                shapes.push_back({c[0], c[1], g, 0, 0});
         }
-        const long long resident = (long long)ctx->dev_sms * std::max(1, tb::slot_kernel_blocks_per_sm(SW_STAGE_MAX)) * TB_WARPS_PER_BLOCK;
+        const long long resident = (long long)ctx->dev_sms * std::max(1, tb::slot_kernel_blocks_per_sm(SW_STAGE)) * TB_WARPS_PER_BLOCK;
         const int lanes0 = s.H + s.S <= 2 * resident ? 1 : 32;
         for (size_t k = 0; k < shapes.size(); k++)
-            if (shapes[k].lanes == lanes0 && shapes[k].stage == SW_STAGE_MAX)
+            if (shapes[k].lanes == lanes0 && shapes[k].stage == SW_STAGE)
                 best = k;
     }
     if (shapes.empty())
-        shapes.push_back({ctx->host_lanes, ctx->stage_cap, ctx->grid, 0});
-    const int probe = 64, period = 6;
+        shapes.push_back({ctx->host_lanes, ctx->stage_cap, ctx->grid, 0, 0});
+    const int probe = 64, period = 12;
     const int run_slots = shapes.size() > 1 ? std::min(ctx->max_slots_per_launch, 1024) : ctx->max_slots_per_launch;
     long long launches = 0, since = 0;
     // the running worlds' units: rebuilt when a world finishes (or the shape changes), so that a
@@ -1237,7 +1238,7 @@ int tb_run(tb_ctx *ctx, long long max_slots)
         std::vector<double> per_slot(shapes.size(), -1);
         for (size_t k = 0; k < shapes.size(); k++)
         {
-            if (!explore && k != best)
+            if ((!explore && k != best) || (explore && k != best && shapes[k].strikes >= 2))
                 continue;
             Shape &sh = shapes[k];
             int grid = sh.grid;
@@ -1288,6 +1289,9 @@ int tb_run(tb_ctx *ctx, long long max_slots)
             for (size_t k = 0; k < shapes.size(); k++)
                 if (per_slot[k] > 0 && (per_slot[b] <= 0 || per_slot[k] < 0.95 * per_slot[b]))
                     b = k;
+            for (size_t k = 0; k < shapes.size(); k++)
+                if (per_slot[k] > 0 && per_slot[b] > 0 && per_slot[k] > 1.3 * per_slot[b])
+                    shapes[k].strikes++;
             best = b;
             since = 0;
         }

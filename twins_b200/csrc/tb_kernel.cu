@@ -12,6 +12,7 @@
 #include "tb_switch.cuh"
 #include "tb_kernel.h"
 
+#include <algorithm>
 #include <climits>
 #include <cuda_runtime.h>
 
@@ -479,11 +480,23 @@ static bool smem_attr()
     return ok;
 }
 
+// The preferred shared-memory carveout, in percent of the SM's maximum: the shared memory of the
+// blocks a launch puts on one SM and no more, so that the rest of the SM's unified L1 / shared
+// memory is L1, where the units' records, ring heads and prefetched lines stay between slots.
+static int carveout = -1; // the last one set (-1: none)
+static void set_carveout(int pct)
+{
+    if (pct != carveout && cudaFuncSetAttribute(slot_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, pct) == cudaSuccess)
+        carveout = pct;
+}
+
 int slot_kernel_blocks_per_sm(int stage_cap)
 {
     int n = 0;
-    if (stage_cap < 1 || stage_cap > SW_STAGE_MAX || !smem_attr() ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, slot_kernel, WARPS_PER_BLOCK * 32, smem_bytes(stage_cap)) != cudaSuccess)
+    if (stage_cap < 1 || stage_cap > SW_STAGE_MAX || !smem_attr())
+        return 0;
+    set_carveout(100); // (occupancy with all of the shared memory)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, slot_kernel, WARPS_PER_BLOCK * 32, smem_bytes(stage_cap)) != cudaSuccess)
         return 0;
     return n;
 }
@@ -492,8 +505,22 @@ int launch_slots(const Sim &s, int grid, int max_slots_per_launch, int host_lane
 {
     if (!smem_attr() || stage_cap < 1 || stage_cap > SW_STAGE_MAX)
         return (int)cudaErrorInvalidValue;
+    int dev = 0, sms = 1, max_smem = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    const long long per_sm = (grid + sms - 1) / sms;
+    const long long need = per_sm * (long long)(smem_bytes(stage_cap) + 2048); // (+ the block's reserved and static shared memory)
+    set_carveout((int)std::min<long long>(100, (need * 100 + max_smem - 1) / max_smem));
     void *args[] = {(void *)&s, (void *)&max_slots_per_launch, (void *)&host_lanes, (void *)&stage_cap};
     cudaError_t e = cudaLaunchCooperativeKernel((const void *)slot_kernel, dim3(grid), dim3(WARPS_PER_BLOCK * 32), args, smem_bytes(stage_cap), stream);
+    if (e == cudaErrorCooperativeLaunchTooLarge)
+    {
+        // (the carveout left too little shared memory for the blocks to be resident at once)
+        cudaGetLastError();
+        set_carveout(100);
+        e = cudaLaunchCooperativeKernel((const void *)slot_kernel, dim3(grid), dim3(WARPS_PER_BLOCK * 32), args, smem_bytes(stage_cap), stream);
+    }
     return e == cudaSuccess ? 0 : (int)e;
 }
 

@@ -121,7 +121,7 @@ struct tb_server
     std::map<long long, std::unique_ptr<Req>> reqs;
     std::vector<long long> slot_req; // world slot -> running request (0: none)
     long long next_id = 1;
-    int lanes = 1, stage = SW_STAGE_MAX, grid = 0;
+    int lanes = 1, stage = SW_STAGE, grid = 0;
     int *d_units = nullptr;      // the batch's units (device)
     bool units_stale = true;     // admissions or retirements since the list was built
     // statistics
@@ -537,9 +537,9 @@ int server_alloc(tb_server *v)
     // the resident warps about once, else 32 hosts per warp with the smaller staging area
     cudaDeviceGetAttribute(&c.dev_sms, cudaDevAttrMultiProcessorCount, v->device);
     c.sim = s;
-    const long long resident = (long long)c.dev_sms * std::max(1, tb::slot_kernel_blocks_per_sm(SW_STAGE_MAX)) * TB_WARPS_PER_BLOCK;
+    const long long resident = (long long)c.dev_sms * std::max(1, tb::slot_kernel_blocks_per_sm(SW_STAGE)) * TB_WARPS_PER_BLOCK;
     v->lanes = s.H + s.S <= 2 * resident ? 1 : 32;
-    v->stage = v->lanes == 1 ? SW_STAGE_MAX : 96;
+    v->stage = v->lanes == 1 ? SW_STAGE : SW_STAGE_SMALL;
     if ((v->grid = grid_for(&c, v->lanes, v->stage)) <= 0)
         return fail(TB_ERR_CUDA, "the slot kernel does not fit on the device");
     v->a_world.init(k.worlds);

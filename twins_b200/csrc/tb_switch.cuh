@@ -24,16 +24,15 @@ struct SwShared
     int off2[32], off1[32]; // where they start in `fr` (staged)
     int staged, total;
     int cap;
-    // the staging arrays, addressed from the scratch itself (so that the compiler keeps them in
-    // the shared address space): frames [cap], then each egress region's arrival times [cap] and
-    // sources [cap] (staged slots)
-    TB_D Frame *fr() { return reinterpret_cast<Frame *>(reinterpret_cast<unsigned char *>(this) + header()); }
-    TB_D const Frame *fr() const { return reinterpret_cast<const Frame *>(reinterpret_cast<const unsigned char *>(this) + header()); }
-    TB_D int64_t *ets() { return reinterpret_cast<int64_t *>(reinterpret_cast<unsigned char *>(this) + header() + (size_t)cap * sizeof(Frame)); }
-    TB_D uint32_t *eref()
-    {
-        return reinterpret_cast<uint32_t *>(reinterpret_cast<unsigned char *>(this) + header() + (size_t)cap * (sizeof(Frame) + 8));
-    }
+    // the arrays after this header, addressed from the scratch itself (so that the compiler keeps
+    // them in the shared address space): the staged frames [cap], then each egress region's
+    // arrival times [cap] and sources [cap] (staged slots)
+    TB_D unsigned char *bytes() { return reinterpret_cast<unsigned char *>(this); }
+    TB_D const unsigned char *bytes() const { return reinterpret_cast<const unsigned char *>(this); }
+    TB_D Frame *fr() { return reinterpret_cast<Frame *>(bytes() + header()); }
+    TB_D const Frame *fr() const { return reinterpret_cast<const Frame *>(bytes() + header()); }
+    TB_D int64_t *ets() { return reinterpret_cast<int64_t *>(bytes() + header() + (size_t)cap * sizeof(Frame)); }
+    TB_D uint32_t *eref() { return reinterpret_cast<uint32_t *>(bytes() + header() + (size_t)cap * (sizeof(Frame) + 8)); }
     static TB_HDI size_t header();
 };
 
