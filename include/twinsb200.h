@@ -149,8 +149,8 @@ int tb_set_launch_shape(tb_ctx *ctx, int host_lanes, int stage_frames, int grid)
 int tb_set_autotune(tb_ctx *ctx, int on);
 
 /* sizeof(tb_topology), sizeof(tb_tcp_params), sizeof(tb_stats), sizeof(tb_serve_caps),
- * sizeof(tb_request_info), sizeof(tb_serve_stats) in out[0..n-1], so that bindings in other
- * languages can check their struct layouts (no counterpart in the reference). */
+ * sizeof(tb_request_info), sizeof(tb_serve_stats), sizeof(tb_qrec) in out[0..n-1], so that
+ * bindings in other languages can check their struct layouts (no counterpart in the reference). */
 int tb_abi_sizes(unsigned long long *out, int n);
 
 /* One TCP world run to completion without allocating device memory (no counterpart in the
@@ -169,6 +169,24 @@ int tb_run_static(int device, const tb_topology *topo, int n_flows, const int *s
                   const long long *size, const long long *start_ns, const long long *conn,
                   const tb_tcp_params *params, long long max_slots, long long *established_ns,
                   long long *completed_ns);
+
+/* ---- the enqueue trace (the reference's --qtrace, src/main.cu:169-174, 985-994, 1077-1100;
+ * record src/model.h:313-320): every packet a queue accepts with from_ps <= its time < until_ps.
+ * Recorded only by the trace build (libtwinsb200_trace.so, front-end twins-trace); the others
+ * return TB_ERR_STATE. */
+typedef struct tb_qrec
+{
+    long long ts;                /* ps */
+    int node, dev, src, dst;     /* ns-3 node (hosts, then switches) and device (NIC 1, port p+1) */
+    unsigned sa;                 /* sequence (data) or acknowledgement number */
+    unsigned short len, qlen;    /* bytes on the wire; the queue disc's length after the enqueue */
+    unsigned char flags, pad[3];
+} tb_qrec;
+
+int tb_has_qtrace(void);
+int tb_set_qtrace(tb_ctx *ctx, unsigned long long capacity, long long from_ps, long long until_ps);
+/* After tb_run: the records (in recording order, at most cap), *n the number recorded (<= capacity). */
+int tb_qtrace(tb_ctx *ctx, tb_qrec *out, unsigned long long cap, unsigned long long *n);
 
 /* ---- serving: requests join a running batch (no counterpart in the reference, which runs one
  * batch fixed at start, src/main.cu:283-325). A server holds device arrays sized by its

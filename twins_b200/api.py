@@ -21,6 +21,8 @@ import numpy as np
 LIB_PATH = Path(__file__).resolve().parent / "lib" / "libtwinsb200.so"
 # the 25-run event-chain build (the reference's twins128)
 LIB25_PATH = Path(__file__).resolve().parent / "lib" / "libtwinsb200_runs25.so"
+# the build that records the enqueue trace (the reference's --qtrace)
+LIB_TRACE_PATH = Path(__file__).resolve().parent / "lib" / "libtwinsb200_trace.so"
 
 TB_OK, TB_WARN_INEXACT = 0, 1
 TB_ERR = {-1: "bad argument", -2: "CUDA error", -3: "HBM budget exceeded", -4: "call out of order",
@@ -59,6 +61,12 @@ class _Stats(ctypes.Structure):
                 ("bytes_h2d", ctypes.c_ulonglong), ("bytes_d2h", ctypes.c_ulonglong),
                 ("grid", ctypes.c_int), ("host_lanes", ctypes.c_int), ("warps_per_block", ctypes.c_int),
                 ("stage_frames", ctypes.c_int), ("autotuned", ctypes.c_int)]
+
+
+class _QRec(ctypes.Structure):
+    _fields_ = [("ts", ctypes.c_longlong), ("node", ctypes.c_int), ("dev", ctypes.c_int), ("src", ctypes.c_int), ("dst", ctypes.c_int),
+                ("sa", ctypes.c_uint), ("len", ctypes.c_ushort), ("qlen", ctypes.c_ushort), ("flags", ctypes.c_ubyte),
+                ("pad", ctypes.c_ubyte * 3)]
 
 
 class _ServeCaps(ctypes.Structure):
@@ -100,6 +108,9 @@ ENTRY_POINTS = [
     ("tb_set_launch_shape", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("tb_set_autotune", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("tb_abi_sizes", ctypes.c_int, [_P(ctypes.c_ulonglong), ctypes.c_int]),
+    ("tb_has_qtrace", ctypes.c_int, []),
+    ("tb_set_qtrace", ctypes.c_int, [ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_longlong, ctypes.c_longlong]),
+    ("tb_qtrace", ctypes.c_int, [ctypes.c_void_p, _P(_QRec), ctypes.c_ulonglong, _P(ctypes.c_ulonglong)]),
     ("tb_server_create", ctypes.c_int, [ctypes.c_int, _P(_ServeCaps), _P(ctypes.c_void_p)]),
     ("tb_server_destroy", ctypes.c_int, [ctypes.c_void_p]),
     ("tb_server_submit_tcp", ctypes.c_int, [ctypes.c_void_p, _P(_Topology), ctypes.c_int, _P(ctypes.c_int), _P(ctypes.c_int),
@@ -133,10 +144,10 @@ def load_library(path: Optional[os.PathLike] = None) -> ctypes.CDLL:
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    sizes = (ctypes.c_ulonglong * 6)()
-    lib.tb_abi_sizes(sizes, 6)
+    sizes = (ctypes.c_ulonglong * 7)()
+    lib.tb_abi_sizes(sizes, 7)
     want = [ctypes.sizeof(_Topology), ctypes.sizeof(_TcpParams), ctypes.sizeof(_Stats), ctypes.sizeof(_ServeCaps),
-            ctypes.sizeof(_RequestInfo), ctypes.sizeof(_ServeStats)]
+            ctypes.sizeof(_RequestInfo), ctypes.sizeof(_ServeStats), ctypes.sizeof(_QRec)]
     if list(sizes) != want:
         raise RuntimeError(f"{p}: struct sizes {list(sizes)} differ from these bindings' {want}: rebuild")
     if path is None:

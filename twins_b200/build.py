@@ -8,6 +8,8 @@ Outputs (git-ignored, they travel with the repository to the GPU machine):
     twins_b200/lib/twins                  the reference's command line over it
     twins_b200/lib/libtwinsb200_runs25.so the same with 25-run chains (128-byte frames), as the
     twins_b200/lib/twins128               reference's twins128 build (-DTWINS_CHAIN_RUNS=25)
+    twins_b200/lib/libtwinsb200_trace.so  the same recording every enqueue (the reference's
+    twins_b200/lib/twins-trace            --qtrace); twins runs twins-trace when given --qtrace
 """
 from __future__ import annotations
 
@@ -24,8 +26,10 @@ SO = LIB / "libtwinsb200.so"
 CLI = LIB / "twins"
 SO25 = LIB / "libtwinsb200_runs25.so"
 CLI25 = LIB / "twins128"
-# (library, front-end, extra flags) per event-chain length
-VARIANTS = [(SO, CLI, []), (SO25, CLI25, ["-DTB_CHAIN_RUNS=25"])]
+SO_TRACE = LIB / "libtwinsb200_trace.so"
+CLI_TRACE = LIB / "twins-trace"
+# (library, front-end, extra flags): 9-run chains, 25-run chains, 9-run chains with the enqueue trace
+VARIANTS = [(SO, CLI, []), (SO25, CLI25, ["-DTB_CHAIN_RUNS=25"]), (SO_TRACE, CLI_TRACE, ["-DTB_QTRACE"])]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # exactness: no floating-point contraction (fma() is written where ns-3 fuses), IEEE division

@@ -542,6 +542,8 @@ struct tb_ctx
     int host_lanes = 1, grid_req = 0, grid = 0;
     int stage_cap = SW_STAGE;     // frames staged per warp
     int *d_units = nullptr;       // the running units' list (tb_run)
+    unsigned long long qtrace_cap = 0; // the enqueue trace (trace build): records kept, window (ps)
+    long long qtrace_from = 0, qtrace_until = 0;
     bool autotune = true;         // pick the launch shape per launch by measured throughput
     int dev_sms = 0;
     cudaStream_t stream = nullptr;
@@ -889,6 +891,72 @@ int grid_for(const tb_ctx *c, int host_lanes, int stage, int units = -1)
     return c->grid_req > 0 ? std::min(c->grid_req, most) : std::min(need, most);
 }
 
+// Launch-shape autotuning, for tb_run and the server. A shape is the hosts per warp and the
+// frames a warp stages per slot; no shape changes a result. It starts from one host per warp
+// while the entities fit the resident warps about once (latency-bound: each host's serial events
+// are the slot's critical path), else 32 hosts per warp (throughput-bound: the lanes' memory
+// accesses overlap). Every `period` launches each shape still in the running runs a probe of
+// `probe` slots, and one whose device time per slot beats the current one's by more than 5%
+// takes over; a shape that loses a probe by more than 30% twice is not probed again.
+struct ShapeTuner
+{
+    struct Shape
+    {
+        int lanes, stage;
+        long long slots;
+        int strikes;
+    };
+    std::vector<Shape> shapes;
+    size_t best = 0;
+    long long since = 0;
+    int period = 12, probe = 64;
+
+    void init(const tb_ctx *c, bool autotune, int lanes, int stage, long long entities)
+    {
+        shapes.clear();
+        best = 0;
+        since = 0;
+        if (autotune)
+        {
+            const int cand[][2] = {{1, SW_STAGE}, {4, SW_STAGE}, {32, SW_STAGE}, {1, SW_STAGE_SMALL}, {32, SW_STAGE_SMALL}, {1, SW_STAGE_MAX}};
+            for (auto &x : cand)
+                if (grid_for(c, x[0], x[1]) > 0)
+                    shapes.push_back({x[0], x[1], 0, 0});
+            const long long resident = (long long)c->dev_sms * std::max(1, tb::slot_kernel_blocks_per_sm(SW_STAGE)) * TB_WARPS_PER_BLOCK;
+            const int lanes0 = entities <= 2 * resident ? 1 : 32;
+            for (size_t k = 0; k < shapes.size(); k++)
+                if (shapes[k].lanes == lanes0 && shapes[k].stage == SW_STAGE)
+                    best = k;
+        }
+        if (shapes.empty())
+            shapes.push_back({lanes, stage, 0, 0});
+    }
+    bool explore() const { return shapes.size() > 1 && since >= period; }
+    bool probes(size_t k) const { return k == best || shapes[k].strikes < 2; }
+    // after a round of probes (per_slot[k]: ms per slot, <= 0 where no probe ran)
+    void decide(const std::vector<double> &per_slot)
+    {
+        size_t b = best;
+        for (size_t k = 0; k < shapes.size(); k++)
+            if (per_slot[k] > 0 && (per_slot[b] <= 0 || per_slot[k] < 0.95 * per_slot[b]))
+                b = k;
+        for (size_t k = 0; k < shapes.size(); k++)
+            if (per_slot[k] > 0 && per_slot[b] > 0 && per_slot[k] > 1.3 * per_slot[b])
+                shapes[k].strikes++;
+        best = b;
+        since = 0;
+    }
+    // the shape that ran the most slots
+    size_t most() const
+    {
+        size_t m = 0;
+        for (size_t k = 1; k < shapes.size(); k++)
+            if (shapes[k].slots > shapes[m].slots)
+                m = k;
+        return m;
+    }
+};
+
 int prepare(tb_ctx *c)
 {
     if (c->prepared)
@@ -1045,6 +1113,14 @@ int prepare(tb_ctx *c)
     }
     if (!c->arena && (r = c->alloc(&c->d_units, (size_t)H + S, false)))
         return r;
+    if (c->qtrace_cap)
+    {
+        if ((r = c->alloc(&s.qtrace, c->qtrace_cap, false)) || (r = c->alloc(&s.qtrace_cnt, 1, true)))
+            return r;
+        s.qtrace_n = c->qtrace_cap;
+        s.qtrace_from = c->qtrace_from;
+        s.qtrace_until = c->qtrace_until;
+    }
     // snapshots of the initial state
     for (auto &sn : c->snaps)
         if (cudaMemcpy(sn.src, sn.dst, sn.bytes, cudaMemcpyDeviceToDevice) != cudaSuccess)
@@ -1186,41 +1262,10 @@ int tb_run(tb_ctx *ctx, long long max_slots)
     Sim s = ctx->sim;
     s.max_slots = max_slots > 0 ? max_slots : 2000000;
     SlotCtl ctl{};
-    // Launch shapes: hosts per warp and frames staged per warp (a smaller staging area leaves room
-    // for more resident blocks). The results do not depend on the shape. Autotuning starts from
-    // one host per warp while the hosts fit the resident warps about once (latency-bound: each
-    // host's serial events are the slot's critical path), else 32 hosts per warp (throughput-
-    // bound: the lanes' memory accesses overlap). Every `period` launches, each shape runs a
-    // probe of `probe` slots, and a shape whose device time per slot beats the current one's by
-    // more than 5% takes over.
-    struct Shape
-    {
-        int lanes, stage, grid;
-        long long slots;
-        int strikes; // probes it lost by more than 30% (it is not probed again after two)
-    };
-    std::vector<Shape> shapes;
-    size_t best = 0;
-    if (ctx->autotune)
-    {
-        const int cand[][2] = {{1, SW_STAGE}, {4, SW_STAGE}, {32, SW_STAGE}, {1, SW_STAGE_SMALL}, {32, SW_STAGE_SMALL}, {1, SW_STAGE_MAX}};
-        for (auto &c : cand)
-        {
-            int g = grid_for(ctx, c[0], c[1]);
-            if (g > 0)
-                shapes.push_back({c[0], c[1], g, 0, 0});
-        }
-        const long long resident = (long long)ctx->dev_sms * std::max(1, tb::slot_kernel_blocks_per_sm(SW_STAGE)) * TB_WARPS_PER_BLOCK;
-        const int lanes0 = s.H + s.S <= 2 * resident ? 1 : 32;
-        for (size_t k = 0; k < shapes.size(); k++)
-            if (shapes[k].lanes == lanes0 && shapes[k].stage == SW_STAGE)
-                best = k;
-    }
-    if (shapes.empty())
-        shapes.push_back({ctx->host_lanes, ctx->stage_cap, ctx->grid, 0, 0});
-    const int probe = 64, period = 12;
-    const int run_slots = shapes.size() > 1 ? std::min(ctx->max_slots_per_launch, 1024) : ctx->max_slots_per_launch;
-    long long launches = 0, since = 0;
+    ShapeTuner tu;
+    tu.init(ctx, ctx->autotune, ctx->host_lanes, ctx->stage_cap, (long long)s.H + s.S);
+    const int run_slots = tu.shapes.size() > 1 ? std::min(ctx->max_slots_per_launch, 1024) : ctx->max_slots_per_launch;
+    long long launches = 0;
     // the running worlds' units: rebuilt when a world finishes (or the shape changes), so that a
     // finished world's entities cost a launch nothing and the grid shrinks with the work
     std::vector<std::array<int, 4>> wr(s.W);
@@ -1234,14 +1279,14 @@ int tb_run(tb_ctx *ctx, long long max_slots)
     cudaEventRecord(ctx->ev0, ctx->stream);
     for (;;)
     {
-        const bool explore = shapes.size() > 1 && since >= period;
-        std::vector<double> per_slot(shapes.size(), -1);
-        for (size_t k = 0; k < shapes.size(); k++)
+        const bool explore = tu.explore();
+        std::vector<double> per_slot(tu.shapes.size(), -1);
+        for (size_t k = 0; k < tu.shapes.size(); k++)
         {
-            if ((!explore && k != best) || (explore && k != best && shapes[k].strikes >= 2))
+            if (explore ? !tu.probes(k) : k != tu.best)
                 continue;
-            Shape &sh = shapes[k];
-            int grid = sh.grid;
+            ShapeTuner::Shape &sh = tu.shapes[k];
+            int grid = ctx->grid_req > 0 && !ctx->autotune ? ctx->grid : grid_for(ctx, sh.lanes, sh.stage);
             if (ctx->d_units && alive < s.W)
             {
                 if (alive != list_alive || sh.lanes != list_lanes)
@@ -1259,7 +1304,7 @@ int tb_run(tb_ctx *ctx, long long max_slots)
             }
             const long long slots_before = ctl.slots_run;
             cudaEventRecord(ctx->la, ctx->stream);
-            int e = tb::launch_slots(s, grid, explore ? probe : run_slots, sh.lanes, sh.stage, ctx->stream);
+            int e = tb::launch_slots(s, grid, explore ? tu.probe : run_slots, sh.lanes, sh.stage, ctx->stream);
             if (e)
                 return fail(TB_ERR_CUDA, std::string("slot kernel launch: ") + cudaGetErrorString((cudaError_t)e));
             cudaEventRecord(ctx->lb, ctx->stream);
@@ -1278,25 +1323,15 @@ int tb_run(tb_ctx *ctx, long long max_slots)
             sh.slots += ran;
             float lms = 0;
             cudaEventElapsedTime(&lms, ctx->la, ctx->lb);
-            if (ran >= probe / 2)
+            if (ran >= tu.probe / 2)
                 per_slot[k] = lms / (double)ran;
             if (ctl.finished || ctl.error)
                 break;
         }
         if (explore)
-        {
-            size_t b = best;
-            for (size_t k = 0; k < shapes.size(); k++)
-                if (per_slot[k] > 0 && (per_slot[b] <= 0 || per_slot[k] < 0.95 * per_slot[b]))
-                    b = k;
-            for (size_t k = 0; k < shapes.size(); k++)
-                if (per_slot[k] > 0 && per_slot[b] > 0 && per_slot[k] > 1.3 * per_slot[b])
-                    shapes[k].strikes++;
-            best = b;
-            since = 0;
-        }
+            tu.decide(per_slot);
         else
-            since++;
+            tu.since++;
         if (ctl.finished || ctl.error)
             break;
     }
@@ -1305,11 +1340,8 @@ int tb_run(tb_ctx *ctx, long long max_slots)
     float ms = 0;
     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
     ctx->ran = true;
-    // the shape that ran the most slots
-    size_t most = 0;
-    for (size_t k = 1; k < shapes.size(); k++)
-        if (shapes[k].slots > shapes[most].slots)
-            most = k;
+    const ShapeTuner::Shape &most = tu.shapes[tu.most()];
+    const int most_grid = grid_for(ctx, most.lanes, most.stage);
 #ifdef TB_PROFILE
     if (ctl.slots_run > 1)
     {
@@ -1338,11 +1370,11 @@ int tb_run(tb_ctx *ctx, long long max_slots)
     st.host_frames = ev[EV_HOST_FRAMES];
     st.switch_events = ev[EV_SW_PKT];
     st.packet_events = st.host_events + st.switch_events;
-    st.grid = shapes[most].grid;
-    st.host_lanes = shapes[most].lanes;
+    st.grid = ctx->grid_req > 0 && !ctx->autotune ? ctx->grid : most_grid;
+    st.host_lanes = most.lanes;
     st.warps_per_block = TB_WARPS_PER_BLOCK;
-    st.stage_frames = shapes[most].stage;
-    st.autotuned = shapes.size() > 1;
+    st.stage_frames = most.stage;
+    st.autotuned = tu.shapes.size() > 1;
     st.bytes_d2h = 0;
     if (ctl.error)
         return fail(TB_ERR_TIMEOUT, "a device-side barrier wait ran out; the run was abandoned");
@@ -1405,10 +1437,50 @@ int tb_hashes(tb_ctx *ctx, int world, unsigned *hash_data, unsigned *hash_ack)
 
 int tb_abi_sizes(unsigned long long *out, int n)
 {
-    const unsigned long long v[6] = {sizeof(tb_topology),   sizeof(tb_tcp_params),   sizeof(tb_stats),
-                                     sizeof(tb_serve_caps), sizeof(tb_request_info), sizeof(tb_serve_stats)};
-    for (int i = 0; i < n && i < 6; i++)
+    const unsigned long long v[7] = {sizeof(tb_topology),     sizeof(tb_tcp_params),  sizeof(tb_stats), sizeof(tb_serve_caps),
+                                     sizeof(tb_request_info), sizeof(tb_serve_stats), sizeof(tb_qrec)};
+    for (int i = 0; i < n && i < 7; i++)
         out[i] = v[i];
+    return TB_OK;
+}
+
+int tb_has_qtrace(void)
+{
+#ifdef TB_QTRACE
+    return 1;
+#else
+    return 0;
+#endif
+}
+
+int tb_set_qtrace(tb_ctx *ctx, unsigned long long capacity, long long from_ps, long long until_ps)
+{
+    if (!ctx)
+        return fail(TB_ERR_ARG, "ctx is NULL");
+    if (!tb_has_qtrace())
+        return fail(TB_ERR_STATE, "this library records no enqueue trace: load libtwinsb200_trace.so (or run twins-trace)");
+    if (ctx->prepared)
+        return fail(TB_ERR_STATE, "set the trace before tb_prepare");
+    ctx->qtrace_cap = capacity;
+    ctx->qtrace_from = from_ps;
+    ctx->qtrace_until = until_ps;
+    return TB_OK;
+}
+
+int tb_qtrace(tb_ctx *ctx, tb_qrec *out, unsigned long long cap, unsigned long long *n)
+{
+    static_assert(sizeof(tb_qrec) == sizeof(QRec), "tb_qrec is QRec's public twin");
+    if (!ctx || !n)
+        return fail(TB_ERR_ARG, "ctx and n are required");
+    if (!ctx->ran || !ctx->sim.qtrace)
+        return fail(TB_ERR_STATE, "no traced run");
+    unsigned long long cnt = 0;
+    if (cudaMemcpy(&cnt, ctx->sim.qtrace_cnt, 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return fail(TB_ERR_CUDA, "cudaMemcpy failed");
+    cnt = std::min<unsigned long long>(cnt, ctx->sim.qtrace_n);
+    *n = cnt;
+    if (out && cap && cudaMemcpy(out, ctx->sim.qtrace, sizeof(QRec) * std::min(cnt, cap), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return fail(TB_ERR_CUDA, "cudaMemcpy failed");
     return TB_OK;
 }
 

@@ -104,6 +104,10 @@ struct Egress
     Frame *out; // this slot's link message
     int sent;
     unsigned drops, marks, ovf, emitted;
+#ifdef TB_QTRACE
+    const Sim *qs; // the trace's sink; the queue's ns-3 node and device
+    int qnode, qdev;
+#endif
 
     // start every frame whose transmission begins by `until` and within this slot
     TB_D void advance(int64_t until)
@@ -165,6 +169,30 @@ struct Egress
             drops++;
             return false;
         }
+#ifdef TB_QTRACE
+        if (qs->qtrace && now < qs->qtrace_until && now >= qs->qtrace_from)
+        {
+#if defined(__CUDA_ARCH__)
+            const unsigned long long i = atomicAdd(qs->qtrace_cnt, 1ull);
+#else
+            const unsigned long long i = (*qs->qtrace_cnt)++;
+#endif
+            if (i < qs->qtrace_n)
+            {
+                QRec &r = qs->qtrace[i];
+                const SndRec &S = qs->snd[g.flow];
+                r.ts = now;
+                r.node = qnode;
+                r.dev = qdev;
+                r.src = g.to_sender ? S.dst_local : S.src_local;
+                r.dst = g.to_sender ? S.src_local : S.dst_local;
+                r.sa = g.sa;
+                r.len = g.len;
+                r.qlen = (uint16_t)(nq + 1);
+                r.flags = g.flags;
+            }
+        }
+#endif
         if (size >= cap)
         {
             ovf++;

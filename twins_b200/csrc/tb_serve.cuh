@@ -124,6 +124,9 @@ struct tb_server
     int lanes = 1, stage = SW_STAGE, grid = 0;
     int *d_units = nullptr;      // the batch's units (device)
     bool units_stale = true;     // admissions or retirements since the list was built
+    int list_lanes = 0;          // the hosts per unit the list was built for
+    long long batch_entities = 0;
+    ShapeTuner tuner;            // the launch shape, per launch
     // statistics
     long long launches = 0, slots_run = 0, admitted = 0, retired = 0;
     double kernel_ms = 0;
@@ -374,9 +377,9 @@ int serve_round(tb_server *v, int *running)
     }
     if (in_batch)
     {
-        if (v->units_stale)
-        {
-            // the units of the worlds in the batch (free entities are not visited)
+        // the units of the worlds in the batch (free entities are not visited), for a shape's
+        // hosts per warp; world slots in place order, so that host units come out ascending
+        auto build_list = [&](int lanes) -> int {
             std::vector<std::array<int, 4>> wr(s.W, std::array<int, 4>{0, 0, 0, 0});
             std::vector<WorldCtl> live(s.W);
             {
@@ -391,53 +394,90 @@ int serve_round(tb_server *v, int *running)
                     }
                 }
             }
-            // (world slots in place order: the host units come out ascending)
             std::vector<int> order(s.W);
             for (int i = 0; i < s.W; i++)
                 order[i] = i;
             std::sort(order.begin(), order.end(), [&](int a, int b) { return wr[a][0] < wr[b][0]; });
             std::vector<std::array<int, 4>> wr2(s.W);
             std::vector<WorldCtl> live2(s.W);
+            long long entities = 0;
             for (int i = 0; i < s.W; i++)
             {
                 wr2[i] = wr[order[i]];
                 live2[i] = live[order[i]];
+                entities += wr2[i][1] + wr2[i][3];
             }
+            v->batch_entities = entities;
             std::vector<int> ulist;
-            running_units(live2, wr2, v->lanes, s.H, ulist);
+            running_units(live2, wr2, lanes, s.H, ulist);
             if (!ulist.empty() &&
                 cudaMemcpyAsync(v->d_units, ulist.data(), sizeof(int) * ulist.size(), cudaMemcpyHostToDevice, v->dev.stream) != cudaSuccess)
                 return fail(TB_ERR_CUDA, "cudaMemcpyAsync failed");
             s.unit_list = v->d_units;
             s.n_list = (int)ulist.size();
-            v->grid = grid_for(&v->dev, v->lanes, v->stage, s.n_list);
+            v->list_lanes = lanes;
             v->units_stale = false;
+            return TB_OK;
+        };
+        // one launch of `slots` slots with shape k; *per_slot: its device ms per slot run
+        long long before_all = ctl.slots_run;
+        auto launch = [&](size_t k, int slots, double *per_slot) -> int {
+            ShapeTuner::Shape &sh = v->tuner.shapes[k];
+            if (v->units_stale || v->list_lanes != sh.lanes)
+            {
+                int rr = build_list(sh.lanes);
+                if (rr)
+                    return rr;
+            }
+            v->lanes = sh.lanes;
+            v->stage = sh.stage;
+            v->grid = grid_for(&v->dev, sh.lanes, sh.stage, s.n_list);
+            // the kernel stops early when every world in the batch is done
+            ctl.finished = 0;
+            if (cudaMemcpyAsync(&s.ctl->finished, &ctl.finished, sizeof(int), cudaMemcpyHostToDevice, v->dev.stream) != cudaSuccess)
+                return fail(TB_ERR_CUDA, "cudaMemcpyAsync failed");
+            const long long before = ctl.slots_run;
+            cudaEventRecord(v->dev.la, v->dev.stream);
+            int e = tb::launch_slots(s, v->grid, slots, sh.lanes, sh.stage, v->dev.stream);
+            if (e)
+                return fail(TB_ERR_CUDA, std::string("slot kernel launch: ") + cudaGetErrorString((cudaError_t)e));
+            cudaEventRecord(v->dev.lb, v->dev.stream);
+            if (cudaMemcpyAsync(&ctl, s.ctl, sizeof ctl, cudaMemcpyDeviceToHost, v->dev.stream) != cudaSuccess ||
+                cudaStreamSynchronize(v->dev.stream) != cudaSuccess)
+                return fail(TB_ERR_CUDA, std::string("slot kernel: ") + cudaGetErrorString(cudaGetLastError()));
+            if (ctl.error)
+                return fail(TB_ERR_TIMEOUT, "a device-side barrier wait ran out");
+            float ms = 0;
+            cudaEventElapsedTime(&ms, v->dev.la, v->dev.lb);
+            const long long ran = ctl.slots_run - before;
+            sh.slots += ran;
+            v->kernel_ms += ms;
+            v->launches++;
+            if (per_slot)
+                *per_slot = ran >= v->tuner.probe / 2 ? ms / (double)ran : -1;
+            return TB_OK;
+        };
+        if (v->tuner.explore())
+        {
+            std::vector<double> per_slot(v->tuner.shapes.size(), -1);
+            for (size_t k = 0; k < v->tuner.shapes.size() && !ctl.finished; k++)
+                if (v->tuner.probes(k) && (r = launch(k, v->tuner.probe, &per_slot[k])))
+                    return r;
+            v->tuner.decide(per_slot);
         }
-        // run: the kernel stops early when every world in the batch is done
-        ctl.finished = 0;
-        if (cudaMemcpyAsync(&s.ctl->finished, &ctl.finished, sizeof(int), cudaMemcpyHostToDevice, v->dev.stream) != cudaSuccess)
-            return fail(TB_ERR_CUDA, "cudaMemcpyAsync failed");
-        cudaEventRecord(v->dev.la, v->dev.stream);
-        int e = tb::launch_slots(s, v->grid, v->caps.slots_per_launch, v->lanes, v->stage, v->dev.stream);
-        if (e)
-            return fail(TB_ERR_CUDA, std::string("slot kernel launch: ") + cudaGetErrorString((cudaError_t)e));
-        cudaEventRecord(v->dev.lb, v->dev.stream);
-        const long long before = ctl.slots_run;
+        else
+        {
+            if ((r = launch(v->tuner.best, v->caps.slots_per_launch, nullptr)))
+                return r;
+            v->tuner.since++;
+        }
         std::vector<WorldCtl> wc(s.W);
         std::vector<unsigned long long> ev(EV_N);
-        if (cudaMemcpyAsync(&ctl, s.ctl, sizeof ctl, cudaMemcpyDeviceToHost, v->dev.stream) != cudaSuccess ||
-            cudaMemcpyAsync(wc.data(), s.wctl, sizeof(WorldCtl) * s.W, cudaMemcpyDeviceToHost, v->dev.stream) != cudaSuccess ||
-            cudaMemcpyAsync(ev.data(), s.ev, 8 * EV_N, cudaMemcpyDeviceToHost, v->dev.stream) != cudaSuccess ||
-            cudaStreamSynchronize(v->dev.stream) != cudaSuccess)
-            return fail(TB_ERR_CUDA, std::string("slot kernel: ") + cudaGetErrorString(cudaGetLastError()));
-        if (ctl.error)
-            return fail(TB_ERR_TIMEOUT, "a device-side barrier wait ran out");
-        float ms = 0;
-        cudaEventElapsedTime(&ms, v->dev.la, v->dev.lb);
+        if (cudaMemcpy(wc.data(), s.wctl, sizeof(WorldCtl) * s.W, cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(ev.data(), s.ev, 8 * EV_N, cudaMemcpyDeviceToHost) != cudaSuccess)
+            return fail(TB_ERR_CUDA, "cudaMemcpy failed");
         std::lock_guard<std::mutex> g(v->mu);
-        v->launches++;
-        v->slots_run += ctl.slots_run - before;
-        v->kernel_ms += ms;
+        v->slots_run += ctl.slots_run - before_all;
         v->events = ev[EV_HOST_PKT] + ev[EV_SW_PKT];
         for (int wi = 0; wi < s.W; wi++)
             if (v->slot_req[wi] && wc[wi].next == INT64_MAX)
@@ -533,13 +573,13 @@ int server_alloc(tb_server *v)
     if ((r = park(v, 0, s.H, 0, s.S)))
         return r;
     cudaStreamSynchronize(c.stream);
-    // the launch shape (as tb_run's autotuner starts): one host per warp while the entities fit
-    // the resident warps about once, else 32 hosts per warp with the smaller staging area
     cudaDeviceGetAttribute(&c.dev_sms, cudaDevAttrMultiProcessorCount, v->device);
     c.sim = s;
-    const long long resident = (long long)c.dev_sms * std::max(1, tb::slot_kernel_blocks_per_sm(SW_STAGE)) * TB_WARPS_PER_BLOCK;
-    v->lanes = s.H + s.S <= 2 * resident ? 1 : 32;
-    v->stage = v->lanes == 1 ? SW_STAGE : SW_STAGE_SMALL;
+    v->tuner.init(&c, true, 1, SW_STAGE, (long long)s.H + s.S);
+    v->tuner.period = 8;
+    v->tuner.probe = 32;
+    v->lanes = v->tuner.shapes[v->tuner.best].lanes;
+    v->stage = v->tuner.shapes[v->tuner.best].stage;
     if ((v->grid = grid_for(&c, v->lanes, v->stage)) <= 0)
         return fail(TB_ERR_CUDA, "the slot kernel does not fit on the device");
     v->a_world.init(k.worlds);

@@ -105,6 +105,11 @@ TB_D bool host_step(const Sim &s, int h, int64_t t, int64_t gt, int64_t *wake, u
     nic.out = s.msg + msg_index(s, gt, h) * MAX_TX;
     nic.sent = 0;
     nic.drops = nic.marks = nic.ovf = nic.emitted = 0;
+#ifdef TB_QTRACE
+    nic.qs = &s;
+    nic.qnode = hr.local;
+    nic.qdev = 1;
+#endif
     unsigned ties = 0;
 
     TB_PHASE(0)

@@ -189,6 +189,20 @@ struct WorldCtl
     int64_t t0;
 };
 
+// one enqueue at an egress queue, as the reference's --qtrace records it (src/model.h:313-320):
+// the enqueue time (ps), the ns-3 node (hosts 0..H-1, then switches) and device (a host's NIC 1,
+// switch port p + 1), the packet's source and destination host, its sequence (data) or ack
+// number, length, the queue disc's length after the enqueue and the flags. Recorded by the trace
+// build (TB_QTRACE) only.
+struct QRec
+{
+    int64_t ts;
+    int32_t node, dev, src, dst;
+    uint32_t sa;
+    uint16_t len, qlen;
+    uint8_t flags, pad[3];
+};
+
 #if defined(TB_PROFILE) && defined(__CUDACC__)
 __device__ __forceinline__ unsigned long long prof_now()
 {
@@ -248,6 +262,11 @@ struct Sim
     // running, then host_units + switch; rebuilt between launches
     const int *unit_list;
     int n_list;
+    // the enqueue trace (trace build; null: off): records of enqueues with from <= time < until
+    QRec *qtrace;
+    unsigned long long *qtrace_cnt;
+    unsigned long long qtrace_n;
+    int64_t qtrace_from, qtrace_until;
 };
 
 } // namespace tb

@@ -352,6 +352,11 @@ TB_D bool sw_phase_egress(const SwCtx &x, SwShared &sh, int e, unsigned &ties, u
     eg.out = s.msg + msg_index(s, x.gt, out_link) * MAX_TX;
     eg.sent = 0;
     eg.drops = eg.marks = eg.ovf = eg.emitted = 0;
+#ifdef TB_QTRACE
+    eg.qs = &s;
+    eg.qnode = x.wd->H1 + x.sr->local;
+    eg.qdev = e + 1;
+#endif
     for (int i = 0; i < n; i++)
     {
         Frame p;

@@ -3,16 +3,21 @@
 //          [--fail=T:sA:sB[:up],...]) (--flows=<csv> [--out=csv] | --worlds=<file>)
 //         [--tcp=dctcp|newreno|cubic] [--ecnK=30] [--queue=200] [--fin=0|1] [--spray=0|1]
 //         [--RngSeed=1] [--RngRun=1] [--ecmp_from=csv [--hash_check=1]] [--max_slots=N]
-//         [--host_lanes=N] [--hbm_budget_gb=G]
+//         [--host_lanes=N] [--hbm_budget_gb=G] [--qtrace=F --qtrace_until=ps [--qtrace_from=ps]]
+// --qtrace: every enqueue with from <= time < until (ps), as the reference writes it
+// (src/main.cu:1077-1100); recorded by the trace build, which this front-end runs (twins-trace)
+// when it was built without it.
 // A worlds file holds one world per line: flows=..,tcp=..,ecnK=..,queue=..,fin=..,ecmp_from=..,out=..
 // Output: fct.csv per world (src,dst,flow_size,start_ns,established_ns,completed_ns); stdout:
 // "Simulation Duration", "Executed Slots" and a counter line, as the reference prints them.
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <sstream>
 #include <string>
+#include <unistd.h>
 #include <vector>
 
 #include "../../include/twinsb200.h"
@@ -94,8 +99,9 @@ struct World
 
 int main(int argc, char **argv)
 {
-    int k = 4, leaves = 16, spines = 8, hpl = 16, ecn_k = 30, queue = 200, fin = 0, spray = 0, hash_check = 0, host_lanes = 1;
-    long long seed = 1, run = 1, max_slots = 2000000;
+    int k = 4, leaves = 16, spines = 8, hpl = 16, ecn_k = 30, queue = 200, fin = 0, spray = 0, hash_check = 0, host_lanes = 0;
+    long long seed = 1, run = 1, max_slots = 2000000, qtrace_from = 0, qtrace_until = 0;
+    std::string qtrace_file;
     double budget_gb = 0;
     std::string flow_file, out = "fct.csv", tcp = "dctcp", topo = "fattree", topofile, fail_spec, worlds_file, ecmp_from;
     for (int i = 1; i < argc; i++)
@@ -147,6 +153,12 @@ int main(int argc, char **argv)
             host_lanes = std::stoi(val("--host_lanes="));
         else if (has("--hbm_budget_gb="))
             budget_gb = std::stod(val("--hbm_budget_gb="));
+        else if (has("--qtrace="))
+            qtrace_file = val("--qtrace=");
+        else if (has("--qtrace_from="))
+            qtrace_from = std::stoll(val("--qtrace_from="));
+        else if (has("--qtrace_until="))
+            qtrace_until = std::stoll(val("--qtrace_until="));
         else if (a == "--general" || has("--ooo_segs=") || has("--rtt_ring=") || has("--graph_k="))
             ; // the reference's tuning flags: this build sizes its rings itself
         else
@@ -154,6 +166,17 @@ int main(int argc, char **argv)
             fprintf(stderr, "unknown argument %s\n", a.c_str());
             return 1;
         }
+    }
+    if (!qtrace_file.empty() && !tb_has_qtrace())
+    {
+        // the trace build, beside this program
+        char self[4096];
+        ssize_t n = readlink("/proc/self/exe", self, sizeof self - 1);
+        std::string path = n > 0 ? std::string(self, n) : std::string(argv[0]);
+        path = path.substr(0, path.find_last_of('/') + 1) + "twins-trace";
+        execv(path.c_str(), argv);
+        fprintf(stderr, "twins: --qtrace needs %s\n", path.c_str());
+        return 1;
     }
     // the topology
     tb_topology T;
@@ -301,7 +324,13 @@ int main(int argc, char **argv)
         fprintf(stderr, "twins: %s\n", tb_last_error());
         return 1;
     }
-    tb_set_launch(ctx, host_lanes, 0);
+    if (host_lanes > 0)
+        tb_set_launch(ctx, host_lanes, 0); // (else the launch shape is autotuned)
+    if (!qtrace_file.empty() && tb_set_qtrace(ctx, 20000000, qtrace_from, qtrace_until) != TB_OK)
+    {
+        fprintf(stderr, "twins: %s\n", tb_last_error());
+        return 1;
+    }
     std::vector<Flows> flows(worlds.size());
     int hash_same = 0, hash_n = 0;
     for (size_t w = 0; w < worlds.size(); w++)
@@ -393,6 +422,34 @@ int main(int argc, char **argv)
            st.slots_run, st.launches, tot[7], tot[8], tot[9], tot[10], tot[11], tot[4]);
     if (r == TB_WARN_INEXACT)
         fprintf(stderr, "warning: a capacity overflowed; the results may differ from the reference\n");
+    if (!qtrace_file.empty())
+    {
+        unsigned long long n = 0;
+        tb_qtrace(ctx, nullptr, 0, &n);
+        std::vector<tb_qrec> q(n);
+        tb_qtrace(ctx, q.data(), n, &n);
+        std::stable_sort(q.begin(), q.end(), [](const tb_qrec &a, const tb_qrec &b) {
+            if (a.ts != b.ts)
+                return a.ts < b.ts;
+            if (a.node != b.node)
+                return a.node < b.node;
+            return a.dev < b.dev;
+        });
+        FILE *o = fopen(qtrace_file.c_str(), "w");
+        if (!o)
+        {
+            fprintf(stderr, "cannot write %s\n", qtrace_file.c_str());
+            return 1;
+        }
+        for (const tb_qrec &x : q)
+        {
+            // data, SYN-ACK, SYN, else an ACK (FIN, FIN-ACK and pure ACKs)
+            const char *kind = (x.flags & 32) ? "D" : (x.flags & 2) ? ((x.flags & 1) ? "SA" : "S") : "A";
+            fprintf(o, "%lld %d %d %d %d %s %u %d\n", x.ts, x.node, x.dev, x.src, x.dst, kind, x.sa, (int)x.qlen);
+        }
+        fclose(o);
+        printf("qtrace: %llu records\n", n);
+    }
     if (worlds.size() > 1)
         printf("worlds %zu\n", worlds.size());
     tb_ctx_destroy(ctx);
