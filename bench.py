@@ -26,6 +26,7 @@ import json
 import os
 import statistics
 import subprocess
+import tempfile
 import sys
 import threading
 import time
@@ -160,7 +161,7 @@ def write_flows(worlds, d: Path):
 def cpu_sample(worlds, slots: int, threads: int):
     """The oracle on the first `slots` slots of every world, one world per process."""
     binary = oracle_bin()
-    d = ROOT / "gpurun_out" / "bench_flows" if (ROOT / "gpurun_out").exists() else Path("/tmp") / "twins_bench_flows"
+    d = Path(tempfile.gettempdir()) / "twins_bench_flows"
     d.mkdir(parents=True, exist_ok=True)
     paths = write_flows(worlds, d)
     t0 = time.perf_counter()
@@ -425,7 +426,7 @@ def main():
         plain = plain_sample(worlds, args.plain_sample, local_rank, len(worlds) / (ms_max / 1000.0))
     ref_gpu = None
     if not args.no_ref_gpu and rank == 0:
-        d = Path("/tmp") / "twins_bench_ref"
+        d = Path(tempfile.gettempdir()) / "twins_bench_ref"
         d.mkdir(exist_ok=True)
         try:
             # (C4: the plain path's sample of worlds, one at a time as the reference runs them)
