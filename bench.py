@@ -222,8 +222,12 @@ def serve_bench(args):
     torch.cuda.set_device(local_rank)
     reqs = workloads.served_stream(seed=1, n=args.requests + 3, rate_per_s=args.rate)
     warm, reqs = reqs[:3], reqs[3:]
-    caps = dict(worlds=48, hosts=24000, switches=8000, ports=80000, connections=120000, messages=120000,
-                sent_list_entries=1 << 28, ooo_blocks=1 << 26, slots_per_launch=128, hbm_budget_bytes=160 * 10 ** 9)
+    # capacities for about `--serve-worlds` requests of the mix at once (500 hosts, 170 switches,
+    # 1,700 ports and 2,500 connections per request on average, with room), within 160 GB
+    n = args.serve_worlds
+    caps = dict(worlds=n, hosts=500 * n, switches=170 * n, ports=1700 * n, connections=2500 * n, messages=2500 * n,
+                sent_list_entries=min(1 << 30, 2_800_000 * n), ooo_blocks=min(1 << 28, 700_000 * n), slots_per_launch=128,
+                hbm_budget_bytes=160 * 10 ** 9)
     with api.Server(device=local_rank, **caps) as srv:
         srv.start()
         for r in warm:  # warm-up requests (untimed)
@@ -286,6 +290,7 @@ def main():
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c2s", "c4", "c5"])
     ap.add_argument("--requests", type=int, default=200, help="C5: requests in the served stream")
     ap.add_argument("--rate", type=float, default=100.0, help="C5: request arrivals per second (Poisson)")
+    ap.add_argument("--serve-worlds", type=int, default=256, help="C5: requests the server holds at once")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--ref-slots", type=int, default=2500, help="reference arm: slots of each world per step")
     ap.add_argument("--cpu-slots", type=int, default=6000, help="cpu_baseline: slots of the sample world")
