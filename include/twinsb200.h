@@ -85,6 +85,7 @@ typedef struct tb_stats
     int grid, host_lanes, warps_per_block; /* the launch shape that ran the most slots */
     int stage_frames;        /* frames a warp stages in shared memory in that shape */
     int autotuned;           /* 1: the shape was picked per launch by measured throughput */
+    int port_local;          /* 1: that shape keeps switch ports' slot state in shared memory */
 } tb_stats;
 
 /* A context on CUDA device `device`, admitting batches up to hbm_budget_bytes of device memory
@@ -143,6 +144,10 @@ int tb_set_launch(tb_ctx *ctx, int host_lanes, int grid);
  * build; default 192; fewer leave room for more resident blocks per SM, more stage the slots of
  * big switches). */
 int tb_set_launch_shape(tb_ctx *ctx, int host_lanes, int stage_frames, int grid);
+/* A fixed shape's switch egress: 1 keeps each port's transmission chain and last enqueued frame in
+ * shared memory for the slot (faster where big switches are the critical path), 0 (default) reads
+ * them from the port's record. Autotuning picks it per launch. */
+int tb_set_port_local(tb_ctx *ctx, int on);
 /* Autotuning (on by default): tb_run picks each launch's shape (hosts per warp, staging size)
  * among a fixed set by the packet-events per ms that short probe launches of each achieve. The
  * results never depend on the shape (no counterpart in the reference). */

@@ -124,15 +124,18 @@ def test_max_slots_stops_early(native_lib):
 
 @pytest.mark.parametrize("name", ["k8_a2a30_dctcp_spray", "k8_r30_cubic_sprayfin", "jf32f_a2a50_newreno_spray"])
 def test_launch_shapes_identical(native_lib, name):
-    """Every launch shape (hosts per warp, frames staged per warp: 8 leaves most slots unstaged)
-    gives the same results and event counts as ns-3 and as each other."""
+    """Every launch shape (hosts per warp, frames staged per warp: 8 leaves most slots unstaged;
+    switch egress with or without the ports' slot copies) gives the same results and event counts
+    as ns-3 and as each other."""
     case = next(c for c in CASES if c["name"] == name)
     want_est, want_done = ns3(case)
     events = set()
-    for lanes, stage in [(1, 192), (1, 8), (1, 96), (1, 384), (4, 96), (32, 192), (7, 64)]:
-        est, done, ctr, stats = api.run_world(*world_of(case), host_lanes=lanes, stage_frames=stage)
-        assert (est == want_est).all() and (done == want_done).all(), (lanes, stage)
+    for lanes, stage, pl in [(1, 192, 0), (1, 8, 0), (1, 96, 0), (1, 384, 0), (4, 96, 0), (32, 192, 0), (7, 64, 0), (1, 384, 1),
+                             (1, 8, 1), (32, 96, 1)]:
+        est, done, ctr, stats = api.run_world(*world_of(case), host_lanes=lanes, stage_frames=stage, port_local=bool(pl))
+        assert (est == want_est).all() and (done == want_done).all(), (lanes, stage, pl)
         assert stats["host_lanes"] == lanes and stats["stage_frames"] == stage and not stats["autotuned"]
+        assert stats["port_local"] == pl
         events.add(stats["packet_events"])
     assert len(events) == 1
 

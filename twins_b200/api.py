@@ -60,7 +60,7 @@ class _Stats(ctypes.Structure):
                 ("host_sender_events", ctypes.c_ulonglong), ("host_frames", ctypes.c_ulonglong),
                 ("bytes_h2d", ctypes.c_ulonglong), ("bytes_d2h", ctypes.c_ulonglong),
                 ("grid", ctypes.c_int), ("host_lanes", ctypes.c_int), ("warps_per_block", ctypes.c_int),
-                ("stage_frames", ctypes.c_int), ("autotuned", ctypes.c_int)]
+                ("stage_frames", ctypes.c_int), ("autotuned", ctypes.c_int), ("port_local", ctypes.c_int)]
 
 
 class _QRec(ctypes.Structure):
@@ -107,6 +107,7 @@ ENTRY_POINTS = [
     ("tb_set_launch", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     ("tb_set_launch_shape", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("tb_set_autotune", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    ("tb_set_port_local", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("tb_abi_sizes", ctypes.c_int, [_P(ctypes.c_ulonglong), ctypes.c_int]),
     ("tb_has_qtrace", ctypes.c_int, []),
     ("tb_set_qtrace", ctypes.c_int, [ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_longlong, ctypes.c_longlong]),
@@ -318,7 +319,7 @@ class Simulator:
     """A batch of worlds on one GPU: add worlds, run, read results (tb_* of the C ABI)."""
 
     def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, host_lanes: Optional[int] = None, grid: int = 0,
-                 stage_frames: int = 192, chain_runs: int = 9):
+                 stage_frames: int = 192, chain_runs: int = 9, port_local: bool = False):
         """host_lanes None: the launch shape is autotuned per launch; else that fixed shape.
         chain_runs 25: the 25-run event-chain build (the reference's twins128)."""
         if chain_runs not in (9, 25):
@@ -328,6 +329,7 @@ class Simulator:
         self._check(self.lib.tb_ctx_create(device, hbm_budget_bytes, ctypes.byref(self.ctx)))
         if host_lanes is not None:
             self._check(self.lib.tb_set_launch_shape(self.ctx, host_lanes, stage_frames, grid))
+            self._check(self.lib.tb_set_port_local(self.ctx, int(port_local)))
         self.sizes: list[int] = []
         self.last_status = TB_OK
 

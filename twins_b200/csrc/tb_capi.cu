@@ -545,6 +545,7 @@ struct tb_ctx
     unsigned long long qtrace_cap = 0; // the enqueue trace (trace build): records kept, window (ps)
     long long qtrace_from = 0, qtrace_until = 0;
     bool autotune = true;         // pick the launch shape per launch by measured throughput
+    bool port_local = false;      // a fixed shape's switch egress (tb_set_port_local)
     int dev_sms = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, la = nullptr, lb = nullptr;
@@ -879,9 +880,9 @@ void running_units(const std::vector<WorldCtl> &wc, const std::vector<std::array
 }
 
 // the grid of a launch shape: a warp per unit, at most what is co-resident (0: does not fit)
-int grid_for(const tb_ctx *c, int host_lanes, int stage, int units = -1)
+int grid_for(const tb_ctx *c, int host_lanes, int stage, int units = -1, bool port_local = false)
 {
-    int per_sm = tb::slot_kernel_blocks_per_sm(stage);
+    int per_sm = tb::slot_kernel_blocks_per_sm(stage, port_local);
     if (per_sm <= 0 || c->dev_sms <= 0)
         return 0;
     if (units < 0)
@@ -905,31 +906,42 @@ struct ShapeTuner
         int lanes, stage;
         long long slots;
         int strikes;
+        bool port_local; // switch ports' slot copies in shared memory (PortEgress)
     };
     std::vector<Shape> shapes;
     size_t best = 0;
-    long long since = 0;
-    int period = 12, probe = 64;
+    long long since = 0, rounds = 0;
+    int period = 12, probe = 128;
 
-    void init(const tb_ctx *c, bool autotune, int lanes, int stage, long long entities)
+    // entities: hosts and switches to run; kmax: the most ports a switch has
+    void init(const tb_ctx *c, bool autotune, int lanes, int stage, long long entities, int kmax = 0)
     {
         shapes.clear();
         best = 0;
         since = 0;
+        rounds = 0;
         if (autotune)
         {
-            const int cand[][2] = {{1, SW_STAGE}, {4, SW_STAGE}, {32, SW_STAGE}, {1, SW_STAGE_SMALL}, {32, SW_STAGE_SMALL}, {1, SW_STAGE_MAX}};
+            // (lanes, stage, port-local)
+            const int cand[][3] = {{1, SW_STAGE_TWO, 0}, {1, SW_STAGE, 0}, {4, SW_STAGE, 0}, {32, SW_STAGE, 0}, {1, SW_STAGE_SMALL, 0},
+                                   {32, SW_STAGE_SMALL, 0}, {1, SW_STAGE_MAX, 0}, {1, SW_STAGE_MAX, 1}, {1, SW_STAGE_TWO - 32, 1}};
             for (auto &x : cand)
-                if (grid_for(c, x[0], x[1]) > 0)
-                    shapes.push_back({x[0], x[1], 0, 0});
+                if (grid_for(c, x[0], x[1], -1, x[2] != 0) > 0)
+                    shapes.push_back({x[0], x[1], 0, 0, x[2] != 0});
             const long long resident = (long long)c->dev_sms * std::max(1, tb::slot_kernel_blocks_per_sm(SW_STAGE)) * TB_WARPS_PER_BLOCK;
+            // (one host per warp: with big switches (16 ports or more), whose ports' serial
+            // enqueues are the critical path, the port-local egress and the largest staging; else
+            // the largest staging that keeps two blocks per SM. 32 hosts per warp: the smallest
+            // staging, for four blocks per SM)
             const int lanes0 = entities <= 2 * resident ? 1 : 32;
+            const bool pl0 = lanes0 == 1 && kmax >= 16;
+            const int stage0 = lanes0 == 1 ? (pl0 ? SW_STAGE_MAX : SW_STAGE_TWO) : SW_STAGE_SMALL;
             for (size_t k = 0; k < shapes.size(); k++)
-                if (shapes[k].lanes == lanes0 && shapes[k].stage == SW_STAGE)
+                if (shapes[k].lanes == lanes0 && shapes[k].stage == stage0 && shapes[k].port_local == pl0)
                     best = k;
         }
         if (shapes.empty())
-            shapes.push_back({lanes, stage, 0, 0});
+            shapes.push_back({lanes, stage, 0, 0, c->port_local});
     }
     bool explore() const { return shapes.size() > 1 && since >= period; }
     bool probes(size_t k) const { return k == best || shapes[k].strikes < 2; }
@@ -945,6 +957,10 @@ struct ShapeTuner
                 shapes[k].strikes++;
         best = b;
         since = 0;
+        // (the load changes along a run: every fourth round probes every shape again)
+        if (++rounds % 4 == 0)
+            for (auto &x : shapes)
+                x.strikes = 0;
     }
     // the shape that ran the most slots
     size_t most() const
@@ -1241,6 +1257,16 @@ int tb_set_launch_shape(tb_ctx *ctx, int host_lanes, int stage_frames, int grid)
 
 int tb_set_launch(tb_ctx *ctx, int host_lanes, int grid) { return tb_set_launch_shape(ctx, host_lanes, SW_STAGE, grid); }
 
+int tb_set_port_local(tb_ctx *ctx, int on)
+{
+    if (!ctx)
+        return fail(TB_ERR_ARG, "ctx is NULL");
+    ctx->port_local = on != 0;
+    if (ctx->prepared && !ctx->autotune && (ctx->grid = grid_for(ctx, ctx->host_lanes, ctx->stage_cap, -1, ctx->port_local)) <= 0)
+        return fail(TB_ERR_CUDA, "the slot kernel does not fit on the device with this shape");
+    return TB_OK;
+}
+
 int tb_set_autotune(tb_ctx *ctx, int on)
 {
     if (!ctx)
@@ -1263,7 +1289,7 @@ int tb_run(tb_ctx *ctx, long long max_slots)
     s.max_slots = max_slots > 0 ? max_slots : 2000000;
     SlotCtl ctl{};
     ShapeTuner tu;
-    tu.init(ctx, ctx->autotune, ctx->host_lanes, ctx->stage_cap, (long long)s.H + s.S);
+    tu.init(ctx, ctx->autotune, ctx->host_lanes, ctx->stage_cap, (long long)s.H + s.S, s.kmax);
     const int run_slots = tu.shapes.size() > 1 ? std::min(ctx->max_slots_per_launch, 1024) : ctx->max_slots_per_launch;
     long long launches = 0;
     // the running worlds' units: rebuilt when a world finishes (or the shape changes), so that a
@@ -1286,7 +1312,7 @@ int tb_run(tb_ctx *ctx, long long max_slots)
             if (explore ? !tu.probes(k) : k != tu.best)
                 continue;
             ShapeTuner::Shape &sh = tu.shapes[k];
-            int grid = ctx->grid_req > 0 && !ctx->autotune ? ctx->grid : grid_for(ctx, sh.lanes, sh.stage);
+            int grid = ctx->grid_req > 0 && !ctx->autotune ? ctx->grid : grid_for(ctx, sh.lanes, sh.stage, -1, sh.port_local);
             if (ctx->d_units && alive < s.W)
             {
                 if (alive != list_alive || sh.lanes != list_lanes)
@@ -1300,11 +1326,11 @@ int tb_run(tb_ctx *ctx, long long max_slots)
                 }
                 s.unit_list = ctx->d_units;
                 s.n_list = (int)ulist.size();
-                grid = grid_for(ctx, sh.lanes, sh.stage, s.n_list);
+                grid = grid_for(ctx, sh.lanes, sh.stage, s.n_list, sh.port_local);
             }
             const long long slots_before = ctl.slots_run;
             cudaEventRecord(ctx->la, ctx->stream);
-            int e = tb::launch_slots(s, grid, explore ? tu.probe : run_slots, sh.lanes, sh.stage, ctx->stream);
+            int e = tb::launch_slots(s, grid, explore ? tu.probe : run_slots, sh.lanes, sh.stage, sh.port_local, ctx->stream);
             if (e)
                 return fail(TB_ERR_CUDA, std::string("slot kernel launch: ") + cudaGetErrorString((cudaError_t)e));
             cudaEventRecord(ctx->lb, ctx->stream);
@@ -1341,7 +1367,7 @@ int tb_run(tb_ctx *ctx, long long max_slots)
     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
     ctx->ran = true;
     const ShapeTuner::Shape &most = tu.shapes[tu.most()];
-    const int most_grid = grid_for(ctx, most.lanes, most.stage);
+    const int most_grid = grid_for(ctx, most.lanes, most.stage, -1, most.port_local);
 #ifdef TB_PROFILE
     if (ctl.slots_run > 1)
     {
@@ -1375,6 +1401,7 @@ int tb_run(tb_ctx *ctx, long long max_slots)
     st.warps_per_block = TB_WARPS_PER_BLOCK;
     st.stage_frames = most.stage;
     st.autotuned = tu.shapes.size() > 1;
+    st.port_local = most.port_local;
     st.bytes_d2h = 0;
     if (ctl.error)
         return fail(TB_ERR_TIMEOUT, "a device-side barrier wait ran out; the run was abandoned");
@@ -1556,7 +1583,7 @@ extern "C" int tb_run_static(int device, const tb_topology *topo, int n_flows, c
     SlotCtl ctl{};
     for (;;)
     {
-        int e = tb::launch_slots(s, c.grid, c.max_slots_per_launch, c.host_lanes, c.stage_cap, 0);
+        int e = tb::launch_slots(s, c.grid, c.max_slots_per_launch, c.host_lanes, c.stage_cap, false, 0);
         if (e)
             return fail(TB_ERR_CUDA, std::string("slot kernel launch: ") + cudaGetErrorString((cudaError_t)e));
         if (cudaMemcpy(&ctl, s.ctl, sizeof ctl, cudaMemcpyDeviceToHost) != cudaSuccess)

@@ -244,6 +244,7 @@ __device__ __forceinline__ void host_unit(const Sim &s, int u, int host_lanes, i
 
 // one switch, one slot (launch slot gt), by its warp (lanes >= k idle but take part in the warp
 // barriers); nothing when its world does not run this slot
+template <bool PORT_LOCAL>
 __device__ bool switch_step(const Sim &s, int sw, int64_t gt, int lane, SwShared &sh, unsigned &ties)
 {
     const SwRec &sr = s.sws[sw];
@@ -307,7 +308,7 @@ __device__ bool switch_step(const Sim &s, int sw, int64_t gt, int lane, SwShared
 #endif
     bool act = false;
     if (on)
-        act = sw_phase_egress(x, sh, lane, my_ties, drops, marks, ovf);
+        act = sw_phase_egress<PORT_LOCAL>(x, sh, lane, my_ties, drops, marks, ovf);
     __syncwarp();
 #ifdef TB_PROFILE
     if (lane == 0)
@@ -335,6 +336,9 @@ __device__ bool switch_step(const Sim &s, int sw, int64_t gt, int lane, SwShared
     return any;
 }
 
+// PORT_LOCAL: switch ports keep the slot's transmission chain and last enqueued frame in shared
+// memory (PortEgress); a separate instantiation, chosen per launch
+template <bool PORT_LOCAL>
 __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, TB_MIN_BLOCKS) slot_kernel(Sim s, int max_slots_per_launch, int host_lanes, int stage_cap)
 {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
@@ -346,7 +350,7 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, TB_MIN_BLOCKS) slot_kern
     const int gwarp = blockIdx.x * WARPS_PER_BLOCK + warp, nwarps = gridDim.x * WARPS_PER_BLOCK;
     const int host_units = (s.H + host_lanes - 1) / host_lanes;
     const int units = host_units + s.S;
-    SwShared &sh = *sw_shared_at(dyn_smem + (size_t)warp * sw_shared_bytes(stage_cap), stage_cap); // the warp's scratch
+    SwShared &sh = *sw_shared_at(dyn_smem + (size_t)warp * sw_shared_bytes(stage_cap, PORT_LOCAL), stage_cap); // the warp's scratch
     __syncwarp();
     SlotCtl *ctl = s.ctl;
     volatile SlotCtl *vc = ctl;
@@ -372,7 +376,7 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, TB_MIN_BLOCKS) slot_kern
             else
             {
                 const int sw = u - host_units;
-                if (switch_step(s, sw, t, lane, sh, ties) && lane == 0)
+                if (switch_step<PORT_LOCAL>(s, sw, t, lane, sh, ties) && lane == 0)
                     atomicOr(&s.wctl[s.sws[sw].world].act, 1u);
             }
 #ifdef TB_PROFILE
@@ -472,54 +476,61 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, TB_MIN_BLOCKS) slot_kern
 }
 
 // dynamic shared memory of a block: one switch scratch (with its staging area) per warp
-static size_t smem_bytes(int stage_cap) { return sw_shared_bytes(stage_cap) * WARPS_PER_BLOCK; }
+static size_t smem_bytes(int stage_cap, bool port_local) { return sw_shared_bytes(stage_cap, port_local) * WARPS_PER_BLOCK; }
 
-static bool smem_attr()
+static const void *kernel_of(bool port_local) { return port_local ? (const void *)slot_kernel<true> : (const void *)slot_kernel<false>; }
+
+static bool smem_attr(bool port_local)
 {
-    static bool ok = cudaFuncSetAttribute(slot_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes(SW_STAGE_MAX)) == cudaSuccess;
-    return ok;
+    static const bool ok[2] = {
+        cudaFuncSetAttribute(slot_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes(SW_STAGE_MAX, false)) == cudaSuccess,
+        cudaFuncSetAttribute(slot_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes(SW_STAGE_MAX, true)) == cudaSuccess};
+    return ok[port_local];
 }
 
 // The preferred shared-memory carveout, in percent of the SM's maximum: the shared memory of the
 // blocks a launch puts on one SM and no more, so that the rest of the SM's unified L1 / shared
 // memory is L1, where the units' records, ring heads and prefetched lines stay between slots.
-static int carveout = -1; // the last one set (-1: none)
-static void set_carveout(int pct)
+static int carveout[2] = {-1, -1}; // the last ones set (-1: none)
+static void set_carveout(bool port_local, int pct)
 {
-    if (pct != carveout && cudaFuncSetAttribute(slot_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, pct) == cudaSuccess)
-        carveout = pct;
+    if (pct != carveout[port_local] &&
+        cudaFuncSetAttribute(kernel_of(port_local), cudaFuncAttributePreferredSharedMemoryCarveout, pct) == cudaSuccess)
+        carveout[port_local] = pct;
 }
 
-int slot_kernel_blocks_per_sm(int stage_cap)
+int slot_kernel_blocks_per_sm(int stage_cap, bool port_local)
 {
     int n = 0;
-    if (stage_cap < 1 || stage_cap > SW_STAGE_MAX || !smem_attr())
+    if (stage_cap < 1 || stage_cap > SW_STAGE_MAX || !smem_attr(port_local))
         return 0;
-    set_carveout(100); // (occupancy with all of the shared memory)
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, slot_kernel, WARPS_PER_BLOCK * 32, smem_bytes(stage_cap)) != cudaSuccess)
+    set_carveout(port_local, 100); // (occupancy with all of the shared memory)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel_of(port_local), WARPS_PER_BLOCK * 32, smem_bytes(stage_cap, port_local)) !=
+        cudaSuccess)
         return 0;
     return n;
 }
 
-int launch_slots(const Sim &s, int grid, int max_slots_per_launch, int host_lanes, int stage_cap, cudaStream_t stream)
+int launch_slots(const Sim &s, int grid, int max_slots_per_launch, int host_lanes, int stage_cap, bool port_local, cudaStream_t stream)
 {
-    if (!smem_attr() || stage_cap < 1 || stage_cap > SW_STAGE_MAX)
+    if (!smem_attr(port_local) || stage_cap < 1 || stage_cap > SW_STAGE_MAX)
         return (int)cudaErrorInvalidValue;
     int dev = 0, sms = 1, max_smem = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
     const long long per_sm = (grid + sms - 1) / sms;
-    const long long need = per_sm * (long long)(smem_bytes(stage_cap) + 2048); // (+ the block's reserved and static shared memory)
-    set_carveout((int)std::min<long long>(100, (need * 100 + max_smem - 1) / max_smem));
+    const size_t bytes = smem_bytes(stage_cap, port_local);
+    const long long need = per_sm * (long long)(bytes + 2048); // (+ the block's reserved and static shared memory)
+    set_carveout(port_local, (int)std::min<long long>(100, (need * 100 + max_smem - 1) / max_smem));
     void *args[] = {(void *)&s, (void *)&max_slots_per_launch, (void *)&host_lanes, (void *)&stage_cap};
-    cudaError_t e = cudaLaunchCooperativeKernel((const void *)slot_kernel, dim3(grid), dim3(WARPS_PER_BLOCK * 32), args, smem_bytes(stage_cap), stream);
+    cudaError_t e = cudaLaunchCooperativeKernel(kernel_of(port_local), dim3(grid), dim3(WARPS_PER_BLOCK * 32), args, bytes, stream);
     if (e == cudaErrorCooperativeLaunchTooLarge)
     {
         // (the carveout left too little shared memory for the blocks to be resident at once)
         cudaGetLastError();
-        set_carveout(100);
-        e = cudaLaunchCooperativeKernel((const void *)slot_kernel, dim3(grid), dim3(WARPS_PER_BLOCK * 32), args, smem_bytes(stage_cap), stream);
+        set_carveout(port_local, 100);
+        e = cudaLaunchCooperativeKernel(kernel_of(port_local), dim3(grid), dim3(WARPS_PER_BLOCK * 32), args, bytes, stream);
     }
     return e == cudaSuccess ? 0 : (int)e;
 }

@@ -10,7 +10,8 @@ namespace tb
 {
 struct Sim;
 // blocks of the slot kernel that fit on one SM at once (0 on error)
-int slot_kernel_blocks_per_sm(int stage_cap);
+int slot_kernel_blocks_per_sm(int stage_cap, bool port_local = false);
 // one cooperative launch of up to max_slots_per_launch slots; 0 or a cudaError_t
-int launch_slots(const Sim &s, int grid, int max_slots_per_launch, int host_lanes, int stage_cap, cudaStream_t stream);
+// port_local: switch ports keep the slot's transmission chain and last enqueued frame in shared memory
+int launch_slots(const Sim &s, int grid, int max_slots_per_launch, int host_lanes, int stage_cap, bool port_local, cudaStream_t stream);
 } // namespace tb

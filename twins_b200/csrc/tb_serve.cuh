@@ -431,14 +431,14 @@ int serve_round(tb_server *v, int *running)
             }
             v->lanes = sh.lanes;
             v->stage = sh.stage;
-            v->grid = grid_for(&v->dev, sh.lanes, sh.stage, s.n_list);
+            v->grid = grid_for(&v->dev, sh.lanes, sh.stage, s.n_list, sh.port_local);
             // the kernel stops early when every world in the batch is done
             ctl.finished = 0;
             if (cudaMemcpyAsync(&s.ctl->finished, &ctl.finished, sizeof(int), cudaMemcpyHostToDevice, v->dev.stream) != cudaSuccess)
                 return fail(TB_ERR_CUDA, "cudaMemcpyAsync failed");
             const long long before = ctl.slots_run;
             cudaEventRecord(v->dev.la, v->dev.stream);
-            int e = tb::launch_slots(s, v->grid, slots, sh.lanes, sh.stage, v->dev.stream);
+            int e = tb::launch_slots(s, v->grid, slots, sh.lanes, sh.stage, sh.port_local, v->dev.stream);
             if (e)
                 return fail(TB_ERR_CUDA, std::string("slot kernel launch: ") + cudaGetErrorString((cudaError_t)e));
             cudaEventRecord(v->dev.lb, v->dev.stream);

@@ -20,6 +20,7 @@ namespace tb
 constexpr int SW_STAGE = 192;
 constexpr int SW_STAGE_MAX = RUNS > 9 ? 256 : 384; // (what four warps' scratch fits in 227 KB)
 constexpr int SW_STAGE_SMALL = 96;
+constexpr int SW_STAGE_TWO = 288; // the most with which two blocks of four warps fit on an SM
 
 // a world's topology and parameters (read-only on the device)
 struct WorldDesc

@@ -9,6 +9,8 @@
 #pragma once
 #include "tb_slot.cuh"
 
+#include <type_traits>
+
 namespace tb
 {
 
@@ -33,12 +35,21 @@ struct SwShared
     TB_D const Frame *fr() const { return reinterpret_cast<const Frame *>(bytes() + header()); }
     TB_D int64_t *ets() { return reinterpret_cast<int64_t *>(bytes() + header() + (size_t)cap * sizeof(Frame)); }
     TB_D uint32_t *eref() { return reinterpret_cast<uint32_t *>(bytes() + header() + (size_t)cap * (sizeof(Frame) + 8)); }
+    // (port-local egress) each port's frame last enqueued [32] and transmission chain [32]
+    TB_D Frame *eg_tail() { return reinterpret_cast<Frame *>(bytes() + ports_at(cap)); }
+    TB_D Chain *eg_last() { return reinterpret_cast<Chain *>(bytes() + ports_at(cap) + 32 * sizeof(Frame)); }
     static TB_HDI size_t header();
+    static TB_HDI size_t ports_at(int cap);
 };
 
 TB_HDI size_t SwShared::header() { return (sizeof(SwShared) + 15) & ~(size_t)15; }
-// bytes of one warp's scratch with `cap` staged frames (16-byte multiple)
-TB_HDI size_t sw_shared_bytes(int cap) { return (SwShared::header() + (size_t)cap * (sizeof(Frame) + 8 + 4) + 15) & ~(size_t)15; }
+TB_HDI size_t SwShared::ports_at(int cap) { return (header() + (size_t)cap * (sizeof(Frame) + 8 + 4) + 15) & ~(size_t)15; }
+// bytes of one warp's scratch with `cap` staged frames (16-byte multiple), and the ports' slot
+// copies of the port-local egress
+TB_HDI size_t sw_shared_bytes(int cap, bool port_local = false)
+{
+    return SwShared::ports_at(cap) + (port_local ? (32 * (sizeof(Frame) + sizeof(Chain)) + 15) & ~(size_t)15 : 0);
+}
 // a warp's scratch at `p` (every lane may call it: the same value is written)
 TB_D SwShared *sw_shared_at(unsigned char *p, int cap)
 {
@@ -293,6 +304,7 @@ TB_D void sw_phase_scatter(const SwCtx &x, SwShared &sh, int q)
 // phase 7 (lane e): egress e's arrivals in time order (ties: ns-3's order, insertion sort in
 // ingress order), each enqueued (RED) with its arrival event's chain; then the starts of the
 // slot. Returns true if the port sent or holds frames.
+template <bool PORT_LOCAL>
 TB_D bool sw_phase_egress(const SwCtx &x, SwShared &sh, int e, unsigned &ties, unsigned &drops, unsigned &marks,
                           unsigned &ovf)
 {
@@ -335,14 +347,22 @@ TB_D bool sw_phase_egress(const SwCtx &x, SwShared &sh, int e, unsigned &ties, u
     }
     PortRec &pr = x.ports[e];
     const int port = x.sr->port0 + e;
-    Egress eg;
+    typename std::conditional<PORT_LOCAL, PortEgress, Egress>::type eg;
     eg.ring = s.port_ring + (size_t)port * s.ring;
     eg.cap = s.ring;
     eg.head = pr.q_head;
     eg.size = pr.q_size;
     eg.link_free = pr.link_free;
     eg.last_start = pr.last_start;
-    eg.last = &pr.last;
+    if constexpr (PORT_LOCAL)
+    {
+        sh.eg_last()[e] = pr.last;
+        eg.last = &sh.eg_last()[e];
+        eg.tailp = &sh.eg_tail()[e];
+        eg.tail_at = -1;
+    }
+    else
+        eg.last = &pr.last;
     eg.red_k = pr.red_k;
     eg.qcap = pr.qcap;
     eg.woke = -1;
@@ -370,6 +390,8 @@ TB_D bool sw_phase_egress(const SwCtx &x, SwShared &sh, int e, unsigned &ties, u
     pr.q_size = eg.size;
     pr.link_free = eg.link_free;
     pr.last_start = eg.last_start;
+    if constexpr (PORT_LOCAL)
+        pr.last = *eg.last;
     drops += eg.drops;
     marks += eg.marks;
     ovf += eg.ovf;
