@@ -115,6 +115,8 @@ class Clocks:
 
 def load_worlds(name: str, rank: int):
     from twins_b200 import workloads
+    if name == "c5":  # (the served stream's requests as worlds: the reference arm's sample)
+        return [workloads.World(r.name, r.topo, r.flows, r.params) for r in workloads.served_stream(1 + rank, n=200)]
     return workloads.WORKLOADS[name](1 + rank)
 
 
@@ -122,7 +124,18 @@ def topo_flags(topo):
     from twins_b200 import api
     if topo.kind == api.TOPO_FATTREE:
         return [f"--k={topo.k}"]
-    return ["--topo=leafspine", f"--leaves={topo.leaves}", f"--spines={topo.spines}", f"--hpl={topo.hpl}"]
+    if topo.kind == api.TOPO_LEAFSPINE:
+        return ["--topo=leafspine", f"--leaves={topo.leaves}", f"--spines={topo.spines}", f"--hpl={topo.hpl}"]
+    # a topology file (hosts / switches / link lines) in the temp directory, and its failures
+    name = lambda x: f"h{x}" if x >= 0 else f"s{-1 - x}"
+    text = f"hosts {topo.n_hosts}\nswitches {topo.n_switches}\n" + "".join(f"link {name(a)} {name(b)}\n" for a, b in topo.links)
+    path = Path(tempfile.gettempdir()) / f"twins_topo_{abs(hash(text)) % 10 ** 12}.txt"
+    if not path.exists():
+        path.write_text(text)
+    flags = ["--topo=graph", f"--topofile={path}"]
+    if topo.fails:
+        flags.append("--fail=" + ",".join(f"{t}:s{a}:s{b}" + (":up" if up else "") for t, a, b, up in topo.fails))
+    return flags
 
 
 def world_flags(w):
@@ -306,16 +319,19 @@ def main():
         args.warmup_slots = 400 if args.workload == "c4" else 0
     args.warmup = max(args.warmup, 3)
 
-    if args.workload == "c5":
-        return serve_bench(args)
     rank = int(os.environ.get("RANK", 0))
+    if args.workload == "c5" and args.impl == "ours":
+        if rank == 0:  # (one server on one GPU; other ranks have nothing to add)
+            serve_bench(args)
+        return
     world_size = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     worlds = load_worlds(args.workload, rank)
     config = {"workload": {"c1": "FatTree k=4, 240 flows, DCTCP (C1)",
                            "c2": "FatTree k=8, 10,000 flows x {NewReno, DCTCP, Cubic}, FIN, spraying (C2)",
                            "c2s": "FatTree k=8, 1,500 flows x {NewReno, DCTCP, Cubic}, FIN, spraying (C2 shape, small)",
-                           "c4": "256 leaf-spine worlds, 1k-20k flows each (C4)"}[args.workload],
+                           "c4": "256 leaf-spine worlds, 1k-20k flows each (C4)",
+                           "c5": "200 served-stream requests (C5 shape, TCP) as worlds"}[args.workload],
               "worlds": len(worlds), "flows_per_step": int(sum(len(w.flows) for w in worlds)),
               "l2": "flushed between steps (256 MiB write); state restored device-to-device before each step",
               "seed": 1}
