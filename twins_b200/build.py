@@ -57,6 +57,8 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     deps = list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + \
         [ROOT / "include" / "twinsb200.h", Path(__file__)]
     nvcc = _nvcc()
+    # every stale library's objects compile at once (each is one nvcc process), then link
+    jobs, links = [], []
     for so, cli, extra in VARIANTS:
         if force or _stale(so, deps):
             objs = []
@@ -65,12 +67,17 @@ def build(force: bool = False, verbose: bool = False) -> Path:
                 cmd = [nvcc, *NVFLAGS, *extra, "-c", str(CSRC / src), "-o", str(obj)]
                 if verbose:
                     print(" ".join(cmd))
-                subprocess.run(cmd, check=True)
+                jobs.append(subprocess.Popen(cmd))
                 objs.append(str(obj))
-            cmd = [nvcc, *ARCH, "-shared", "-o", str(so), *objs, "-lcudart"]
-            subprocess.run(cmd, check=True)
-            for o in objs:
-                Path(o).unlink(missing_ok=True)
+            links.append((so, objs))
+    failed = [j.args for j in jobs if j.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, failed[0])
+    for so, objs in links:
+        subprocess.run([nvcc, *ARCH, "-shared", "-o", str(so), *objs, "-lcudart"], check=True)
+        for o in objs:
+            Path(o).unlink(missing_ok=True)
+    for so, cli, extra in VARIANTS:
         if force or _stale(cli, deps + [so]):
             cmd = ["g++", "-std=c++17", "-O2", "-o", str(cli), str(CSRC / "twins_cli.cpp"),
                    f"-L{LIB}", f"-l{so.stem[3:]}", f"-Wl,-rpath,$ORIGIN"]

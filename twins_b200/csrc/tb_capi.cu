@@ -882,7 +882,7 @@ void running_units(const std::vector<WorldCtl> &wc, const std::vector<std::array
 // the grid of a launch shape: a warp per unit, at most what is co-resident (0: does not fit)
 int grid_for(const tb_ctx *c, int host_lanes, int stage, int units = -1, bool port_local = false)
 {
-    int per_sm = tb::slot_kernel_blocks_per_sm(stage, port_local);
+    int per_sm = tb::slot_kernel_blocks_per_sm(stage, port_local, host_lanes);
     if (per_sm <= 0 || c->dev_sms <= 0)
         return 0;
     if (units < 0)
@@ -928,7 +928,7 @@ struct ShapeTuner
             for (auto &x : cand)
                 if (grid_for(c, x[0], x[1], -1, x[2] != 0) > 0)
                     shapes.push_back({x[0], x[1], 0, 0, x[2] != 0});
-            const long long resident = (long long)c->dev_sms * std::max(1, tb::slot_kernel_blocks_per_sm(SW_STAGE)) * TB_WARPS_PER_BLOCK;
+            const long long resident = (long long)c->dev_sms * std::max(1, tb::slot_kernel_blocks_per_sm(SW_STAGE, false, 1)) * TB_WARPS_PER_BLOCK;
             // (one host per warp: with big switches (16 ports or more), whose ports' serial
             // enqueues are the critical path, the port-local egress and the largest staging; else
             // the largest staging that keeps two blocks per SM. 32 hosts per warp: the smallest

@@ -20,9 +20,10 @@ namespace tb
 {
 
 constexpr int WARPS_PER_BLOCK = TB_WARPS_PER_BLOCK;
-#ifndef TB_MIN_BLOCKS
-#define TB_MIN_BLOCKS 4 // resident blocks per SM the register budget allows (with the smaller staging areas)
-#endif
+// resident blocks per SM that each instantiation's register budget allows: 4 for several hosts
+// per warp (with the smaller staging areas, four blocks fit an SM), 2 for one host per warp (two
+// blocks at most fit with its staging areas; more registers spare the host's event loop spills)
+constexpr int MIN_BLOCKS_MANY = 4, MIN_BLOCKS_ONE = 2;
 constexpr long long BARRIER_SPIN_LIMIT = 1ll << 22; // polls of >= 64 ns: several seconds
 
 __device__ __forceinline__ unsigned long long globaltimer()
@@ -337,9 +338,9 @@ __device__ bool switch_step(const Sim &s, int sw, int64_t gt, int lane, SwShared
 }
 
 // PORT_LOCAL: switch ports keep the slot's transmission chain and last enqueued frame in shared
-// memory (PortEgress); a separate instantiation, chosen per launch
-template <bool PORT_LOCAL>
-__global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, TB_MIN_BLOCKS) slot_kernel(Sim s, int max_slots_per_launch, int host_lanes, int stage_cap)
+// memory (PortEgress); MIN_BLOCKS: the register budget. Separate instantiations, chosen per launch.
+template <bool PORT_LOCAL, int MIN_BLOCKS>
+__global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, MIN_BLOCKS) slot_kernel(Sim s, int max_slots_per_launch, int host_lanes, int stage_cap)
 {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     __shared__ unsigned blk_done;
@@ -478,42 +479,57 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, TB_MIN_BLOCKS) slot_kern
 // dynamic shared memory of a block: one switch scratch (with its staging area) per warp
 static size_t smem_bytes(int stage_cap, bool port_local) { return sw_shared_bytes(stage_cap, port_local) * WARPS_PER_BLOCK; }
 
-static const void *kernel_of(bool port_local) { return port_local ? (const void *)slot_kernel<true> : (const void *)slot_kernel<false>; }
-
-static bool smem_attr(bool port_local)
+// the instantiation of a launch shape: several hosts per warp, one host per warp, one host per
+// warp with port-local switch egress
+enum
 {
-    static const bool ok[2] = {
-        cudaFuncSetAttribute(slot_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes(SW_STAGE_MAX, false)) == cudaSuccess,
-        cudaFuncSetAttribute(slot_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes(SW_STAGE_MAX, true)) == cudaSuccess};
-    return ok[port_local];
+    K_MANY,
+    K_ONE,
+    K_ONE_PL,
+    K_N
+};
+static int kind_of(int host_lanes, bool port_local) { return host_lanes > 1 ? K_MANY : port_local ? K_ONE_PL : K_ONE; }
+static const void *kernel_of(int k)
+{
+    return k == K_MANY ? (const void *)slot_kernel<false, MIN_BLOCKS_MANY>
+                       : k == K_ONE ? (const void *)slot_kernel<false, MIN_BLOCKS_ONE> : (const void *)slot_kernel<true, MIN_BLOCKS_ONE>;
+}
+
+static bool smem_attr(int k)
+{
+    static const bool ok[K_N] = {
+        cudaFuncSetAttribute(kernel_of(K_MANY), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes(SW_STAGE_MAX, false)) == cudaSuccess,
+        cudaFuncSetAttribute(kernel_of(K_ONE), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes(SW_STAGE_MAX, false)) == cudaSuccess,
+        cudaFuncSetAttribute(kernel_of(K_ONE_PL), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes(SW_STAGE_MAX, true)) == cudaSuccess};
+    return ok[k];
 }
 
 // The preferred shared-memory carveout, in percent of the SM's maximum: the shared memory of the
 // blocks a launch puts on one SM and no more, so that the rest of the SM's unified L1 / shared
 // memory is L1, where the units' records, ring heads and prefetched lines stay between slots.
-static int carveout[2] = {-1, -1}; // the last ones set (-1: none)
-static void set_carveout(bool port_local, int pct)
+static int carveout[K_N] = {-1, -1, -1}; // the last ones set (-1: none)
+static void set_carveout(int k, int pct)
 {
-    if (pct != carveout[port_local] &&
-        cudaFuncSetAttribute(kernel_of(port_local), cudaFuncAttributePreferredSharedMemoryCarveout, pct) == cudaSuccess)
-        carveout[port_local] = pct;
+    if (pct != carveout[k] && cudaFuncSetAttribute(kernel_of(k), cudaFuncAttributePreferredSharedMemoryCarveout, pct) == cudaSuccess)
+        carveout[k] = pct;
 }
 
-int slot_kernel_blocks_per_sm(int stage_cap, bool port_local)
+int slot_kernel_blocks_per_sm(int stage_cap, bool port_local, int host_lanes)
 {
     int n = 0;
-    if (stage_cap < 1 || stage_cap > SW_STAGE_MAX || !smem_attr(port_local))
+    const int k = kind_of(host_lanes, port_local);
+    if (stage_cap < 1 || stage_cap > SW_STAGE_MAX || !smem_attr(k))
         return 0;
-    set_carveout(port_local, 100); // (occupancy with all of the shared memory)
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel_of(port_local), WARPS_PER_BLOCK * 32, smem_bytes(stage_cap, port_local)) !=
-        cudaSuccess)
+    set_carveout(k, 100); // (occupancy with all of the shared memory)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel_of(k), WARPS_PER_BLOCK * 32, smem_bytes(stage_cap, port_local)) != cudaSuccess)
         return 0;
     return n;
 }
 
 int launch_slots(const Sim &s, int grid, int max_slots_per_launch, int host_lanes, int stage_cap, bool port_local, cudaStream_t stream)
 {
-    if (!smem_attr(port_local) || stage_cap < 1 || stage_cap > SW_STAGE_MAX)
+    const int k = kind_of(host_lanes, port_local);
+    if (!smem_attr(k) || stage_cap < 1 || stage_cap > SW_STAGE_MAX)
         return (int)cudaErrorInvalidValue;
     int dev = 0, sms = 1, max_smem = 1;
     cudaGetDevice(&dev);
@@ -522,15 +538,15 @@ int launch_slots(const Sim &s, int grid, int max_slots_per_launch, int host_lane
     const long long per_sm = (grid + sms - 1) / sms;
     const size_t bytes = smem_bytes(stage_cap, port_local);
     const long long need = per_sm * (long long)(bytes + 2048); // (+ the block's reserved and static shared memory)
-    set_carveout(port_local, (int)std::min<long long>(100, (need * 100 + max_smem - 1) / max_smem));
+    set_carveout(k, (int)std::min<long long>(100, (need * 100 + max_smem - 1) / max_smem));
     void *args[] = {(void *)&s, (void *)&max_slots_per_launch, (void *)&host_lanes, (void *)&stage_cap};
-    cudaError_t e = cudaLaunchCooperativeKernel(kernel_of(port_local), dim3(grid), dim3(WARPS_PER_BLOCK * 32), args, bytes, stream);
+    cudaError_t e = cudaLaunchCooperativeKernel(kernel_of(k), dim3(grid), dim3(WARPS_PER_BLOCK * 32), args, bytes, stream);
     if (e == cudaErrorCooperativeLaunchTooLarge)
     {
         // (the carveout left too little shared memory for the blocks to be resident at once)
         cudaGetLastError();
-        set_carveout(port_local, 100);
-        e = cudaLaunchCooperativeKernel(kernel_of(port_local), dim3(grid), dim3(WARPS_PER_BLOCK * 32), args, bytes, stream);
+        set_carveout(k, 100);
+        e = cudaLaunchCooperativeKernel(kernel_of(k), dim3(grid), dim3(WARPS_PER_BLOCK * 32), args, bytes, stream);
     }
     return e == cudaSuccess ? 0 : (int)e;
 }

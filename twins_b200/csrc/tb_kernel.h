@@ -10,7 +10,7 @@ namespace tb
 {
 struct Sim;
 // blocks of the slot kernel that fit on one SM at once (0 on error)
-int slot_kernel_blocks_per_sm(int stage_cap, bool port_local = false);
+int slot_kernel_blocks_per_sm(int stage_cap, bool port_local = false, int host_lanes = 1);
 // one cooperative launch of up to max_slots_per_launch slots; 0 or a cudaError_t
 // port_local: switch ports keep the slot's transmission chain and last enqueued frame in shared memory
 int launch_slots(const Sim &s, int grid, int max_slots_per_launch, int host_lanes, int stage_cap, bool port_local, cudaStream_t stream);
