@@ -171,3 +171,29 @@ def test_chain_runs_25(native_lib, name):
     want_est, want_done = ns3(case)
     assert (est == want_est).all() and (done == want_done).all()
     assert ctr["undecided_ties"] == 0
+
+
+def test_edge_worlds(native_lib, oracle_bin, tmp_path):
+    """Edge cases in one batch and alone: a world without flows, a single flow that starts 5 ms
+    in (the idle skip jumps there), a one-byte flow, and a normal small world. Each equals its
+    standalone run; the single flows equal the oracle."""
+    empty = api.Flows.from_arrays([], [], [], [])
+    late = api.Flows.from_arrays([3], [12], [150_000], [5_000_000])
+    tiny = api.Flows.from_arrays([0, 5], [9, 0], [1, 2], [1_000, 1_000])
+    small = workloads.c1()[0].flows
+    topo = api.Topology.fattree(4)
+    p = api.TcpParams("dctcp", 30, 200)
+    worlds = [(topo, empty, p), (topo, late, p), (topo, tiny, api.TcpParams("cubic", 30, 200, fin=True)), (topo, small, p)]
+    alone = [api.run_world(*w) for w in worlds]
+    assert len(alone[0][0]) == 0
+    for i in (1, 2):
+        w = workloads.World(f"edge{i}", topo, worlds[i][1], worlds[i][2])
+        want_est, want_done, _ = oracle_run(oracle_bin, tmp_path, w)
+        assert (alone[i][0] == want_est).all() and (alone[i][1] == want_done).all()
+        assert (alone[i][1] >= 0).all()
+    with api.Simulator() as sim:
+        ids = [sim.add_world(*w) for w in worlds]
+        sim.run()
+        for (est, done, ctr, _), i in zip(alone, ids):
+            e2, d2 = sim.results(i)
+            assert (est == e2).all() and (done == d2).all()
