@@ -477,6 +477,7 @@ def main():
                          "sample": f"oracle on the first {args.cpu_slots} slots of {sample_world.name}"},
         "clocks": clocks.summary(),
         "gpu_launches": launches,
+        "graph_launches": stats["graph_launches"],
         "launch": {"grid": stats["grid"], "host_lanes": stats["host_lanes"], "warps_per_block": stats["warps_per_block"],
                    "stage_frames": stats["stage_frames"], "autotuned": bool(stats["autotuned"])},
     }

@@ -86,6 +86,7 @@ typedef struct tb_stats
     int stage_frames;        /* frames a warp stages in shared memory in that shape */
     int autotuned;           /* 1: the shape was picked per launch by measured throughput */
     int port_local;          /* 1: that shape keeps switch ports' slot state in shared memory */
+    long long graph_launches; /* launches replayed from a captured CUDA graph */
 } tb_stats;
 
 /* A context on CUDA device `device`, admitting batches up to hbm_budget_bytes of device memory

@@ -81,6 +81,7 @@ def test_c1_equals_oracle(native_lib, oracle_bin, tmp_path):
     assert (est == want_est).all() and (done == want_done).all()
     assert (done >= 0).all()
     assert stats["packet_events"] == events
+    assert stats["graph_launches"] >= 1  # (the steady launches replay a captured CUDA graph)
 
 
 @pytest.mark.parametrize("tcp", ["newreno", "dctcp", "cubic"])

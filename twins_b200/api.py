@@ -60,7 +60,8 @@ class _Stats(ctypes.Structure):
                 ("host_sender_events", ctypes.c_ulonglong), ("host_frames", ctypes.c_ulonglong),
                 ("bytes_h2d", ctypes.c_ulonglong), ("bytes_d2h", ctypes.c_ulonglong),
                 ("grid", ctypes.c_int), ("host_lanes", ctypes.c_int), ("warps_per_block", ctypes.c_int),
-                ("stage_frames", ctypes.c_int), ("autotuned", ctypes.c_int), ("port_local", ctypes.c_int)]
+                ("stage_frames", ctypes.c_int), ("autotuned", ctypes.c_int), ("port_local", ctypes.c_int),
+                ("graph_launches", ctypes.c_longlong)]
 
 
 class _QRec(ctypes.Structure):

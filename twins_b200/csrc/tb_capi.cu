@@ -1302,6 +1302,12 @@ int tb_run(tb_ctx *ctx, long long max_slots)
     int alive = s.W, list_alive = s.W, list_lanes = 0;
     s.unit_list = nullptr;
     s.n_list = 0;
+    tb::SlotGraph graph;
+    struct GraphRelease
+    {
+        tb::SlotGraph &g;
+        ~GraphRelease() { tb::release_graph(g); }
+    } graph_release{graph};
     cudaEventRecord(ctx->ev0, ctx->stream);
     for (;;)
     {
@@ -1330,7 +1336,9 @@ int tb_run(tb_ctx *ctx, long long max_slots)
             }
             const long long slots_before = ctl.slots_run;
             cudaEventRecord(ctx->la, ctx->stream);
-            int e = tb::launch_slots(s, grid, explore ? tu.probe : run_slots, sh.lanes, sh.stage, sh.port_local, ctx->stream);
+            // (the steady launches replay a captured graph; the short probes launch directly)
+            int e = explore ? tb::launch_slots(s, grid, tu.probe, sh.lanes, sh.stage, sh.port_local, ctx->stream)
+                            : tb::launch_slots_graph(graph, s, grid, run_slots, sh.lanes, sh.stage, sh.port_local, ctx->stream);
             if (e)
                 return fail(TB_ERR_CUDA, std::string("slot kernel launch: ") + cudaGetErrorString((cudaError_t)e));
             cudaEventRecord(ctx->lb, ctx->stream);
@@ -1402,6 +1410,7 @@ int tb_run(tb_ctx *ctx, long long max_slots)
     st.stage_frames = most.stage;
     st.autotuned = tu.shapes.size() > 1;
     st.port_local = most.port_local;
+    st.graph_launches = graph.replays;
     st.bytes_d2h = 0;
     if (ctl.error)
         return fail(TB_ERR_TIMEOUT, "a device-side barrier wait ran out; the run was abandoned");

@@ -14,6 +14,8 @@
 
 #include <algorithm>
 #include <climits>
+#include <cstdint>
+#include <cstring>
 #include <cuda_runtime.h>
 
 namespace tb
@@ -549,6 +551,55 @@ int launch_slots(const Sim &s, int grid, int max_slots_per_launch, int host_lane
         e = cudaLaunchCooperativeKernel(kernel_of(k), dim3(grid), dim3(WARPS_PER_BLOCK * 32), args, bytes, stream);
     }
     return e == cudaSuccess ? 0 : (int)e;
+}
+
+// A launch as a CUDA graph: the launch is captured once per shape, slot count and unit list and
+// replayed as a graph; where capturing or instantiating fails, plain launches follow for good.
+int launch_slots_graph(SlotGraph &g, const Sim &s, int grid, int max_slots_per_launch, int host_lanes, int stage_cap, bool port_local,
+                       cudaStream_t stream)
+{
+    const unsigned long long key[8] = {(unsigned long long)grid, (unsigned long long)max_slots_per_launch, (unsigned long long)host_lanes,
+                                       (unsigned long long)stage_cap, (unsigned long long)port_local, (unsigned long long)(uintptr_t)s.unit_list,
+                                       (unsigned long long)s.n_list, (unsigned long long)s.max_slots};
+    if (g.broken)
+        return launch_slots(s, grid, max_slots_per_launch, host_lanes, stage_cap, port_local, stream);
+    if (!g.exec || memcmp(key, g.key, sizeof key) != 0)
+    {
+        if (g.exec)
+            cudaGraphExecDestroy((cudaGraphExec_t)g.exec);
+        g.exec = nullptr;
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        int e = 1;
+        if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess)
+        {
+            e = launch_slots(s, grid, max_slots_per_launch, host_lanes, stage_cap, port_local, stream);
+            if (cudaStreamEndCapture(stream, &graph) != cudaSuccess)
+                e = 1;
+        }
+        if (e == 0 && graph && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess)
+        {
+            g.exec = exec;
+            memcpy(g.key, key, sizeof key);
+        }
+        if (graph)
+            cudaGraphDestroy(graph);
+        if (!g.exec)
+        {
+            cudaGetLastError(); // (the failed capture's error)
+            g.broken = true;
+            return launch_slots(s, grid, max_slots_per_launch, host_lanes, stage_cap, port_local, stream);
+        }
+    }
+    g.replays++;
+    return cudaGraphLaunch((cudaGraphExec_t)g.exec, stream) == cudaSuccess ? 0 : (int)cudaGetLastError();
+}
+
+void release_graph(SlotGraph &g)
+{
+    if (g.exec)
+        cudaGraphExecDestroy((cudaGraphExec_t)g.exec);
+    g.exec = nullptr;
 }
 
 } // namespace tb
