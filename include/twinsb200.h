@@ -145,9 +145,9 @@ int tb_set_launch(tb_ctx *ctx, int host_lanes, int grid);
  * build; default 192; fewer leave room for more resident blocks per SM, more stage the slots of
  * big switches). */
 int tb_set_launch_shape(tb_ctx *ctx, int host_lanes, int stage_frames, int grid);
-/* A fixed shape's switch egress: 1 keeps each port's transmission chain and last enqueued frame in
- * shared memory for the slot (faster where big switches are the critical path), 0 (default) reads
- * them from the port's record. Autotuning picks it per launch. */
+/* A fixed shape's switch egress (one host per warp only): 1 keeps each port's transmission chain
+ * and last enqueued frame in shared memory for the slot (faster where big switches are the
+ * critical path), 0 (default) reads them from the port's record. Autotuning picks it per launch. */
 int tb_set_port_local(tb_ctx *ctx, int on);
 /* Autotuning (on by default): tb_run picks each launch's shape (hosts per warp, staging size)
  * among a fixed set by the packet-events per ms that short probe launches of each achieve. The

@@ -1409,7 +1409,7 @@ int tb_run(tb_ctx *ctx, long long max_slots)
     st.warps_per_block = TB_WARPS_PER_BLOCK;
     st.stage_frames = most.stage;
     st.autotuned = tu.shapes.size() > 1;
-    st.port_local = most.port_local;
+    st.port_local = most.port_local && most.lanes == 1;
     st.graph_launches = graph.replays;
     st.bytes_d2h = 0;
     if (ctl.error)

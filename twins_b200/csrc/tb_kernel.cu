@@ -152,6 +152,7 @@ __device__ __forceinline__ void host_report(const Sim &s, int w, int64_t t0, boo
 // histories, the head frames of the host's egress queue, and the timers of its active
 // connections; then lane 0 runs the host's slot (host_step) on the staged frames, or in place
 // when they do not fit. With several hosts per warp each lane runs its own host in place.
+template <bool MANY>
 __device__ __forceinline__ void host_unit(const Sim &s, int u, int host_lanes, int64_t t, int lane, SwShared &sh, unsigned &ties,
                                           unsigned &blk_done)
 {
@@ -159,7 +160,7 @@ __device__ __forceinline__ void host_unit(const Sim &s, int u, int host_lanes, i
     int64_t t0 = 0;
     bool run = false;
     const Frame *stage = nullptr;
-    if (host_lanes == 1)
+    if constexpr (!MANY)
     {
         h = u;
         const HostRec &hr = s.hosts[h];
@@ -228,9 +229,29 @@ __device__ __forceinline__ void host_unit(const Sim &s, int u, int host_lanes, i
         h = u * host_lanes + lane;
         if (lane < host_lanes && h < s.H)
         {
-            w = s.hosts[h].world;
+            const HostRec &hr = s.hosts[h];
+            w = hr.world;
             t0 = world_t0(s, w);
             run = t >= world_next(s, w);
+            if (run)
+            {
+                // all lanes at once: the tags of the host's link messages, then the records of
+                // the connections of its first arrivals into L1 (the lanes' event loops diverge
+                // next, and would each wait for these one after the other)
+                const int link = hr.in_link;
+                n2 = t >= 2 ? msg_count(s, t - 2, link) : 0;
+                n1 = t >= 1 ? msg_count(s, t - 1, link) : 0;
+                const Frame *m2 = msg_frames(s, t - 2, link), *m1 = msg_frames(s, t - 1, link);
+                for (int j = 0; j < 4 && j < n2 + n1; j++)
+                {
+                    const Frame *f = j < n2 ? &m2[j] : &m1[j - n2];
+                    const uint32_t flow = __ldcg(&f->flow);
+                    const uint8_t to_snd = __ldcg(&f->to_sender);
+                    prefetch_l1(to_snd ? (const void *)&s.snd[flow] : (const void *)&s.rcv[flow]);
+                }
+                if (hr.q_size > 0)
+                    prefetch_l1(&s.host_ring[(size_t)h * s.ring + hr.q_head]);
+            }
         }
     }
     if (run)
@@ -375,7 +396,7 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, MIN_BLOCKS) slot_kernel(
             unsigned long long p0 = globaltimer();
 #endif
             if (u < host_units)
-                host_unit(s, u, host_lanes, t, lane, sh, ties, blk_done);
+                host_unit<MIN_BLOCKS == MIN_BLOCKS_MANY>(s, u, host_lanes, t, lane, sh, ties, blk_done);
             else
             {
                 const int sw = u - host_units;
@@ -519,6 +540,7 @@ static void set_carveout(int k, int pct)
 int slot_kernel_blocks_per_sm(int stage_cap, bool port_local, int host_lanes)
 {
     int n = 0;
+    port_local = port_local && host_lanes == 1;
     const int k = kind_of(host_lanes, port_local);
     if (stage_cap < 1 || stage_cap > SW_STAGE_MAX || !smem_attr(k))
         return 0;
@@ -530,6 +552,7 @@ int slot_kernel_blocks_per_sm(int stage_cap, bool port_local, int host_lanes)
 
 int launch_slots(const Sim &s, int grid, int max_slots_per_launch, int host_lanes, int stage_cap, bool port_local, cudaStream_t stream)
 {
+    port_local = port_local && host_lanes == 1; // (several hosts per warp: the plain egress)
     const int k = kind_of(host_lanes, port_local);
     if (!smem_attr(k) || stage_cap < 1 || stage_cap > SW_STAGE_MAX)
         return (int)cudaErrorInvalidValue;
