@@ -857,121 +857,22 @@ int make_world(const tb_topology *topo, int n_flows, const int *src, const int *
     return TB_OK;
 }
 
-// The units of the worlds still running (WorldCtl::next != INT64_MAX), hosts grouped `lanes` to
-// a unit: host units in order, then host_units + switch. `worlds`: (host0, hosts, sw0, switches)
-// of each world slot.
-void running_units(const std::vector<WorldCtl> &wc, const std::vector<std::array<int, 4>> &worlds, int lanes, int H,
-                   std::vector<int> &out)
-{
-    out.clear();
-    const int host_units = (H + lanes - 1) / lanes;
-    for (size_t w = 0; w < worlds.size(); w++)
-    {
-        if (wc[w].next == INT64_MAX || worlds[w][1] == 0)
-            continue;
-        for (int u = worlds[w][0] / lanes; u <= (worlds[w][0] + worlds[w][1] - 1) / lanes; u++)
-            if (out.empty() || out.back() < u)
-                out.push_back(u);
-    }
-    for (size_t w = 0; w < worlds.size(); w++)
-        if (wc[w].next != INT64_MAX)
-            for (int x = 0; x < worlds[w][3]; x++)
-                out.push_back(host_units + worlds[w][2] + x);
-}
-
 // the grid of a launch shape: a warp per unit, at most what is co-resident (0: does not fit)
 int grid_for(const tb_ctx *c, int host_lanes, int stage, int units = -1, bool port_local = false)
 {
-    int per_sm = tb::slot_kernel_blocks_per_sm(stage, port_local, host_lanes);
-    if (per_sm <= 0 || c->dev_sms <= 0)
-        return 0;
     if (units < 0)
         units = (c->sim.H + host_lanes - 1) / host_lanes + c->sim.S;
-    int need = std::max(1, (units + TB_WARPS_PER_BLOCK - 1) / TB_WARPS_PER_BLOCK);
-    int most = c->dev_sms * per_sm;
-    return c->grid_req > 0 ? std::min(c->grid_req, most) : std::min(need, most);
+    return grid_of(units, TB_WARPS_PER_BLOCK, tb::slot_kernel_blocks_per_sm(stage, port_local, host_lanes), c->dev_sms, c->grid_req);
 }
 
-// Launch-shape autotuning, for tb_run and the server. A shape is the hosts per warp and the
-// frames a warp stages per slot; no shape changes a result. It starts from one host per warp
-// while the entities fit the resident warps about once (latency-bound: each host's serial events
-// are the slot's critical path), else 32 hosts per warp (throughput-bound: the lanes' memory
-// accesses overlap). Every `period` launches each shape still in the running runs a probe of
-// `probe` slots, and one whose device time per slot beats the current one's by more than 5%
-// takes over; a shape that loses a probe by more than 30% twice is not probed again.
-struct ShapeTuner
+// the launch-shape tuner's start, on this context's device: the candidates that fit, and the warps
+// co-resident at one host per warp and the default staging
+void tuner_init(ShapeTuner &tu, const tb_ctx *c, bool autotune, int lanes, int stage, long long entities, int kmax = 0)
 {
-    struct Shape
-    {
-        int lanes, stage;
-        long long slots;
-        int strikes;
-        bool port_local; // switch ports' slot copies in shared memory (PortEgress)
-    };
-    std::vector<Shape> shapes;
-    size_t best = 0;
-    long long since = 0, rounds = 0;
-    int period = 12, probe = 128;
-
-    // entities: hosts and switches to run; kmax: the most ports a switch has
-    void init(const tb_ctx *c, bool autotune, int lanes, int stage, long long entities, int kmax = 0)
-    {
-        shapes.clear();
-        best = 0;
-        since = 0;
-        rounds = 0;
-        if (autotune)
-        {
-            // (lanes, stage, port-local)
-            const int cand[][3] = {{1, SW_STAGE_TWO, 0}, {1, SW_STAGE, 0}, {4, SW_STAGE, 0}, {32, SW_STAGE, 0}, {1, SW_STAGE_SMALL, 0},
-                                   {32, SW_STAGE_SMALL, 0}, {1, SW_STAGE_MAX, 0}, {1, SW_STAGE_MAX, 1}, {1, SW_STAGE_TWO - 32, 1}};
-            for (auto &x : cand)
-                if (grid_for(c, x[0], x[1], -1, x[2] != 0) > 0)
-                    shapes.push_back({x[0], x[1], 0, 0, x[2] != 0});
-            const long long resident = (long long)c->dev_sms * std::max(1, tb::slot_kernel_blocks_per_sm(SW_STAGE, false, 1)) * TB_WARPS_PER_BLOCK;
-            // (one host per warp: with big switches (16 ports or more), whose ports' serial
-            // enqueues are the critical path, the port-local egress and the largest staging; else
-            // the largest staging that keeps two blocks per SM. 32 hosts per warp: the smallest
-            // staging, for four blocks per SM)
-            const int lanes0 = entities <= 2 * resident ? 1 : 32;
-            const bool pl0 = lanes0 == 1 && kmax >= 16;
-            const int stage0 = lanes0 == 1 ? (pl0 ? SW_STAGE_MAX : SW_STAGE_TWO) : SW_STAGE_SMALL;
-            for (size_t k = 0; k < shapes.size(); k++)
-                if (shapes[k].lanes == lanes0 && shapes[k].stage == stage0 && shapes[k].port_local == pl0)
-                    best = k;
-        }
-        if (shapes.empty())
-            shapes.push_back({lanes, stage, 0, 0, c->port_local});
-    }
-    bool explore() const { return shapes.size() > 1 && since >= period; }
-    bool probes(size_t k) const { return k == best || shapes[k].strikes < 2; }
-    // after a round of probes (per_slot[k]: ms per slot, <= 0 where no probe ran)
-    void decide(const std::vector<double> &per_slot)
-    {
-        size_t b = best;
-        for (size_t k = 0; k < shapes.size(); k++)
-            if (per_slot[k] > 0 && (per_slot[b] <= 0 || per_slot[k] < 0.95 * per_slot[b]))
-                b = k;
-        for (size_t k = 0; k < shapes.size(); k++)
-            if (per_slot[k] > 0 && per_slot[b] > 0 && per_slot[k] > 1.3 * per_slot[b])
-                shapes[k].strikes++;
-        best = b;
-        since = 0;
-        // (the load changes along a run: every fourth round probes every shape again)
-        if (++rounds % 4 == 0)
-            for (auto &x : shapes)
-                x.strikes = 0;
-    }
-    // the shape that ran the most slots
-    size_t most() const
-    {
-        size_t m = 0;
-        for (size_t k = 1; k < shapes.size(); k++)
-            if (shapes[k].slots > shapes[m].slots)
-                m = k;
-        return m;
-    }
-};
+    const long long resident = (long long)c->dev_sms * std::max(1, tb::slot_kernel_blocks_per_sm(SW_STAGE, false, 1)) * TB_WARPS_PER_BLOCK;
+    tu.init(autotune, lanes, stage, c->port_local, entities, kmax, resident,
+            [c](int l, int st, bool pl) { return grid_for(c, l, st, -1, pl) > 0; });
+}
 
 int prepare(tb_ctx *c)
 {
@@ -1289,7 +1190,7 @@ int tb_run(tb_ctx *ctx, long long max_slots)
     s.max_slots = max_slots > 0 ? max_slots : 2000000;
     SlotCtl ctl{};
     ShapeTuner tu;
-    tu.init(ctx, ctx->autotune, ctx->host_lanes, ctx->stage_cap, (long long)s.H + s.S, s.kmax);
+    tuner_init(tu, ctx, ctx->autotune, ctx->host_lanes, ctx->stage_cap, (long long)s.H + s.S, s.kmax);
     const int run_slots = tu.shapes.size() > 1 ? std::min(ctx->max_slots_per_launch, 1024) : ctx->max_slots_per_launch;
     long long launches = 0;
     // the running worlds' units: rebuilt when a world finishes (or the shape changes), so that a
@@ -1323,7 +1224,7 @@ int tb_run(tb_ctx *ctx, long long max_slots)
             {
                 if (alive != list_alive || sh.lanes != list_lanes)
                 {
-                    running_units(wc, wr, sh.lanes, s.H, ulist);
+                    running_units([&wc](size_t w) { return wc[w].next != INT64_MAX; }, wr, sh.lanes, s.H, ulist);
                     if (!ulist.empty() &&
                         cudaMemcpyAsync(ctx->d_units, ulist.data(), sizeof(int) * ulist.size(), cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
                         return fail(TB_ERR_CUDA, "cudaMemcpyAsync failed");

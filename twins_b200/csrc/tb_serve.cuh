@@ -24,62 +24,6 @@
 
 namespace
 {
-// first-fit ranges of [0, cap)
-struct RangeAlloc
-{
-    std::map<uint64_t, uint64_t> free_; // start -> length
-    uint64_t cap = 0, used = 0;
-    void init(uint64_t n)
-    {
-        cap = n;
-        used = 0;
-        free_.clear();
-        if (n)
-            free_[0] = n;
-    }
-    // the start of n free entries, or -1
-    long long take(uint64_t n)
-    {
-        if (n == 0)
-            return 0;
-        for (auto it = free_.begin(); it != free_.end(); ++it)
-            if (it->second >= n)
-            {
-                uint64_t at = it->first, len = it->second;
-                free_.erase(it);
-                if (len > n)
-                    free_[at + n] = len - n;
-                used += n;
-                return (long long)at;
-            }
-        return -1;
-    }
-    void give(uint64_t at, uint64_t n)
-    {
-        if (n == 0)
-            return;
-        used -= n;
-        auto next = free_.lower_bound(at);
-        if (next != free_.begin())
-        {
-            auto prev = std::prev(next);
-            if (prev->first + prev->second == at)
-            {
-                at = prev->first;
-                n += prev->second;
-                free_.erase(prev);
-            }
-        }
-        next = free_.lower_bound(at);
-        if (next != free_.end() && at + n == next->first)
-        {
-            n += next->second;
-            free_.erase(next);
-        }
-        free_[at] = n;
-    }
-};
-
 double now_s()
 {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
@@ -409,7 +353,7 @@ int serve_round(tb_server *v, int *running)
             }
             v->batch_entities = entities;
             std::vector<int> ulist;
-            running_units(live2, wr2, lanes, s.H, ulist);
+            running_units([&live2](size_t w) { return live2[w].next != INT64_MAX; }, wr2, lanes, s.H, ulist);
             if (!ulist.empty() &&
                 cudaMemcpyAsync(v->d_units, ulist.data(), sizeof(int) * ulist.size(), cudaMemcpyHostToDevice, v->dev.stream) != cudaSuccess)
                 return fail(TB_ERR_CUDA, "cudaMemcpyAsync failed");
@@ -575,7 +519,7 @@ int server_alloc(tb_server *v)
     cudaStreamSynchronize(c.stream);
     cudaDeviceGetAttribute(&c.dev_sms, cudaDevAttrMultiProcessorCount, v->device);
     c.sim = s;
-    v->tuner.init(&c, true, 1, SW_STAGE, (long long)s.H + s.S);
+    tuner_init(v->tuner, &c, true, 1, SW_STAGE, (long long)s.H + s.S);
     v->tuner.period = 8;
     v->tuner.probe = 32;
     v->lanes = v->tuner.shapes[v->tuner.best].lanes;

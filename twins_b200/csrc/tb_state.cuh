@@ -10,17 +10,10 @@
 //   messages    MsgRec[M]: the application's flows over connections
 #pragma once
 #include "tb_common.cuh"
+#include "tb_host.h" // (the staging sizes SW_STAGE*)
 
 namespace tb
 {
-
-// frames a warp stages in shared memory per switch (or host) and slot: the default staging area
-// and the largest; a launch may use a smaller one (more resident warps per SM, fewer slots
-// staged) or a larger one (big switches' slots staged, fewer resident warps)
-constexpr int SW_STAGE = 192;
-constexpr int SW_STAGE_MAX = RUNS > 9 ? 256 : 384; // (what four warps' scratch fits in 227 KB)
-constexpr int SW_STAGE_SMALL = 96;
-constexpr int SW_STAGE_TWO = 288; // the most with which two blocks of four warps fit on an SM
 
 // a world's topology and parameters (read-only on the device)
 struct WorldDesc
