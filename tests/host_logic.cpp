@@ -64,6 +64,8 @@ int hl_tuner_best(void *t) { return (int)((ShapeTuner *)t)->best; }
 int hl_tuner_explore(void *t) { return ((ShapeTuner *)t)->explore(); }
 int hl_tuner_probes(void *t, int k) { return ((ShapeTuner *)t)->probes(k); }
 int hl_tuner_period(void *t) { return ((ShapeTuner *)t)->period; }
+void hl_tuner_backoff(void *t, int most) { ((ShapeTuner *)t)->backoff(most); }
+void hl_tuner_load_changed(void *t) { ((ShapeTuner *)t)->load_changed(); }
 void hl_tuner_tick(void *t) { ((ShapeTuner *)t)->since++; }
 void hl_tuner_add_slots(void *t, int k, long long n) { ((ShapeTuner *)t)->shapes[k].slots += n; }
 int hl_tuner_most(void *t) { return (int)((ShapeTuner *)t)->most(); }

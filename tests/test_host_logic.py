@@ -37,6 +37,8 @@ def hl(tmp_path_factory):
         "hl_tuner_explore": (C.c_int, [vp]),
         "hl_tuner_probes": (C.c_int, [vp, C.c_int]),
         "hl_tuner_period": (C.c_int, [vp]),
+        "hl_tuner_backoff": (None, [vp, C.c_int]),
+        "hl_tuner_load_changed": (None, [vp]),
         "hl_tuner_tick": (None, [vp]),
         "hl_tuner_add_slots": (None, [vp, C.c_int, ll]),
         "hl_tuner_most": (C.c_int, [vp]),
@@ -155,6 +157,33 @@ def test_tuner_hysteresis_strikes_and_expiry(hl):
     assert all(not hl.hl_tuner_probes(t, k) for k in slow)
     decide(hl, t, skip)
     assert all(hl.hl_tuner_probes(t, k) for k in range(n))
+    hl.hl_tuner_free(t)
+
+
+def test_tuner_backoff(hl):
+    t, shapes = tuner(hl, 208)
+    n = len(shapes)
+    p0 = hl.hl_tuner_period(t)
+    # without backoff the period stays
+    decide(hl, t, [1.0] * n)
+    assert hl.hl_tuner_period(t) == p0
+    hl.hl_tuner_backoff(t, 4 * p0)
+    b0 = hl.hl_tuner_best(t)
+    keep = [1.0 if k == b0 else 1.2 for k in range(n)]
+    periods = []
+    for _ in range(4):
+        decide(hl, t, keep)
+        periods.append(hl.hl_tuner_period(t))
+    assert periods == [2 * p0, 4 * p0, 4 * p0, 4 * p0] and hl.hl_tuner_best(t) == b0
+    # a change of the load restores the first period; so does a new shape
+    hl.hl_tuner_load_changed(t)
+    assert hl.hl_tuner_period(t) == p0
+    decide(hl, t, keep)
+    assert hl.hl_tuner_period(t) == 2 * p0
+    new = list(keep)
+    new[(b0 + 1) % n] = 0.5
+    decide(hl, t, new)
+    assert hl.hl_tuner_best(t) == (b0 + 1) % n and hl.hl_tuner_period(t) == p0
     hl.hl_tuner_free(t)
 
 

@@ -1191,6 +1191,7 @@ int tb_run(tb_ctx *ctx, long long max_slots)
     SlotCtl ctl{};
     ShapeTuner tu;
     tuner_init(tu, ctx, ctx->autotune, ctx->host_lanes, ctx->stage_cap, (long long)s.H + s.S, s.kmax);
+    tu.backoff(96);
     const int run_slots = tu.shapes.size() > 1 ? std::min(ctx->max_slots_per_launch, 1024) : ctx->max_slots_per_launch;
     long long launches = 0;
     // the running worlds' units: rebuilt when a world finishes (or the shape changes), so that a
@@ -1200,7 +1201,7 @@ int tb_run(tb_ctx *ctx, long long max_slots)
         wr[i] = {ctx->worlds[i].host0, ctx->worlds[i].H1, ctx->worlds[i].sw0, ctx->worlds[i].S1};
     std::vector<WorldCtl> wc(s.W);
     std::vector<int> ulist;
-    int alive = s.W, list_alive = s.W, list_lanes = 0;
+    int alive = s.W, list_alive = s.W, list_lanes = 0, tuned_alive = s.W;
     s.unit_list = nullptr;
     s.n_list = 0;
     tb::SlotGraph graph;
@@ -1269,6 +1270,11 @@ int tb_run(tb_ctx *ctx, long long max_slots)
             tu.since++;
         if (ctl.finished || ctl.error)
             break;
+        if (4 * (tuned_alive - alive) > tuned_alive)
+        {
+            tu.load_changed();
+            tuned_alive = alive;
+        }
     }
     cudaEventRecord(ctx->ev1, ctx->stream);
     cudaEventSynchronize(ctx->ev1);

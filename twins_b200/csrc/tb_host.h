@@ -66,6 +66,8 @@ void running_units(Alive alive, const std::vector<std::array<int, 4>> &worlds, i
 // runs a probe of `probe` slots, and one whose device time per slot beats the current one's by
 // more than 5% takes over; a shape that loses a probe by more than 30% twice is not probed again
 // until every fourth round of probes, which probes all shapes (the load changes along a run).
+// With backoff, a round that keeps the shape doubles the period (up to a bound: probes of losing
+// shapes cost time), and a new shape or a change of the load (load_changed) restores it.
 struct ShapeTuner
 {
     struct Shape
@@ -79,6 +81,7 @@ struct ShapeTuner
     size_t best = 0;
     long long since = 0, rounds = 0;
     int period = 12, probe = 128;
+    int period0 = 12, most_period = 0; // (backoff: the first period and the bound; 0: none)
 
     // the candidates: (lanes, stage, port-local)
     static constexpr int N_CAND = 9;
@@ -116,6 +119,18 @@ struct ShapeTuner
         if (shapes.empty())
             shapes.push_back({lanes, stage, 0, 0, port_local});
     }
+    // the period doubles after each round that keeps the shape, up to `most` launches
+    void backoff(int most)
+    {
+        period0 = period;
+        most_period = most;
+    }
+    // the running worlds' entities changed much: probe again at the first period
+    void load_changed()
+    {
+        if (most_period > 0)
+            period = period0;
+    }
     bool explore() const { return shapes.size() > 1 && since >= period; }
     bool probes(size_t k) const { return k == best || shapes[k].strikes < 2; }
     // after a round of probes (per_slot[k]: ms per slot, <= 0 where no probe ran)
@@ -128,6 +143,8 @@ struct ShapeTuner
         for (size_t k = 0; k < shapes.size(); k++)
             if (per_slot[k] > 0 && per_slot[b] > 0 && per_slot[k] > 1.3 * per_slot[b])
                 shapes[k].strikes++;
+        if (most_period > 0)
+            period = b == best ? std::min(2 * period, most_period) : period0;
         best = b;
         since = 0;
         if (++rounds % 4 == 0)
