@@ -138,17 +138,21 @@ def test_tuner_hysteresis_strikes_and_expiry(hl):
         assert not hl.hl_tuner_explore(t)
         hl.hl_tuner_tick(t)
     assert hl.hl_tuner_explore(t)
-    # a shape 4% faster does not take over; every shape more than 30% slower takes a strike
-    ps = [1.0 if k == b0 else 2.0 for k in range(n)]
+    # a shape 4% faster does not take over; every shape more than 30% slower takes a strike, and
+    # one more than 60% slower two (it is not probed again)
+    ps = [1.0 if k == b0 else 1.4 for k in range(n)]
     other = (b0 + 1) % n
-    ps[other] = 0.96
+    far = (b0 + 2) % n
+    ps[other], ps[far] = 0.96, 1.7
     decide(hl, t, ps)
     assert hl.hl_tuner_best(t) == b0 and not hl.hl_tuner_explore(t)
+    assert not hl.hl_tuner_probes(t, far)
+    assert all(hl.hl_tuner_probes(t, k) for k in range(n) if k != far)
     # second round: 6% faster takes over, and the slow ones take their second strike
     ps[other] = 0.94
     decide(hl, t, ps)
     assert hl.hl_tuner_best(t) == other
-    slow = [k for k in range(n) if ps[k] == 2.0]
+    slow = [k for k in range(n) if ps[k] >= 1.4]
     assert slow and all(not hl.hl_tuner_probes(t, k) for k in slow)
     assert hl.hl_tuner_probes(t, b0) and hl.hl_tuner_probes(t, other)
     # rounds 3 and 4 without probes of the struck shapes; the fourth round clears every strike

@@ -64,8 +64,8 @@ void running_units(Alive alive, const std::vector<std::array<int, 4>> &worlds, i
 // host's serial events are the slot's critical path), else 32 hosts per warp (throughput-bound:
 // the lanes' memory accesses overlap). Every `period` launches each shape still in the running
 // runs a probe of `probe` slots, and one whose device time per slot beats the current one's by
-// more than 5% takes over; a shape that loses a probe by more than 30% twice is not probed again
-// until every fourth round of probes, which probes all shapes (the load changes along a run).
+// more than 5% takes over; a shape that loses a probe by more than 30% twice, or by more than 60%
+// once, is not probed again until every fourth round of probes, which probes all shapes (the load changes along a run).
 // With backoff, a round that keeps the shape doubles the period (up to a bound: probes of losing
 // shapes cost time), and a new shape or a change of the load (load_changed) restores it.
 struct ShapeTuner
@@ -142,7 +142,7 @@ struct ShapeTuner
                 b = k;
         for (size_t k = 0; k < shapes.size(); k++)
             if (per_slot[k] > 0 && per_slot[b] > 0 && per_slot[k] > 1.3 * per_slot[b])
-                shapes[k].strikes++;
+                shapes[k].strikes += per_slot[k] > 1.6 * per_slot[b] ? 2 : 1;
         if (most_period > 0)
             period = b == best ? std::min(2 * period, most_period) : period0;
         best = b;
