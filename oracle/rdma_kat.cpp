@@ -1,0 +1,296 @@
+// Test infrastructure, not product code: known answers of the reference's RDMA arithmetic.
+//
+// Built by `make -C oracle ref-rdma-kat` against the reference's own device code
+// (src/rdma/rstep.cuh, compiled for the CPU with its TWINS_CPU shim, src/gpu_runtime.h), so that
+// every answer below is the reference's. It prints one JSON object per case on stdout:
+//   {"fn": name, ...inputs..., ...outputs...}
+// with every double as the hex string of its IEEE-754 bits. tests/golden/make_rdma_kat.py turns
+// the output into tests/golden/rdma_kat.json, against which tests/test_rdma_cc.py checks the
+// restatement in twins_b200/csrc/tr_cc.cuh.
+//
+// Cases: ns_seconds, tx times (ns-3.17 and ns-3.36), node addresses, ECMP hashes, INT hop words,
+// HPCC's per-hop utilisation, and sequences of events on one queue pair for DCQCN (CNPs and the
+// three timers), DCTCP (ACKs) and HPCC (ACKs with INT hops, fast react, sample feedback).
+#include <climits>
+#include <cstdio>
+#include <cstring>
+
+#include "rdma/rstep.cuh"
+
+thread_local twins_dim3 threadIdx, blockIdx, blockDim, gridDim;
+uint64_t g_tail_side = 0;
+
+namespace
+{
+uint64_t rng_state = 0x2545F4914F6CDD1Dull;
+uint64_t next64()
+{
+    uint64_t z = (rng_state += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+uint64_t below(uint64_t n) { return next64() % n; }
+double unit() { return (double)(next64() >> 11) * (1.0 / 9007199254740992.0); }
+
+const char *hx(double d, char *buf)
+{
+    uint64_t b;
+    memcpy(&b, &d, 8);
+    snprintf(buf, 24, "0x%016llx", (unsigned long long)b);
+    return buf;
+}
+
+const uint64_t RATES[5] = {25000000000ull, 50000000000ull, 100000000000ull, 200000000000ull, 400000000000ull};
+
+void kat_time()
+{
+    char a[24];
+    const double fixed[] = {0.0, 1e-9, 1e-6, 1.5e-6, 0.25, 1.0, 2.0 / 3.0, 1e-3 + 1e-12, 123.456789, 4096.0 / 1e11};
+    for (double x : fixed)
+        printf("{\"fn\":\"ns_seconds\",\"x\":\"%s\",\"ns\":%lld}\n", hx(x, a), (long long)rdma::ns_seconds(x));
+    for (int i = 0; i < 200; i++)
+    {
+        const double x = i % 3 == 0 ? unit() * 1e-3 : i % 3 == 1 ? unit() * 10 : (double)below(1u << 30) * 1e-9;
+        printf("{\"fn\":\"ns_seconds\",\"x\":\"%s\",\"ns\":%lld}\n", hx(x, a), (long long)rdma::ns_seconds(x));
+    }
+    for (int i = 0; i < 200; i++)
+    {
+        const uint64_t bps = i % 2 ? RATES[below(5)] : (1 + below(400)) * 1000000000ull + below(1000) * 1000000ull;
+        const uint32_t bytes = (uint32_t)(i % 4 == 0 ? below(10000) : below(70000));
+        printf("{\"fn\":\"tx\",\"bps\":%llu,\"bytes\":%u,\"ns17\":%lld,\"ns36\":%lld}\n", (unsigned long long)bps, bytes,
+               (long long)rdma::tx_ns(bps, bytes), (long long)rdma::tx_ns36(bps, bytes));
+    }
+}
+
+void kat_hash()
+{
+    for (int i = 0; i < 200; i++)
+    {
+        const int x = i < 100 ? (int)below(70000) : i;
+        const uint32_t w0 = i % 2 ? rdma::node_ip(x) : (uint32_t)next64(), w1 = (uint32_t)next64(), w2 = (uint32_t)next64(),
+                       seed = (uint32_t)below(5000);
+        printf("{\"fn\":\"ecmp\",\"id\":%d,\"ip\":%u,\"w\":[%u,%u,%u],\"seed\":%u,\"h\":%u}\n", x, rdma::node_ip(x), w0, w1, w2, seed,
+               rdma::ecmp_hash(w0, w1, w2, seed));
+    }
+}
+
+void kat_hops()
+{
+    char a[24];
+    for (int i = 0; i < 200; i++)
+    {
+        const uint32_t multi = i % 3 == 0 ? 1 : (uint32_t)(1 + below(4));
+        const uint64_t rate = RATES[below(5)];
+        const uint64_t t0 = below(1ull << 25), b0 = below(1ull << 30), t1 = t0 + 1 + below(20000), b1 = b0 + below(1ull << 22);
+        const uint32_t q0 = (uint32_t)below(1u << 22), q1 = (uint32_t)below(1u << 22);
+        const uint64_t h0 = rdma::hop_make(t0, b0, q0, rate, multi), h1 = rdma::hop_make(t1, b1, q1, rate, multi);
+        rdma::Params P{};
+        P.int_multi = multi;
+        const uint64_t max_rate = RATES[below(5)];
+        const uint32_t win = (uint32_t)(10000 + below(200000));
+        double U;
+        uint64_t dt;
+        rdma::hpcc_hops(P, &h1, 1, &h0, max_rate, win, &U, &dt);
+        printf("{\"fn\":\"hop\",\"t\":[%llu,%llu],\"b\":[%llu,%llu],\"q\":[%u,%u],\"rate\":%llu,\"multi\":%u,\"h\":[%llu,%llu],"
+               "\"dtime\":%llu,\"dbytes\":%llu,\"max_rate\":%llu,\"win\":%u,\"U\":\"%s\",\"dt\":%llu}\n",
+               (unsigned long long)t0, (unsigned long long)t1, (unsigned long long)b0, (unsigned long long)b1, q0, q1,
+               (unsigned long long)rate, multi, (unsigned long long)h0, (unsigned long long)h1,
+               (unsigned long long)rdma::hop_time_delta(h1, h0), (unsigned long long)rdma::hop_bytes_delta(h1, h0, multi),
+               (unsigned long long)max_rate, win, hx(U, a), (unsigned long long)dt);
+    }
+}
+
+// the rate state printed after each event
+void print_state(const char *fn, int seq, int step, int ev, const rdma::SndQP &q, unsigned started, int set)
+{
+    char a[24], b[24];
+    printf("{\"fn\":\"%s\",\"seq\":%d,\"step\":%d,\"ev\":%d,\"rate\":%llu,\"target\":%llu,\"alpha\":\"%s\",\"rp_stage\":%u,"
+           "\"alpha_cnp\":%u,\"dec_cnp\":%u,\"first_cnp\":%u,\"started\":%u,\"lus\":%u,\"inc\":%d,\"cur_rate\":%llu,\"u\":\"%s\","
+           "\"hop\":[%llu,%llu,%llu,%llu,%llu],\"set\":%d,\"next_avail\":%lld}\n",
+           fn, seq, step, ev, (unsigned long long)q.rate, (unsigned long long)q.target, hx(q.alpha, a), q.rp_stage, q.alpha_cnp,
+           q.dec_cnp, q.first_cnp, started, q.last_update_seq, q.inc_stage, (unsigned long long)q.cur_rate, hx(q.u, b),
+           (unsigned long long)q.hop[0], (unsigned long long)q.hop[1], (unsigned long long)q.hop[2], (unsigned long long)q.hop[3],
+           (unsigned long long)q.hop[4], set, (long long)q.next_avail);
+}
+
+struct Harness
+{
+    rdma::Sim s{};
+    rdma::Params P{};
+    rdma::SndQP qp[1]{};
+    rdma::QPChains qc[1]{};
+    rdma::HCtx<1> c{};
+    Harness()
+    {
+        s.qp = qp;
+        s.qc = qc;
+        c.s = &s;
+        c.P = &P;
+        c.now = 1000000;
+        c.stv[0].ns_at = -1;
+        c.stv[0].due_min = INT64_MAX;
+    }
+    void params_line(const char *fn, int seq)
+    {
+        char a[24], b[24], d[24];
+        printf("{\"fn\":\"%s_params\",\"seq\":%d,\"g\":\"%s\",\"rate_first_cnp\":\"%s\",\"clamp\":%d,\"rpg_threshold\":%u,"
+               "\"rai\":%llu,\"rhai\":%llu,\"min_rate\":%llu,\"dctcp_rai\":%llu,\"u_target\":\"%s\",\"mi_thresh\":%u,"
+               "\"sample_feedback\":%d,\"int_multi\":%u,\"mtu\":%u}\n",
+               fn, seq, hx(P.g, a), hx(P.rate_first_cnp, b), P.clamp, P.rpg_threshold, (unsigned long long)P.rai,
+               (unsigned long long)P.rhai, (unsigned long long)P.min_rate, (unsigned long long)P.dctcp_rai, hx(P.u_target, d),
+               P.mi_thresh, P.sample_feedback, P.int_multi, P.mtu);
+    }
+    void qp_line(const char *fn, int seq)
+    {
+        const rdma::SndQP &q = qp[0];
+        printf("{\"fn\":\"%s_qp\",\"seq\":%d,\"rate\":%llu,\"max_rate\":%llu,\"snd_nxt\":%llu,\"base_rtt\":%llu,\"win\":%u,"
+               "\"last_pkt\":%u,\"next_avail\":%lld}\n",
+               fn, seq, (unsigned long long)q.rate, (unsigned long long)q.max_rate, (unsigned long long)q.snd_nxt,
+               (unsigned long long)q.base_rtt, q.win, q.last_pkt, (long long)q.next_avail);
+    }
+};
+
+void kat_dcqcn()
+{
+    for (int seq = 0; seq < 32; seq++)
+    {
+        Harness H;
+        H.P.g = 1.0 / (double)(16 << below(4));
+        H.P.rate_first_cnp = seq % 2 ? 1.0 : 0.5 + 0.5 * unit();
+        H.P.clamp = (int)below(2);
+        H.P.alpha_int = 1 + (int64_t)below(100000);
+        H.P.dec_int = 1 + (int64_t)below(100000);
+        H.P.rp_int = 1 + (int64_t)below(100000);
+        H.P.rpg_threshold = (uint32_t)(1 + below(6));
+        H.P.rai = (1 + below(100)) * 1000000ull;
+        H.P.rhai = (1 + below(1000)) * 1000000ull;
+        H.P.min_rate = (1 + below(1000)) * 1000000ull;
+        rdma::SndQP &q = H.qp[0];
+        q.max_rate = RATES[below(5)];
+        q.rate = q.max_rate;
+        q.target = q.max_rate;
+        q.first_cnp = 1;
+        q.alpha = 1;
+        H.params_line("dcqcn", seq);
+        H.qp_line("dcqcn", seq);
+        for (int step = 0; step < 20; step++)
+        {
+            const int ev = (int)below(4); // 0 CNP, 1 alpha timer, 2 decrease check, 3 increase timer
+            q.t_alpha = q.t_dec = q.t_rp = -1;
+            if (ev == 0)
+                rdma::dcqcn_cnp(H.c, 0, q);
+            else
+                rdma::dcqcn_timer(H.c, 0, ev - 1);
+            const unsigned started = (q.t_alpha >= 0 ? 1u : 0u) | (q.t_dec >= 0 ? 2u : 0u) | (q.t_rp >= 0 ? 4u : 0u);
+            print_state("dcqcn", seq, step, ev, q, started, 0);
+            H.c.now += 1 + (int64_t)below(50000);
+        }
+    }
+}
+
+void kat_dctcp()
+{
+    for (int seq = 0; seq < 32; seq++)
+    {
+        Harness H;
+        H.P.g = 1.0 / (double)(16 << below(4));
+        H.P.min_rate = (1 + below(1000)) * 1000000ull;
+        H.P.dctcp_rai = (1 + below(1000)) * 1000000ull;
+        H.P.mtu = 1000 + (uint32_t)below(8) * 500;
+        rdma::SndQP &q = H.qp[0];
+        q.max_rate = RATES[below(5)];
+        q.rate = q.max_rate;
+        q.snd_nxt = H.P.mtu * (1 + below(20));
+        H.params_line("dctcp", seq);
+        H.qp_line("dctcp", seq);
+        uint32_t acked = 0;
+        for (int step = 0; step < 20; step++)
+        {
+            rdma::Pkt p{};
+            // the sender runs ahead; an ACK covers up to what was sent (or, after a NACK, less)
+            q.snd_nxt += H.P.mtu * below(6);
+            acked += (uint32_t)(H.P.mtu * below(4));
+            if (acked > q.snd_nxt)
+                acked = (uint32_t)q.snd_nxt;
+            p.seq = step % 7 == 6 ? (uint32_t)q.snd_nxt + H.P.mtu : acked;
+            p.cnp = (uint8_t)(below(3) == 0);
+            rdma::dctcp_ack(H.c, q, p);
+            printf("{\"fn\":\"dctcp\",\"seq\":%d,\"step\":%d,\"ack\":%u,\"cnp\":%u,\"snd_nxt\":%llu,\"rate\":%llu,\"alpha\":\"", seq, step,
+                   p.seq, p.cnp, (unsigned long long)q.snd_nxt, (unsigned long long)q.rate);
+            char a[24];
+            printf("%s\",\"lus\":%u,\"batch\":%u,\"ecn_cnt\":%u,\"ca_state\":%u,\"high_seq\":%u}\n", hx(q.alpha, a), q.last_update_seq,
+                   q.batch, q.ecn_cnt, q.ca_state, q.high_seq);
+        }
+    }
+}
+
+void kat_hpcc()
+{
+    for (int seq = 0; seq < 32; seq++)
+    {
+        Harness H;
+        H.P.u_target = 0.95;
+        H.P.mi_thresh = (uint32_t)below(6);
+        H.P.rai = (1 + below(100)) * 1000000ull;
+        H.P.min_rate = (1 + below(1000)) * 1000000ull;
+        H.P.sample_feedback = seq % 4 == 3;
+        H.P.int_multi = seq % 3 == 0 ? 1 : (uint32_t)(1 + below(4));
+        H.P.mtu = 1000;
+        rdma::SndQP &q = H.qp[0];
+        q.max_rate = RATES[below(5)];
+        q.rate = q.max_rate;
+        q.cur_rate = q.max_rate;
+        q.base_rtt = 2000 + below(20000);
+        q.win = (uint32_t)(q.max_rate / 8 * q.base_rtt / 1000000000ull) + 1000;
+        q.u = 1;
+        q.last_pkt = 1048;
+        q.next_avail = 5000000;
+        q.snd_nxt = 1000;
+        H.params_line("hpcc", seq);
+        H.qp_line("hpcc", seq);
+        const int nhop = 1 + (int)below(5);
+        uint64_t t[5], b[5];
+        uint64_t rate[5];
+        for (int i = 0; i < nhop; i++)
+        {
+            t[i] = below(1ull << 24);
+            b[i] = below(1ull << 26);
+            rate[i] = RATES[below(5)];
+        }
+        for (int step = 0; step < 20; step++)
+        {
+            rdma::Pkt p{};
+            p.nhop = (uint16_t)nhop;
+            for (int i = 0; i < nhop; i++)
+            {
+                t[i] += 200 + below(4000);
+                b[i] += below(rate[i] / 8 / 1000000ull * 4);
+                const uint32_t ql = below(3) == 0 ? 0 : (uint32_t)below(400000);
+                p.hop[i] = rdma::hop_make(t[i], b[i], ql, rate[i], H.P.int_multi);
+            }
+            q.snd_nxt += 1000 * below(8);
+            const bool fast = below(2) == 1;
+            q.tx_rate = 12345; // (change_rate leaves the new rate here: whether it ran)
+            q.tx_size = 0;
+            rdma::hpcc_update(H.c, q, p, fast);
+            const int set = q.tx_rate != 12345;
+            printf("{\"fn\":\"hpcc_ack\",\"seq\":%d,\"step\":%d,\"fast\":%d,\"nhop\":%d,\"snd_nxt\":%llu,\"hops\":[%llu,%llu,%llu,%llu,%llu]}\n",
+                   seq, step, (int)fast, nhop, (unsigned long long)q.snd_nxt, (unsigned long long)p.hop[0], (unsigned long long)p.hop[1],
+                   (unsigned long long)p.hop[2], (unsigned long long)p.hop[3], (unsigned long long)p.hop[4]);
+            print_state("hpcc", seq, step, fast, q, 0, set);
+        }
+    }
+}
+} // namespace
+
+int main()
+{
+    kat_time();
+    kat_hash();
+    kat_hops();
+    kat_dcqcn();
+    kat_dctcp();
+    kat_hpcc();
+    return 0;
+}

@@ -1,0 +1,35 @@
+"""Writes tests/golden/rdma_kat.json: known answers of the reference's RDMA arithmetic (time and tx
+times, node addresses, ECMP hashes, INT hop words, HPCC's per-hop utilisation, and event sequences
+of DCQCN, DCTCP and HPCC on one queue pair), printed by oracle/_ref/rdma_kat, which
+`make -C oracle ref-rdma-kat` builds from the reference's own src/rdma/rstep.cuh for the CPU.
+
+The fixture groups the harness's lines by function: {fn: {"keys": [...], "rows": [[...], ...]}}.
+Doubles stay as the hex strings of their bits.
+
+    python tests/golden/make_rdma_kat.py
+"""
+import json
+import subprocess
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parents[2]
+EXE = ROOT / "oracle" / "_ref" / "rdma_kat"
+OUT = Path(__file__).resolve().parent / "rdma_kat.json"
+
+
+def main():
+    subprocess.run(["make", "-C", str(ROOT / "oracle"), "ref-rdma-kat"], check=True)
+    lines = subprocess.run([str(EXE)], check=True, capture_output=True, text=True).stdout.splitlines()
+    out = {}
+    for line in lines:
+        d = json.loads(line)
+        fn = d.pop("fn")
+        g = out.setdefault(fn, {"keys": list(d), "rows": []})
+        assert list(d) == g["keys"], fn
+        g["rows"].append([d[k] for k in g["keys"]])
+    OUT.write_text(json.dumps(out, separators=(",", ":")) + "\n")
+    print(OUT, {k: len(v["rows"]) for k, v in out.items()}, OUT.stat().st_size, "bytes")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,65 @@
+// A C shim over the RDMA arithmetic (twins_b200/csrc/tr_cc.cuh), built by tests/test_rdma_cc.py
+// with g++ (no floating-point contraction: the rules' fma() calls are explicit) and checked there
+// against the reference's known answers.
+#include "tr_cc.cuh"
+
+using namespace tr;
+
+extern "C" {
+
+void rc_sizes(int *out)
+{
+    out[0] = (int)sizeof(QpRate);
+    out[1] = (int)sizeof(CcParams);
+}
+
+long long rc_ns_seconds(double x) { return ns_seconds(x); }
+long long rc_tx(unsigned long long bps, unsigned bytes, int ns336) { return tx_time(ns336 != 0, bps, bytes); }
+unsigned rc_node_ip(int id) { return node_ip(id); }
+unsigned rc_ecmp(unsigned a, unsigned b, unsigned c, unsigned seed) { return ecmp_hash(a, b, c, seed); }
+
+unsigned long long rc_hop_make(unsigned long long t, unsigned long long b, unsigned q, unsigned long long rate, unsigned multi)
+{
+    return hop_make(t, b, q, rate, multi);
+}
+unsigned long long rc_hop_time_delta(unsigned long long now, unsigned long long was) { return hop_time_delta(now, was); }
+unsigned long long rc_hop_bytes_delta(unsigned long long now, unsigned long long was, unsigned multi) { return hop_bytes_delta(now, was, multi); }
+double rc_hop_u(unsigned long long now, unsigned long long was, unsigned multi, unsigned long long max_rate, unsigned win, unsigned long long *tau)
+{
+    uint64_t t;
+    const double u = hpcc_hop_u(now, was, multi, max_rate, win, &t);
+    *tau = t;
+    return u;
+}
+
+// DCQCN events: 0 a CNP, 1 the alpha timer, 2 the decrease check, 3 the increase timer
+unsigned rc_dcqcn(QpRate *q, const CcParams *P, int ev)
+{
+    switch (ev)
+    {
+    case 0:
+        return dcqcn_cnp(*q, *P);
+    case 1:
+        return dcqcn_alpha(*q, *P);
+    case 2:
+        return dcqcn_decrease(*q, *P);
+    default:
+        return dcqcn_increase(*q, *P);
+    }
+}
+
+void rc_dctcp(QpRate *q, const CcParams *P, unsigned seq, int cnp) { dctcp_ack(*q, *P, seq, cnp != 0); }
+
+int rc_hpcc(QpRate *q, const CcParams *P, const unsigned long long *hops, int nhop, int fast)
+{
+    uint64_t h[MAX_HOP];
+    for (int i = 0; i < MAX_HOP; i++)
+        h[i] = hops[i];
+    return hpcc_ack(*q, *P, h, nhop, fast != 0);
+}
+
+long long rc_paced(long long next_avail, int ns336, unsigned long long old_rate, unsigned long long new_rate, unsigned last_pkt)
+{
+    return paced_after_change(next_avail, ns336 != 0, old_rate, new_rate, last_pkt);
+}
+}
