@@ -82,7 +82,12 @@ void kat_hops()
     {
         const uint32_t multi = i % 3 == 0 ? 1 : (uint32_t)(1 + below(4));
         const uint64_t rate = RATES[below(5)];
-        const uint64_t t0 = below(1ull << 25), b0 = below(1ull << 30), t1 = t0 + 1 + below(20000), b1 = b0 + below(1ull << 22);
+        // (odd cases: the time and byte counters wrap between the two words)
+        const bool wrap = i % 2 == 1;
+        const uint64_t unit_b = 128ull * multi;
+        const uint64_t t0 = wrap ? (1ull << 24) * (1 + below(2)) - 1 - below(20000) : below(1ull << 25);
+        const uint64_t b0 = wrap ? (1ull << 20) * unit_b * (1 + below(2)) - below(1ull << 21) : below(1ull << 30);
+        const uint64_t t1 = t0 + 1 + below(20000), b1 = b0 + below(1ull << 22);
         const uint32_t q0 = (uint32_t)below(1u << 22), q1 = (uint32_t)below(1u << 22);
         const uint64_t h0 = rdma::hop_make(t0, b0, q0, rate, multi), h1 = rdma::hop_make(t1, b1, q1, rate, multi);
         rdma::Params P{};
@@ -153,7 +158,7 @@ struct Harness
 
 void kat_dcqcn()
 {
-    for (int seq = 0; seq < 32; seq++)
+    for (int seq = 0; seq < 24; seq++)
     {
         Harness H;
         H.P.g = 1.0 / (double)(16 << below(4));
@@ -174,7 +179,7 @@ void kat_dcqcn()
         q.alpha = 1;
         H.params_line("dcqcn", seq);
         H.qp_line("dcqcn", seq);
-        for (int step = 0; step < 20; step++)
+        for (int step = 0; step < 16; step++)
         {
             const int ev = (int)below(4); // 0 CNP, 1 alpha timer, 2 decrease check, 3 increase timer
             q.t_alpha = q.t_dec = q.t_rp = -1;
@@ -191,7 +196,7 @@ void kat_dcqcn()
 
 void kat_dctcp()
 {
-    for (int seq = 0; seq < 32; seq++)
+    for (int seq = 0; seq < 24; seq++)
     {
         Harness H;
         H.P.g = 1.0 / (double)(16 << below(4));
@@ -205,7 +210,7 @@ void kat_dctcp()
         H.params_line("dctcp", seq);
         H.qp_line("dctcp", seq);
         uint32_t acked = 0;
-        for (int step = 0; step < 20; step++)
+        for (int step = 0; step < 16; step++)
         {
             rdma::Pkt p{};
             // the sender runs ahead; an ACK covers up to what was sent (or, after a NACK, less)
@@ -227,7 +232,7 @@ void kat_dctcp()
 
 void kat_hpcc()
 {
-    for (int seq = 0; seq < 32; seq++)
+    for (int seq = 0; seq < 24; seq++)
     {
         Harness H;
         H.P.u_target = 0.95;
@@ -258,7 +263,7 @@ void kat_hpcc()
             b[i] = below(1ull << 26);
             rate[i] = RATES[below(5)];
         }
-        for (int step = 0; step < 20; step++)
+        for (int step = 0; step < 16; step++)
         {
             rdma::Pkt p{};
             p.nhop = (uint16_t)nhop;
@@ -282,6 +287,167 @@ void kat_hpcc()
         }
     }
 }
+// a queue pair's whole rate state, as JSON
+void state_json(const char *key, const rdma::SndQP &q, bool hpcc)
+{
+    char a[24], b[24];
+    printf("\"%s\":{\"rate\":%llu,\"max_rate\":%llu,\"target\":%llu,\"snd_nxt\":%llu,\"base_rtt\":%llu,\"win\":%u,"
+           "\"alpha_cnp\":%u,\"dec_cnp\":%u,\"first_cnp\":%u,\"rp_stage\":%u,\"alpha\":\"%s\",\"lus\":%u,\"inc\":%d,",
+           key, (unsigned long long)q.rate, (unsigned long long)q.max_rate, (unsigned long long)q.target, (unsigned long long)q.snd_nxt,
+           (unsigned long long)q.base_rtt, q.win, q.alpha_cnp, q.dec_cnp, q.first_cnp, q.rp_stage, hx(q.alpha, a), q.last_update_seq,
+           q.inc_stage);
+    // (HPCC's and DCTCP's fields share their room in the reference's queue pair)
+    if (hpcc)
+        printf("\"cur_rate\":%llu,\"u\":\"%s\",", (unsigned long long)q.cur_rate, hx(q.u, b));
+    else
+        printf("\"high_seq\":%u,\"ecn_cnt\":%u,\"batch\":%u,\"ca_state\":%u,", q.high_seq, q.ecn_cnt, q.batch, q.ca_state);
+    printf("\"hop\":[%llu,%llu,%llu,%llu,%llu],\"next_avail\":%lld,\"last_pkt\":%u}", (unsigned long long)q.hop[0],
+           (unsigned long long)q.hop[1], (unsigned long long)q.hop[2], (unsigned long long)q.hop[3], (unsigned long long)q.hop[4],
+           (long long)q.next_avail, q.last_pkt);
+}
+
+void random_params(rdma::Params &P)
+{
+    P.g = 1.0 / 1024 + unit() * 0.12;
+    P.rate_first_cnp = 0.3 + 0.7 * unit();
+    P.clamp = (int)below(2);
+    P.alpha_int = P.dec_int = P.rp_int = 55;
+    P.rpg_threshold = (uint32_t)(1 + below(6));
+    P.rai = (1 + below(100)) * 1000000ull + below(1000);
+    P.rhai = (1 + below(1000)) * 1000000ull + below(1000);
+    P.min_rate = (1 + below(1000)) * 1000000ull;
+    P.dctcp_rai = (1 + below(1000)) * 1000000ull;
+    P.u_target = 0.5 + 0.5 * unit();
+    P.mi_thresh = (uint32_t)below(8);
+    P.sample_feedback = (int)below(2);
+    P.int_multi = (uint32_t)(1 + below(4));
+    P.mtu = 500 + (uint32_t)below(4000);
+}
+
+void params_json(const rdma::Params &P)
+{
+    char a[24], b[24], d[24];
+    printf("\"P\":{\"g\":\"%s\",\"rate_first_cnp\":\"%s\",\"clamp\":%d,\"rpg_threshold\":%u,\"rai\":%llu,\"rhai\":%llu,"
+           "\"min_rate\":%llu,\"dctcp_rai\":%llu,\"u_target\":\"%s\",\"mi_thresh\":%u,\"sample_feedback\":%d,\"int_multi\":%u,"
+           "\"mtu\":%u}",
+           hx(P.g, a), hx(P.rate_first_cnp, b), P.clamp, P.rpg_threshold, (unsigned long long)P.rai, (unsigned long long)P.rhai,
+           (unsigned long long)P.min_rate, (unsigned long long)P.dctcp_rai, hx(P.u_target, d), P.mi_thresh, P.sample_feedback,
+           P.int_multi, P.mtu);
+}
+
+// one event on a queue pair in a random state, for each rule
+void kat_single()
+{
+    for (int i = 0; i < 900; i++)
+    {
+        Harness H;
+        random_params(H.P);
+        rdma::SndQP &q = H.qp[0];
+        q.max_rate = RATES[below(5)];
+        q.rate = H.P.min_rate + below(q.max_rate - H.P.min_rate + 1);
+        q.target = below(q.max_rate + 1);
+        q.snd_nxt = below(1ull << 31);
+        q.base_rtt = 1000 + below(30000);
+        q.win = (uint32_t)(1000 + below(1u << 22));
+        q.last_pkt = (uint32_t)(64 + below(9000));
+        q.next_avail = (int64_t)below(1ull << 40);
+        const int kind = i % 3; // 0 DCQCN, 1 DCTCP, 2 HPCC
+        if (kind == 0)
+        {
+            q.alpha = unit();
+            q.rp_stage = (uint32_t)below(10);
+            q.alpha_cnp = (uint8_t)below(2);
+            q.dec_cnp = (uint8_t)below(2);
+            q.first_cnp = (uint8_t)below(2);
+            const int ev = (int)below(4);
+            printf("{\"fn\":\"dcqcn1\",\"ev\":%d,", ev);
+            params_json(H.P);
+            printf(",");
+            state_json("a", q, false);
+            q.t_alpha = q.t_dec = q.t_rp = -1;
+            if (ev == 0)
+                rdma::dcqcn_cnp(H.c, 0, q);
+            else
+                rdma::dcqcn_timer(H.c, 0, ev - 1);
+            const unsigned started = (q.t_alpha >= 0 ? 1u : 0u) | (q.t_dec >= 0 ? 2u : 0u) | (q.t_rp >= 0 ? 4u : 0u);
+            printf(",\"started\":%u,", started);
+            state_json("b", q, false);
+            printf("}\n");
+        }
+        else if (kind == 1)
+        {
+            q.alpha = unit();
+            q.last_update_seq = below(4) == 0 ? 0 : (uint32_t)below(1u << 31);
+            q.batch = (uint32_t)(1 + below(100));
+            q.ecn_cnt = (uint32_t)below(q.batch + 5);
+            q.ca_state = (uint32_t)below(2);
+            q.high_seq = (uint32_t)below(1u << 31);
+            rdma::Pkt p{};
+            p.seq = below(2) ? (uint32_t)below(1u << 31) : (uint32_t)(q.snd_nxt - below(1u << 16));
+            p.cnp = (uint8_t)below(2);
+            printf("{\"fn\":\"dctcp1\",\"ack\":%u,\"cnp\":%u,", p.seq, p.cnp);
+            params_json(H.P);
+            printf(",");
+            state_json("a", q, false);
+            rdma::dctcp_ack(H.c, q, p);
+            printf(",");
+            state_json("b", q, false);
+            printf("}\n");
+        }
+        else
+        {
+            q.u = unit() * 3;
+            q.inc_stage = (int32_t)below(9);
+            q.cur_rate = H.P.min_rate + below(q.max_rate - H.P.min_rate + 1);
+            q.last_update_seq = below(5) == 0 ? 0 : (uint32_t)below(1u << 31);
+            rdma::Pkt p{};
+            p.nhop = (uint16_t)(below(8) == 0 ? 6 : 1 + below(5)); // (more than MAX_HOP: ignored)
+            for (int k = 0; k < 5; k++)
+            {
+                const uint64_t rate = RATES[below(5)];
+                const uint64_t t0 = below(1ull << 24), b0 = below(1ull << 30);
+                q.hop[k] = rdma::hop_make(t0, b0, (uint32_t)below(1u << 21), rate, H.P.int_multi);
+                p.hop[k] = rdma::hop_make(t0 + 1 + below(30000), b0 + below(1ull << 22), below(3) == 0 ? 0 : (uint32_t)below(1u << 21),
+                                          rate, H.P.int_multi);
+            }
+            // ties: hop 1 has hop 0's utilisation over twice the interval (the first of equal hops
+            // sets dt); idle hops: no bytes and an empty queue (utilisation 0 sets nothing)
+            const int shape = (int)below(4);
+            if (shape == 1 && p.nhop >= 2)
+            {
+                const uint64_t rate = RATES[below(5)], unit_b = 128ull * H.P.int_multi;
+                const uint64_t tau = 1 + below(8000), db = below(2000) * unit_b, t0 = below(1ull << 23), t1 = below(1ull << 23);
+                const uint64_t b0 = below(1ull << 12) * unit_b, b1 = below(1ull << 12) * unit_b;
+                const uint32_t qa = (uint32_t)below(1u << 20), qb = (uint32_t)below(1u << 20);
+                q.hop[0] = rdma::hop_make(t0, b0, qa, rate, H.P.int_multi);
+                p.hop[0] = rdma::hop_make(t0 + tau, b0 + db, qb, rate, H.P.int_multi);
+                q.hop[1] = rdma::hop_make(t1, b1, qa, rate, H.P.int_multi);
+                p.hop[1] = rdma::hop_make(t1 + 2 * tau, b1 + 2 * db, qb, rate, H.P.int_multi);
+            }
+            else if (shape == 2)
+                for (int k = 0; k < p.nhop && k < 5; k++)
+                    if (below(2))
+                    {
+                        const uint64_t rate = RATES[below(5)], t0 = below(1ull << 23), b0 = below(1ull << 30);
+                        q.hop[k] = rdma::hop_make(t0, b0, (uint32_t)below(1u << 20), rate, H.P.int_multi);
+                        p.hop[k] = rdma::hop_make(t0 + 1 + below(8000), b0, 0, rate, H.P.int_multi);
+                    }
+            const int fast = (int)below(2);
+            printf("{\"fn\":\"hpcc1\",\"fast\":%d,\"nhop\":%d,\"hops\":[%llu,%llu,%llu,%llu,%llu],", fast, p.nhop,
+                   (unsigned long long)p.hop[0], (unsigned long long)p.hop[1], (unsigned long long)p.hop[2], (unsigned long long)p.hop[3],
+                   (unsigned long long)p.hop[4]);
+            params_json(H.P);
+            printf(",");
+            state_json("a", q, true);
+            q.tx_rate = 12345;
+            q.tx_size = 0;
+            rdma::hpcc_update(H.c, q, p, fast != 0);
+            printf(",\"set\":%d,", q.tx_rate != 12345 ? 1 : 0);
+            state_json("b", q, true);
+            printf("}\n");
+        }
+    }
+}
 } // namespace
 
 int main()
@@ -292,5 +458,6 @@ int main()
     kat_dcqcn();
     kat_dctcp();
     kat_hpcc();
+    kat_single();
     return 0;
 }

@@ -3,7 +3,8 @@ times, node addresses, ECMP hashes, INT hop words, HPCC's per-hop utilisation, a
 of DCQCN, DCTCP and HPCC on one queue pair), printed by oracle/_ref/rdma_kat, which
 `make -C oracle ref-rdma-kat` builds from the reference's own src/rdma/rstep.cuh for the CPU.
 
-The fixture groups the harness's lines by function: {fn: {"keys": [...], "rows": [[...], ...]}}.
+The fixture groups the harness's lines by function: {fn: {"keys": [...], "rows": [[...], ...]}},
+nested objects flattened to dotted keys ("a.rate": the rate before the event, "b.rate" after).
 Doubles stay as the hex strings of their bits.
 
     python tests/golden/make_rdma_kat.py
@@ -17,12 +18,22 @@ EXE = ROOT / "oracle" / "_ref" / "rdma_kat"
 OUT = Path(__file__).resolve().parent / "rdma_kat.json"
 
 
+def flat(d, pre=""):
+    out = {}
+    for k, v in d.items():
+        if isinstance(v, dict):
+            out.update(flat(v, pre + k + "."))
+        else:
+            out[pre + k] = v
+    return out
+
+
 def main():
     subprocess.run(["make", "-C", str(ROOT / "oracle"), "ref-rdma-kat"], check=True)
     lines = subprocess.run([str(EXE)], check=True, capture_output=True, text=True).stdout.splitlines()
     out = {}
     for line in lines:
-        d = json.loads(line)
+        d = flat(json.loads(line))
         fn = d.pop("fn")
         g = out.setdefault(fn, {"keys": list(d), "rows": []})
         assert list(d) == g["keys"], fn
