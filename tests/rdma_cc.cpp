@@ -7,6 +7,8 @@ using namespace tr;
 
 extern "C" {
 
+int rc_failed() { return 0; }
+
 void rc_sizes(int *out)
 {
     out[0] = (int)sizeof(QpRate);

@@ -3,7 +3,9 @@
 tests/golden/make_rdma_kat.py), bit for bit: ns-3.17 time and tx times (and ns-3.36's), node
 addresses, ECMP hashes, INT hop words and HPCC's per-hop utilisation, and event sequences on one
 queue pair for DCQCN (CNPs, alpha / decrease / increase timers), DCTCP-RDMA and HPCC (fast react,
-sample feedback, pacing after a rate change)."""
+sample feedback, pacing after a rate change). Every check runs twice: on the CPU (the header built
+with g++) and, marked gpu, on a B200 (the same header built with nvcc for sm_100a, each function run
+in a kernel)."""
 import ctypes as C
 import json
 import shutil
@@ -15,6 +17,7 @@ import pytest
 from conftest import GOLDEN, ROOT
 
 SHIM = ROOT / "tests" / "rdma_cc.cpp"
+SHIM_GPU = ROOT / "tests" / "rdma_cc_gpu.cu"
 CSRC = ROOT / "twins_b200" / "csrc"
 U64, U32, U8 = C.c_uint64, C.c_uint32, C.c_uint8
 
@@ -40,16 +43,21 @@ def bits(x):
     return "0x%016x" % struct.unpack("<Q", struct.pack("<d", x))[0]
 
 
-@pytest.fixture(scope="module")
-def rc(tmp_path_factory):
-    if shutil.which("g++") is None:
-        pytest.skip("g++ is not here")
-    so = tmp_path_factory.mktemp("rc") / "librc.so"
-    subprocess.run(["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-fno-fast-math", "-shared", "-fPIC", f"-I{CSRC}", "-o", str(so),
-                    str(SHIM)], check=True)
+@pytest.fixture(scope="module", params=["cpu", pytest.param("gpu", marks=pytest.mark.gpu)])
+def rc(request, tmp_path_factory):
+    so = tmp_path_factory.mktemp("rc") / f"librc_{request.param}.so"
+    if request.param == "cpu":
+        if shutil.which("g++") is None:
+            pytest.skip("g++ is not here")
+        cmd = ["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-fno-fast-math", "-shared", "-fPIC", f"-I{CSRC}", "-o", str(so), str(SHIM)]
+    else:
+        cmd = ["nvcc", "-std=c++17", "-O2", "--fmad=false", "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-Xcompiler", "-fPIC",
+               f"-I{CSRC}", "-o", str(so), str(SHIM_GPU)]
+    subprocess.run(cmd, check=True)
     lib = C.CDLL(str(so))
     ull, qp, pp = C.c_ulonglong, C.POINTER(QpRate), C.POINTER(CcParams)
     sig = {
+        "rc_failed": (C.c_int, []),
         "rc_sizes": (None, [C.POINTER(C.c_int)]),
         "rc_ns_seconds": (C.c_longlong, [C.c_double]),
         "rc_tx": (C.c_longlong, [ull, C.c_uint, C.c_int]),
@@ -70,7 +78,8 @@ def rc(tmp_path_factory):
     sizes = (C.c_int * 2)()
     lib.rc_sizes(sizes)
     assert (sizes[0], sizes[1]) == (C.sizeof(QpRate), C.sizeof(CcParams))
-    return lib
+    yield lib
+    assert lib.rc_failed() == 0  # (a CUDA call of the device shim failed)
 
 
 @pytest.fixture(scope="module")
