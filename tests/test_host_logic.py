@@ -179,9 +179,13 @@ def test_tuner_backoff(hl):
         decide(hl, t, keep)
         periods.append(hl.hl_tuner_period(t))
     assert periods == [2 * p0, 4 * p0, 4 * p0, 4 * p0] and hl.hl_tuner_best(t) == b0
-    # a change of the load restores the first period; so does a new shape
+    # a change of the load restores the first period and clears the strikes; a new shape restores the period
+    far = [1.0 if k == b0 else 2.0 for k in range(n)]
+    decide(hl, t, far)
+    assert all(not hl.hl_tuner_probes(t, k) for k in range(n) if k != b0)
     hl.hl_tuner_load_changed(t)
     assert hl.hl_tuner_period(t) == p0
+    assert all(hl.hl_tuner_probes(t, k) for k in range(n))
     decide(hl, t, keep)
     assert hl.hl_tuner_period(t) == 2 * p0
     new = list(keep)

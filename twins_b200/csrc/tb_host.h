@@ -67,7 +67,8 @@ void running_units(Alive alive, const std::vector<std::array<int, 4>> &worlds, i
 // more than 5% takes over; a shape that loses a probe by more than 30% twice, or by more than 60%
 // once, is not probed again until every fourth round of probes, which probes all shapes (the load changes along a run).
 // With backoff, a round that keeps the shape doubles the period (up to a bound: probes of losing
-// shapes cost time), and a new shape or a change of the load (load_changed) restores it.
+// shapes cost time), and a new shape or a change of the load (load_changed) restores it; a change
+// of the load also clears the strikes.
 struct ShapeTuner
 {
     struct Shape
@@ -125,11 +126,14 @@ struct ShapeTuner
         period0 = period;
         most_period = most;
     }
-    // the running worlds' entities changed much: probe again at the first period
+    // the running worlds' entities changed much: earlier losses say little now; probe every shape
+    // again, at the first period
     void load_changed()
     {
         if (most_period > 0)
             period = period0;
+        for (auto &x : shapes)
+            x.strikes = 0;
     }
     bool explore() const { return shapes.size() > 1 && since >= period; }
     bool probes(size_t k) const { return k == best || shapes[k].strikes < 2; }
