@@ -5,7 +5,7 @@
 // every answer below is the reference's. It prints one JSON object per case on stdout:
 //   {"fn": name, ...inputs..., ...outputs...}
 // with every double as the hex string of its IEEE-754 bits. tests/golden/make_rdma_kat.py turns
-// the output into tests/golden/rdma_kat.json, against which tests/test_rdma_cc.py checks the
+// the output into tests/golden/rdma_kat.json.gz, against which tests/test_rdma_cc.py checks the
 // restatement in twins_b200/csrc/tr_cc.cuh.
 //
 // Cases: ns_seconds, tx times (ns-3.17 and ns-3.36), node addresses, ECMP hashes, INT hop words,
@@ -448,6 +448,196 @@ void kat_single()
         }
     }
 }
+// the NIC: frame sizes, the window, the round robin, the receiver's check, ACK handling
+void kat_nic()
+{
+    for (int extra = 0; extra <= 4; extra += 4)
+        for (int isz = 0; isz <= 42; isz += 42)
+        {
+            rdma::Params P{};
+            P.seq_extra = (uint32_t)extra;
+            P.int_size = isz;
+            const uint32_t payload = (uint32_t)below(4097);
+            printf("{\"fn\":\"sizes\",\"seq_extra\":%d,\"int_size\":%d,\"payload\":%u,\"data\":%u,\"ack\":%u}\n", extra, isz, payload,
+                   rdma::data_size(P, payload), rdma::ack_size(P));
+        }
+    // the round robin over a NIC's queue pairs
+    for (int i = 0; i < 250; i++)
+    {
+        Harness H;
+        H.P.var_win = (int)below(2);
+        H.P.ack_high_prio = (int)below(2);
+        const int n = 1 + (int)below(8);
+        static rdma::SndQP qps[8];
+        static int list[8];
+        H.s.qp = qps;
+        H.s.qps = list;
+        H.s.qps_cap = 8;
+        const int64_t now = 1000000 + (int64_t)below(1000);
+        printf("{\"fn\":\"rr\",\"var_win\":%d,\"ack_high_prio\":%d,\"now\":%lld,\"qps\":[", H.P.var_win, H.P.ack_high_prio, (long long)now);
+        for (int k = 0; k < 8; k++)
+        {
+            rdma::SndQP &q = qps[k];
+            q = rdma::SndQP{};
+            q.size = 1 + below(100000);
+            const int st = (int)below(5); // done, all sent, window-bound, late, ready
+            q.snd_una = st == 0 ? q.size : below(q.size);
+            q.snd_nxt = st <= 1 ? q.size : q.snd_una + below(q.size - q.snd_una);
+            q.max_rate = RATES[below(5)];
+            q.rate = 1 + below(q.max_rate);
+            q.win = below(4) == 0 ? 0 : (uint32_t)(1 + below(st == 2 ? q.snd_nxt - q.snd_una + 1 : 200000));
+            // (due exactly now, or one ns later, a third of the time)
+            q.next_avail = st == 3 ? now + 1 + (below(3) ? (int64_t)below(1000) : 0) : now - (below(3) ? (int64_t)below(1000) : 0);
+            printf("%s[%llu,%llu,%llu,%llu,%llu,%u,%lld]", k ? "," : "", (unsigned long long)q.size, (unsigned long long)q.snd_nxt,
+                   (unsigned long long)q.snd_una, (unsigned long long)q.rate, (unsigned long long)q.max_rate, q.win, (long long)q.next_avail);
+        }
+        for (int k = 0; k < 8; k++)
+            list[k] = k;
+        for (int k = 7; k > 0; k--) // (a shuffled list)
+        {
+            const int j = (int)below(k + 1), t = list[k];
+            list[k] = list[j], list[j] = t;
+        }
+        rdma::Host &h = H.c.stv[0];
+        h.paused = below(4) == 0 ? (uint32_t)below(16) : 0;
+        h.ackq_n = below(3) == 0 ? (int)below(3) : 0;
+        h.qp_n = n;
+        h.rr = (int)below(40);
+        H.c.now = now;
+        printf("],\"paused\":%u,\"ackq_n\":%d,\"n\":%d,\"rr\":%d,\"list\":[", h.paused, h.ackq_n, n, h.rr);
+        for (int k = 0; k < n; k++)
+            printf("%s%d", k ? "," : "", list[k]);
+        const int pick = rdma::next_qindex(H.c);
+        printf("],\"pick\":%d,\"n_after\":%d,\"list_after\":[", pick, h.qp_n);
+        for (int k = 0; k < h.qp_n; k++)
+            printf("%s%d", k ? "," : "", list[k]);
+        printf("]}\n");
+    }
+    // a data frame at the receiver (ReceiverCheckSeq) and the ACK or NACK it queues
+    for (int i = 0; i < 400; i++)
+    {
+        Harness H;
+        static rdma::RcvQP rx[1];
+        static rdma::FlowInfo fi[1];
+        static rdma::Pkt ackq[8];
+        static unsigned long long ev[64];
+        H.s.rx = rx;
+        H.s.fi = fi;
+        H.s.ackq = ackq;
+        H.s.ackq_cap = 8;
+        H.s.ev = ev;
+        H.P.seq_extra = below(2) ? 4 : 0;
+        H.P.int_size = below(2) ? 42 : 0;
+        H.P.ack_interval = below(2) ? 1 : (uint32_t)(1 + below(20000));
+        H.P.chunk = below(2) ? 0 : (uint32_t)(1000 * (1 + below(4)));
+        H.P.nack_interval = 500000;
+        fi[0] = rdma::FlowInfo{};
+        fi[0].size = 1ull << 40;
+        rx[0].expected = (uint32_t)(1000 * below(30));
+        rx[0].last_nack = below(2) ? rx[0].expected : (uint32_t)(1000 * below(30));
+        rx[0].nack_timer = below(4) == 0 ? 1000000 : (int64_t)below(2000000); // (at times expiring exactly now)
+        H.c.stv[0].tc_at = 1; // (the device is busy: the ACK stays queued)
+        H.c.stv[0].ackq_head = (int)below(8);
+        H.c.stv[0].ackq_n = 0;
+        H.c.now = 1000000;
+        rdma::Pkt p{};
+        p.kind = rdma::K_DATA;
+        const uint32_t payload = 1 + (uint32_t)below(1000);
+        p.size = (uint16_t)rdma::data_size(H.P, payload);
+        p.seq = below(3) == 0 ? rx[0].expected : (uint32_t)(1000 * below(30));
+        p.ecn = below(2) ? 3 : 0;
+        printf("{\"fn\":\"rx\",\"seq_extra\":%u,\"int_size\":%d,\"ack_interval\":%u,\"chunk\":%u,\"nack_interval\":%lld,\"now\":%lld,"
+               "\"expected\":%u,\"last_nack\":%u,\"nack_timer\":%lld,\"seq\":%u,\"payload\":%u,\"ecn\":%u,",
+               H.P.seq_extra, H.P.int_size, H.P.ack_interval, H.P.chunk, (long long)H.P.nack_interval, (long long)H.c.now, rx[0].expected,
+               rx[0].last_nack, (long long)rx[0].nack_timer, p.seq, payload, p.ecn);
+        rdma::h_data(H.c, p);
+        const rdma::Pkt &a = ackq[H.c.stv[0].ackq_head];
+        const int queued = H.c.stv[0].ackq_n;
+        printf("\"expected_after\":%u,\"last_nack_after\":%u,\"nack_timer_after\":%lld,\"queued\":%d,\"kind\":%u,\"ack_seq\":%u,"
+               "\"cnp\":%u,\"size\":%u}\n",
+               rx[0].expected, rx[0].last_nack, (long long)rx[0].nack_timer, queued, queued ? a.kind : 0, queued ? a.seq : 0,
+               queued ? a.cnp : 0, queued ? a.size : 0);
+    }
+    // an ACK or NACK at the sender, with each congestion control
+    for (int i = 0; i < 360; i++)
+    {
+        Harness H;
+        static rdma::FlowInfo fi[1];
+        static int64_t fct[1];
+        static unsigned done_n;
+        static unsigned long long ev[64];
+        random_params(H.P);
+        H.s.fi = fi;
+        H.s.fct = fct;
+        H.s.flows_done = &done_n;
+        H.s.ev = ev;
+        H.s.dag = 0;
+        fi[0] = rdma::FlowInfo{};
+        fi[0].start = 1000;
+        fct[0] = -1;
+        const int ccs[3] = {1, 3, 8};
+        H.P.cc = ccs[i % 3];
+        H.P.fast_react = (int)below(2);
+        H.c.stv[0].tc_at = 1;
+        rdma::SndQP &q = H.qp[0];
+        q.max_rate = RATES[below(5)];
+        q.rate = H.P.min_rate + below(q.max_rate - H.P.min_rate + 1);
+        q.target = q.max_rate;
+        q.size = 1000 + below(1u << 20);
+        q.snd_una = below(q.size);
+        q.snd_nxt = q.snd_una + below(q.size - q.snd_una + 1);
+        q.base_rtt = 1000 + below(30000);
+        q.win = (uint32_t)(1000 + below(1u << 22));
+        q.last_pkt = (uint32_t)(64 + below(9000));
+        q.next_avail = (int64_t)below(1ull << 40);
+        q.first_cnp = (uint8_t)below(2);
+        q.alpha = unit();
+        q.t_alpha = q.t_dec = q.t_rp = -1;
+        if (H.P.cc == 3)
+        {
+            q.u = unit() * 2;
+            q.cur_rate = q.rate;
+            q.inc_stage = (int32_t)below(6);
+            q.last_update_seq = below(5) == 0 ? 0 : (uint32_t)below(q.size + 1);
+        }
+        else if (H.P.cc == 8)
+        {
+            q.last_update_seq = below(4) == 0 ? 0 : (uint32_t)below(q.size + 1);
+            q.batch = (uint32_t)(1 + below(100));
+            q.ecn_cnt = (uint32_t)below(q.batch + 5);
+            q.ca_state = (uint32_t)below(2);
+            q.high_seq = (uint32_t)below(q.size + 1);
+        }
+        rdma::Pkt p{};
+        p.kind = below(4) == 0 ? rdma::K_NACK : rdma::K_ACK;
+        p.seq = below(6) == 0 ? (uint32_t)q.size : (uint32_t)below(q.snd_nxt + 1);
+        p.cnp = (uint8_t)below(2);
+        p.nhop = (uint16_t)(1 + below(5));
+        for (int k = 0; k < 5; k++)
+        {
+            const uint64_t rate = RATES[below(5)];
+            const uint64_t t0 = below(1ull << 24), b0 = below(1ull << 30);
+            q.hop[k] = rdma::hop_make(t0, b0, (uint32_t)below(1u << 21), rate, H.P.int_multi);
+            p.hop[k] = rdma::hop_make(t0 + 1 + below(30000), b0 + below(1ull << 22), (uint32_t)below(1u << 21), rate, H.P.int_multi);
+        }
+        // (HPCC's state has other fields: its cases are "ack_hp")
+        printf("{\"fn\":\"%s\",\"cc\":%d,\"fast_react\":%d,\"nack\":%d,\"seq\":%u,\"cnp\":%u,\"nhop\":%u,"
+               "\"hops\":[%llu,%llu,%llu,%llu,%llu],\"size\":%llu,\"snd_una\":%llu,",
+               H.P.cc == 3 ? "ack_hp" : "ack", H.P.cc, H.P.fast_react, p.kind == rdma::K_NACK, p.seq, p.cnp, p.nhop, (unsigned long long)p.hop[0], (unsigned long long)p.hop[1],
+               (unsigned long long)p.hop[2], (unsigned long long)p.hop[3], (unsigned long long)p.hop[4], (unsigned long long)q.size,
+               (unsigned long long)q.snd_una);
+        params_json(H.P);
+        printf(",");
+        state_json("a", q, H.P.cc == 3);
+        H.c.now = 5000000;
+        rdma::h_ack(H.c, p);
+        const unsigned started = (q.t_alpha >= 0 ? 1u : 0u) | (q.t_dec >= 0 ? 2u : 0u) | (q.t_rp >= 0 ? 4u : 0u);
+        printf(",\"snd_una_after\":%llu,\"done\":%u,\"fct\":%lld,\"started\":%u,", (unsigned long long)q.snd_una, q.done,
+               (long long)fct[0], started);
+        state_json("b", q, H.P.cc == 3);
+        printf("}\n");
+    }
+}
 } // namespace
 
 int main()
@@ -459,5 +649,6 @@ int main()
     kat_dctcp();
     kat_hpcc();
     kat_single();
+    kat_nic();
     return 0;
 }

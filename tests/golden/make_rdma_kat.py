@@ -1,4 +1,4 @@
-"""Writes tests/golden/rdma_kat.json: known answers of the reference's RDMA arithmetic (time and tx
+"""Writes tests/golden/rdma_kat.json.gz: known answers of the reference's RDMA arithmetic (time and tx
 times, node addresses, ECMP hashes, INT hop words, HPCC's per-hop utilisation, and event sequences
 of DCQCN, DCTCP and HPCC on one queue pair), printed by oracle/_ref/rdma_kat, which
 `make -C oracle ref-rdma-kat` builds from the reference's own src/rdma/rstep.cuh for the CPU.
@@ -9,13 +9,14 @@ Doubles stay as the hex strings of their bits.
 
     python tests/golden/make_rdma_kat.py
 """
+import gzip
 import json
 import subprocess
 from pathlib import Path
 
 ROOT = Path(__file__).resolve().parents[2]
 EXE = ROOT / "oracle" / "_ref" / "rdma_kat"
-OUT = Path(__file__).resolve().parent / "rdma_kat.json"
+OUT = Path(__file__).resolve().parent / "rdma_kat.json.gz"
 
 
 def flat(d, pre=""):
@@ -38,7 +39,8 @@ def main():
         g = out.setdefault(fn, {"keys": list(d), "rows": []})
         assert list(d) == g["keys"], fn
         g["rows"].append([d[k] for k in g["keys"]])
-    OUT.write_text(json.dumps(out, separators=(",", ":")) + "\n")
+    # (mtime 0: the same answers give the same bytes)
+    OUT.write_bytes(gzip.compress((json.dumps(out, separators=(",", ":")) + "\n").encode(), mtime=0))
     print(OUT, {k: len(v["rows"]) for k, v in out.items()}, OUT.stat().st_size, "bytes")
 
 

@@ -65,3 +65,39 @@ long long rc_paced(long long next_avail, int ns336, unsigned long long old_rate,
     return paced_after_change(next_avail, ns336 != 0, old_rate, new_rate, last_pkt);
 }
 }
+
+// ------------------------------------------------------------------ the NIC rules (tr_nic.cuh)
+#include "tr_nic.cuh"
+
+extern "C" {
+
+void rc_nic_sizes(int *out)
+{
+    out[0] = (int)sizeof(NicParams);
+    out[1] = (int)sizeof(QpSend);
+    out[2] = (int)sizeof(RxQp);
+}
+
+void rc_frame_sizes(const NicParams *P, unsigned payload, unsigned *out)
+{
+    out[0] = data_size(*P, payload);
+    out[1] = ack_size(*P);
+}
+
+int rc_next_qindex(const NicParams *P, unsigned paused, int ackq_n, int *list, int *n, int rr, long long now, const QpRate *rates,
+                   const QpSend *sends)
+{
+    return next_qindex(*P, paused, ackq_n, list, n, rr, now, [rates, sends](int f) { return QpView{rates[f], sends[f]}; });
+}
+
+int rc_rx_check(const NicParams *P, RxQp *r, unsigned seq, unsigned payload, long long now) { return rx_check(*P, *r, seq, payload, now); }
+
+unsigned rc_ack_received(const NicParams *P, const CcParams *C, QpRate *r, QpSend *q, unsigned seq, int nack, int cnp,
+                         const unsigned long long *hops, int nhop)
+{
+    uint64_t h[MAX_HOP];
+    for (int i = 0; i < MAX_HOP; i++)
+        h[i] = hops[i];
+    return ack_received(*P, *C, *r, *q, seq, nack != 0, cnp != 0, h, nhop);
+}
+}

@@ -1,0 +1,27 @@
+// Built by tests/test_rdma_nic.py with nvcc for sm_100a (compiled, not run): every NIC rule of
+// twins_b200/csrc/tr_nic.cuh instantiated in a kernel.
+#include "tr_nic.cuh"
+
+using namespace tr;
+
+struct NicCase
+{
+    NicParams P;
+    CcParams C;
+    QpRate rate[4];
+    QpSend send[4];
+    RxQp rx;
+    int list[4], n;
+    uint64_t hops[MAX_HOP];
+    unsigned out[4];
+};
+
+__global__ void nic_rules(NicCase *c)
+{
+    c->out[0] = data_size(c->P, 1000) + ack_size(c->P);
+    const QpRate *r = c->rate;
+    const QpSend *s = c->send;
+    c->out[1] = (unsigned)next_qindex(c->P, 0, 0, c->list, &c->n, 0, 0, [r, s](int f) { return QpView{r[f], s[f]}; });
+    c->out[2] = (unsigned)rx_check(c->P, c->rx, 0, 1000, 0);
+    c->out[3] = ack_received(c->P, c->C, c->rate[0], c->send[0], 1000, false, true, c->hops, 1);
+}

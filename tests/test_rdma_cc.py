@@ -1,5 +1,5 @@
 """The RDMA model's arithmetic (twins_b200/csrc/tr_cc.cuh) against the reference's own answers
-(tests/golden/rdma_kat.json, printed by the reference's src/rdma/rstep.cuh built for the CPU:
+(tests/golden/rdma_kat.json.gz, printed by the reference's src/rdma/rstep.cuh built for the CPU:
 tests/golden/make_rdma_kat.py), bit for bit: ns-3.17 time and tx times (and ns-3.36's), node
 addresses, ECMP hashes, INT hop words and HPCC's per-hop utilisation, and event sequences on one
 queue pair for DCQCN (CNPs, alpha / decrease / increase timers), DCTCP-RDMA and HPCC (fast react,
@@ -7,6 +7,7 @@ sample feedback, pacing after a rate change). Every check runs twice: on the CPU
 with g++) and, marked gpu, on a B200 (the same header built with nvcc for sm_100a, each function run
 in a kernel)."""
 import ctypes as C
+import gzip
 import json
 import shutil
 import struct
@@ -84,7 +85,7 @@ def rc(request, tmp_path_factory):
 
 @pytest.fixture(scope="module")
 def kat():
-    raw = json.loads((GOLDEN / "rdma_kat.json").read_text())
+    raw = json.loads(gzip.decompress((GOLDEN / "rdma_kat.json.gz").read_bytes()))
     return {fn: [dict(zip(g["keys"], r)) for r in g["rows"]] for fn, g in raw.items()}
 
 

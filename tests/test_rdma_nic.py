@@ -1,0 +1,127 @@
+"""The RDMA model's NIC rules (twins_b200/csrc/tr_nic.cuh) against the reference's own answers
+(tests/golden/rdma_kat.json.gz, printed by the reference's src/rdma/rstep.cuh built for the CPU),
+bit for bit: frame sizes, the queue pairs' round robin with the window and pacing (and the removal
+of finished queue pairs), the receiver's go-back-N check with the ACK or NACK it queues, and the
+sender's handling of an ACK or NACK with DCQCN, HPCC and DCTCP. The rules run on the CPU here
+(g++); that the same header builds for sm_100a is checked with nvcc."""
+import ctypes as C
+import shutil
+import subprocess
+
+import pytest
+
+from conftest import ROOT
+from test_rdma_cc import CSRC, SHIM, CcParams, QpRate, bits, dbl, kat, params, same, state, sub  # noqa: F401
+
+U64, U32, U8 = C.c_uint64, C.c_uint32, C.c_uint8
+RC_NIC = ROOT / "tests" / "rdma_nic_compile.cu"
+
+
+class NicParams(C.Structure):
+    _fields_ = [("mtu", U32), ("ack_interval", U32), ("chunk", U32), ("nack_interval", C.c_int64), ("seq_extra", U32), ("int_size", C.c_int),
+                ("var_win", C.c_int), ("ack_high_prio", C.c_int), ("cc", C.c_int), ("fast_react", C.c_int), ("ns336", C.c_int)]
+
+
+class QpSend(C.Structure):
+    _fields_ = [("size", U64), ("snd_una", U64), ("next_avail", C.c_int64), ("last_pkt", U32), ("done", U8)]
+
+
+class RxQp(C.Structure):
+    _fields_ = [("expected", U32), ("last_nack", U32), ("nack_timer", C.c_int64)]
+
+
+@pytest.fixture(scope="module")
+def nic(tmp_path_factory):
+    if shutil.which("g++") is None:
+        pytest.skip("g++ is not here")
+    so = tmp_path_factory.mktemp("nic") / "libnic.so"
+    subprocess.run(["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-fno-fast-math", "-shared", "-fPIC", f"-I{CSRC}", "-o", str(so), str(SHIM)],
+                   check=True)
+    lib = C.CDLL(str(so))
+    ull, np_, qr, qs = C.c_ulonglong, C.POINTER(NicParams), C.POINTER(QpRate), C.POINTER(QpSend)
+    sig = {
+        "rc_nic_sizes": (None, [C.POINTER(C.c_int)]),
+        "rc_frame_sizes": (None, [np_, C.c_uint, C.POINTER(C.c_uint)]),
+        "rc_next_qindex": (C.c_int, [np_, C.c_uint, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int, C.c_longlong, qr, qs]),
+        "rc_rx_check": (C.c_int, [np_, C.POINTER(RxQp), C.c_uint, C.c_uint, C.c_longlong]),
+        "rc_ack_received": (C.c_uint, [np_, C.POINTER(CcParams), qr, qs, C.c_uint, C.c_int, C.c_int, C.POINTER(ull), C.c_int]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype, f.argtypes = res, args
+    sizes = (C.c_int * 3)()
+    lib.rc_nic_sizes(sizes)
+    assert list(sizes) == [C.sizeof(NicParams), C.sizeof(QpSend), C.sizeof(RxQp)]
+    return lib
+
+
+def test_frame_sizes(nic, kat):
+    for r in kat["sizes"]:
+        P = NicParams(seq_extra=r["seq_extra"], int_size=r["int_size"])
+        out = (C.c_uint * 2)()
+        nic.rc_frame_sizes(C.byref(P), r["payload"], out)
+        assert list(out) == [r["data"], r["ack"]], r
+
+
+def test_round_robin(nic, kat):
+    picks = set()
+    for r in kat["rr"]:
+        P = NicParams(var_win=r["var_win"], ack_high_prio=r["ack_high_prio"])
+        k = len(r["qps"])
+        rates, sends = (QpRate * k)(), (QpSend * k)()
+        for i, (size, nxt, una, rate, max_rate, win, na) in enumerate(r["qps"]):
+            rates[i].snd_nxt, rates[i].rate, rates[i].max_rate, rates[i].win = nxt, rate, max_rate, win
+            sends[i].size, sends[i].snd_una, sends[i].next_avail = size, una, na
+        lst = (C.c_int * k)(*(r["list"] + [0] * (k - r["n"])))
+        n = C.c_int(r["n"])
+        pick = nic.rc_next_qindex(C.byref(P), r["paused"], r["ackq_n"], lst, C.byref(n), r["rr"], r["now"], rates, sends)
+        assert (pick, n.value, list(lst[:n.value])) == (r["pick"], r["n_after"], r["list_after"]), r
+        picks.add(pick if pick < 0 else 0)
+    assert picks == {-1, -1024, 0}
+
+
+def test_receiver_check(nic, kat):
+    seen = set()
+    for r in kat["rx"]:
+        P = NicParams(seq_extra=r["seq_extra"], int_size=r["int_size"], ack_interval=r["ack_interval"], chunk=r["chunk"],
+                      nack_interval=r["nack_interval"])
+        rx = RxQp(r["expected"], r["last_nack"], r["nack_timer"])
+        x = nic.rc_rx_check(C.byref(P), C.byref(rx), r["seq"], r["payload"], r["now"])
+        seen.add(x)
+        assert (rx.expected, rx.last_nack, rx.nack_timer) == (r["expected_after"], r["last_nack_after"], r["nack_timer_after"]), r
+        # an ACK (1) or a NACK (2) is queued, carrying the expected byte and the frame's ECN as a CNP
+        assert r["queued"] == (x in (1, 2)), r
+        if x in (1, 2):
+            out = (C.c_uint * 2)()
+            nic.rc_frame_sizes(C.byref(P), 0, out)
+            assert (r["kind"], r["ack_seq"], r["cnp"], r["size"]) == (x, rx.expected, 1 if r["ecn"] else 0, out[1]), r
+    assert seen == {1, 2, 3, 4, 5}
+
+
+@pytest.mark.parametrize("fn", ["ack", "ack_hp"])
+def test_ack_received(nic, kat, fn):
+    n_done = 0
+    for r in kat[fn]:
+        P = NicParams(cc=r["cc"], fast_react=r["fast_react"])
+        Cp, a = params(sub(r, "P.")), sub(r, "a.")
+        q = state(a)
+        s = QpSend(size=r["size"], snd_una=r["snd_una"], next_avail=a["next_avail"], last_pkt=a["last_pkt"])
+        hops = (C.c_ulonglong * 5)(*r["hops"])
+        out = nic.rc_ack_received(C.byref(P), C.byref(Cp), C.byref(q), C.byref(s), r["seq"], r["nack"], r["cnp"], hops, r["nhop"])
+        b = sub(r, "b.")
+        assert same(q, b), r
+        assert s.next_avail == b["next_avail"] and s.snd_una == r["snd_una_after"] and s.done == r["done"], r
+        # completion: the reference stamps the flow's completion time and stops the DCQCN timers
+        assert bool(out & 1) == (r["fct"] >= 0) == bool(r["done"]), r
+        started = 0 if out & 1 else out >> 4
+        assert started == r["started"], r
+        n_done += s.done
+    assert n_done > 10
+
+
+def test_nic_rules_build_for_sm100a(tmp_path):
+    """The rules are host and device functions: the header builds for sm_100a."""
+    if shutil.which("nvcc") is None:
+        pytest.skip("nvcc is not here")
+    subprocess.run(["nvcc", "-std=c++17", "--fmad=false", "-gencode", "arch=compute_100a,code=sm_100a", "-c", f"-I{CSRC}", "-o",
+                    str(tmp_path / "nic.o"), str(RC_NIC)], check=True)
