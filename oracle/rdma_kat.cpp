@@ -638,6 +638,267 @@ void kat_nic()
         printf("}\n");
     }
 }
+// a switch of 4 ports for the buffer rules: every port busy transmitting unless a case frees one
+struct SwHarness
+{
+    rdma::Sim s{};
+    rdma::Params P{};
+    rdma::SCtx c{};
+    rdma::SwPortLds w[4]{};
+    rdma::Chain tc[4]{}, zero{};
+    rdma::PortCfg pc[4]{};
+    int pbase[1] = {0};
+    rdma::Pkt q0[32]{}, q3[32]{};
+    unsigned long long ev[64]{};
+    unsigned pend[8]{};
+    rdma::LFrame msg[4]{};
+    SwHarness()
+    {
+        s.pc = pc;
+        s.pbase = pbase;
+        s.q0 = q0;
+        s.q3 = q3;
+        s.q0_cap = s.q3_cap = 8;
+        s.ev = ev;
+        s.R = 1; // (one link rate: tx times from the table, all 0 here)
+        s.fD = rdma::fdiv_make(1000);
+        s.fpend = rdma::fdiv_make(8);
+        s.pend = pend;
+        s.msg = msg;
+        P.delay = 1000;
+        c.s = &s;
+        c.P = &P;
+        c.x = 0;
+        c.node = 10;
+        c.w = w;
+        c.tc = tc;
+        c.cur_src = &zero;
+        c.now = 5000;
+        const rdma::FDiv one = rdma::fdiv_make(1);
+        for (int k = 0; k < 4; k++)
+        {
+            w[k].pt.tc_at = 1;
+            w[k].out_delay = 1000;
+            w[k].ob.nb = 1;
+            w[k].ob.nb_m = one.m;
+            w[k].ob.nb_sh = (uint8_t)one.sh;
+            w[k].ob.nb_add = (uint8_t)one.add;
+            w[k].ob.cap = 4;
+        }
+    }
+};
+
+void random_switch(SwHarness &S)
+{
+    S.P.buffer_size = (uint32_t)((1 + below(32)) << 20);
+    S.c.sw.total_rsrv = 4 * 4096;
+    S.c.sw.total_hdrm = (uint32_t)below(S.P.buffer_size / 4);
+    S.c.sw.shared_used = (uint32_t)below(S.P.buffer_size - S.c.sw.total_hdrm - S.c.sw.total_rsrv + 1);
+    S.c.nvs = below(8) == 0;
+    for (int k = 0; k < 4; k++)
+    {
+        rdma::PortCfg &pc = S.pc[k];
+        pc.bps = RATES[below(5)];
+        pc.hdrm_cap = (uint32_t)(10000 + below(200000));
+        pc.shift = (uint32_t)below(4);
+        pc.kmin = (uint32_t)below(100000);
+        pc.kmax = pc.kmin + 1 + (uint32_t)below(400000);
+        pc.pmax = unit();
+        S.w[k].kmin = pc.kmin;
+        S.w[k].kmax = pc.kmax;
+        rdma::Port &pt = S.w[k].pt;
+        const int shape = (int)below(3); // in the reserve, in the shared pool, in the headroom
+        pt.ing = shape == 0 ? (uint32_t)below(4097) : 4096 + (uint32_t)below(400000);
+        pt.hdrm = shape == 2 ? (uint32_t)below(pc.hdrm_cap + 1) : 0;
+        pt.egr = (uint32_t)below(600000);
+        pt.mmu_paused = (uint32_t)below(2);
+        pt.tx_bytes = below(1ull << 40);
+        pt.bytes_total = (uint32_t)below(1u << 22);
+        for (int i = 0; i < 6; i++)
+            pt.rng.s[i] = (double)(1 + below(4294944000ull));
+    }
+}
+
+void port_json(const char *key, const rdma::Port &pt)
+{
+    printf("\"%s\":[%u,%u,%u,%u,%llu,%u,%d]", key, pt.ing, pt.hdrm, pt.egr, pt.mmu_paused, (unsigned long long)pt.tx_bytes, pt.bytes_total,
+           pt.q0_n);
+}
+
+void switch_json(const SwHarness &S)
+{
+    printf("\"buffer\":%u,\"sw\":[%u,%u,%u],\"nvs\":%d,\"cfg\":[", S.P.buffer_size, S.c.sw.shared_used, S.c.sw.total_hdrm, S.c.sw.total_rsrv,
+           (int)S.c.nvs);
+    char a[24];
+    for (int k = 0; k < 4; k++)
+        printf("%s[%llu,%u,%u,%u,%u,\"%s\"]", k ? "," : "", (unsigned long long)S.pc[k].bps, S.pc[k].hdrm_cap, S.pc[k].shift, S.pc[k].kmin,
+               S.pc[k].kmax, hx(S.pc[k].pmax, a));
+    printf("]");
+}
+
+// the buffer rules: admission (SwitchNode's forwarding with the egress busy, so the frame queues),
+// release at dequeue (the frame goes out onto its link), and the ECMP choice
+void kat_mmu()
+{
+    for (int i = 0; i < 500; i++)
+    {
+        SwHarness S;
+        random_switch(S);
+        const int in = (int)below(4), out = (in + 1 + (int)below(3)) % 4;
+        rdma::Pkt p{};
+        p.kind = rdma::K_DATA;
+        p.size = (uint16_t)(64 + below(9000));
+        rdma::Port &pi = S.w[in].pt;
+        const int edge = (int)below(8);
+        const uint32_t free_b = S.P.buffer_size - S.c.sw.total_hdrm - S.c.sw.total_rsrv;
+        if (edge == 0) // (a nearly full buffer and headroom: the frame may be dropped)
+        {
+            pi.hdrm = S.pc[in].hdrm_cap - (uint32_t)below(p.size);
+            pi.ing = 4096 + (uint32_t)below(100000);
+            S.c.sw.shared_used = free_b - (uint32_t)below(1u << 16);
+        }
+        else if (edge == 1) // (the headroom exactly full with the frame, the shared part above the threshold)
+        {
+            const uint32_t th = (free_b - S.c.sw.shared_used) >> S.pc[in].shift;
+            pi.hdrm = S.pc[in].hdrm_cap - p.size;
+            pi.ing = 4096 + th + (uint32_t)below(2);
+        }
+        else if (edge == 2) // (the frame fills the shared part exactly to the threshold)
+        {
+            const uint32_t th = (free_b - S.c.sw.shared_used) >> S.pc[in].shift;
+            pi.hdrm = 0;
+            pi.mmu_paused = 0;
+            if (th >= p.size)
+                pi.ing = 4096 + th - p.size;
+        }
+        else if (edge == 3) // (a threshold of 0 and the frame in the reserve)
+        {
+            pi.hdrm = 0;
+            pi.mmu_paused = 0;
+            pi.ing = (uint32_t)below(4096 - p.size + 1);
+            S.c.sw.shared_used = free_b - (uint32_t)below(1u << S.pc[in].shift);
+        }
+        printf("{\"fn\":\"admit\",\"in\":%d,\"out\":%d,\"size\":%u,", in, out, p.size);
+        switch_json(S);
+        printf(",");
+        port_json("pin", S.w[in].pt);
+        printf(",");
+        port_json("pout", S.w[out].pt);
+        const unsigned long long drop0 = S.ev[0], pause0 = S.ev[2];
+        rdma::s_forward(S.c, in, p, out, rdma::PG);
+        printf(",\"shared_after\":%u,\"drop\":%llu,\"pause\":%llu,", S.c.sw.shared_used, S.ev[0] - drop0, S.ev[2] - pause0);
+        port_json("pin_after", S.w[in].pt);
+        printf(",");
+        port_json("pout_after", S.w[out].pt);
+        printf("}\n");
+    }
+    for (int i = 0; i < 500; i++)
+    {
+        SwHarness S;
+        random_switch(S);
+        S.P.ecn = (int)below(4) != 0;
+        S.P.cc = below(2) ? 3 : 1;
+        S.P.int_multi = (uint32_t)(1 + below(4));
+        const int in = (int)below(4), out = (in + 1 + (int)below(3)) % 4;
+        rdma::Pkt p{};
+        p.kind = below(4) ? rdma::K_DATA : rdma::K_ACK;
+        p.size = (uint16_t)(64 + below(9000));
+        p.inport = (uint8_t)in;
+        p.nhop = (uint16_t)(below(10) == 0 ? 0xFFFF : below(8));
+        for (int k = 0; k < 5; k++)
+            p.hop[k] = next64();
+        // (the frame's bytes are in the counters it leaves: at least its size)
+        rdma::Port &pi = S.w[in].pt, &po = S.w[out].pt;
+        if (pi.hdrm + pi.ing < p.size)
+            pi.ing += p.size;
+        if (po.egr < p.size)
+            po.egr += p.size;
+        const int edge = (int)below(6);
+        if (edge == 0) // (the ingress counters near the resume condition)
+        {
+            pi.hdrm = below(2) ? 0 : (uint32_t)below(p.size + 1);
+            pi.ing = 4096 + (uint32_t)below(2 * 4096) + (pi.hdrm < p.size ? p.size - pi.hdrm : 0);
+            pi.mmu_paused = 1;
+        }
+        else if (edge == 1) // (after it leaves, the shared part exactly RESUME_OFFSET below the threshold)
+        {
+            const uint32_t x = (uint32_t)below(1000);
+            S.pc[in].shift = 0;
+            pi.hdrm = 0;
+            pi.mmu_paused = 1;
+            pi.ing = 4096 + x + p.size;
+            S.c.sw.shared_used = S.P.buffer_size - S.c.sw.total_hdrm - S.c.sw.total_rsrv + p.size - x - 3072 - (uint32_t)below(2);
+        }
+        else if (edge == 2) // (after it leaves, the egress queue exactly at kmax)
+            po.egr = S.w[out].kmax + p.size;
+        else if (edge == 3) // (after it leaves, the egress queue exactly at kmin)
+            po.egr = S.w[out].kmin + p.size;
+        po.tc_at = -1;
+        nsm_rng::State probe = po.rng;
+        const double u = nsm_rng::rand_u01(probe);
+        const nsm_rng::State rng0 = po.rng;
+        char a[24];
+        printf("{\"fn\":\"release\",\"in\":%d,\"out\":%d,\"size\":%u,\"kind\":%u,\"ecn\":%d,\"cc\":%d,\"multi\":%u,\"nhop\":%u,"
+               "\"hops\":[%llu,%llu,%llu,%llu,%llu],\"now\":%lld,\"u\":\"%s\",",
+               in, out, p.size, p.kind, S.P.ecn, S.P.cc, S.P.int_multi, p.nhop, (unsigned long long)p.hop[0], (unsigned long long)p.hop[1],
+               (unsigned long long)p.hop[2], (unsigned long long)p.hop[3], (unsigned long long)p.hop[4], (long long)S.c.now, hx(u, a));
+        switch_json(S);
+        printf(",");
+        port_json("pin", pi);
+        printf(",");
+        port_json("pout", po);
+        const unsigned long long mark0 = S.ev[1], resume0 = S.ev[3];
+        rdma::s_start_q3(S.c, out, p);
+        const int drawn = memcmp(&rng0, &po.rng, sizeof rng0) != 0;
+        const rdma::Pkt &f = S.msg[0].p;
+        printf(",\"shared_after\":%u,\"mark\":%llu,\"resume\":%llu,\"drawn\":%d,\"sent_ecn\":%u,\"sent_nhop\":%u,"
+               "\"sent_hops\":[%llu,%llu,%llu,%llu,%llu],",
+               S.c.sw.shared_used, S.ev[1] - mark0, S.ev[3] - resume0, drawn, f.ecn, f.nhop, (unsigned long long)f.hop[0],
+               (unsigned long long)f.hop[1], (unsigned long long)f.hop[2], (unsigned long long)f.hop[3], (unsigned long long)f.hop[4]);
+        port_json("pin_after", pi);
+        printf(",");
+        port_json("pout_after", po);
+        printf("}\n");
+    }
+    // ECMP: a switch's equal-cost ports towards each host
+    for (int i = 0; i < 300; i++)
+    {
+        rdma::Sim s{};
+        rdma::Params P{};
+        rdma::SwInfo si{};
+        rdma::Route rt[16];
+        uint8_t rtp[64];
+        si.seed = (uint32_t)below(3000);
+        si.hbase = (int)below(100);
+        si.rt_off = 0;
+        int off = 0;
+        for (int h = 0; h < 16; h++)
+        {
+            rt[h].off = (uint32_t)off;
+            rt[h].n = (uint32_t)(below(8) == 0 ? 0 : 1 + below(4));
+            for (uint32_t k = 0; k < rt[h].n; k++)
+                rtp[off++] = (uint8_t)below(32);
+        }
+        s.si = &si;
+        s.rt = rt;
+        s.rtp = rtp;
+        P.ack_high_prio = (int)below(2);
+        rdma::Pkt p{};
+        p.kind = below(2) ? rdma::K_DATA : rdma::K_ACK;
+        p.src = (uint16_t)(si.hbase + below(16));
+        p.dst = (uint16_t)(si.hbase + below(16));
+        p.sport = (uint16_t)(10000 + below(50000));
+        int q = -1;
+        const int port = rdma::s_route(s, P, 0, p, &q);
+        const int d = (p.kind == rdma::K_DATA ? p.dst : p.src) - si.hbase;
+        printf("{\"fn\":\"route\",\"data\":%d,\"src\":%d,\"dst\":%d,\"sport\":%u,\"seed\":%u,\"ack_high_prio\":%d,\"n\":%u,"
+               "\"ports\":[",
+               p.kind == rdma::K_DATA, p.src - si.hbase, p.dst - si.hbase, p.sport, si.seed, P.ack_high_prio, rt[d].n);
+        for (uint32_t k = 0; k < rt[d].n; k++)
+            printf("%s%u", k ? "," : "", rtp[rt[d].off + k]);
+        printf("],\"port\":%d,\"q\":%d}\n", port, q);
+    }
+}
 } // namespace
 
 int main()
@@ -650,5 +911,6 @@ int main()
     kat_hpcc();
     kat_single();
     kat_nic();
+    kat_mmu();
     return 0;
 }

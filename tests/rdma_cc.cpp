@@ -101,3 +101,40 @@ unsigned rc_ack_received(const NicParams *P, const CcParams *C, QpRate *r, QpSen
     return ack_received(*P, *C, *r, *q, seq, nack != 0, cnp != 0, h, nhop);
 }
 }
+
+// ------------------------------------------------------------------ the buffer rules (tr_mmu.cuh)
+#include "tr_mmu.cuh"
+
+extern "C" {
+
+unsigned rc_mmu_admit(unsigned buffer, MmuSwitch *sw, MmuPort *in, unsigned hdrm_cap, unsigned shift, MmuPort *out, unsigned size, int nvs)
+{
+    return mmu_admit(buffer, *sw, *in, hdrm_cap, shift, *out, size, nvs != 0);
+}
+
+// (u: the stream's next uniform number; *drawn: whether the rule took it)
+unsigned rc_mmu_release(unsigned buffer, MmuSwitch *sw, MmuPort *in, unsigned in_shift, MmuPort *out, unsigned size, int ecn, unsigned kmin,
+                        unsigned kmax, double pmax, int nvs, double u, int *drawn)
+{
+    *drawn = 0;
+    return mmu_release(buffer, *sw, *in, in_shift, *out, size, ecn != 0, kmin, kmax, pmax, nvs != 0, [u, drawn]() {
+        *drawn = 1;
+        return u;
+    });
+}
+
+void rc_int_stamp(unsigned long long *hops, unsigned short *nhop, long long now, unsigned long long tx_bytes, unsigned queue_bytes,
+                  unsigned long long bps, unsigned multi)
+{
+    uint64_t h[MAX_HOP];
+    for (int i = 0; i < MAX_HOP; i++)
+        h[i] = hops[i];
+    uint16_t n = *nhop;
+    int_stamp(h, n, now, tx_bytes, queue_bytes, bps, multi);
+    for (int i = 0; i < MAX_HOP; i++)
+        hops[i] = h[i];
+    *nhop = n;
+}
+
+int rc_ecmp_choice(int src, int dst, unsigned sport, int data, unsigned seed, int n) { return ecmp_choice(src, dst, sport, data != 0, seed, n); }
+}

@@ -25,3 +25,15 @@ __global__ void nic_rules(NicCase *c)
     c->out[2] = (unsigned)rx_check(c->P, c->rx, 0, 1000, 0);
     c->out[3] = ack_received(c->P, c->C, c->rate[0], c->send[0], 1000, false, true, c->hops, 1);
 }
+
+// (and the buffer rules of tr_mmu.cuh)
+#include "tr_mmu.cuh"
+
+__global__ void mmu_rules(MmuSwitch *sw, MmuPort *p, uint64_t *hops, unsigned *out)
+{
+    out[0] = mmu_admit(1 << 20, *sw, p[0], 100000, 2, p[1], 1000, false);
+    out[1] = mmu_release(1 << 20, *sw, p[0], 2, p[1], 1000, true, 100, 1000, 0.5, false, [] { return 0.25; });
+    uint16_t n = 0;
+    int_stamp(hops, n, 5000, 1 << 20, 4096, 100000000000ull, 1);
+    out[2] = (unsigned)ecmp_choice(1, 2, 10000, true, 7, 4) + n;
+}
