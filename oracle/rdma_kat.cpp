@@ -11,14 +11,21 @@
 // Cases: ns_seconds, tx times (ns-3.17 and ns-3.36), node addresses, ECMP hashes, INT hop words,
 // HPCC's per-hop utilisation, and sequences of events on one queue pair for DCQCN (CNPs and the
 // three timers), DCTCP (ACKs) and HPCC (ACKs with INT hops, fast react, sample feedback).
+#include <algorithm>
 #include <climits>
 #include <cstdio>
 #include <cstring>
+#include <vector>
 
 #include "rdma/rstep.cuh"
 
 thread_local twins_dim3 threadIdx, blockIdx, blockDim, gridDim;
+namespace rdma
+{
+// (the CPU build's island hooks: every tail node here is this process's own)
 uint64_t g_tail_side = 0;
+TailNode island_remote(uint64_t) { return TailNode{}; }
+} // namespace rdma
 
 namespace
 {
@@ -899,6 +906,176 @@ void kat_mmu()
         printf("],\"port\":%d,\"q\":%d}\n", port, q);
     }
 }
+// the event order: chains grown with the reference's cpush from flows' start chains, compared by its
+// ccmp (with and without a virtual push on either side); each case prints both chains' runs as
+// the cursor reads them, newest first
+void runs_json(const char *key, const rdma::Chain &c, uint32_t code0)
+{
+    rdma::RunCursor cur;
+    cur.init(c, code0);
+    printf("\"%s\":[", key);
+    for (int k = 0; cur.code; k++)
+    {
+        printf("%s[%u,%u]", k ? "," : "", cur.code, cur.left);
+        cur.left = 0;
+        cur.next();
+    }
+    printf("]");
+}
+
+void kat_chain()
+{
+    static rdma::TailNode tail[1 << 16];
+    static unsigned long long tail_cnt;
+    static unsigned long long memo_t[1 << 16], memo_walk[1 << 12];
+    rdma::g_tail.n = tail;
+    rdma::g_tail.cnt = &tail_cnt;
+    rdma::g_tail.mask = (1 << 16) - 1;
+    rdma::g_memo.t = memo_t;
+    rdma::g_memo.mask = (1 << 16) - 1;
+    rdma::g_memo.walk = memo_walk;
+    rdma::g_memo.walk_mask = (1 << 12) - 1;
+    for (int world = 0; world < 6; world++)
+    {
+        memset(memo_t, 0, sizeof memo_t);
+        memset(memo_walk, 0, sizeof memo_walk);
+        // flows' start chains as the reference's driver makes them: the gap since the previous
+        // start time, the flow's place among those starting together, StartApplication; their
+        // hashes 0 (a chain's hash covers what follows its start)
+        const int F = 12;
+        std::vector<rdma::Chain> pool;
+        int64_t prev_t = 0;
+        int prev_n = 0;
+        for (int f = 0; f < F;)
+        {
+            const int together = 1 + (int)below(3);
+            const int64_t t = prev_t + (int64_t)below(3) * 1000;
+            for (int m = 0; m < together && f < F; m++, f++)
+            {
+                rdma::Chain c{}, c2, c3;
+                rdma::cpush(&c2, rdma::ccode(t - prev_t, prev_n), c);
+                rdma::cpush(&c3, rdma::ccode(0, m), c2);
+                rdma::cpush(&c, rdma::ccode(0, 0), c3);
+                c.root = (uint32_t)(f + 1);
+                c.hash = 0;
+                for (int k = 0; k < rdma::NANC; k++)
+                    c.anc[k] = 0;
+                pool.push_back(c);
+            }
+            prev_n = together;
+            prev_t = t;
+        }
+        // the rank of the start chains (the reference's driver's rule): their leads newest first,
+        // the first differing one larger first, a shorter chain first, then the root
+        std::vector<uint32_t> rank(F);
+        {
+            auto leads = [](const rdma::Chain &c) {
+                std::vector<uint32_t> v;
+                for (int i = 0; i < rdma::RUNS && c.r[i].code; i++)
+                    for (uint32_t k = 0; k < c.r[i].cnt; k++)
+                        v.push_back(c.r[i].code >> rdma::CODE_ORD_BITS);
+                return v;
+            };
+            std::vector<int> idx(F);
+            for (int f = 0; f < F; f++)
+                idx[f] = f;
+            std::sort(idx.begin(), idx.end(), [&](int x, int y) {
+                const std::vector<uint32_t> lx = leads(pool[x]), ly = leads(pool[y]);
+                for (size_t i = 0; i < lx.size() && i < ly.size(); i++)
+                    if (lx[i] != ly[i])
+                        return lx[i] > ly[i];
+                if (lx.size() != ly.size())
+                    return lx.size() < ly.size();
+                return pool[x].root < pool[y].root;
+            });
+            for (int i = 0; i < F; i++)
+                rank[idx[i]] = (uint32_t)i;
+        }
+        rdma::Sim s{};
+        s.root_rank = rank.data();
+        printf("{\"fn\":\"chain_rank\",\"world\":%d,\"rank\":[", world);
+        for (int f = 0; f < F; f++)
+            printf("%s%u", f ? "," : "", rank[f]);
+        printf("]}\n");
+        // events: a child of a random event, with a lead from a small set (ties are common) and
+        // a small ordinal; lockstep lineages: the same pushes on two chains
+        const int64_t leads[6] = {0, 1, 80, 1000, 2048 + 1000, 4096};
+        for (int e = 0; e < 400; e++)
+        {
+            const size_t at = pool.size() < 40 || below(3) ? pool.size() - 1 - below(pool.size() < 40 ? pool.size() : 40) : below(pool.size());
+            const uint32_t code = rdma::ccode(leads[below(6)], (int)below(3));
+            rdma::Chain c;
+            rdma::cpush(&c, code, pool[at]);
+            pool.push_back(c);
+            if (below(4) == 0)
+            {
+                const size_t other = below(pool.size());
+                rdma::Chain d;
+                rdma::cpush(&d, code, pool[other]);
+                pool.push_back(d);
+            }
+        }
+        // lineages in lockstep: the same pushes on two flows' start chains (equal hashes where the
+        // starts' leads are equal)
+        std::vector<std::pair<size_t, size_t>> lock;
+        for (int i = 0; i < 30; i++)
+        {
+            const int f1 = (int)below(F), f2 = (f1 + 1 + (int)below(F - 1)) % F;
+            rdma::Chain a = pool[f1], b = pool[f2];
+            const int depth = 1 + (int)below(25);
+            for (int k = 0; k < depth; k++)
+            {
+                const uint32_t code = rdma::ccode(leads[below(6)], (int)below(3));
+                rdma::Chain a2, b2;
+                rdma::cpush(&a2, code, a);
+                rdma::cpush(&b2, below(8) ? code : rdma::ccode(leads[below(6)], (int)below(3)), b);
+                a = a2, b = b2;
+            }
+            pool.push_back(a);
+            pool.push_back(b);
+            lock.push_back({pool.size() - 2, pool.size() - 1});
+        }
+        // siblings at two depths: equal leads from a common ancestor, ordinals that differ at both
+        // (the deeper difference decides)
+        for (int i = 0; i < 30; i++)
+        {
+            const rdma::Chain &anc = pool[below(pool.size())];
+            const int64_t l1 = leads[below(6)], l2 = leads[below(6)];
+            const int o1 = (int)below(3), o2 = (int)below(3);
+            rdma::Chain a1, a2, b1, b2;
+            rdma::cpush(&a1, rdma::ccode(l1, o1), anc);
+            rdma::cpush(&a2, rdma::ccode(l2, o2), a1);
+            rdma::cpush(&b1, rdma::ccode(l1, (o1 + 1 + (int)below(2)) % 3), anc);
+            rdma::cpush(&b2, rdma::ccode(l2, (o2 + 1 + (int)below(2)) % 3), b1);
+            pool.push_back(a2);
+            pool.push_back(b2);
+            lock.push_back({pool.size() - 2, pool.size() - 1});
+        }
+        for (int i = 0; i < 200; i++)
+        {
+            size_t x = below(pool.size()), y = below(3) == 0 ? x : below(pool.size());
+            if (i < (int)lock.size())
+                x = lock[i].first, y = lock[i].second;
+            const uint32_t pa = below(3) == 0 ? rdma::ccode(leads[below(6)], (int)below(3)) : 0;
+            const uint32_t pb = below(3) == 0 ? (below(2) ? pa : rdma::ccode(leads[below(6)], (int)below(3))) : 0;
+            bool inexact = false, inexact_walk = false;
+            const int r = rdma::ccmp(s, pa, pool[x], pb, pool[y], &inexact);
+            const uint64_t ha = pa ? rdma::chash(pool[x].hash, pa) : pool[x].hash, hb = pb ? rdma::chash(pool[y].hash, pb) : pool[y].hash;
+            // the same comparison without the memo of decisions: the root-rank rule, else the walk
+            // (a memo key made of ancestors' hashes can be 0 for every chain that starts at a flow's
+            // start, whose hash is 0: there an unrelated decision answers)
+            const uint32_t ra = pool[x].root, rb = pool[y].root;
+            const int walk = ra && rb && ra != rb && ha == hb ? (rank[ra - 1] < rank[rb - 1] ? -1 : 1)
+                                                             : rdma::ccmp_walk(pa, pool[x], pb, pool[y], &inexact_walk);
+            printf("{\"fn\":\"chain\",\"world\":%d,\"root\":[%u,%u],\"hash\":[\"0x%016llx\",\"0x%016llx\"],", world, pool[x].root,
+                   pool[y].root, (unsigned long long)ha, (unsigned long long)hb);
+            runs_json("a", pool[x], pa);
+            printf(",");
+            runs_json("b", pool[y], pb);
+            printf(",\"order\":%d,\"walk\":%d,\"inexact\":%d}\n", r, walk, (int)(inexact || inexact_walk));
+        }
+    }
+}
 } // namespace
 
 int main()
@@ -912,5 +1089,6 @@ int main()
     kat_single();
     kat_nic();
     kat_mmu();
+    kat_chain();
     return 0;
 }

@@ -138,3 +138,20 @@ void rc_int_stamp(unsigned long long *hops, unsigned short *nhop, long long now,
 
 int rc_ecmp_choice(int src, int dst, unsigned sport, int data, unsigned seed, int n) { return ecmp_choice(src, dst, sport, data != 0, seed, n); }
 }
+
+// ------------------------------------------------------------------ the event order (tr_chain.cuh)
+#include "tr_chain.cuh"
+
+extern "C" {
+
+unsigned rc_event_code(long long lead, int ord) { return event_code(lead, ord); }
+unsigned long long rc_chain_hash(unsigned long long h, unsigned code) { return chain_hash(h, code); }
+
+// runs as (code, count) pairs, newest first
+int rc_chain_order(const unsigned *ra, int na, unsigned root_a, unsigned long long hash_a, const unsigned *rb, int nb, unsigned root_b,
+                   unsigned long long hash_b, const unsigned *root_rank)
+{
+    const ChainView a{(const ChainRun *)ra, na, root_a, hash_a}, b{(const ChainRun *)rb, nb, root_b, hash_b};
+    return chain_order(a, b, root_rank);
+}
+}

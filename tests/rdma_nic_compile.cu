@@ -37,3 +37,11 @@ __global__ void mmu_rules(MmuSwitch *sw, MmuPort *p, uint64_t *hops, unsigned *o
     int_stamp(hops, n, 5000, 1 << 20, 4096, 100000000000ull, 1);
     out[2] = (unsigned)ecmp_choice(1, 2, 10000, true, 7, 4) + n;
 }
+
+// (and the event order of tr_chain.cuh)
+#include "tr_chain.cuh"
+
+__global__ void chain_rules(const ChainRun *ra, const ChainRun *rb, const uint32_t *rank, int *out)
+{
+    out[0] = chain_order(ChainView{ra, 3, 1, chain_hash(0, event_code(1000, 0))}, ChainView{rb, 2, 2, 7}, rank);
+}
