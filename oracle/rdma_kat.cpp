@@ -645,6 +645,134 @@ void kat_nic()
         printf("}\n");
     }
 }
+// the NIC's dequeue (DequeueAndTransmit): its pick's next data frame goes out onto a one-slot link
+// buffer, or, with none ready, the next send is scheduled; and a queue pair's start
+void kat_dequeue()
+{
+    for (int i = 0; i < 400; i++)
+    {
+        Harness H;
+        static rdma::SndQP qps[8];
+        static int list[8];
+        static rdma::FlowInfo fi[8];
+        static rdma::Chain h_tc[1], h_ns[1];
+        static rdma::Pkt ackq[4];
+        static unsigned long long ev[64];
+        static unsigned pend[8];
+        static rdma::LFrame msg[4];
+        static int64_t first_sent[8];
+        for (int k = 0; k < 8; k++)
+            first_sent[k] = -1;
+        H.s.sent = first_sent;
+        H.s.qp = qps;
+        H.s.qps = list;
+        H.s.qps_cap = 8;
+        H.s.fi = fi;
+        H.s.h_tc = h_tc;
+        H.s.h_ns = h_ns;
+        H.s.ackq = ackq;
+        H.s.ackq_cap = 4;
+        H.s.ev = ev;
+        H.s.R = 1;
+        H.s.fD = rdma::fdiv_make(1000);
+        H.s.fpend = rdma::fdiv_make(8);
+        H.s.pend = pend;
+        H.s.msg = msg;
+        H.P.delay = 1000;
+        H.P.simai = (int)below(2);
+        H.P.seq_extra = H.P.simai ? 4 : 0;
+        H.P.int_size = below(2) ? 42 : 0;
+        H.P.mtu = 500 + (uint32_t)below(4000);
+        H.P.var_win = (int)below(2);
+        H.P.rate_bound = (int)below(2);
+        const rdma::FDiv one = rdma::fdiv_make(1);
+        rdma::OutBucket &o = H.c.obv[0];
+        o = rdma::OutBucket{};
+        o.nb = 1;
+        o.nb_m = one.m;
+        o.nb_sh = (uint8_t)one.sh;
+        o.nb_add = (uint8_t)one.add;
+        o.cap = 4;
+        H.c.ldl[0] = 1000;
+        msg[0] = rdma::LFrame{};
+        const int64_t now = 5000 + (int64_t)below(3);
+        H.c.now = now;
+        const int n = 1 + (int)below(8);
+        printf("{\"fn\":\"dequeue\",\"simai\":%d,\"int_size\":%d,\"mtu\":%u,\"var_win\":%d,\"rate_bound\":%d,\"now\":%lld,\"qps\":[",
+               H.P.simai, H.P.int_size, H.P.mtu, H.P.var_win, H.P.rate_bound, (long long)now);
+        for (int k = 0; k < 8; k++)
+        {
+            rdma::SndQP &q = qps[k];
+            q = rdma::SndQP{};
+            q.size = 1 + below(20000);
+            const int st = (int)below(4); // done / all sent, window-bound, late, ready
+            q.snd_una = st == 0 ? (below(2) ? q.size : below(q.size)) : below(q.size);
+            q.snd_nxt = st == 0 ? q.size : q.snd_una + below(q.size - q.snd_una);
+            q.max_rate = RATES[below(5)];
+            q.rate = 1000000000ull + below(q.max_rate - 1000000000ull);
+            q.win = st == 1 ? (uint32_t)(q.snd_nxt - q.snd_una + 1 - below(2)) : 0;
+            // (at times due exactly now, or one ns later)
+            q.next_avail = st == 2 ? now + 1 + (below(3) ? (int64_t)below(1000) : 0) : now - (below(3) ? (int64_t)below(1000) : 0);
+            fi[k] = rdma::FlowInfo{};
+            printf("%s[%llu,%llu,%llu,%llu,%llu,%u,%lld]", k ? "," : "", (unsigned long long)q.size, (unsigned long long)q.snd_nxt,
+                   (unsigned long long)q.snd_una, (unsigned long long)q.rate, (unsigned long long)q.max_rate, q.win, (long long)q.next_avail);
+        }
+        for (int k = 0; k < 8; k++)
+            list[k] = k;
+        rdma::Host &h = H.c.stv[0];
+        h.tc_at = -1;
+        h.ns_at = below(3) == 0 ? now + 5000 : -1;
+        h.qp_n = n;
+        h.rr = (int)below(16);
+        printf("],\"n\":%d,\"rr\":%d,\"ns_at\":%lld,", n, h.rr, (long long)h.ns_at);
+        rdma::h_dequeue(H.c);
+        const rdma::Pkt &f = msg[0].p;
+        const bool sent = f.size != 0;
+        printf("\"sent\":%d,\"flow\":%u,\"seq\":%u,\"size\":%u,\"rr_after\":%d,\"ns_at_after\":%lld,\"n_after\":%d,\"after\":[", (int)sent,
+               sent ? f.flow : 0, sent ? f.seq : 0, f.size, h.rr, (long long)h.ns_at, h.qp_n);
+        for (int k = 0; k < 8; k++)
+            printf("%s[%llu,%u,%lld]", k ? "," : "", (unsigned long long)qps[k].snd_nxt, qps[k].last_pkt, (long long)qps[k].next_avail);
+        printf("]}\n");
+    }
+    // a queue pair's start (the NIC busy: nothing is sent)
+    for (int i = 0; i < 60; i++)
+    {
+        Harness H;
+        static rdma::SndQP qps[1];
+        static int list[4];
+        static rdma::FlowInfo fi[1];
+        static rdma::LinkInfo li[2];
+        static unsigned long long ev[64];
+        H.s.qp = qps;
+        H.s.qps = list;
+        H.s.qps_cap = 4;
+        H.s.fi = fi;
+        H.s.li = li;
+        H.s.ev = ev;
+        H.P.cc = i % 3 == 0 ? 1 : i % 3 == 1 ? 3 : 8;
+        fi[0] = rdma::FlowInfo{};
+        fi[0].size = 1 + below(1u << 30);
+        fi[0].win = (uint32_t)below(1u << 20);
+        fi[0].base_rtt = below(100000);
+        li[1].bps = RATES[below(5)];
+        H.c.lk[0] = 1;
+        H.c.stv[0].tc_at = 1;
+        H.c.now = (int64_t)below(1ull << 30);
+        qps[0] = rdma::SndQP{};
+        qps[0].snd_nxt = 77; // (overwritten)
+        rdma::h_start(H.c, 0);
+        const rdma::SndQP &q = qps[0];
+        char a[24], b[24];
+        printf("{\"fn\":\"qp_start\",\"cc\":%d,\"size\":%llu,\"win\":%u,\"base_rtt\":%llu,\"bps\":%llu,\"now\":%lld,\"rate\":%llu,"
+               "\"max_rate\":%llu,\"target\":%llu,\"q_win\":%u,\"q_base_rtt\":%llu,\"alpha\":\"%s\",\"first_cnp\":%u,\"cur_rate\":%llu,"
+               "\"u\":\"%s\",\"next_avail\":%lld,\"snd_nxt\":%llu,\"listed\":%d}\n",
+               H.P.cc, (unsigned long long)fi[0].size, fi[0].win, (unsigned long long)fi[0].base_rtt, (unsigned long long)li[1].bps,
+               (long long)H.c.now, (unsigned long long)q.rate, (unsigned long long)q.max_rate, (unsigned long long)q.target, q.win,
+               (unsigned long long)q.base_rtt, hx(q.alpha, a), q.first_cnp, (unsigned long long)q.cur_rate, hx(q.u, b), (long long)q.next_avail,
+               (unsigned long long)q.snd_nxt, H.c.stv[0].qp_n);
+    }
+}
+
 // a switch of 4 ports for the buffer rules: every port busy transmitting unless a case frees one
 struct SwHarness
 {
@@ -1090,5 +1218,6 @@ int main()
     kat_nic();
     kat_mmu();
     kat_chain();
+    kat_dequeue();
     return 0;
 }

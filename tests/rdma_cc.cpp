@@ -155,3 +155,23 @@ int rc_chain_order(const unsigned *ra, int na, unsigned root_a, unsigned long lo
     return chain_order(a, b, root_rank);
 }
 }
+
+// (the NIC's start, next frame and next send: tr_nic.cuh)
+extern "C" {
+
+void rc_qp_start(const NicParams *P, QpRate *r, QpSend *q, unsigned long long size, unsigned long long bps, unsigned win, unsigned long long base_rtt,
+                 long long now)
+{
+    qp_start(*P, *r, *q, size, bps, win, base_rtt, now);
+}
+
+unsigned rc_next_data(const NicParams *P, QpRate *r, QpSend *q, long long now, int rate_bound, unsigned *seq)
+{
+    return next_data(*P, *r, *q, now, rate_bound != 0, seq);
+}
+
+long long rc_next_send_at(const NicParams *P, const int *list, int n, long long now, const QpRate *rates, const QpSend *sends)
+{
+    return next_send_at(*P, list, n, now, [rates, sends](int f) { return QpView{rates[f], sends[f]}; });
+}
+}

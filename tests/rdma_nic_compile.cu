@@ -24,6 +24,10 @@ __global__ void nic_rules(NicCase *c)
     c->out[1] = (unsigned)next_qindex(c->P, 0, 0, c->list, &c->n, 0, 0, [r, s](int f) { return QpView{r[f], s[f]}; });
     c->out[2] = (unsigned)rx_check(c->P, c->rx, 0, 1000, 0);
     c->out[3] = ack_received(c->P, c->C, c->rate[0], c->send[0], 1000, false, true, c->hops, 1);
+    uint32_t seq;
+    c->out[0] += next_data(c->P, c->rate[1], c->send[1], 0, true, &seq) + seq;
+    c->out[1] += (unsigned)next_send_at(c->P, c->list, c->n, 0, [r, s](int f) { return QpView{r[f], s[f]}; });
+    qp_start(c->P, c->rate[2], c->send[2], 1000, 100000000000ull, 1 << 20, 10000, 0);
 }
 
 // (and the buffer rules of tr_mmu.cuh)

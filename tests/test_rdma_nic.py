@@ -1,9 +1,10 @@
 """The RDMA model's NIC rules (twins_b200/csrc/tr_nic.cuh) against the reference's own answers
 (tests/golden/rdma_kat.json.gz, printed by the reference's src/rdma/rstep.cuh built for the CPU),
 bit for bit: frame sizes, the queue pairs' round robin with the window and pacing (and the removal
-of finished queue pairs), the receiver's go-back-N check with the ACK or NACK it queues, and the
-sender's handling of an ACK or NACK with DCQCN, HPCC and DCTCP. The rules run on the CPU here
-(g++); that the same header builds for sm_100a is checked with nvcc."""
+of finished queue pairs), a queue pair's start, the dequeue's next data frame and pacing or the
+NIC's next send, the receiver's go-back-N check with the ACK or NACK it queues, and the sender's
+handling of an ACK or NACK with DCQCN, HPCC and DCTCP. The rules run on the CPU here (g++); that
+the same headers build for sm_100a is checked with nvcc."""
 import ctypes as C
 import shutil
 import subprocess
@@ -45,6 +46,9 @@ def nic(tmp_path_factory):
         "rc_next_qindex": (C.c_int, [np_, C.c_uint, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int, C.c_longlong, qr, qs]),
         "rc_rx_check": (C.c_int, [np_, C.POINTER(RxQp), C.c_uint, C.c_uint, C.c_longlong]),
         "rc_ack_received": (C.c_uint, [np_, C.POINTER(CcParams), qr, qs, C.c_uint, C.c_int, C.c_int, C.POINTER(ull), C.c_int]),
+        "rc_qp_start": (None, [np_, qr, qs, ull, ull, C.c_uint, ull, C.c_longlong]),
+        "rc_next_data": (C.c_uint, [np_, qr, qs, C.c_longlong, C.c_int, C.POINTER(C.c_uint)]),
+        "rc_next_send_at": (C.c_longlong, [np_, C.POINTER(C.c_int), C.c_int, C.c_longlong, qr, qs]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -117,6 +121,49 @@ def test_ack_received(nic, kat, fn):
         assert started == r["started"], r
         n_done += s.done
     assert n_done > 10
+
+
+def test_dequeue(nic, kat):
+    """The NIC's dequeue: the round robin's pick sends its next data frame (sequence number, size,
+    snd_nxt, the pacing of its next send); with none ready, the next send is scheduled at the
+    earliest queue pair's time (unless one is pending)."""
+    sent = scheduled = 0
+    for r in kat["dequeue"]:
+        P = NicParams(mtu=r["mtu"], seq_extra=4 if r["simai"] else 0, int_size=r["int_size"], var_win=r["var_win"], ns336=r["simai"])
+        k = len(r["qps"])
+        rates, sends = (QpRate * k)(), (QpSend * k)()
+        for i, (size, nxt, una, rate, max_rate, win, na) in enumerate(r["qps"]):
+            rates[i].snd_nxt, rates[i].rate, rates[i].max_rate, rates[i].win = nxt, rate, max_rate, win
+            sends[i].size, sends[i].snd_una, sends[i].next_avail = size, una, na
+        lst = (C.c_int * k)(*range(k))
+        n = C.c_int(r["n"])
+        pick = nic.rc_next_qindex(C.byref(P), 0, 0, lst, C.byref(n), r["rr"], r["now"], rates, sends)
+        assert n.value == r["n_after"], r
+        if pick >= 0:
+            f = lst[pick]
+            seq = C.c_uint()
+            size = nic.rc_next_data(C.byref(P), C.byref(rates[f]), C.byref(sends[f]), r["now"], r["rate_bound"], C.byref(seq))
+            assert (r["sent"], r["flow"], r["seq"], r["size"], r["rr_after"]) == (1, f, seq.value, size, pick), r
+            sent += 1
+        else:
+            assert not r["sent"] and r["rr_after"] == r["rr"], r
+            t = nic.rc_next_send_at(C.byref(P), lst, n.value, r["now"], rates, sends)
+            want = r["ns_at"] if r["ns_at"] >= 0 or t < 0 else t
+            assert r["ns_at_after"] == want, r
+            scheduled += r["ns_at"] < 0 and t >= 0
+        assert [[rates[i].snd_nxt, sends[i].last_pkt, sends[i].next_avail] for i in range(k)] == r["after"], r
+    assert sent > 100 and scheduled > 10, (sent, scheduled)
+
+
+def test_qp_start(nic, kat):
+    for r in kat["qp_start"]:
+        P = NicParams(cc=r["cc"])
+        q, s = QpRate(snd_nxt=77), QpSend()
+        nic.rc_qp_start(C.byref(P), C.byref(q), C.byref(s), r["size"], r["bps"], r["win"], r["base_rtt"], r["now"])
+        got = (q.rate, q.max_rate, q.target, q.win, q.base_rtt, bits(q.alpha), q.first_cnp, q.cur_rate, bits(q.u), s.next_avail, q.snd_nxt, s.size)
+        want = (r["rate"], r["max_rate"], r["target"], r["q_win"], r["q_base_rtt"], r["alpha"], r["first_cnp"], r["cur_rate"], r["u"],
+                r["next_avail"], r["snd_nxt"], r["size"])
+        assert got == want, r
 
 
 def test_nic_rules_build_for_sm100a(tmp_path):

@@ -1,7 +1,8 @@
 // twins-b200: the RDMA model's NIC rules (RdmaHw, RdmaEgressQueue, RdmaQueuePair of the HPCC fork
 // of ns-3.17 that the reference's twins-rdma restates): frame sizes, the send window, the queue
 // pairs' round robin, the receiver's go-back-N check and the sender's handling of an ACK or NACK
-// with its congestion-control dispatch. Host and device functions of a queue pair's state; the
+// with its congestion-control dispatch, a queue pair's start, its next data frame and the NIC's
+// next send time. Host and device functions of a queue pair's state; the
 // caller owns queues, links, timers and event order. Bit-exact with the reference's functions
 // (src/rdma/rstep.cuh), which the oracle's known-answer vectors pin.
 #pragma once
@@ -119,6 +120,59 @@ TR_HD int next_qindex(const NicParams &P, uint32_t paused, int ackq_n, int *list
         *n = keep;
     }
     return pick;
+}
+
+// a queue pair starts (RdmaHw::AddQueuePair): the NIC's line rate as rate, line rate and DCQCN
+// target, the flow's window and base RTT, alpha 1 before a first CNP, HPCC's reference rate and
+// utilisation, sending from now (reference: src/rdma/rstep.cuh:1548-1587)
+TR_HD void qp_start(const NicParams &P, QpRate &r, QpSend &q, uint64_t size, uint64_t nic_bps, uint32_t win, uint64_t base_rtt, int64_t now)
+{
+    r = QpRate{};
+    q = QpSend{};
+    q.size = size;
+    r.rate = r.max_rate = r.target = nic_bps;
+    r.win = win;
+    r.base_rtt = base_rtt;
+    r.alpha = 1;
+    r.first_cnp = 1;
+    if (P.cc == 3)
+    {
+        r.cur_rate = nic_bps;
+        r.u = 1;
+    }
+    q.next_avail = now;
+}
+
+// the next data frame of a queue pair (RdmaHw::GetNxtPacket, PktSent, UpdateNextAvail): its
+// sequence number (*seq) and size; snd_nxt moves past its payload, and the next send waits its tx
+// time at the rate (or the line rate without RATE_BOUND) (reference: src/rdma/rstep.cuh:1162-1181)
+TR_HD uint32_t next_data(const NicParams &P, QpRate &r, QpSend &q, int64_t now, bool rate_bound, uint32_t *seq)
+{
+    const uint64_t left = bytes_left(r, q);
+    const uint32_t payload = left < P.mtu ? (uint32_t)left : P.mtu;
+    const uint32_t size = data_size(P, payload) & 0xFFFF;
+    *seq = (uint32_t)r.snd_nxt;
+    r.snd_nxt += payload;
+    q.last_pkt = size;
+    q.next_avail = now + tx_time(P.ns336 != 0, rate_bound ? r.rate : r.max_rate, size);
+    return size;
+}
+
+// no queue pair can send now: the earliest next_avail among list[0 .. n) (those with data left;
+// all of them under ns-3.36), when later than now, is the NIC's next send; else -1 (reference:
+// src/rdma/rstep.cuh:1182-1192)
+template <class Qp>
+TR_HD int64_t next_send_at(const NicParams &P, const int *list, int n, int64_t now, Qp qp)
+{
+    int64_t t = INT64_MAX;
+    for (int i = 0; i < n; i++)
+    {
+        const QpView v = qp(list[i]);
+        if (bytes_left(v.rate, v.send) == 0 && !P.ns336)
+            continue;
+        t = v.send.next_avail < t ? v.send.next_avail : t;
+    }
+    return t < INT64_MAX && t > now ? t : -1;
 }
 
 // the receiving queue pair's state (expected byte, last NACKed byte, NACK timer)
