@@ -32,3 +32,20 @@ def native_lib():
     from twins_b200 import build
     build.build()
     return build.SO
+
+
+@pytest.fixture(scope="session")
+def rdma_kat():
+    """The reference's known answers for the RDMA rules."""
+    import rdma_shim
+    return rdma_shim.load_kat()
+
+
+@pytest.fixture(scope="session")
+def rdma_lib(tmp_path_factory):
+    """The RDMA rules' C shim, built with g++ (the CPU build of the rules)."""
+    import shutil
+    import rdma_shim
+    if shutil.which("g++") is None:
+        pytest.skip("g++ is not here")
+    return rdma_shim.build(tmp_path_factory.mktemp("rdma_shim"))

@@ -7,86 +7,23 @@ sample feedback, pacing after a rate change). Every check runs twice: on the CPU
 with g++) and, marked gpu, on a B200 (the same header built with nvcc for sm_100a, each function run
 in a kernel)."""
 import ctypes as C
-import gzip
-import json
-import shutil
-import struct
-import subprocess
 
 import pytest
 
-from conftest import GOLDEN, ROOT
-
-SHIM = ROOT / "tests" / "rdma_cc.cpp"
-SHIM_GPU = ROOT / "tests" / "rdma_cc_gpu.cu"
-CSRC = ROOT / "twins_b200" / "csrc"
-U64, U32, U8 = C.c_uint64, C.c_uint32, C.c_uint8
-
-
-class QpRate(C.Structure):
-    _fields_ = [("rate", U64), ("max_rate", U64), ("target", U64), ("snd_nxt", U64), ("base_rtt", U64), ("win", U32),
-                ("alpha_cnp", U8), ("dec_cnp", U8), ("first_cnp", U8), ("rp_stage", U32), ("alpha", C.c_double),
-                ("last_update_seq", U32), ("inc_stage", C.c_int32), ("cur_rate", U64), ("u", C.c_double), ("hop", U64 * 5),
-                ("high_seq", U32), ("ecn_cnt", U32), ("batch", U32), ("ca_state", U32)]
-
-
-class CcParams(C.Structure):
-    _fields_ = [("g", C.c_double), ("rate_first_cnp", C.c_double), ("clamp", C.c_int), ("rpg_threshold", U32), ("rai", U64),
-                ("rhai", U64), ("min_rate", U64), ("dctcp_rai", U64), ("u_target", C.c_double), ("mi_thresh", U32),
-                ("sample_feedback", C.c_int), ("int_multi", U32), ("mtu", U32)]
-
-
-def dbl(h):
-    return struct.unpack("<d", struct.pack("<Q", int(h, 16)))[0]
-
-
-def bits(x):
-    return "0x%016x" % struct.unpack("<Q", struct.pack("<d", x))[0]
+import rdma_shim
+from rdma_shim import QpRate, bits, dbl, params, same, state, sub
 
 
 @pytest.fixture(scope="module", params=["cpu", pytest.param("gpu", marks=pytest.mark.gpu)])
 def rc(request, tmp_path_factory):
-    so = tmp_path_factory.mktemp("rc") / f"librc_{request.param}.so"
-    if request.param == "cpu":
-        if shutil.which("g++") is None:
-            pytest.skip("g++ is not here")
-        cmd = ["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-fno-fast-math", "-shared", "-fPIC", f"-I{CSRC}", "-o", str(so), str(SHIM)]
-    else:
-        cmd = ["nvcc", "-std=c++17", "-O2", "--fmad=false", "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-Xcompiler", "-fPIC",
-               f"-I{CSRC}", "-o", str(so), str(SHIM_GPU)]
-    subprocess.run(cmd, check=True)
-    lib = C.CDLL(str(so))
-    ull, qp, pp = C.c_ulonglong, C.POINTER(QpRate), C.POINTER(CcParams)
-    sig = {
-        "rc_failed": (C.c_int, []),
-        "rc_sizes": (None, [C.POINTER(C.c_int)]),
-        "rc_ns_seconds": (C.c_longlong, [C.c_double]),
-        "rc_tx": (C.c_longlong, [ull, C.c_uint, C.c_int]),
-        "rc_node_ip": (C.c_uint, [C.c_int]),
-        "rc_ecmp": (C.c_uint, [C.c_uint] * 4),
-        "rc_hop_make": (ull, [ull, ull, C.c_uint, ull, C.c_uint]),
-        "rc_hop_time_delta": (ull, [ull, ull]),
-        "rc_hop_bytes_delta": (ull, [ull, ull, C.c_uint]),
-        "rc_hop_u": (C.c_double, [ull, ull, C.c_uint, ull, C.c_uint, C.POINTER(ull)]),
-        "rc_dcqcn": (C.c_uint, [qp, pp, C.c_int]),
-        "rc_dctcp": (None, [qp, pp, C.c_uint, C.c_int]),
-        "rc_hpcc": (C.c_int, [qp, pp, C.POINTER(ull), C.c_int, C.c_int]),
-        "rc_paced": (C.c_longlong, [C.c_longlong, C.c_int, ull, ull, C.c_uint]),
-    }
-    for name, (res, args) in sig.items():
-        f = getattr(lib, name)
-        f.restype, f.argtypes = res, args
-    sizes = (C.c_int * 2)()
-    lib.rc_sizes(sizes)
-    assert (sizes[0], sizes[1]) == (C.sizeof(QpRate), C.sizeof(CcParams))
+    lib = request.getfixturevalue("rdma_lib") if request.param == "cpu" else rdma_shim.build(tmp_path_factory.mktemp("rc_gpu"), gpu=True)
     yield lib
     assert lib.rc_failed() == 0  # (a CUDA call of the device shim failed)
 
 
 @pytest.fixture(scope="module")
-def kat():
-    raw = json.loads(gzip.decompress((GOLDEN / "rdma_kat.json.gz").read_bytes()))
-    return {fn: [dict(zip(g["keys"], r)) for r in g["rows"]] for fn, g in raw.items()}
+def kat(rdma_kat):
+    return rdma_kat
 
 
 def test_time_and_tx(rc, kat):
@@ -117,44 +54,12 @@ def test_int_hops(rc, kat):
         assert bits(U) == r["U"] and dt == r["dt"], r
 
 
-def params(row):
-    P = CcParams()
-    for k in ("rpg_threshold", "rai", "rhai", "min_rate", "dctcp_rai", "mi_thresh", "sample_feedback", "int_multi", "mtu", "clamp"):
-        setattr(P, k, row[k])
-    for k in ("g", "rate_first_cnp", "u_target"):
-        setattr(P, k, dbl(row[k]))
-    return P
 
 
-def sub(row, pre):
-    return {k[len(pre):]: v for k, v in row.items() if k.startswith(pre)}
 
 
-def state(d):
-    """A queue pair's rate state from the fixture's fields (before or after an event)."""
-    q = QpRate()
-    for k in ("rate", "max_rate", "target", "snd_nxt", "base_rtt", "win", "alpha_cnp", "dec_cnp", "first_cnp", "rp_stage", "cur_rate",
-              "high_seq", "ecn_cnt", "batch", "ca_state"):
-        if k in d:
-            setattr(q, k, d[k])
-    q.alpha = dbl(d["alpha"])
-    if "u" in d:
-        q.u = dbl(d["u"])
-    q.last_update_seq, q.inc_stage = d["lus"], d["inc"]
-    q.hop[:] = d["hop"]
-    return q
 
 
-def same(q, d):
-    """The fields of q that the fixture's state holds, against it."""
-    want = dict(d)
-    got = {k: getattr(q, k) for k in want if hasattr(q, k) and k not in ("alpha", "u", "hop")}
-    got.update(alpha=bits(q.alpha), lus=q.last_update_seq, inc=q.inc_stage, hop=list(q.hop))
-    if "u" in want:
-        got["u"] = bits(q.u)
-    for k in ("next_avail", "last_pkt"):
-        got[k] = want[k]  # (pacing: checked by the caller)
-    return got == want
 
 
 def test_single_events(rc, kat):

@@ -6,28 +6,18 @@ and the chains' hashes against a fold of chain_hash over the events after their 
 The rules run on the CPU here (g++); tests/test_rdma_nic.py builds them for sm_100a."""
 import collections
 import ctypes as C
-import shutil
-import subprocess
 
 import pytest
 
-from test_rdma_cc import CSRC, SHIM, kat  # noqa: F401
+
+@pytest.fixture(scope="module")
+def ch(rdma_lib):
+    return rdma_lib
 
 
 @pytest.fixture(scope="module")
-def ch(tmp_path_factory):
-    if shutil.which("g++") is None:
-        pytest.skip("g++ is not here")
-    so = tmp_path_factory.mktemp("chain") / "libchain.so"
-    subprocess.run(["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-fno-fast-math", "-shared", "-fPIC", f"-I{CSRC}", "-o", str(so), str(SHIM)],
-                   check=True)
-    lib = C.CDLL(str(so))
-    u32p = C.POINTER(C.c_uint)
-    lib.rc_event_code.restype, lib.rc_event_code.argtypes = C.c_uint, [C.c_longlong, C.c_int]
-    lib.rc_chain_hash.restype, lib.rc_chain_hash.argtypes = C.c_ulonglong, [C.c_ulonglong, C.c_uint]
-    lib.rc_chain_order.restype = C.c_int
-    lib.rc_chain_order.argtypes = [u32p, C.c_int, C.c_uint, C.c_ulonglong, u32p, C.c_int, C.c_uint, C.c_ulonglong, u32p]
-    return lib
+def kat(rdma_kat):
+    return rdma_kat
 
 
 def flat_runs(runs):

@@ -5,44 +5,20 @@ through the reserve, the shared pool and the headroom, drops, PAUSE and RESUME, 
 dequeue with the port's random stream, the INT stamp of HPCC data, and the egress port of data
 and ACKs. The rules run on the CPU here (g++); tests/test_rdma_nic.py builds them for sm_100a."""
 import ctypes as C
-import shutil
-import subprocess
 
 import pytest
 
-from test_rdma_cc import CSRC, SHIM, bits, dbl, kat  # noqa: F401
-
-U32 = C.c_uint32
-
-
-class MmuPort(C.Structure):
-    _fields_ = [("ing", U32), ("hdrm", U32), ("egr", U32), ("paused", U32)]
-
-
-class MmuSwitch(C.Structure):
-    _fields_ = [("shared_used", U32), ("total_hdrm", U32), ("total_rsrv", U32)]
+from rdma_shim import MmuPort, MmuSwitch, dbl
 
 
 @pytest.fixture(scope="module")
-def mmu(tmp_path_factory):
-    if shutil.which("g++") is None:
-        pytest.skip("g++ is not here")
-    so = tmp_path_factory.mktemp("mmu") / "libmmu.so"
-    subprocess.run(["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-fno-fast-math", "-shared", "-fPIC", f"-I{CSRC}", "-o", str(so), str(SHIM)],
-                   check=True)
-    lib = C.CDLL(str(so))
-    sw, pt, ull = C.POINTER(MmuSwitch), C.POINTER(MmuPort), C.c_ulonglong
-    sig = {
-        "rc_mmu_admit": (C.c_uint, [C.c_uint, sw, pt, C.c_uint, C.c_uint, pt, C.c_uint, C.c_int]),
-        "rc_mmu_release": (C.c_uint, [C.c_uint, sw, pt, C.c_uint, pt, C.c_uint, C.c_int, C.c_uint, C.c_uint, C.c_double, C.c_int, C.c_double,
-                                      C.POINTER(C.c_int)]),
-        "rc_int_stamp": (None, [C.POINTER(ull), C.POINTER(C.c_ushort), C.c_longlong, ull, C.c_uint, ull, C.c_uint]),
-        "rc_ecmp_choice": (C.c_int, [C.c_int, C.c_int, C.c_uint, C.c_int, C.c_uint, C.c_int]),
-    }
-    for name, (res, args) in sig.items():
-        f = getattr(lib, name)
-        f.restype, f.argtypes = res, args
-    return lib
+def mmu(rdma_lib):
+    return rdma_lib
+
+
+@pytest.fixture(scope="module")
+def kat(rdma_kat):
+    return rdma_kat
 
 
 def ports(r, key):

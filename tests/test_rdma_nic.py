@@ -12,51 +12,19 @@ import subprocess
 import pytest
 
 from conftest import ROOT
-from test_rdma_cc import CSRC, SHIM, CcParams, QpRate, bits, dbl, kat, params, same, state, sub  # noqa: F401
+from rdma_shim import CSRC, NicParams, QpRate, QpSend, RxQp, bits, params, same, state, sub
 
-U64, U32, U8 = C.c_uint64, C.c_uint32, C.c_uint8
 RC_NIC = ROOT / "tests" / "rdma_nic_compile.cu"
 
 
-class NicParams(C.Structure):
-    _fields_ = [("mtu", U32), ("ack_interval", U32), ("chunk", U32), ("nack_interval", C.c_int64), ("seq_extra", U32), ("int_size", C.c_int),
-                ("var_win", C.c_int), ("ack_high_prio", C.c_int), ("cc", C.c_int), ("fast_react", C.c_int), ("ns336", C.c_int)]
-
-
-class QpSend(C.Structure):
-    _fields_ = [("size", U64), ("snd_una", U64), ("next_avail", C.c_int64), ("last_pkt", U32), ("done", U8)]
-
-
-class RxQp(C.Structure):
-    _fields_ = [("expected", U32), ("last_nack", U32), ("nack_timer", C.c_int64)]
+@pytest.fixture(scope="module")
+def nic(rdma_lib):
+    return rdma_lib
 
 
 @pytest.fixture(scope="module")
-def nic(tmp_path_factory):
-    if shutil.which("g++") is None:
-        pytest.skip("g++ is not here")
-    so = tmp_path_factory.mktemp("nic") / "libnic.so"
-    subprocess.run(["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-fno-fast-math", "-shared", "-fPIC", f"-I{CSRC}", "-o", str(so), str(SHIM)],
-                   check=True)
-    lib = C.CDLL(str(so))
-    ull, np_, qr, qs = C.c_ulonglong, C.POINTER(NicParams), C.POINTER(QpRate), C.POINTER(QpSend)
-    sig = {
-        "rc_nic_sizes": (None, [C.POINTER(C.c_int)]),
-        "rc_frame_sizes": (None, [np_, C.c_uint, C.POINTER(C.c_uint)]),
-        "rc_next_qindex": (C.c_int, [np_, C.c_uint, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int, C.c_longlong, qr, qs]),
-        "rc_rx_check": (C.c_int, [np_, C.POINTER(RxQp), C.c_uint, C.c_uint, C.c_longlong]),
-        "rc_ack_received": (C.c_uint, [np_, C.POINTER(CcParams), qr, qs, C.c_uint, C.c_int, C.c_int, C.POINTER(ull), C.c_int]),
-        "rc_qp_start": (None, [np_, qr, qs, ull, ull, C.c_uint, ull, C.c_longlong]),
-        "rc_next_data": (C.c_uint, [np_, qr, qs, C.c_longlong, C.c_int, C.POINTER(C.c_uint)]),
-        "rc_next_send_at": (C.c_longlong, [np_, C.POINTER(C.c_int), C.c_int, C.c_longlong, qr, qs]),
-    }
-    for name, (res, args) in sig.items():
-        f = getattr(lib, name)
-        f.restype, f.argtypes = res, args
-    sizes = (C.c_int * 3)()
-    lib.rc_nic_sizes(sizes)
-    assert list(sizes) == [C.sizeof(NicParams), C.sizeof(QpSend), C.sizeof(RxQp)]
-    return lib
+def kat(rdma_kat):
+    return rdma_kat
 
 
 def test_frame_sizes(nic, kat):
