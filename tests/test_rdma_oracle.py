@@ -1,0 +1,56 @@
+"""The RDMA oracle's fixtures (tests/golden/rdma/: small worlds under DCQCN, HPCC and DCTCP, with
+ECN marks and PFC pauses, and the flow completion times that the reference's twins-rdma gives
+for them, run on the CPU): every flow completes, each output line matches its flow, and, where
+the CPU build of the reference is here (`make -C oracle ref-rdma-cpu`), it reproduces every
+fixture exactly."""
+import json
+import shutil
+import subprocess
+
+import pytest
+
+from conftest import GOLDEN, ROOT
+
+RDMA = GOLDEN / "rdma"
+EXE = ROOT / "oracle" / "_ref" / "twins-rdma-cpu"
+
+
+def cases():
+    return json.loads((RDMA / "manifest.json").read_text())
+
+
+def flows(name):
+    lines = (RDMA / f"{name}.csv").read_text().splitlines()[1:]
+    return [tuple(int(x) for x in l.split(",")) for l in lines]
+
+
+def fct(path):
+    return [tuple(int(x) for x in l.split()) for l in path.read_text().splitlines() if l.strip()]
+
+
+@pytest.mark.parametrize("case", cases(), ids=lambda c: c["name"])
+def test_fixture_consistent(case):
+    fl, out = flows(case["name"]), fct(RDMA / f"{case['name']}.fct")
+    assert len(fl) == len(out) == case["flows"]
+    for i, ((src, dst, size, start), (fid, start_ns, fct_ns)) in enumerate(zip(fl, out)):
+        assert fid == i and start_ns == start and fct_ns > 0
+    assert "overflows: tx 0 queue 0 ackq 0 qps 0 due 0" in case["counters"]
+
+
+def test_coverage():
+    cs = cases()
+    counters = " ".join(c["counters"] for c in cs)
+    assert {"dcqcn", "hpcc", "dctcp"} <= {n for c in cs for n in c["name"].split("_")}
+    assert any(" pauses 0 " not in c["counters"] for c in cs) and any(" marks 0 " not in c["counters"] for c in cs), counters
+
+
+@pytest.mark.skipif(not EXE.exists(), reason="the CPU build of the reference's twins-rdma (make -C oracle ref-rdma-cpu) is not here")
+@pytest.mark.parametrize("case", cases(), ids=lambda c: c["name"])
+def test_oracle_reproduces(case, tmp_path):
+    name = case["name"]
+    for ext in ("cfg", "topo", "csv"):
+        shutil.copy(RDMA / f"{name}.{ext}", tmp_path)
+    r = subprocess.run([str(EXE), f"{name}.cfg", f"--topo={name}.topo", f"--flows={name}.csv", f"--out={name}.fct"], cwd=tmp_path,
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-500:]
+    assert fct(tmp_path / f"{name}.fct") == fct(RDMA / f"{name}.fct")
