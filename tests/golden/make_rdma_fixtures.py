@@ -90,6 +90,12 @@ def cases():
     # PFC: a small buffer under an incast
     out.append(("ft4_incast15_hpcc_pfc", ft4, incast(rng, 16, 15, 300_000), {"CC_MODE": "3", "BUFFER_SIZE": "1"}))
     out.append(("ft4_incast15_dcqcn_pfc", ft4, incast(rng, 16, 15, 300_000), {"CC_MODE": "1", "BUFFER_SIZE": "1"}))
+    # FatTree k=8 (128 hosts): 600 flows, and a 32-sender incast
+    ft8 = fattree(8)
+    for cc, name in [(1, "dcqcn"), (3, "hpcc"), (8, "dctcp")]:
+        out.append((f"ft8_uniform600_{name}", ft8, uniform(rng, 128, 600, 400_000), {"CC_MODE": str(cc)}))
+    out.append(("ft8_incast32_hpcc", ft8, incast(rng, 128, 32, 262_144), {"CC_MODE": "3"}))
+    out.append(("ft8_incast32_dcqcn_pfc", ft8, incast(rng, 128, 32, 262_144), {"CC_MODE": "1", "BUFFER_SIZE": "2"}))
     return out
 
 

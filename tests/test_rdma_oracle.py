@@ -1,4 +1,5 @@
-"""The RDMA oracle's fixtures (tests/golden/rdma/: small worlds under DCQCN, HPCC and DCTCP, with
+"""The RDMA oracle's fixtures (tests/golden/rdma/: FatTree k=4 and k=8 and leaf-spine worlds under
+DCQCN, HPCC and DCTCP, with
 ECN marks and PFC pauses, and the flow completion times that the reference's twins-rdma gives
 for them, run on the CPU): every flow completes, each output line matches its flow, and, where
 the CPU build of the reference is here (`make -C oracle ref-rdma-cpu`), it reproduces every
