@@ -55,3 +55,16 @@ def test_oracle_reproduces(case, tmp_path):
                        capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-500:]
     assert fct(tmp_path / f"{name}.fct") == fct(RDMA / f"{name}.fct")
+
+
+@pytest.mark.skipif(not EXE.exists(), reason="the CPU build of the reference's twins-rdma (make -C oracle ref-rdma-cpu) is not here")
+def test_oracle_refuses_wide_switches(tmp_path):
+    """Switches of more than 32 ports run in the GPU's wide blocks: the CPU build refuses them."""
+    hpl = 40
+    links = [f"link h{l * hpl + j} s{l}\n" for l in range(2) for j in range(hpl)] + [f"link s{l} s{2 + s}\n" for l in range(2) for s in range(2)]
+    (tmp_path / "w.topo").write_text(f"hosts {2 * hpl}\nswitches 4\n" + "".join(links))
+    (tmp_path / "w.csv").write_text("src,dst,flow_size,start_ns\n0,79,10000,1000\n")
+    shutil.copy(RDMA / "ft4_incast15_hpcc.cfg", tmp_path / "w.cfg")
+    r = subprocess.run([str(EXE), "w.cfg", "--topo=w.topo", "--flows=w.csv", "--out=w.fct"], cwd=tmp_path, capture_output=True, text=True,
+                       timeout=120)
+    assert r.returncode == 3 and "wide switches" in r.stderr
