@@ -5,10 +5,13 @@ own src/rdma/rmain.cu). They pin the RDMA model where no GPU is at hand.
 
 Each case: <name>.cfg (the reference's KEY VALUE config), <name>.topo, <name>.csv (flows:
 src,dst,flow_size,start_ns), <name>.fct (the reference's output: id start_ns fct_ns), and a line
-in manifest.json with the reference's counters line.
+in manifest.json with the reference's counters line and, per field of the world the reference's
+build_world makes of it (oracle/_ref/rdma_world_kat: parameters, wiring, ECMP routes, port
+configurations), the SHA-256 of the field's JSON.
 
     python tests/golden/make_rdma_fixtures.py
 """
+import hashlib
 import json
 import subprocess
 from pathlib import Path
@@ -17,6 +20,7 @@ import numpy as np
 
 ROOT = Path(__file__).resolve().parents[2]
 EXE = ROOT / "oracle" / "_ref" / "twins-rdma-cpu"
+WORLD_KAT = ROOT / "oracle" / "_ref" / "rdma_world_kat"
 OUT = Path(__file__).resolve().parent / "rdma"
 
 # the HPCC fork's parameters, as its example configuration sets them (the file format is the
@@ -99,8 +103,15 @@ def cases():
     return out
 
 
+def world_digests(name):
+    """The reference's world of a case, each field's JSON digested."""
+    r = subprocess.run([str(WORLD_KAT), f"{name}.cfg", f"{name}.topo", f"{name}.csv"], cwd=OUT, capture_output=True, text=True, timeout=600,
+                       check=True)
+    return {k: hashlib.sha256(json.dumps(v, separators=(",", ":")).encode()).hexdigest() for k, v in json.loads(r.stdout).items()}
+
+
 def main():
-    subprocess.run(["make", "-C", str(ROOT / "oracle"), "ref-rdma-cpu"], check=True)
+    subprocess.run(["make", "-C", str(ROOT / "oracle"), "ref-rdma-cpu", "ref-rdma-world"], check=True)
     OUT.mkdir(exist_ok=True)
     manifest = []
     for name, topo, flows, over in cases():
@@ -112,7 +123,7 @@ def main():
                            capture_output=True, text=True, timeout=600)
         assert r.returncode == 0, (name, r.returncode, r.stderr[-500:])
         counters = [x for x in (r.stdout + r.stderr).splitlines() if x.startswith("drops ")]
-        manifest.append({"name": name, "flows": len(flows), "counters": counters[-1] if counters else ""})
+        manifest.append({"name": name, "flows": len(flows), "counters": counters[-1] if counters else "", "world": world_digests(name)})
         print(name, manifest[-1]["counters"])
     (OUT / "manifest.json").write_text(json.dumps(manifest, indent=1) + "\n")
 
