@@ -3,7 +3,8 @@
 // Built by `make -C oracle ref-rdma-world` from the reference's own src/rdma/rmain.cu (its main
 // renamed away; the CPU build of rdma_cpu/rdma/island.h): for a config, a topology file and a flow
 // file, it runs the reference's build_world and prints, as one JSON object, the world's parameters,
-// its link wiring, its switches' ECMP route tables and port configurations, and maxRtt / maxBdp.
+// its link wiring, its switches' ECMP route tables and port configurations, maxRtt / maxBdp, and
+// its flows (in file order, with their ports, start order and start chains) and start lists.
 // tests/golden/make_rdma_fixtures.py stores a digest of each field per world, against which
 // tests/test_rdma_world.py checks twins_b200/csrc/tr_world.h.
 #define main twins_rdma_main
@@ -62,7 +63,22 @@ int main(int argc, char **argv)
         printf("%s\"%a\"", i ? "," : "", c.pmax);
     }
     printf("],");
-    arr("pcfg", pc, false);
+    arr("pcfg", pc);
+    // flows: src, dst, size, start, sport, order, win, base_rtt, snic, rnic, then their start
+    // chains' root and runs (code, count), newest first
+    printf("\"flows\":[");
+    for (size_t i = 0; i < w.fi.size(); i++)
+    {
+        const FlowInfo &x = w.fi[i];
+        printf("%s[%d,%d,%llu,%lld,%u,%u,%u,%llu,%u,%u,%u", i ? "," : "", x.src, x.dst, (unsigned long long)x.size, (long long)x.start, x.sport,
+               x.order, x.win, (unsigned long long)x.base_rtt, x.snic, x.rnic, x.start_chain.root);
+        for (int r = 0; r < RUNS && x.start_chain.r[r].code; r++)
+            printf(",%u,%u", x.start_chain.r[r].code, x.start_chain.r[r].cnt);
+        printf("]");
+    }
+    printf("],");
+    arr("start_list", w.start_list);
+    arr("start_off", w.start_off, false);
     printf("}\n");
     return 0;
 }

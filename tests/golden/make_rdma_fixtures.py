@@ -100,6 +100,11 @@ def cases():
         out.append((f"ft8_uniform600_{name}", ft8, uniform(rng, 128, 600, 400_000), {"CC_MODE": str(cc)}))
     out.append(("ft8_incast32_hpcc", ft8, incast(rng, 128, 32, 262_144), {"CC_MODE": "3"}))
     out.append(("ft8_incast32_dcqcn_pfc", ft8, incast(rng, 128, 32, 262_144), {"CC_MODE": "1", "BUFFER_SIZE": "2"}))
+    # flows that start together (one ScheduleFlowInputs each time) and host pairs with several flows
+    same = [(int(a), int(b), int(rng.integers(1000, 100_000)), int(1000 * rng.integers(1, 4)))
+            for a, b in (rng.choice(16, 2, replace=False) for _ in range(60))]
+    same += [(3, 7, 5000, 2000)] * 4
+    out.append(("ft4_sametime64_dcqcn", ft4, same, {"CC_MODE": "1"}))
     return out
 
 

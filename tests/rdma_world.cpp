@@ -36,13 +36,13 @@ void arr(const char *key, const std::vector<T> &v, bool comma = true)
 
 extern "C" {
 
-// the world of a configuration and a topology (100 Gb/s, 1 us links) as JSON; NULL and the
-// reason in *err where it is refused
-const char *rw_world(const char *config, const char *topo, const char **err)
+// the world of a configuration, a topology (100 Gb/s, 1 us links) and a flow file as JSON; NULL
+// and the reason in *err where it is refused
+const char *rw_world(const char *config, const char *topo, const char *flows, const char **err)
 {
     RdmaWorld w;
     out.clear();
-    if (!build_rdma_world(w, parse_rdma_config(config), topo, 100000000000ull, 1000))
+    if (!build_rdma_world(w, parse_rdma_config(config), topo, 100000000000ull, 1000) || !build_rdma_flows(w, flows))
     {
         out = w.error;
         *err = out.c_str();
@@ -74,7 +74,20 @@ const char *rw_world(const char *config, const char *topo, const char **err)
         add("%s\"%a\"", i ? "," : "", c.pmax);
     }
     add("],");
-    arr("pcfg", pc, false);
+    arr("pcfg", pc);
+    add("\"flows\":[");
+    for (size_t i = 0; i < w.flows.size(); i++)
+    {
+        const RdmaFlow &x = w.flows[i];
+        add("%s[%d,%d,%llu,%lld,%u,%u,%u,%llu,%u,%u,%u", i ? "," : "", x.src, x.dst, (unsigned long long)x.size, (long long)x.start, x.sport,
+            x.order, x.win, (unsigned long long)x.base_rtt, x.snic, x.rnic, x.root);
+        for (auto &r : x.runs)
+            add(",%u,%u", r.first, r.second);
+        add("]");
+    }
+    add("],");
+    arr("start_list", w.start_list);
+    arr("start_off", w.start_off, false);
     add("}");
     *err = nullptr;
     return out.c_str();

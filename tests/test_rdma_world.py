@@ -1,8 +1,9 @@
 """The RDMA world set-up (twins_b200/csrc/tr_world.h) against the reference's build_world on every
 RDMA fixture world (tests/golden/rdma/manifest.json holds, per world, the SHA-256 of each field of
 the reference's world, printed by oracle/rdma_world_kat.cpp): the HPCC fork's parameters from the
-config, the link wiring and port numbering, the switches' ECMP route tables, maxRtt / maxBdp, and
-every switch port's headroom, PFC threshold shift and ECN thresholds."""
+config, the link wiring and port numbering, the switches' ECMP route tables, maxRtt / maxBdp,
+every switch port's headroom, PFC threshold shift and ECN thresholds, and the flows (source ports,
+start order, start chains) with the hosts' start lists."""
 import ctypes as C
 import hashlib
 import json
@@ -25,13 +26,13 @@ def rw(tmp_path_factory):
     so = tmp_path_factory.mktemp("rw") / "librw.so"
     subprocess.run(["g++", "-std=c++17", "-O1", "-shared", "-fPIC", f"-I{CSRC}", "-o", str(so), str(SHIM)], check=True)
     lib = C.CDLL(str(so))
-    lib.rw_world.restype, lib.rw_world.argtypes = C.c_char_p, [C.c_char_p, C.c_char_p, C.POINTER(C.c_char_p)]
+    lib.rw_world.restype, lib.rw_world.argtypes = C.c_char_p, [C.c_char_p, C.c_char_p, C.c_char_p, C.POINTER(C.c_char_p)]
     return lib
 
 
-def world(rw, cfg, topo):
+def world(rw, cfg, topo, flows="src,dst,flow_size,start_ns\n0,1,1000,1000\n"):
     err = C.c_char_p()
-    out = rw.rw_world(cfg.encode(), topo.encode(), C.byref(err))
+    out = rw.rw_world(cfg.encode(), topo.encode(), flows.encode(), C.byref(err))
     return (json.loads(out), None) if out is not None else (None, err.value.decode())
 
 
@@ -42,7 +43,7 @@ def cases():
 @pytest.mark.parametrize("case", cases(), ids=lambda c: c["name"])
 def test_world_equals_reference(rw, case):
     name = case["name"]
-    w, err = world(rw, (RDMA / f"{name}.cfg").read_text(), (RDMA / f"{name}.topo").read_text())
+    w, err = world(rw, (RDMA / f"{name}.cfg").read_text(), (RDMA / f"{name}.topo").read_text(), (RDMA / f"{name}.csv").read_text())
     assert err is None, err
     got = {k: hashlib.sha256(json.dumps(v, separators=(",", ":")).encode()).hexdigest() for k, v in w.items()}
     assert got.keys() == case["world"].keys()
@@ -56,6 +57,7 @@ def test_world_refusals(rw):
     assert "CC_MODE" in world(rw, cfg.replace("CC_MODE 3", "CC_MODE 2"), topo)[1]
     assert "L2_ACK_INTERVAL" in world(rw, cfg.replace("L2_ACK_INTERVAL 1", "L2_ACK_INTERVAL 0"), topo)[1]
     assert "one link" in world(rw, cfg, topo + "link h0 s1\n")[1]
+    assert "not hosts" in world(rw, cfg, topo, "src,dst,flow_size,start_ns\n0,16,1000,1000\n")[1]
     # HPCC's INT header holds 5 hops: a chain of 7 switches between two hosts is refused
     chain = "hosts 2\nswitches 7\nlink h0 s0\n" + "".join(f"link s{i} s{i + 1}\n" for i in range(6)) + "link h1 s6\n"
     assert "5 switches" in world(rw, cfg, chain)[1]

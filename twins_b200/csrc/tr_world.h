@@ -2,12 +2,14 @@
 // KEY VALUE configuration, the topology (TwiNS's "hosts / switches / link" format), the link
 // wiring and port numbering, the switches' ECMP route tables (ns-3's CalculateRoute: BFS from each
 // host), maxRtt / maxBdp (the window and base RTT of every flow under GLOBAL_T), and each switch
-// port's PFC headroom and threshold shift and ECN thresholds. Equal, field by field, to the
-// reference's build_world (src/rdma/rmain.cu:364-720), which the oracle's digests pin.
+// port's PFC headroom and threshold shift and ECN thresholds; and the flows with their source ports,
+// start order and start chains. Equal, field by field, to the reference's build_world
+// (src/rdma/rmain.cu:364-1021), which the oracle's digests pin.
 #pragma once
 #include <algorithm>
 #include <climits>
 #include <cstdint>
+#include <cstdio>
 #include <cstdlib>
 #include <map>
 #include <sstream>
@@ -18,6 +20,17 @@ namespace tr
 {
 
 using RdmaConfig = std::map<std::string, std::vector<std::string>>;
+
+// an event's code in a chain: (lead + 1) << 5 | (31 - ordinal), both saturating (as
+// tr_chain.cuh's event_code, which device code uses)
+inline uint32_t start_code(int64_t lead, int ord)
+{
+    uint64_t l = (uint64_t)lead + 1;
+    const uint64_t most = (1ull << 27) - 2;
+    if (l > most)
+        l = most;
+    return (uint32_t)(l << 5 | (31u - (uint32_t)(ord < 31 ? ord : 31)));
+}
 
 // "KEY v1 v2 ..." per line (reference: src/rdma/rmain.cu:111-135)
 inline RdmaConfig parse_rdma_config(const std::string &text)
@@ -78,6 +91,20 @@ struct RdmaPortCfg
     double pmax;
 };
 
+// a flow as the set-up leaves it: its ends, size and start, source port (per host pair from 10000,
+// in start order), place in start order, window and base RTT, devices, and the chain of its
+// StartApplication (root = 1 + its place; runs newest first, as tr_chain.cuh reads them)
+struct RdmaFlow
+{
+    int src, dst;
+    uint64_t size;
+    int64_t start;
+    uint32_t sport, order, win;
+    uint64_t base_rtt;
+    uint32_t snic, rnic, root;
+    std::vector<std::pair<uint32_t, uint32_t>> runs;
+};
+
 struct RdmaWorld
 {
     RdmaWorldParams P{};
@@ -88,8 +115,85 @@ struct RdmaWorld
     std::vector<uint32_t> rt;                                       // [S H] (first port, count)
     std::vector<uint8_t> rtp;                                       // the route tables' ports
     std::vector<RdmaPortCfg> pcfg;                                  // every switch's ports in turn
+    std::vector<RdmaFlow> flows;                                    // in file order
+    std::vector<int> start_list, start_off;                         // per host, its flows in start order
     std::string error;
 };
+
+// The flows of a flow file ("src,dst,flow_size,start_ns" after a header line; lines that do not
+// parse are skipped) in a world made by build_rdma_world (reference: src/rdma/rmain.cu:842-1021,
+// for hosts of one link). ns-3 starts them through one ScheduleFlowInputs event per start time,
+// each scheduled by the previous one (or by main), then Application::Start, then StartApplication:
+// their start chains.
+inline bool build_rdma_flows(RdmaWorld &w, const std::string &csv)
+{
+    std::istringstream f(csv);
+    std::string line;
+    std::getline(f, line);
+    w.flows.clear();
+    while (std::getline(f, line))
+    {
+        unsigned a, b;
+        unsigned long long sz, st;
+        if (sscanf(line.c_str(), "%u,%u,%llu,%llu", &a, &b, &sz, &st) != 4)
+            continue;
+        RdmaFlow x{};
+        x.src = (int)a, x.dst = (int)b, x.size = sz, x.start = (int64_t)st;
+        w.flows.push_back(x);
+    }
+    const int F = (int)w.flows.size(), H = w.H;
+    for (RdmaFlow &x : w.flows)
+    {
+        if (x.src >= H || x.dst >= H)
+            return w.error = "a flow between nodes that are not hosts", false;
+        x.win = w.P.win;
+        x.base_rtt = w.P.base_rtt;
+    }
+    std::vector<int> order(F);
+    for (int i = 0; i < F; i++)
+        order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return w.flows[a].start < w.flows[b].start; });
+    std::map<std::pair<int, int>, uint32_t> port;
+    int64_t prev_t = 0;
+    int prev_n = 0, k = 0;
+    for (int i = 0; i < F;)
+    {
+        int j = i;
+        while (j < F && w.flows[order[j]].start == w.flows[order[i]].start)
+            j++;
+        const int64_t t = w.flows[order[i]].start;
+        for (int m = i; m < j; m++)
+        {
+            RdmaFlow &x = w.flows[order[m]];
+            auto it = port.emplace(std::make_pair(x.src, x.dst), 10000u).first;
+            x.sport = it->second++;
+            x.order = (uint32_t)m;
+            x.root = (uint32_t)(m + 1);
+            // its start chain: three events, newest first, equal codes in one run
+            const uint32_t codes[3] = {start_code(t - prev_t, k == 0 ? 0 : prev_n), start_code(0, m - i), start_code(0, 0)};
+            x.runs.clear();
+            for (uint32_t c : codes)
+                if (!x.runs.empty() && x.runs.front().first == c)
+                    x.runs.front().second++;
+                else
+                    x.runs.insert(x.runs.begin(), {c, 1u});
+        }
+        prev_t = t;
+        prev_n = j - i;
+        k++;
+        i = j;
+    }
+    w.start_list.assign(F, 0);
+    w.start_off.assign(H + 1, 0);
+    for (int i = 0; i < F; i++)
+        w.start_off[w.flows[order[i]].src + 1]++;
+    for (int h = 0; h < H; h++)
+        w.start_off[h + 1] += w.start_off[h];
+    std::vector<int> pos(w.start_off.begin(), w.start_off.end() - 1);
+    for (int i = 0; i < F; i++)
+        w.start_list[pos[w.flows[order[i]].src]++] = order[i];
+    return true;
+}
 
 // The world of a configuration and a topology, every link at bps with delay ns. Returns false
 // (and error) where the reference refuses it.
