@@ -1,7 +1,7 @@
 #!/usr/bin/env python3
 """Benchmark: packet-events/s (and worlds/s) of the batched slot kernels on one B200 per rank.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2|c1|c4] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2|c1|c4|c5] [--impl ours|reference]
 
 A step simulates every world of the workload to completion (all flows done). The default
 workload is C2: FatTree k=8, 10,000 flows (web-search-like sizes, Poisson at 50% load, 25% of
@@ -12,10 +12,16 @@ ours:       `value`  = packet-events per second of device time (CUDA events on t
                        stream), state resident in HBM (restored by a device-to-device copy before
                        each step, outside the timed region; L2 flushed between steps);
             `e2e`    = the same metric through the C ABI from host buffers: world set-up, upload,
-                       run and the download of every flow's result inside the timed region.
+                       run and the download of every flow's result inside the timed region;
+            `parity` = every flow of the step against the oracle run on the whole workload (and
+                       against the reference's own CUDA build's fct.csv);
+            `c4`, `c5`, `sweep_k8` (default run, one GPU): the batched sweep of 256 worlds against
+                       the plain path, the served stream with p50/p99 latency against the requests
+                       run alone, and the reference's k=8 golden sweep (138 worlds) as one batch,
+                       each result compared.
 reference:  the reference's CPU path for this model, the oracle port (the reference TwiNS has no
-            CPU build of its TCP model), on the host cores, one world per process, each step a
-            bounded sample of the workload (the first --ref-slots slots of every world).
+            CPU build of its TCP model), on the host cores, one process per world, each step the
+            whole workload.
 Multi-GPU (torchrun): every rank runs its own copy of the workload (seeded by rank), no
 collective on the data path; time is the max over ranks ("scaling": "weak").
 """
@@ -184,70 +190,209 @@ def cpu_sample(worlds, slots: int, threads: int):
     return sum(r[0] for r in res), wall, res
 
 
-def reference_gpu(worlds, d: Path):
+def read_fct(path: Path):
+    """Columns 5-6 (established_ns, completed_ns) of an fct.csv as int64 arrays."""
+    rows = path.read_text().splitlines()[1:]
+    est = np.array([int(r.split(",")[4]) for r in rows], dtype=np.int64)
+    done = np.array([int(r.split(",")[5]) for r in rows], dtype=np.int64)
+    return est, done
+
+
+def reference_gpu(worlds, d: Path, ours=None):
     """The reference's own CUDA build (oracle/_ref/twins, built for sm_100a from its sources) on
-    each world, one at a time as it runs them: its event-loop time ("Simulation Duration")."""
+    the worlds, batched as it batches them: worlds that share a topology and the global flags run
+    as one --worlds file (its src/main.cu:267-325), timed by its "Simulation Duration" line. With
+    `ours` (name -> (est, done)), every world's fct.csv is compared with this build's results."""
     binary = ROOT / "oracle" / "_ref" / "twins"
     if not binary.exists():
         return None
     paths = write_flows(worlds, d)
-    total = 0.0
+    groups = {}
     for w, p in zip(worlds, paths):
-        r = subprocess.run([str(binary), *world_flags(w), f"--flows={p}", f"--out={d / (w.name + '.ref.csv')}"], capture_output=True,
-                           text=True, timeout=600)
+        flags = tuple(f for f in world_flags(w) if not f.startswith(("--tcp=", "--ecnK=", "--queue=", "--fin=")))
+        groups.setdefault(flags, []).append((w, p))
+    total, equal, flows = 0.0, 0, 0
+    for flags, members in groups.items():
+        wf = d / f"worlds_{abs(hash(flags)) % 10 ** 9}.txt"
+        wf.write_text("".join(f"flows={p},tcp={w.params.tcp},ecnK={w.params.ecn_k},queue={w.params.queue},fin={int(w.params.fin)},"
+                              f"out={d / (w.name + '.ref.csv')}\n" for w, p in members))
+        r = subprocess.run([str(binary), *flags, f"--worlds={wf}"], capture_output=True, text=True, timeout=1200)
         if r.returncode != 0:
             return {"error": r.stderr.strip()[-200:]}
         for line in r.stdout.splitlines():
             if line.startswith("Simulation Duration:"):
                 total += float(line.split(":")[1].strip().rstrip("s"))
-    return {"seconds_per_step": total, "binary": "oracle/_ref/twins (reference src/main.cu, nvcc sm_100a)"}
+        if ours is not None:
+            for w, _ in members:
+                est, done = read_fct(d / (w.name + ".ref.csv"))
+                a = ours[w.name]
+                equal += int(((est == a[0]) & (done == a[1])).sum())
+                flows += len(est)
+    out = {"seconds_per_step": total, "batches": len(groups),
+           "binary": "oracle/_ref/twins (reference src/main.cu, nvcc sm_100a), same-topology worlds batched with --worlds"}
+    if ours is not None:
+        out["flows_equal"] = f"{equal}/{flows}"
+    return out
 
 
-def plain_sample(worlds, n, device, batched_wps):
+class OracleRuns:
+    """The oracle (CPU restatement, test infrastructure) on whole worlds, one process per world,
+    started in the background: the parity check of every flow and the CPU baseline."""
+
+    def __init__(self, worlds, d: Path):
+        binary = oracle_bin()
+        self.worlds = worlds
+        self.d = d
+        paths = write_flows(worlds, d)
+        self.t0 = time.perf_counter()
+        self.procs = [subprocess.Popen([str(binary), *world_flags(w), f"--flows={p}", f"--out={d / (w.name + '.oracle.csv')}"],
+                                       stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True) for w, p in zip(worlds, paths)]
+
+    def collect(self):
+        events, secs, res = 0, [], {}
+        for w, p in zip(self.worlds, self.procs):
+            out, err = p.communicate()
+            if p.returncode != 0:
+                raise RuntimeError(f"oracle failed on {w.name}: {err[-200:]}")
+            f = out.strip().splitlines()[-1].split()
+            events += int(f[f.index("events") + 1])
+            secs.append(float(f[f.index("seconds") + 1]))
+            res[w.name] = read_fct(self.d / (w.name + ".oracle.csv"))
+        return events, secs, res
+
+
+def compare_all(worlds, ours, want):
+    """Flows whose established and completed times are identical, over all worlds."""
+    equal = total = 0
+    for w in worlds:
+        a, b = ours[w.name], want[w.name]
+        equal += int(((a[0] == b[0]) & (a[1] == b[1])).sum())
+        total += len(a[0])
+    return equal, total
+
+
+def plain_sample(worlds, n, device, batched_wps, batched=None):
     """The plain path: worlds run one at a time on the same GPU (each its own context and run),
-    on every (len / n)-th world; worlds/s = sample size / summed device time of the sample."""
+    on every (len / n)-th world; worlds/s = sample size / summed device time of the sample. With
+    `batched` (world index -> (est, done) from the batch), each sampled world's plain result is
+    compared with its batched one."""
     from twins_b200 import api
     step = max(1, len(worlds) // max(1, n))
     idx = list(range(0, len(worlds), step))[:n]
-    ms, events = [], 0
+    ms, events, equal = [], 0, 0
     for i in idx:
         w = worlds[i]
         with api.Simulator(device=device) as sim:
             sim.add_world(w.topo, w.flows, w.params)
             sim.run()
             st = sim.stats()
+            est, done = sim.results(0)
+        if batched is not None:
+            equal += int((est == batched[i][0]).all() and (done == batched[i][1]).all())
         ms.append(st["kernel_ms"])
         events += st["packet_events"]
     wps = len(idx) / (sum(ms) / 1000.0)
-    return {"worlds_per_s": wps, "events_per_s": events / (sum(ms) / 1000.0), "sample_worlds": idx,
-            "sample": f"{len(idx)} of {len(worlds)} worlds (every {step}th), each alone, device time summed",
-            "batched_over_plain_worlds_per_s": batched_wps / wps}
+    out = {"worlds_per_s": wps, "events_per_s": events / (sum(ms) / 1000.0), "sample_worlds": idx,
+           "sample": f"{len(idx)} of {len(worlds)} worlds (every {step}th), each alone, device time summed",
+           "batched_over_plain_worlds_per_s": batched_wps / wps}
+    if batched is not None:
+        out["batched_equal_plain"] = f"{equal}/{len(idx)}"
+    return out
 
 
-def serve_bench(args):
-    """C5: a seeded Poisson stream of simulation requests served by continuous batching (requests
-    join the running batch between launches), against the same requests run one at a time.
-    Latency = completion - submission on the server's clock; worlds/s = requests / (last
-    completion - first submission). One GPU (each rank would serve its own stream)."""
+def c4_leg(device: int, plain_n: int, warmup: int, warmup_slots: int):
+    """C4: 256 leaf-spine worlds of uneven size in one batch (one step, device time), against the
+    plain path on a sample of the same worlds, each sampled world's results compared."""
     import torch
     from twins_b200 import api, workloads
-    local_rank = int(os.environ.get("LOCAL_RANK", 0))
-    torch.cuda.set_device(local_rank)
-    reqs = workloads.served_stream(seed=1, n=args.requests + 3, rate_per_s=args.rate)
+    worlds = workloads.c4(1)
+    sim = api.Simulator(device=device)
+    for w in worlds:
+        sim.add_world(w.topo, w.flows, w.params)
+    sim.prepare()
+    for _ in range(warmup):
+        sim.run(warmup_slots)
+    sim.reset()
+    torch.cuda.synchronize()
+    sim.run()
+    torch.cuda.synchronize()
+    st = sim.stats()
+    res = {i: sim.results(i) for i in range(len(worlds))}
+    unfinished = int(sum((res[i][1] < 0).sum() for i in res))
+    sim.close()
+    wps = len(worlds) / (st["kernel_ms"] / 1000.0)
+    plain = plain_sample(worlds, plain_n, device, wps, batched=res)
+    return {"config": "256 leaf-spine worlds (4-32 leaves, spines = leaves / 2, 16 hosts per leaf), tcp x ecnK {10,20,40,80} x "
+                      "queue {100,200,400}, 1k-20k web-search-like flows at 30-70% load, one batch",
+            "worlds_per_s": wps, "seconds_per_step": st["kernel_ms"] / 1000.0, "packet_events_per_s": st["packet_events"] / (st["kernel_ms"] / 1000.0),
+            "packet_events": st["packet_events"], "flows": int(sum(len(w.flows) for w in worlds)), "unfinished_flows": unfinished,
+            "steps": 1, "warmup": f"{warmup} runs of {warmup_slots} slots", "plain": plain,
+            "batched_over_plain": plain["batched_over_plain_worlds_per_s"]}
+
+
+def sweep_leg(device: int):
+    """The reference's k=8 parameter sweep (138 ecnK x queue x TCP configurations of FatTree k=8,
+    its data/ns3/sweep_k8 golden set, fixtures under tests/golden/sweep) as one batch of worlds, as
+    its bench/sweep.py runs it (worlds with undecided ties again on the 25-run chain build, time
+    included); worlds/s over device time, and every configuration compared with ns-3."""
+    import torch
+    from twins_b200 import api
+    g = ROOT / "tests" / "golden"
+    index = json.loads((g / "sweep" / "index.json").read_text())["k8"]
+    z = np.load(g / "sweep" / "k8.npz")
+    topo = api.Topology.fattree(8)
+    flows = {c["flows"]: api.Flows.load(g / c["flows"], topo.hosts) for c in index}
+
+    def batch(cfgs, runs):
+        with api.Simulator(device=device, chain_runs=runs) as sim:
+            for c in cfgs:
+                sim.add_world(topo, flows[c["flows"]], api.TcpParams(c["tcp"], c["ecn_k"], c["queue"]))
+            sim.run()
+            torch.cuda.synchronize()
+            return [sim.results(i) for i in range(len(cfgs))], [sim.counters(i)["undecided_ties"] for i in range(len(cfgs))], sim.stats()
+
+    batch(index[:4], 9)  # (warm-up: loads the module, small)
+    res, ties, st = batch(index, 9)
+    ms = st["kernel_ms"]
+    redo = [i for i, t in enumerate(ties) if t]
+    if redo:
+        r2, _, st2 = batch([index[i] for i in redo], 25)
+        ms += st2["kernel_ms"]
+        for j, i in enumerate(redo):
+            res[i] = r2[j]
+    equal, at = 0, 0
+    for c, (est, done) in zip(index, res):
+        n = c["rows"]
+        equal += int((est == z["est"][at:at + n]).all() and (done == z["done"][at:at + n]).all())
+        at += n
+    return {"config": "FatTree k=8 sweep: 138 configurations (k8_a2a30, k8_a2a50w flows) in one batch",
+            "worlds_per_s": len(index) / (ms / 1000.0), "seconds": ms / 1000.0, "rerun_25_runs": len(redo),
+            "identical_to_ns3": f"{equal}/{len(index)}",
+            "published": {"rtx5090_1x138_worlds_per_s": 52.3, "rx9060xt_2x69_worlds_per_s": 22.3,
+                          "source": "reference docs/nvidia.md:126, README.md:257"}}
+
+
+def serve_leg(device: int, requests: int, rate: float, serve_worlds: int):
+    """C5: a seeded Poisson stream of simulation requests served by continuous batching (requests
+    join the running batch between launches), against the same requests run one at a time, each
+    served result compared with its run alone. Latency = completion - submission on the server's
+    clock; worlds/s = requests / (last completion - first submission)."""
+    from twins_b200 import api, workloads
+    reqs = workloads.served_stream(seed=1, n=requests + 3, rate_per_s=rate)
     warm, reqs = reqs[:3], reqs[3:]
-    # capacities for about `--serve-worlds` requests of the mix at once (500 hosts, 170 switches,
+    # capacities for about `serve_worlds` requests of the mix at once (500 hosts, 170 switches,
     # 1,700 ports and 2,500 connections per request on average, with room), within 160 GB
-    n = args.serve_worlds
+    n = serve_worlds
     caps = dict(worlds=n, hosts=500 * n, switches=170 * n, ports=1700 * n, connections=2500 * n, messages=2500 * n,
                 sent_list_entries=min(1 << 30, 2_800_000 * n), ooo_blocks=min(1 << 28, 700_000 * n), slots_per_launch=128,
                 hbm_budget_bytes=160 * 10 ** 9)
-    with api.Server(device=local_rank, **caps) as srv:
+    with api.Server(device=device, **caps) as srv:
         srv.start()
         for r in warm:  # warm-up requests (untimed)
             srv.wait(srv.submit(r.topo, r.flows, r.params), timeout_s=600)
         st0 = srv.stats()
         ids = []
-        with Clocks(local_rank) as clocks:
+        with Clocks(device) as clocks:
             t0 = time.perf_counter()
             for r in reqs:
                 delay = r.arrival_s - reqs[0].arrival_s - (time.perf_counter() - t0)
@@ -257,18 +402,21 @@ def serve_bench(args):
             for i in ids:
                 srv.wait(i, timeout_s=900)
         infos = [srv.info(i) for i in ids]
+        served = [srv.results(i)[:2] for i in ids]
         st = srv.stats()
     lat = np.array([x["t_done"] - x["t_submit"] for x in infos])
     span = max(x["t_done"] for x in infos) - min(x["t_submit"] for x in infos)
     served_wps = len(ids) / span
     events = st["packet_events"] - st0["packet_events"]
     # the plain path: every request alone, one after the other (device time)
-    plain_ms, plain_events = 0.0, 0
-    for r in reqs:
-        with api.Simulator(device=local_rank) as sim:
+    plain_ms, plain_events, equal = 0.0, 0, 0
+    for r, (est_s, done_s) in zip(reqs, served):
+        with api.Simulator(device=device) as sim:
             sim.add_world(r.topo, r.flows, r.params)
             sim.run()
             x = sim.stats()
+            est, done = sim.results(0)
+        equal += int((est == est_s).all() and (done == done_s).all())
         plain_ms += x["kernel_ms"]
         plain_events += x["packet_events"]
     plain_wps = len(reqs) / (plain_ms / 1000.0)
@@ -276,23 +424,45 @@ def serve_bench(args):
     for r in reqs:
         k = r.name.split("_")[2]
         mix[k] = mix.get(k, 0) + 1
-    print(json.dumps({
-        "metric": "worlds/s (served)", "value": served_wps, "unit": "worlds/s", "n_gpus": 1, "steps": 1, "warmup": len(warm),
-        "ms_per_step": 1000 * span, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
-        "data": "synthetic",
-        "config": {"workload": "served stream (C5 shape, TCP requests): Poisson arrivals, 40% FatTree k=4, 30% k=8, 10% k=16, "
-                               "10% Jellyfish 64x8 (4 hosts/switch), 10% Dragonfly 9x4; a tenth with a link failure",
-                   "requests": len(reqs), "rate_per_s": args.rate, "mix": mix, "flows": int(sum(len(r.flows) for r in reqs)),
-                   "capacities": caps},
-        "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)), "max": float(lat.max())},
-        "packet_events_per_s": events / span,
-        "device_busy_frac": (st["kernel_ms"] - st0["kernel_ms"]) / 1000.0 / span,
-        "plain": {"worlds_per_s": plain_wps, "events_per_s": plain_events / (plain_ms / 1000.0),
-                  "sample": "every request alone, one after the other, device time summed"},
-        "served_over_plain_worlds_per_s": served_wps / plain_wps,
-        "server": {k: st[k] for k in ("launches", "slots_run", "admitted", "retired", "hbm_bytes", "host_lanes", "stage_frames", "grid")},
-        "clocks": clocks.summary(),
-    }))
+    return {"config": "served stream (C5 shape, TCP requests): Poisson arrivals, 40% FatTree k=4, 30% k=8, 10% k=16, "
+                      "10% Jellyfish 64x8 (4 hosts/switch), 10% Dragonfly 9x4; a tenth with a link failure",
+            "requests": len(reqs), "rate_per_s": rate, "mix": mix, "flows": int(sum(len(r.flows) for r in reqs)),
+            "worlds_per_s": served_wps, "span_s": span, "warmup_requests": len(warm),
+            "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)), "max": float(lat.max())},
+            "packet_events_per_s": events / span,
+            "device_busy_frac": (st["kernel_ms"] - st0["kernel_ms"]) / 1000.0 / span,
+            "plain": {"worlds_per_s": plain_wps, "events_per_s": plain_events / (plain_ms / 1000.0),
+                      "sample": "every request alone, one after the other, device time summed"},
+            "served_over_plain": served_wps / plain_wps,
+            "served_equal_alone": f"{equal}/{len(reqs)}",
+            "server": {k: st[k] for k in ("launches", "slots_run", "admitted", "retired", "hbm_bytes", "host_lanes", "stage_frames", "grid")},
+            "capacities": caps, "clocks": clocks.summary()}
+
+
+def reference_arm(args, worlds, config):
+    """The reference arm: the reference's CPU path for this model on the host cores, which is the
+    oracle port (the reference has no CPU build of its TCP model): every world of the workload
+    whole, one process per world, all worlds at once; warm-up steps run a short prefix."""
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_sample(worlds, 300, threads)
+    evs, walls = [], []
+    slots = args.ref_slots if args.ref_slots > 0 else 10 ** 12
+    for _ in range(args.steps):
+        ev, wall, _ = cpu_sample(worlds, slots, threads)
+        evs.append(ev)
+        walls.append(wall)
+    value = sum(evs) / sum(walls)
+    what = "whole" if args.ref_slots <= 0 else f"the first {args.ref_slots} slots of each of"
+    sample = f"{what} {len(worlds)} worlds per step ({sum(evs) // len(evs)} packet-events), one process (core) per world, all at once"
+    cores = min(threads, len(worlds))
+    print(json.dumps({"impl": "reference", "metric": METRIC, "value": value, "unit": "events/s", "n_gpus": args.gpus,
+                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * statistics.mean(walls),
+                      "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+                      "data": "synthetic", "config": config,
+                      "cpu_baseline": {"value": value, "unit": "events/s", "cores": cores, "nproc": threads, "kind": "port",
+                                       "sample": sample},
+                      "e2e": {"value": value, "unit": "events/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
 def main():
@@ -305,27 +475,34 @@ def main():
     ap.add_argument("--rate", type=float, default=100.0, help="C5: request arrivals per second (Poisson)")
     ap.add_argument("--serve-worlds", type=int, default=256, help="C5: requests the server holds at once")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--ref-slots", type=int, default=2500, help="reference arm: slots of each world per step")
-    ap.add_argument("--cpu-slots", type=int, default=6000, help="cpu_baseline: slots of the sample world")
+    ap.add_argument("--ref-slots", type=int, default=0, help="reference arm: slots of each world per step (0: whole worlds)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--host-lanes", type=int, default=None, help="fixed hosts per warp (default: autotuned launch shapes)")
     ap.add_argument("--no-ref-gpu", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="C2 alone: no C4, C5 or sweep legs")
+    ap.add_argument("--no-parity", action="store_true", help="no oracle comparison of every flow")
     ap.add_argument("--warmup-slots", type=int, default=None,
-                    help="slots of each warm-up run (default: whole runs; C4: 400)")
+                    help="slots of each warm-up run (default: C2 3000, C4 400; 0: whole runs)")
     ap.add_argument("--plain-sample", type=int, default=16,
                     help="C4: worlds of the plain path (one world at a time) timed, every (256 / n)-th world")
     args = ap.parse_args()
     if args.warmup_slots is None:
-        args.warmup_slots = 400 if args.workload == "c4" else 0
+        args.warmup_slots = 400 if args.workload == "c4" else 3000
     args.warmup = max(args.warmup, 3)
 
     rank = int(os.environ.get("RANK", 0))
-    if args.workload == "c5" and args.impl == "ours":
-        if rank == 0:  # (one server on one GPU; other ranks have nothing to add)
-            serve_bench(args)
-        return
     world_size = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.workload == "c5" and args.impl == "ours":
+        if rank == 0:  # (one server on one GPU; other ranks have nothing to add)
+            import torch
+            torch.cuda.set_device(local_rank)
+            out = serve_leg(local_rank, args.requests, args.rate, args.serve_worlds)
+            print(json.dumps({"metric": "worlds/s (served)", "value": out["worlds_per_s"], "unit": "worlds/s", "n_gpus": 1, "steps": 1,
+                              "warmup": out["warmup_requests"], "ms_per_step": 1000 * out["span_s"], "higher_is_better": True,
+                              "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+                              "config": {"workload": out["config"]}, **{k: v for k, v in out.items() if k != "config"}}))
+        return
     worlds = load_worlds(args.workload, rank)
     config = {"workload": {"c1": "FatTree k=4, 240 flows, DCTCP (C1)",
                            "c2": "FatTree k=8, 10,000 flows x {NewReno, DCTCP, Cubic}, FIN, spraying (C2)",
@@ -337,25 +514,8 @@ def main():
               "seed": 1}
 
     if args.impl == "reference":
-        if rank != 0:
-            return
-        threads = os.cpu_count() or 1
-        for _ in range(args.warmup):
-            cpu_sample(worlds, min(args.ref_slots, 500), threads)
-        evs, walls = [], []
-        for _ in range(args.steps):
-            ev, wall, _ = cpu_sample(worlds, args.ref_slots, threads)
-            evs.append(ev)
-            walls.append(wall)
-        value = sum(evs) / sum(walls)
-        sample = f"the first {args.ref_slots} slots ({args.ref_slots} us simulated) of each of the {len(worlds)} worlds, one process per world"
-        print(json.dumps({"impl": "reference", "metric": METRIC, "value": value, "unit": "events/s", "n_gpus": args.gpus,
-                          "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * statistics.mean(walls),
-                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
-                          "data": "synthetic", "config": config,
-                          "cpu_baseline": {"value": value, "unit": "events/s", "cores": min(threads, len(worlds)), "kind": "port",
-                                           "sample": sample},
-                          "e2e": {"value": value, "unit": "events/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        if rank == 0:
+            reference_arm(args, worlds, config)
         return
 
     import torch
@@ -371,12 +531,14 @@ def main():
         if dist is not None:
             dist.barrier()
 
+    scratch = Path(tempfile.mkdtemp(prefix="twins_bench_"))
     sim = api.Simulator(device=local_rank, host_lanes=args.host_lanes)
     for w in worlds:
         sim.add_world(w.topo, w.flows, w.params)
     sim.prepare()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local_rank}")
     for _ in range(args.warmup):
+        sim.reset()
         sim.run(args.warmup_slots)
     kernel_ms, launches, stats = [], 0, None
     with Clocks(local_rank) as clocks:
@@ -391,14 +553,15 @@ def main():
             kernel_ms.append(stats["kernel_ms"])
             launches += stats["launches"]
     events = stats["packet_events"]
-    for w in range(len(worlds)):
-        est, done = sim.results(w)
-        if (done < 0).any():
-            print(f"warning: world {worlds[w].name}: {(done < 0).sum()} flows unfinished", file=sys.stderr)
+    ours = {w.name: sim.results(i) for i, w in enumerate(worlds)}
+    unfinished = int(sum((d < 0).sum() for _, d in ours.values()))
     ms = statistics.mean(kernel_ms)
     from twins_b200 import shard
     ms_max, events_all = shard.aggregate(ms, float(events), dist, device=f"cuda:{local_rank}")
     value = events_all / (ms_max / 1000.0)
+    # every flow against the oracle: whole worlds on the host cores, one process per world, in the
+    # background while the other legs run (rank 0)
+    oracle = OracleRuns(worlds, scratch) if rank == 0 and not args.no_parity else None
 
     # end to end through the C ABI from host buffers
     e2e_ms, h2d, d2h = [], 0, 0
@@ -413,8 +576,7 @@ def main():
                 s2.results(i)
             st2 = s2.stats()
         e2e_ms.append(1000 * (time.perf_counter() - t0))
-        h2d = st2["bytes_h2d"]
-        d2h = sum(len(w.flows) for w in worlds) * 32
+        h2d, d2h = st2["bytes_h2d"], st2["bytes_d2h"]
     e2e_step = statistics.mean(e2e_ms) if e2e_ms else float("nan")
     if dist is not None:
         t = torch.tensor([e2e_step], dtype=torch.float64, device=f"cuda:{local_rank}")
@@ -438,43 +600,46 @@ def main():
             traffic = tj["dram_bytes_per_event"] * events / max(1, stats["launches"])
         except Exception:
             traffic = None
-    # CPU baseline: the oracle (one core) on a bounded sample of the DCTCP (or first) world
-    sample_world = next((w for w in worlds if w.params.tcp == "dctcp"), worlds[0])
-    ev_cpu, wall_cpu, res = cpu_sample([sample_world], args.cpu_slots, 1)
-    cpu_value = ev_cpu / res[0][1]
-    plain = None
-    if args.workload == "c4":
-        plain = plain_sample(worlds, args.plain_sample, local_rank, len(worlds) / (ms_max / 1000.0))
     ref_gpu = None
-    if not args.no_ref_gpu and rank == 0:
-        d = Path(tempfile.gettempdir()) / "twins_bench_ref"
-        d.mkdir(exist_ok=True)
+    if not args.no_ref_gpu:
         try:
-            # (C4: the plain path's sample of worlds, one at a time as the reference runs them)
-            ref_worlds = [worlds[i] for i in plain["sample_worlds"]] if plain else worlds
-            ref_gpu = reference_gpu(ref_worlds, d)
+            ref_gpu = reference_gpu(worlds, scratch, ours)
             if ref_gpu and "seconds_per_step" in ref_gpu:
-                if plain:
-                    ref_gpu["worlds_per_s"] = len(ref_worlds) / ref_gpu["seconds_per_step"]
-                    ref_gpu["sample_worlds"] = plain["sample_worlds"]
-                else:
-                    ref_gpu["value"] = events / ref_gpu["seconds_per_step"]
-                    ref_gpu["unit"] = "events/s"
+                ref_gpu["value"] = events / ref_gpu["seconds_per_step"]
+                ref_gpu["unit"] = "events/s"
         except Exception as e:
             ref_gpu = {"error": str(e)[:200]}
+    extras = {}
+    if args.workload == "c2" and not args.no_extras and world_size == 1:
+        extras["c4"] = c4_leg(local_rank, args.plain_sample, 3, 200)
+        extras["c5"] = serve_leg(local_rank, args.requests, args.rate, args.serve_worlds)
+        extras["sweep_k8"] = sweep_leg(local_rank)
+    elif args.workload == "c4":
+        extras["plain"] = plain_sample(worlds, args.plain_sample, local_rank, len(worlds) / (ms_max / 1000.0),
+                                       batched=dict(enumerate(ours[w.name] for w in worlds)))
+    parity, cpu = {}, None
+    if oracle is not None:
+        ev_cpu, secs, want = oracle.collect()
+        eq, n = compare_all(worlds, ours, want)
+        parity = {"flows_equal_oracle": f"{eq}/{n}", "oracle_events": ev_cpu, "events_equal_oracle": ev_cpu == events}
+        cpu = {"value": ev_cpu / max(secs), "unit": "events/s", "cores": len(worlds), "nproc": os.cpu_count(), "kind": "port",
+               "sample": f"the oracle on the whole workload ({len(worlds)} worlds, one process per world at once, "
+                         f"event loop {', '.join(f'{s:.1f}' for s in secs)} s)"}
+    if ref_gpu and "flows_equal" in ref_gpu:
+        parity["flows_equal_reference_gpu_build"] = ref_gpu["flows_equal"]
     out = {
         "metric": METRIC, "value": value, "unit": "events/s", "n_gpus": world_size, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
         "data": "synthetic", "config": config,
         "worlds_per_s": len(worlds) * world_size / (ms_max / 1000.0),
-        "packet_events_per_step": events,
+        "packet_events_per_step": events, "unfinished_flows": unfinished,
         "slots_per_step": stats["slots"], "slots_run_per_step": stats["slots_run"],
         "e2e": {"value": e2e_value, "unit": "events/s", "ms_per_step": e2e_step, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
                      "algorithmic_bytes_per_step": alg},
-        "cpu_baseline": {"value": cpu_value, "unit": "events/s", "cores": 1, "kind": "port",
-                         "sample": f"oracle on the first {args.cpu_slots} slots of {sample_world.name}"},
+        "cpu_baseline": cpu,
+        "parity": parity,
         "clocks": clocks.summary(),
         "gpu_launches": launches,
         "graph_launches": stats["graph_launches"],
@@ -483,8 +648,7 @@ def main():
     }
     if ref_gpu is not None:
         out["reference_gpu"] = ref_gpu
-    if plain:
-        out["plain"] = plain
+    out.update(extras)
     print(json.dumps(out))
     sim.close()
     if dist is not None:

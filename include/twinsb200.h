@@ -166,11 +166,14 @@ int tb_abi_sizes(unsigned long long *out, int n);
  * process loading the library holds on each device it uses until it exits; a world that needs
  * more (e.g. a FatTree k=8) is rejected with TB_ERR_MEMORY before anything runs. Arguments are
  * tb_world_add_tcp's and tb_run's (ECMP hashes computed), results as tb_results gives them into
- * the caller's host arrays. The first call on a device sets the area up there (it looks up its
- * device address with that device current), so make that first call before any stream
- * capture. Every call on a device shares the area, which keeps the last call's contents; each
+ * the caller's host arrays. Each call looks up the area's device address with that device
+ * current (the first call on a device loads the module there, so make it before any stream
+ * capture). Every call on a device shares the area, which keeps the last call's contents; each
  * call clears what must start at zero. Calls that overlapped on the GPU would race on the area,
- * so the library makes the calls of one process take turns (a lock held for the whole call). */
+ * so the library makes the calls of one process take turns (a lock held for the whole call).
+ * The call runs its copies and launches on the legacy default stream and returns when they are
+ * done: it waits for earlier work on the caller's blocking streams (as that stream does), but
+ * not for non-blocking streams, and it does not synchronize the whole device. */
 int tb_run_static(int device, const tb_topology *topo, int n_flows, const int *src, const int *dst,
                   const long long *size, const long long *start_ns, const long long *conn,
                   const tb_tcp_params *params, long long max_slots, long long *established_ns,

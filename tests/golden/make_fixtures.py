@@ -7,13 +7,14 @@ arguments in data/flows/<workload>.csv.topo and topology files in data/topo/
 (validation/check_exact.sh reads them the same way). This script copies a subset, unchanged,
 and writes manifest.json listing each case: its flows, its ns-3 output, its topology and flags.
 
-    python tests/golden/make_fixtures.py [/path/to/reference]
+    TWINS_REFERENCE=/path/to/reference python tests/golden/make_fixtures.py
 
 Run here (where the reference tree exists); the tests read only the copies.
 """
 from __future__ import annotations
 
 import json
+import os
 import shutil
 import sys
 from pathlib import Path
@@ -86,4 +87,7 @@ def main(ref: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference"))
+    root = os.environ.get("TWINS_REFERENCE") or (sys.argv[1] if len(sys.argv) > 1 else "")
+    if not root:
+        sys.exit("set TWINS_REFERENCE (or pass the reference tree's path)")
+    main(Path(root))

@@ -9,7 +9,7 @@ in manifest.json with the reference's counters line and, per field of the world 
 build_world makes of it (oracle/_ref/rdma_world_kat: parameters, wiring, ECMP routes, port
 configurations), the SHA-256 of the field's JSON.
 
-    python tests/golden/make_rdma_fixtures.py
+    TWINS_REFERENCE=/path/to/reference python tests/golden/make_rdma_fixtures.py
 """
 import hashlib
 import json

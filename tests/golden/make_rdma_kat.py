@@ -7,7 +7,7 @@ The fixture groups the harness's lines by function: {fn: {"keys": [...], "rows":
 nested objects flattened to dotted keys ("a.rate": the rate before the event, "b.rate" after).
 Doubles stay as the hex strings of their bits.
 
-    python tests/golden/make_rdma_kat.py
+    TWINS_REFERENCE=/path/to/reference python tests/golden/make_rdma_kat.py
 """
 import gzip
 import json

@@ -3,8 +3,10 @@ stored sequential ns-3 outputs the reference validates against (data/ns3/ref, co
 tests/golden/ by make_fixtures.py). Every flow's establishment and completion time and the
 ECMP hashes must be identical. This pins the oracle before it checks the CUDA path."""
 import csv
+import json
 import subprocess
 
+import numpy as np
 import pytest
 
 from conftest import GOLDEN, manifest
@@ -67,3 +69,26 @@ def test_oracle_planted_error_is_caught(oracle_bin, tmp_path):
     with open(out) as f:
         got = [(int(x[4]), int(x[5])) for x in list(csv.reader(f))[1:]]
     assert got != want
+
+
+SWEEP = json.loads((GOLDEN / "sweep" / "index.json").read_text())
+
+
+def sweep_want(sweep, i):
+    z = np.load(GOLDEN / "sweep" / f"{sweep}.npz")
+    at = sum(c["rows"] for c in SWEEP[sweep][:i])
+    n = SWEEP[sweep][i]["rows"]
+    return list(zip(z["est"][at:at + n].tolist(), z["done"][at:at + n].tolist()))
+
+
+@pytest.mark.parametrize("sweep,i", [("k8", 0), ("k8", 70), ("k8", 137), ("k16", 5)])
+def test_oracle_equals_ns3_sweep(oracle_bin, sweep, i, tmp_path):
+    """Sample configurations of the reference's ecnK x queue x TCP sweeps (the golden set of its
+    batching path): the oracle equals the stored ns-3 output, which pins the sweep fixtures."""
+    c = SWEEP[sweep][i]
+    out = tmp_path / "out.csv"
+    subprocess.run([str(oracle_bin), f"--k={c['k']}", f"--flows={GOLDEN / c['flows']}", f"--out={out}", f"--tcp={c['tcp']}",
+                    f"--ecnK={c['ecn_k']}", f"--queue={c['queue']}"], capture_output=True, text=True, check=True)
+    with open(out) as f:
+        got = [(int(x[4]), int(x[5])) for x in list(csv.reader(f))[1:]]
+    assert got == sweep_want(sweep, i)

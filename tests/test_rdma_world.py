@@ -63,3 +63,20 @@ def test_world_refusals(rw):
     assert "5 switches" in world(rw, cfg, chain)[1]
     w, err = world(rw, cfg.replace("CC_MODE 3", "CC_MODE 1"), chain)
     assert err is None and w["params"][9] == 2 * 8 * 1000 + 8 * 80  # maxRtt: twice 8 links of 1 us, and 8 tx times of a 1000-byte frame at 100 Gb/s
+
+
+def test_world_overrides_and_bad_ids(rw):
+    """NVL_BASE_RTT and NVL_WIN replace maxRtt and maxBdp as the reference's build_world does
+    (src/rdma/rmain.cu:687-690: NVL_WIN only with HAS_WIN); negative flow ids and links to nodes that
+    do not exist are refused, not indexed."""
+    cfg = (RDMA / "ft4_incast15_hpcc.cfg").read_text()
+    topo = (RDMA / "ft4_incast15_hpcc.topo").read_text()
+    base, _ = world(rw, cfg, topo)
+    w, err = world(rw, cfg + "NVL_BASE_RTT 12345\nNVL_WIN 777\n", topo)
+    assert err is None and w["params"][9] == 12345 and w["params"][8] == 777
+    assert w["params"][:8] == base["params"][:8]
+    w, err = world(rw, cfg.replace("HAS_WIN 1", "HAS_WIN 0") + "NVL_WIN 777\n", topo)
+    assert err is None and w["params"][8] == 0
+    assert "negative" in world(rw, cfg, topo, "src,dst,flow_size,start_ns\n-1,3,1000,1000\n")[1]
+    assert "does not exist" in world(rw, cfg, topo + "link h0 s99\n")[1]
+    assert "does not exist" in world(rw, cfg, "link h0 s0\n" + topo)[1]

@@ -25,6 +25,21 @@ def test_static_run_equals_tb_run_twice(native_lib):
         assert np.array_equal(s_done, done)
 
 
+def test_static_run_allocates_nothing(native_lib):
+    """Once a first call has loaded the library's module (and its fixed area) on the device, a
+    further call leaves the device's free memory as it was: nothing is allocated for the world."""
+    import torch
+    w = workloads.c1()[0]
+    api.run_world_static(w.topo, w.flows, w.params)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(0)
+    s_est, s_done, status = api.run_world_static(w.topo, w.flows, w.params)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(0)
+    assert status == api.TB_OK and (s_done >= 0).all()
+    assert free0 - free1 <= 2 << 20, f"free device memory dropped by {free0 - free1} bytes"
+
+
 def test_static_run_rejects_a_world_too_large(native_lib):
     w = workloads.c2_small()[1]  # a FatTree k=8 world needs more than the fixed area
     with pytest.raises(api.TwinsError) as e:

@@ -1055,7 +1055,11 @@ int prepare(tb_ctx *c)
     if ((c->grid = grid_for(c, c->host_lanes, c->stage_cap)) <= 0)
         return fail(TB_ERR_CUDA, "the slot kernel does not fit on the device");
     c->prepared = true;
-    cudaDeviceSynchronize();
+    // (tb_run_static: its own work only, on the legacy default stream, not every stream of the device)
+    if (c->arena)
+        cudaStreamSynchronize(0);
+    else
+        cudaDeviceSynchronize();
     c->stats.upload_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return TB_OK;
 }
@@ -1449,8 +1453,7 @@ static __device__ __align__(256) unsigned char tb_static_area[TB_STATIC_AREA_BYT
 
 namespace
 {
-std::mutex g_static_mu;       // calls of this process take turns
-void *g_static_area[64] = {}; // per device: the area's device address (null: not set up yet)
+std::mutex g_static_mu; // calls of this process take turns
 } // namespace
 
 extern "C" int tb_run_static(int device, const tb_topology *topo, int n_flows, const int *src, const int *dst,
@@ -1475,19 +1478,16 @@ extern "C" int tb_run_static(int device, const tb_topology *topo, int n_flows, c
                 cudaSetDevice(d);
         }
     } restore{prev};
-    if (!g_static_area[device])
-    {
-        // once per device, with that device current: the host-side name of the area is not a
-        // device address; the runtime gives the address
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, tb_static_area);
-        if (e != cudaSuccess || !p)
-            return fail(TB_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        g_static_area[device] = p;
-    }
+    // with the device current: the host-side name of the area is not a device address; the runtime
+    // gives the address. Asked on every call (it is cheap), so that a context made anew after a
+    // cudaDeviceReset, which may load the module at another address, is never given a stale one.
+    void *area = nullptr;
+    cudaError_t e0 = cudaGetSymbolAddress(&area, tb_static_area);
+    if (e0 != cudaSuccess || !area)
+        return fail(TB_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e0));
     tb_ctx c;
     c.device = device;
-    c.arena = (unsigned char *)g_static_area[device];
+    c.arena = (unsigned char *)area;
     c.arena_cap = TB_STATIC_AREA_BYTES;
     int r = tb_world_add_tcp(&c, topo, n_flows, src, dst, size, start_ns, conn, nullptr, nullptr, params, nullptr);
     if (r)

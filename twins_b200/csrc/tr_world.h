@@ -72,6 +72,7 @@ struct RdmaWorldParams
     int64_t nack_interval;
     uint64_t bps;
     int64_t delay;
+    double stop_ns; // SIMULATOR_STOP_TIME in ns: the run stops at slot stop_ns / slot length
     uint32_t win;
     uint64_t base_rtt;
     int var_win, rate_bound, ack_high_prio, ecn;
@@ -133,10 +134,12 @@ inline bool build_rdma_flows(RdmaWorld &w, const std::string &csv)
     w.flows.clear();
     while (std::getline(f, line))
     {
-        unsigned a, b;
+        long long a, b;
         unsigned long long sz, st;
-        if (sscanf(line.c_str(), "%u,%u,%llu,%llu", &a, &b, &sz, &st) != 4)
+        if (sscanf(line.c_str(), "%lld,%lld,%llu,%llu", &a, &b, &sz, &st) != 4)
             continue;
+        if (a < 0 || b < 0 || a > INT_MAX || b > INT_MAX)
+            return w.error = "a flow with a negative or out-of-range node id", false;
         RdmaFlow x{};
         x.src = (int)a, x.dst = (int)b, x.size = sz, x.start = (int64_t)st;
         w.flows.push_back(x);
@@ -244,6 +247,8 @@ inline bool build_rdma_world(RdmaWorld &w, const RdmaConfig &cfg, const std::str
     P.ecn_pcnt = 257;
     if (u32("GLOBAL_T", 1) != 1)
         return w.error = "GLOBAL_T 0 (SimAI topologies only)", false;
+    // (in double, as the reference converts it: reference src/rdma/rmain.cu:526)
+    P.stop_ns = num("SIMULATOR_STOP_TIME", 10.0) * 1e9;
 
     // ---- topology: hosts h0.., switches s0..; nodes are hosts, then switches
     std::vector<std::pair<int, int>> links;
@@ -257,11 +262,26 @@ inline bool build_rdma_world(RdmaWorld &w, const RdmaConfig &cfg, const std::str
                 f >> w.S;
             else if (x == "link")
             {
-                f >> a >> b;
-                auto id = [&](const std::string &y) { return (y[0] == 'h' ? 0 : w.H) + atoi(y.c_str() + 1); };
-                links.push_back({id(a), id(b)});
+                if (!(f >> a >> b))
+                    return w.error = "a link line without two ends", false;
+                // h<i> (0 <= i < hosts) or s<j> (0 <= j < switches), after the hosts and switches lines
+                auto id = [&](const std::string &y) -> int {
+                    if (y.size() < 2 || (y[0] != 'h' && y[0] != 's'))
+                        return -1;
+                    char *end = nullptr;
+                    const long v = strtol(y.c_str() + 1, &end, 10);
+                    if (*end || v < 0 || v >= (y[0] == 'h' ? w.H : w.S))
+                        return -1;
+                    return (y[0] == 'h' ? 0 : w.H) + (int)v;
+                };
+                const int ia = id(a), ib = id(b);
+                if (ia < 0 || ib < 0)
+                    return w.error = "a link to a node that does not exist (or before its hosts / switches line)", false;
+                links.push_back({ia, ib});
             }
     }
+    if (w.H <= 0 || w.S < 0)
+        return w.error = "no hosts", false;
     const int H = w.H, S = w.S, N = w.N = H + S, L = w.L = 2 * (int)links.size();
     P.bps = bps;
     w.deg.assign(N, 0);
@@ -361,7 +381,13 @@ inline bool build_rdma_world(RdmaWorld &w, const RdmaConfig &cfg, const std::str
             w.rtp.insert(w.rtp.end(), v.begin(), v.end());
         }
     P.base_rtt = max_rtt;
-    P.win = u32("HAS_WIN", 1) ? (uint32_t)max_bdp : 0;
+    const uint32_t has_win = u32("HAS_WIN", 1);
+    P.win = has_win ? (uint32_t)max_bdp : 0;
+    // a server's world with the whole cluster's maxRtt and maxBdp (reference: src/rdma/rmain.cu:687-690)
+    if (u32("NVL_BASE_RTT", 0))
+        P.base_rtt = u32("NVL_BASE_RTT", 0);
+    if (u32("NVL_WIN", 0) && has_win)
+        P.win = u32("NVL_WIN", 0);
     // ---- switch ports: headroom 3 x rate x delay; the PFC threshold's shift from 3, one less per
     // halving of the rate above the NIC's (host 0's link); ECN thresholds (KB) and probability by rate
     const uint64_t nic_rate = w.lbps[w.out_link[0]];
