@@ -1,0 +1,1301 @@
+// twins-b200: the RDMA model's slot (the network of the HPCC fork of ns-3.17 that the reference's
+// twins-rdma restates): the state of NICs, queue pairs, switch ports and links in HBM, the events of
+// one NIC host or one switch in one slot in ns-3's order, and the slot's end (finish, exact idle
+// skip). Host and device functions: the CUDA kernel (tr_kernel.cu) runs them a warp per entity, and
+// a CPU harness of the tests runs the same code an entity at a time.
+//
+// The model (reference: src/rdma/rstep.cuh, src/rdma/rdma.h). Time runs in slots of D ns, the
+// shortest link delay: a frame that starts in slot s arrives in slot s + 1 or later, so within a slot
+// every NIC and every switch handles its own events alone. A link files its frames by the slot they
+// arrive in (a ring of buckets, each tagged with its slot). Simultaneous events follow ns-3's order:
+// their chains of scheduling leads back to the flows' starts (tr_chain.cuh), here with their oldest
+// runs in a ring of immutable tail nodes shared by all chains.
+//
+// Exactness: integer and IEEE double arithmetic only, no contraction (built with --fmad=false and
+// -ffp-contract=off; fma() where the reference's -march=native build fuses, in tr_cc.cuh).
+#pragma once
+#include "tb_common.cuh"
+#include "tr_chain.cuh"
+#include "tr_mmu.cuh"
+#include "tr_nic.cuh"
+
+#include <climits>
+
+namespace tr
+{
+
+// ------------------------------------------------------------------ records
+constexpr int RUNS = 6;        // a chain's inline runs (newest first); older ones in tail nodes
+constexpr int MAX_DUE = 64;    // DCQCN timers a NIC runs in one slot, at most
+constexpr int PG = 3;          // the data priority's queue
+constexpr uint32_t PFC_BYTES = 43;
+
+enum : uint8_t
+{
+    K_DATA = 0,
+    K_ACK,
+    K_NACK,
+    K_PAUSE,
+    K_RESUME
+};
+
+// an event's chain: its runs newest first, the tail node holding the runs after r[RUNS - 1] (its
+// position + 1; 0: none), the hash of the leads since its root (a flow's StartApplication; 1 + the
+// flow's place in start order, over all worlds)
+struct Chain
+{
+    ChainRun r[RUNS];
+    uint64_t tail;
+    uint64_t hash;
+    uint32_t root, pad;
+};
+static_assert(sizeof(Chain) == 72, "Chain");
+
+// a run spilled out of a chain: immutable once written; pos tells whether the ring has since
+// reused its place
+struct TailNode
+{
+    uint32_t code, cnt;
+    uint64_t next, pos;
+};
+
+// a frame's contents (the reference's wire format: INT hop words, flow, sequence, size, ...)
+struct Pkt
+{
+    uint64_t hop[MAX_HOP];
+    uint32_t flow;
+    uint32_t seq;   // data: its first byte; ACK / NACK: the receiver's next expected byte
+    uint16_t size;  // bytes on the wire
+    uint16_t nhop;
+    uint8_t kind;
+    uint8_t ecn;    // 3: congestion experienced
+    uint8_t cnp;    // ACK / NACK: the ECN echo
+    uint8_t q;      // PFC: the paused queue
+    uint8_t inport; // queued at a switch: its ingress port
+    uint8_t ord;    // on a link: the arrival's ordinal among its sender's event's
+    uint16_t sport;
+    uint16_t src, dst; // hosts (numbered over all worlds)
+};
+static_assert(sizeof(Pkt) == 64, "Pkt");
+
+// a frame on a link: its arrival time, the chain of the event that sent it, its contents
+struct Frame
+{
+    int64_t ts;
+    Chain c;
+    Pkt p;
+};
+static_assert(sizeof(Frame) == 144, "Frame");
+
+// a NIC (QbbNetDevice + RdmaEgressQueue of a host with one link)
+struct Nic
+{
+    int64_t tc_at;        // its TransmitComplete (-1: the device is ready)
+    int64_t ns_at;        // its m_nextSend (-1: none)
+    int64_t wake;         // the earliest time it must run without input
+    int64_t due_min;      // at most its queue pairs' earliest DCQCN timer (INT64_MAX: none)
+    long long ob_last;    // its out link's last bucket tag written (slot << 16 | frames)
+    uint32_t paused;      // PFC-paused queues (bits)
+    int ackq_head, ackq_n;
+    int qp_n, rr;         // its queue-pair list's length; the last one served
+    int next_start, start_end; // its flows, in start order, still to start
+};
+
+// a sending queue pair: its rate state (tr_cc.cuh), its NIC view (tr_nic.cuh), its DCQCN timers
+struct Qp
+{
+    QpRate r;
+    QpSend q;
+    int64_t t[3]; // alpha update, rate-decrease check, rate increase (-1: none)
+};
+struct QpChains
+{
+    Chain c[3];
+};
+
+// a switch port: its transmission, PAUSE state, two queues (0: PFC frames; PG: data and ACKs),
+// byte counters, buffer counters as ingress and egress, ECN random stream
+struct Port
+{
+    int64_t tc_at;
+    long long ob_last;
+    uint64_t tx_bytes;
+    uint32_t paused;
+    int q0_head, q0_n, q3_head, q3_n;
+    uint32_t bytes_total;
+    MmuPort mmu;
+    tb::Rng rng;
+};
+
+struct SwState
+{
+    MmuSwitch mmu;
+};
+
+// static set-up
+struct RWorld
+{
+    NicParams nic;
+    CcParams cc;
+    int ecn, qbb, rate_bound;
+    uint32_t buffer_size;
+    int64_t alpha_int, dec_int, rp_int; // DCQCN timer intervals (ns)
+    int first_flow, n_flows;             // the world's flows (global ids)
+};
+struct HostInfo
+{
+    int world, link_in, link_out;
+};
+struct SwInfo
+{
+    int world, deg, pbase, hbase; // its world, ports, first port, its world's first host
+    uint32_t seed;                 // ECMP hash seed: its node id in its world
+    uint32_t rt_off;               // its routes towards its world's hosts
+};
+struct PortInfo
+{
+    int link_in, link_out;
+    uint64_t bps;                  // its out link's rate
+    uint32_t hdrm_cap, shift, kmin, kmax;
+    double pmax;
+};
+struct LinkInfo
+{
+    int64_t delay;
+    uint64_t bps;
+    uint64_t moff;   // its first frame slot in msg
+    uint32_t coff;   // its first bucket tag in msg_cnt
+    uint16_t nb, cap;
+};
+struct FlowInfo
+{
+    int src, dst;       // hosts over all worlds
+    uint64_t size;
+    int64_t start;
+    uint32_t sport, win;
+    uint64_t base_rtt;
+    Chain start_chain;
+};
+
+// the run's control: the slot, its end, the counters of the slot barrier
+struct RCtl
+{
+    int64_t slot;
+    int64_t slots_run;
+    unsigned long long next_wake;
+    unsigned int flows_done;
+    unsigned int activity;
+    unsigned int arrive, gen;
+    int finished, error;
+};
+
+// counters (the reference's event counters, same indices)
+enum
+{
+    EV_DROP = 0,
+    EV_MARK = 1,
+    EV_PAUSE = 2,
+    EV_RESUME = 3,
+    EV_OVF_TX = 4,
+    EV_OVF_QUEUE = 5,
+    EV_OVF_ACKQ = 6,
+    EV_OVF_QPS = 7,
+    EV_UNDECIDED = 8,
+    EV_LOST_TAIL = 9,
+    EV_ACK_DONE = 10,
+    EV_NACK = 11,
+    EV_OVF_DUE = 12,
+    EV_LATE_DATA = 13,
+    EV_HOST_EVENTS = 20,
+    EV_SWITCH_EVENTS = 21,
+    EV_FRAMES_SENT = 22,
+    EV_HOST_ACK_EVENTS = 23,
+    EV_HOST_DATA_EVENTS = 24,
+    EV_TIMEOUT = 36,
+    EV_N = 40
+};
+
+// every array of a run (device pointers in the kernel, host pointers in the CPU harness)
+struct RSim
+{
+    int H, S, F, W, P; // hosts, switches, flows, worlds, switch ports
+    int64_t D;         // the slot (ns)
+    int64_t max_slots;
+    const RWorld *world;
+    const HostInfo *hinfo;
+    Nic *nic;
+    Chain *h_tc, *h_ns;
+    Pkt *ackq;
+    int ackq_cap;
+    int *qps;
+    int qps_cap;
+    const SwInfo *sinfo;
+    SwState *sw;
+    const PortInfo *pinfo;
+    Port *port;
+    Chain *p_tc;
+    Pkt *q0, *q3;
+    int q0_cap, q3_cap;
+    const uint32_t *rt; // per (switch, host): first port index in rtp, count
+    const uint8_t *rtp;
+    const FlowInfo *flow;
+    const int *start_list;
+    const uint32_t *root_rank;
+    Qp *qp;
+    QpChains *qc;
+    RxQp *rx;
+    int64_t *fct;
+    const LinkInfo *link;
+    Frame *msg;
+    long long *msg_cnt;
+    unsigned int *pend;
+    int pend_n;
+    TailNode *tail;
+    unsigned long long *tail_cnt;
+    uint64_t tail_mask;
+    unsigned long long *ev;
+    RCtl *ctl;
+};
+
+// ------------------------------------------------------------------ memory shared between entities
+// Frames, bucket tags and tail nodes are written by other entities (other SMs) in earlier slots:
+// read from L2, never from a stale L1 line.
+#ifdef __CUDA_ARCH__
+__device__ __forceinline__ long long ld_tag(const long long *p) { return __ldcg(p); }
+__device__ __forceinline__ TailNode ld_tail(const TailNode *p)
+{
+    TailNode n;
+    const uint2 a = __ldcg(reinterpret_cast<const uint2 *>(p));
+    n.code = a.x;
+    n.cnt = a.y;
+    n.next = __ldcg(&p->next);
+    n.pos = __ldcg(&p->pos);
+    return n;
+}
+__device__ __forceinline__ void ld_frame(Frame &f, const Frame *src)
+{
+    const uint4 *s = reinterpret_cast<const uint4 *>(src);
+    uint4 *d = reinterpret_cast<uint4 *>(&f);
+#pragma unroll
+    for (int i = 0; i < (int)(sizeof(Frame) / 16); i++)
+        d[i] = __ldcg(s + i);
+}
+__device__ __forceinline__ unsigned long long atom_add(unsigned long long *p, unsigned long long v) { return atomicAdd(p, v); }
+__device__ __forceinline__ unsigned atom_add(unsigned *p, unsigned v) { return atomicAdd(p, v); }
+__device__ __forceinline__ void atom_min(unsigned long long *p, unsigned long long v) { atomicMin(p, v); }
+#else
+inline long long ld_tag(const long long *p) { return *p; }
+inline TailNode ld_tail(const TailNode *p) { return *p; }
+inline void ld_frame(Frame &f, const Frame *src) { f = *src; }
+inline unsigned long long atom_add(unsigned long long *p, unsigned long long v)
+{
+    const unsigned long long o = *p;
+    *p += v;
+    return o;
+}
+inline unsigned atom_add(unsigned *p, unsigned v)
+{
+    const unsigned o = *p;
+    *p += v;
+    return o;
+}
+inline void atom_min(unsigned long long *p, unsigned long long v)
+{
+    if (v < *p)
+        *p = v;
+}
+#endif
+TR_HD void count(const RSim &s, int i, unsigned long long n = 1) { atom_add(&s.ev[i], n); }
+
+// ------------------------------------------------------------------ event order
+// the chain of an event that the event with chain `par` schedules with `code`; a run pushed out of
+// the inline runs goes to a new tail node (reference: cpush, src/rdma/rstep.cuh:233-290)
+TR_HD void chain_push(const RSim &s, Chain &out, uint32_t code, const Chain &par)
+{
+    Chain c;
+    if (par.r[0].code == code)
+    {
+        c = par;
+        if (c.r[0].cnt != 0xFFFFFFFFu)
+            c.r[0].cnt++;
+    }
+    else
+    {
+        c.r[0].code = code;
+        c.r[0].cnt = 1;
+        for (int i = 1; i < RUNS; i++)
+            c.r[i] = par.r[i - 1];
+        c.root = par.root;
+        c.tail = par.tail;
+        c.pad = 0;
+        if (par.r[RUNS - 1].code)
+        {
+            const uint64_t pos = atom_add(s.tail_cnt, 1ull) + 1;
+            TailNode &n = s.tail[(pos - 1) & s.tail_mask];
+            n.code = par.r[RUNS - 1].code;
+            n.cnt = par.r[RUNS - 1].cnt;
+            n.next = par.tail;
+            n.pos = pos;
+            c.tail = pos;
+        }
+    }
+    c.hash = chain_hash(par.hash, code);
+    out = c;
+}
+
+// a chain's runs, newest first, as a stream of (code, repetitions): a virtual first event `code0`
+// (0: none) merged into the chain's first run when equal, the inline runs, then its tail nodes
+struct RunWalk
+{
+    const Chain *c;
+    int i;          // the inline run (RUNS: in the tail; -1: the virtual event)
+    uint64_t node;  // the tail node's position
+    uint64_t next;
+    uint32_t code;  // 0: the end
+    uint32_t left;
+    bool lost;      // the ring reused a tail node this chain needs
+
+    TR_HD void start(const RSim &s, const Chain &ch, uint32_t code0)
+    {
+        c = &ch;
+        node = next = 0;
+        lost = false;
+        if (code0 && ch.r[0].code == code0)
+        {
+            i = 0;
+            code = code0;
+            left = ch.r[0].cnt == 0xFFFFFFFFu ? ch.r[0].cnt : ch.r[0].cnt + 1;
+        }
+        else if (code0)
+        {
+            i = -1;
+            code = code0;
+            left = 1;
+        }
+        else
+        {
+            i = 0;
+            load(s);
+        }
+    }
+    TR_HD void load(const RSim &s)
+    {
+        if (i < RUNS)
+        {
+            code = c->r[i].code;
+            left = c->r[i].cnt;
+            if (code)
+                return;
+            if (i < RUNS - 1 || c->tail == 0)
+                return; // (the chain ends)
+            i = RUNS;
+            node = c->tail;
+        }
+        if (node == 0)
+        {
+            code = 0;
+            return;
+        }
+        const TailNode n = ld_tail(&s.tail[(node - 1) & s.tail_mask]);
+        if (n.pos != node)
+        {
+            lost = true;
+            code = 0;
+            return;
+        }
+        code = n.code;
+        left = n.cnt;
+        next = n.next;
+    }
+    TR_HD void step(const RSim &s)
+    {
+        if (i < RUNS)
+        {
+            i++;
+            if (i == RUNS)
+                node = c->tail;
+        }
+        else
+            node = next;
+        load(s);
+    }
+};
+
+// which of two simultaneous events ns-3 runs first: < 0 a (its chain cpush(pa, a); pa 0: a itself),
+// > 0 b, 0 undecided; *inexact: the decision met a reused tail node. The order of tr_chain.cuh's
+// chain_order, over chains whose older runs lie in tail nodes (reference: ccmp and ccmp_walk,
+// src/rdma/rstep.cuh:409-560, without its memo of decisions)
+TR_HD int chain_cmp(const RSim &s, uint32_t pa, const Chain &a, uint32_t pb, const Chain &b, bool *inexact)
+{
+    *inexact = false;
+    const uint64_t ha = pa ? chain_hash(a.hash, pa) : a.hash, hb = pb ? chain_hash(b.hash, pb) : b.hash;
+    if (a.root && b.root && a.root != b.root && ha == hb)
+        return s.root_rank[a.root - 1] < s.root_rank[b.root - 1] ? -1 : 1;
+    RunWalk A, B;
+    A.start(s, a, pa);
+    B.start(s, b, pb);
+    int ord = 0;
+    for (;;)
+    {
+        const uint32_t ca = A.code, cb = B.code;
+        if (ca == 0 || cb == 0)
+        {
+            *inexact = (ca == 0 && A.lost) || (cb == 0 && B.lost);
+            if (ca == 0 && cb == 0)
+            {
+                if (a.root && b.root && a.root != b.root)
+                    return a.root < b.root ? -1 : 1;
+                return ord;
+            }
+            if (ca == 0)
+                return A.lost ? ord : -1;
+            return B.lost ? ord : 1;
+        }
+        if (ca >> CODE_ORD_BITS != cb >> CODE_ORD_BITS)
+            return ca > cb ? -1 : 1;
+        if (ca != cb)
+            ord = (ca & CODE_ORD_MAX) > (cb & CODE_ORD_MAX) ? -1 : 1;
+        // one tail node, at one place in it: the rest is a common lineage
+        if (A.i >= RUNS && B.i >= RUNS && A.node == B.node && A.left == B.left)
+            return ord;
+        const uint32_t m = A.left < B.left ? A.left : B.left;
+        A.left -= m;
+        B.left -= m;
+        if (A.left == 0)
+            A.step(s);
+        if (B.left == 0)
+            B.step(s);
+    }
+}
+
+// does event a (time ta, chain cpush(pa, a)) run before event b? Undecided ties keep b, the
+// earlier candidate; they and decisions on reused tail nodes are counted
+TR_HD bool runs_before(const RSim &s, int64_t ta, uint32_t pa, const Chain &a, int64_t tb, uint32_t pb, const Chain &b)
+{
+    if (ta != tb)
+        return ta < tb;
+    bool inexact;
+    const int c = chain_cmp(s, pa, a, pb, b, &inexact);
+    if (inexact)
+        count(s, EV_LOST_TAIL);
+    if (c == 0)
+        count(s, EV_UNDECIDED);
+    return c < 0;
+}
+
+// ------------------------------------------------------------------ links
+TR_HD int64_t link_tx_ns(const LinkInfo &l, uint32_t bytes) { return tx_ns(l.bps, bytes); }
+
+// a sender's place in its out link's ring: the bucket of the slot its frames arrive in
+struct OutLink
+{
+    int link;
+    LinkInfo li;
+    int64_t lo, hi;      // the open bucket's times (hi 0: none open)
+    uint64_t base;       // its first frame in msg
+    uint32_t tag_at;     // its tag in msg_cnt
+    uint32_t n;          // frames in it
+    long long last;      // the last tag written (kept between slots)
+
+    TR_HD void open(const RSim &s, int l, long long last_tag)
+    {
+        link = l;
+        li = s.link[l];
+        hi = 0;
+        last = last_tag;
+    }
+    TR_HD void flush(const RSim &s)
+    {
+        if (hi == 0)
+            return;
+        last = (long long)(lo / s.D) << 16 | n;
+        s.msg_cnt[tag_at] = last;
+        hi = 0;
+    }
+    // room for a frame arriving at ts (null: the bucket is full, counted)
+    TR_HD Frame *push(const RSim &s, int64_t ts)
+    {
+        if (ts >= hi)
+        {
+            flush(s);
+            const int64_t a = ts / s.D;
+            const int b = (int)(a % li.nb);
+            tag_at = li.coff + (uint32_t)b;
+            lo = a * s.D;
+            hi = lo + s.D;
+            base = li.moff + (uint64_t)b * li.cap;
+            n = (last >> 16) == a ? (uint32_t)(last & 0xFFFF) : 0;
+            s.pend[a % s.pend_n] = 1;
+        }
+        if (n >= li.cap)
+        {
+            count(s, EV_OVF_TX);
+            return nullptr;
+        }
+        return s.msg + base + n++;
+    }
+};
+
+// the frames of a link arriving in slot t: their count and first index in msg
+TR_HD int bucket_of(const RSim &s, int link, int64_t t, uint64_t *base)
+{
+    const LinkInfo &l = s.link[link];
+    const int b = (int)(t % l.nb);
+    const long long tag = ld_tag(&s.msg_cnt[l.coff + b]);
+    *base = l.moff + (uint64_t)b * l.cap;
+    return (tag >> 16) == t ? (int)(tag & 0xFFFF) : 0;
+}
+
+// the code of a frame's arrival: lead its tx time + the link's delay, its ordinal
+TR_HD uint32_t arrival_code(const LinkInfo &l, const Frame &f) { return event_code(link_tx_ns(l, f.p.size) + l.delay, f.p.ord); }
+
+// ------------------------------------------------------------------ a NIC host's slot
+struct Due
+{
+    int64_t at;
+    int flow, kind;
+};
+
+// a NIC's running event
+struct HostEv
+{
+    const RSim *s;
+    const RWorld *w;
+    int h;
+    Nic n;
+    OutLink out;
+    int64_t now;
+    Chain cur;
+    int ord;   // events the running event has scheduled
+    int nout;  // frames sent this slot
+};
+
+TR_HD void h_transmit(HostEv &e, Pkt p)
+{
+    const RSim &s = *e.s;
+    const int64_t tx = link_tx_ns(e.out.li, p.size);
+    e.n.tc_at = e.now + tx;
+    chain_push(s, s.h_tc[e.h], event_code(tx, e.ord++), e.cur);
+    p.ord = (uint8_t)(e.ord < 255 ? e.ord : 255);
+    e.ord++;
+    e.nout++;
+    const int64_t ts = e.now + tx + e.out.li.delay;
+    Frame *f = e.out.push(s, ts);
+    if (!f)
+        return;
+    f->ts = ts;
+    f->c = e.cur;
+    f->p = p;
+}
+
+TR_HD void h_next_send(HostEv &e, int64_t at)
+{
+    e.n.ns_at = at;
+    chain_push(*e.s, e.s->h_ns[e.h], event_code(at - e.now, e.ord++), e.cur);
+}
+
+// QbbNetDevice::DequeueAndTransmit of a host: the ACK queue first, then the next queue pair in
+// round robin that can send, else the NIC's next send time
+TR_HD void h_dequeue(HostEv &e)
+{
+    const RSim &s = *e.s;
+    if (e.n.tc_at >= 0)
+        return;
+    int *list = s.qps + (size_t)e.h * s.qps_cap;
+    auto view = [&](int f) { return QpView{s.qp[f].r, s.qp[f].q}; };
+    const int idx = next_qindex(e.w->nic, e.n.paused, e.n.ackq_n, list, &e.n.qp_n, e.n.rr, e.now, view);
+    if (idx == -1)
+    {
+        const Pkt p = s.ackq[(size_t)e.h * s.ackq_cap + e.n.ackq_head];
+        e.n.ackq_head = e.n.ackq_head + 1 == s.ackq_cap ? 0 : e.n.ackq_head + 1;
+        e.n.ackq_n--;
+        h_transmit(e, p);
+        return;
+    }
+    if (idx >= 0)
+    {
+        const int f = list[idx];
+        e.n.rr = idx;
+        Qp &q = s.qp[f];
+        const FlowInfo &fi = s.flow[f];
+        // the frame's size and sequence number first; the queue pair's pacing after its start
+        const uint64_t left = bytes_left(q.r, q.q);
+        const uint32_t payload = left < e.w->nic.mtu ? (uint32_t)left : e.w->nic.mtu;
+        Pkt p = {};
+        p.kind = K_DATA;
+        p.flow = (uint32_t)f;
+        p.src = (uint16_t)fi.src;
+        p.dst = (uint16_t)fi.dst;
+        p.sport = (uint16_t)fi.sport;
+        p.seq = (uint32_t)q.r.snd_nxt;
+        p.size = (uint16_t)data_size(e.w->nic, payload);
+        h_transmit(e, p);
+        uint32_t seq;
+        next_data(e.w->nic, q.r, q.q, e.now, e.w->rate_bound != 0, &seq);
+        return;
+    }
+    const int64_t t = next_send_at(e.w->nic, list, e.n.qp_n, e.now, view);
+    if (e.n.ns_at < 0 && t >= 0)
+        h_next_send(e, t);
+}
+
+// a DCQCN timer of flow f set for t (its NIC's lower bound follows)
+TR_HD void h_timer_set(HostEv &e, int f, int kind, int64_t lead)
+{
+    const RSim &s = *e.s;
+    Qp &q = s.qp[f];
+    q.t[kind] = e.now + lead;
+    if (q.t[kind] < e.n.due_min)
+        e.n.due_min = q.t[kind];
+    chain_push(s, s.qc[f].c[kind], event_code(lead, e.ord++), e.cur);
+}
+
+// RdmaHw::ReceiveAck
+TR_HD void h_ack(HostEv &e, const Pkt &p)
+{
+    const RSim &s = *e.s;
+    const RWorld &w = *e.w;
+    const int f = (int)p.flow;
+    Qp &q = s.qp[f];
+    if (q.q.done)
+    {
+        count(s, EV_ACK_DONE);
+        return;
+    }
+    const unsigned r = ack_received(w.nic, w.cc, q.r, q.q, p.seq, p.kind == K_NACK, p.cnp != 0, p.hop, p.nhop);
+    if (r & ACK_COMPLETED)
+    {
+        q.t[0] = q.t[1] = q.t[2] = -1;
+        s.fct[f] = e.now - s.flow[f].start;
+        atom_add(&s.ctl->flows_done, 1u);
+    }
+    if (r & ACK_CNP)
+    {
+        // the first CNP: the alpha update and, a nanosecond after the decrease interval, its check
+        if (r >> 4 & T_ALPHA)
+            h_timer_set(e, f, 0, w.alpha_int);
+        if (r >> 4 & T_DEC)
+            h_timer_set(e, f, 1, w.dec_int + 1);
+    }
+    if ((r & ACK_RATE_SET) && e.n.ns_at >= 0 && q.q.next_avail < e.n.ns_at)
+        h_next_send(e, q.q.next_avail < e.now ? e.now : q.q.next_avail);
+    h_dequeue(e);
+}
+
+// RdmaHw::ReceiveUdp: the receiver's go-back-N check, an ACK or NACK into the ACK queue
+TR_HD void h_data(HostEv &e, const Pkt &p)
+{
+    const RSim &s = *e.s;
+    RxQp &r = s.rx[p.flow];
+    const uint32_t payload = p.size - data_hdr(e.w->nic);
+    if (r.expected >= s.flow[p.flow].size)
+        count(s, EV_LATE_DATA);
+    const int x = rx_check(e.w->nic, r, p.seq, payload, e.now);
+    if (x != RX_ACK && x != RX_NACK)
+        return;
+    if (x == RX_NACK)
+        count(s, EV_NACK);
+    Pkt a = p;
+    a.kind = x == RX_ACK ? K_ACK : K_NACK;
+    a.seq = r.expected;
+    a.cnp = p.ecn ? 1 : 0;
+    a.ecn = 0;
+    a.size = (uint16_t)ack_size(e.w->nic);
+    if (e.n.ackq_n >= s.ackq_cap)
+    {
+        count(s, EV_OVF_ACKQ);
+        return;
+    }
+    int at = e.n.ackq_head + e.n.ackq_n;
+    if (at >= s.ackq_cap)
+        at -= s.ackq_cap;
+    s.ackq[(size_t)e.h * s.ackq_cap + at] = a;
+    e.n.ackq_n++;
+    h_dequeue(e);
+}
+
+// StartApplication -> AddQueuePair -> NewQp
+TR_HD void h_start(HostEv &e, int f)
+{
+    const RSim &s = *e.s;
+    const FlowInfo &fi = s.flow[f];
+    Qp &q = s.qp[f];
+    qp_start(e.w->nic, q.r, q.q, fi.size, e.out.li.bps, fi.win, fi.base_rtt, e.now);
+    q.t[0] = q.t[1] = q.t[2] = -1;
+    if (e.n.qp_n >= s.qps_cap)
+    {
+        count(s, EV_OVF_QPS);
+        return;
+    }
+    s.qps[(size_t)e.h * s.qps_cap + e.n.qp_n++] = f;
+    h_dequeue(e);
+}
+
+// a DCQCN timer fires (UpdateAlphaMlx, CheckRateDecreaseMlx, RateIncEventTimerMlx): it restarts,
+// the decrease check may start the increase timer
+TR_HD void h_dcqcn_timer(HostEv &e, int f, int kind)
+{
+    const RWorld &w = *e.w;
+    Qp &q = e.s->qp[f];
+    if (kind == 0)
+    {
+        dcqcn_alpha(q.r, w.cc);
+        h_timer_set(e, f, 0, w.alpha_int);
+    }
+    else if (kind == 1)
+    {
+        h_timer_set(e, f, 1, w.dec_int);
+        if (dcqcn_decrease(q.r, w.cc) & T_RP)
+            h_timer_set(e, f, 2, w.rp_int);
+    }
+    else
+    {
+        h_timer_set(e, f, 2, w.rp_int);
+        dcqcn_increase(q.r, w.cc);
+    }
+}
+
+// the DCQCN timers of a NIC due before t1, in event order, into due[] (*n); the NIC's lower bound
+// made exact
+TR_HD void h_collect_due(const RSim &s, int h, Nic &n, int64_t t1, Due *due, int *ndue)
+{
+    *ndue = 0;
+    if (n.due_min >= t1)
+        return;
+    const int *list = s.qps + (size_t)h * s.qps_cap;
+    int64_t mn = INT64_MAX;
+    for (int i = 0; i < n.qp_n; i++)
+    {
+        const int f = list[i];
+        const Qp &q = s.qp[f];
+        for (int k = 0; k < 3; k++)
+            if (q.t[k] >= 0 && q.t[k] < mn)
+                mn = q.t[k];
+        for (int k = 0; k < 3; k++)
+            if (q.t[k] >= 0 && q.t[k] < t1)
+            {
+                if (*ndue == MAX_DUE)
+                {
+                    count(s, EV_OVF_DUE);
+                    continue;
+                }
+                const Due x = {q.t[k], f, k};
+                int j = (*ndue)++;
+                while (j > 0 && runs_before(s, x.at, 0, s.qc[f].c[k], due[j - 1].at, 0, s.qc[due[j - 1].flow].c[due[j - 1].kind]))
+                {
+                    due[j] = due[j - 1];
+                    j--;
+                }
+                due[j] = x;
+            }
+    }
+    n.due_min = mn;
+}
+
+// A NIC host's events of slot t in ns-3's order: arrivals on its in link, its TransmitComplete,
+// its next send, its DCQCN timers and its flows' starts. Returns whether it sent or holds frames;
+// *wake: its earliest event without input (INT64_MAX: none). due: room for MAX_DUE timers.
+// (reference: host_step<1>, src/rdma/rstep.cuh:1649-2114)
+TR_HD bool host_slot(const RSim &s, int h, int64_t t, int64_t *wake, Due *due)
+{
+    const HostInfo hi = s.hinfo[h];
+    const int64_t t1 = (t + 1) * s.D;
+    uint64_t abase;
+    const int na = bucket_of(s, hi.link_in, t, &abase);
+    Nic &ng = s.nic[h];
+    if (na == 0 && ng.wake >= t1)
+    {
+        *wake = ng.wake;
+        return false;
+    }
+    HostEv e;
+    e.s = &s;
+    e.w = &s.world[hi.world];
+    e.h = h;
+    e.n = ng;
+    e.out.open(s, hi.link_out, e.n.ob_last);
+    e.nout = 0;
+    const LinkInfo lin = s.link[hi.link_in];
+    int ndue = 0;
+    if (e.w->nic.cc == 1)
+        h_collect_due(s, h, e.n, t1, due, &ndue);
+    int ai = 0, di = 0;
+    Frame af;           // the next arrival
+    uint32_t acode = 0;
+    bool have_a = false;
+    int sf_at = -1, sf = -1;
+    int64_t sf_t = INT64_MAX;
+    for (;;)
+    {
+        if (!have_a && ai < na)
+        {
+            ld_frame(af, &s.msg[abase + ai]);
+            acode = arrival_code(lin, af);
+            have_a = true;
+        }
+        while (di < ndue && s.qp[due[di].flow].t[due[di].kind] != due[di].at)
+            di++; // (stopped or moved)
+        if (sf_at != e.n.next_start)
+        {
+            sf_at = e.n.next_start;
+            sf = sf_at < e.n.start_end ? s.start_list[sf_at] : -1;
+            sf_t = sf >= 0 ? s.flow[sf].start : INT64_MAX;
+        }
+        // candidates in the reference's order: arrival, TransmitComplete, next send, timer, start
+        int64_t ct[5];
+        ct[0] = have_a ? af.ts : INT64_MAX;
+        ct[1] = e.n.tc_at >= 0 && e.n.tc_at < t1 ? e.n.tc_at : INT64_MAX;
+        ct[2] = e.n.ns_at >= 0 && e.n.ns_at < t1 ? e.n.ns_at : INT64_MAX;
+        ct[3] = di < ndue ? due[di].at : INT64_MAX;
+        ct[4] = sf_t < t1 ? sf_t : INT64_MAX;
+        int64_t tmin = INT64_MAX;
+        for (int k = 0; k < 5; k++)
+            tmin = ct[k] < tmin ? ct[k] : tmin;
+        if (tmin == INT64_MAX)
+            break;
+        auto chain_of = [&](int k) -> const Chain & {
+            return k == 0 ? af.c : k == 1 ? s.h_tc[h] : k == 2 ? s.h_ns[h] : k == 3 ? s.qc[due[di].flow].c[due[di].kind] : s.flow[sf].start_chain;
+        };
+        int bk = -1;
+        for (int k = 0; k < 5; k++)
+        {
+            if (ct[k] != tmin)
+                continue;
+            if (bk < 0 || runs_before(s, tmin, k == 0 ? acode : 0, chain_of(k), tmin, bk == 0 ? acode : 0, chain_of(bk)))
+                bk = k;
+        }
+        e.now = tmin;
+        if (bk == 0)
+            chain_push(s, e.cur, acode, af.c);
+        else
+            e.cur = chain_of(bk);
+        e.ord = 0;
+        count(s, EV_HOST_EVENTS);
+        if (bk == 0)
+        {
+            have_a = false;
+            ai++;
+            const Pkt &p = af.p;
+            if (p.kind == K_DATA)
+            {
+                count(s, EV_HOST_DATA_EVENTS);
+                h_data(e, p);
+            }
+            else if (p.kind == K_ACK || p.kind == K_NACK)
+            {
+                count(s, EV_HOST_ACK_EVENTS);
+                h_ack(e, p);
+            }
+            else if (e.w->qbb)
+            {
+                if (p.kind == K_PAUSE)
+                    e.n.paused |= 1u << p.q;
+                else
+                {
+                    e.n.paused &= ~(1u << p.q);
+                    h_dequeue(e);
+                }
+            }
+        }
+        else if (bk == 1)
+        {
+            e.n.tc_at = -1;
+            h_dequeue(e);
+        }
+        else if (bk == 2)
+        {
+            e.n.ns_at = -1;
+            h_dequeue(e);
+        }
+        else if (bk == 3)
+        {
+            const Due x = due[di++];
+            h_dcqcn_timer(e, x.flow, x.kind);
+        }
+        else
+        {
+            e.n.next_start++;
+            h_start(e, sf);
+        }
+    }
+    bool act = e.nout > 0;
+    int64_t w = INT64_MAX;
+    if (e.n.next_start < e.n.start_end)
+        w = s.flow[s.start_list[e.n.next_start]].start;
+    e.out.flush(s);
+    e.n.ob_last = e.out.last;
+    if (e.n.ackq_n > 0 || e.n.tc_at >= 0)
+        act = true;
+    if (e.n.ns_at >= 0 && e.n.ns_at < w)
+        w = e.n.ns_at;
+    if (e.w->nic.cc == 1)
+    {
+        // (the bound made exact again if a timer of this slot left it behind)
+        if (e.n.due_min < t1)
+        {
+            const int *list = s.qps + (size_t)h * s.qps_cap;
+            int64_t mn = INT64_MAX;
+            for (int i = 0; i < e.n.qp_n; i++)
+                for (int k = 0; k < 3; k++)
+                {
+                    const int64_t x = s.qp[list[i]].t[k];
+                    mn = x >= 0 && x < mn ? x : mn;
+                }
+            e.n.due_min = mn;
+        }
+        if (e.n.due_min < w)
+            w = e.n.due_min;
+    }
+    if (e.n.tc_at >= 0 && e.n.tc_at < w)
+        w = e.n.tc_at;
+    e.n.wake = w;
+    ng = e.n;
+    *wake = w;
+    if (e.nout)
+        count(s, EV_FRAMES_SENT, (unsigned long long)e.nout);
+    return act;
+}
+
+// ------------------------------------------------------------------ a switch's slot
+// a switch port during the slot: its state, its out link, its arrivals' cursor
+struct PortEv
+{
+    Port pt;
+    OutLink out;
+    PortInfo info;
+    LinkInfo lin;
+    uint64_t abase;
+    int an, ai;
+    int nout;
+    bool have_a;
+    uint32_t acode;
+    Frame af;
+};
+
+struct SwEv
+{
+    const RSim *s;
+    const RWorld *w;
+    int x;
+    SwInfo si;
+    SwState sw;
+    PortEv *pe; // [deg]
+    int64_t now;
+    Chain cur;
+    int ord;
+};
+
+TR_HD uint32_t sw_pfc_threshold(const SwEv &e, int port) { return pfc_threshold(e.w->buffer_size, e.sw.mmu, e.pe[port].info.shift); }
+
+TR_HD void s_transmit(SwEv &e, int port, Pkt p)
+{
+    const RSim &s = *e.s;
+    PortEv &pe = e.pe[port];
+    const int64_t tx = link_tx_ns(pe.out.li, p.size);
+    pe.pt.tc_at = e.now + tx;
+    chain_push(s, s.p_tc[e.si.pbase + port], event_code(tx, e.ord++), e.cur);
+    p.ord = (uint8_t)(e.ord < 255 ? e.ord : 255);
+    e.ord++;
+    pe.nout++;
+    const int64_t ts = e.now + tx + pe.out.li.delay;
+    Frame *f = pe.out.push(s, ts);
+    if (!f)
+        return;
+    f->ts = ts;
+    f->c = e.cur;
+    f->p = p;
+}
+
+TR_HD void s_enqueue(SwEv &e, int port, int q, const Pkt &p)
+{
+    const RSim &s = *e.s;
+    Port &pt = e.pe[port].pt;
+    const size_t pi = (size_t)e.si.pbase + port;
+    if (q == 0)
+    {
+        if (pt.q0_n >= s.q0_cap)
+        {
+            count(s, EV_OVF_QUEUE);
+            return;
+        }
+        int at = pt.q0_head + pt.q0_n;
+        if (at >= s.q0_cap)
+            at -= s.q0_cap;
+        s.q0[pi * s.q0_cap + at] = p;
+        pt.q0_n++;
+    }
+    else
+    {
+        if (pt.q3_n >= s.q3_cap)
+        {
+            count(s, EV_OVF_QUEUE);
+            return;
+        }
+        int at = pt.q3_head + pt.q3_n;
+        if (at >= s.q3_cap)
+            at -= s.q3_cap;
+        s.q3[pi * s.q3_cap + at] = p;
+        pt.q3_n++;
+    }
+    pt.bytes_total += p.size;
+}
+
+// queue 0 (PFC frames) goes first; its frames pass no buffer accounting
+TR_HD void s_start_q0(SwEv &e, int port)
+{
+    const RSim &s = *e.s;
+    Port &pt = e.pe[port].pt;
+    if (pt.tc_at >= 0)
+        return;
+    const Pkt p = s.q0[((size_t)e.si.pbase + port) * s.q0_cap + pt.q0_head];
+    pt.q0_head = pt.q0_head + 1 == s.q0_cap ? 0 : pt.q0_head + 1;
+    pt.q0_n--;
+    pt.bytes_total -= p.size;
+    pt.tx_bytes += p.size;
+    s_transmit(e, port, p);
+}
+
+// QbbNetDevice::SendPfc
+TR_HD void s_send_pfc(SwEv &e, int port, bool resume)
+{
+    Pkt p = {};
+    p.kind = resume ? K_RESUME : K_PAUSE;
+    p.q = PG;
+    p.size = (uint16_t)PFC_BYTES;
+    count(*e.s, resume ? EV_RESUME : EV_PAUSE);
+    s_enqueue(e, port, 0, p);
+    if (e.pe[port].pt.q0_n > 0)
+        s_start_q0(e, port);
+}
+
+// a frame of queue PG leaves: the buffer gives its bytes back, ECN may mark it, a paused ingress
+// may resume, an HPCC data frame takes the port's INT word; then TransmitStart
+TR_HD void s_start_q3(SwEv &e, int port, Pkt p)
+{
+    const RWorld &w = *e.w;
+    PortEv &pe = e.pe[port];
+    PortEv &in = e.pe[p.inport];
+    tb::Rng &rng = pe.pt.rng;
+    const unsigned r = mmu_release(w.buffer_size, e.sw.mmu, in.pt.mmu, in.info.shift, pe.pt.mmu, p.size, w.ecn != 0, pe.info.kmin,
+                                   pe.info.kmax, pe.info.pmax, false, [&]() { return tb::rand_u01(rng); });
+    if (r & MMU_MARK)
+    {
+        p.ecn = 3;
+        count(*e.s, EV_MARK);
+    }
+    if (r & MMU_RESUME)
+        s_send_pfc(e, p.inport, true);
+    if (p.kind == K_DATA && w.nic.cc == 3)
+        int_stamp(p.hop, p.nhop, e.now, pe.pt.tx_bytes, pe.pt.bytes_total, pe.info.bps, w.cc.int_multi);
+    pe.pt.tx_bytes += p.size;
+    s_transmit(e, port, p);
+}
+
+// QbbNetDevice::DequeueAndTransmit of a switch port
+TR_HD void s_dequeue(SwEv &e, int port)
+{
+    const RSim &s = *e.s;
+    Port &pt = e.pe[port].pt;
+    if (pt.tc_at >= 0)
+        return;
+    if (pt.q0_n > 0)
+    {
+        s_start_q0(e, port);
+        return;
+    }
+    if ((pt.paused >> PG & 1) || pt.q3_n == 0)
+        return;
+    const Pkt p = s.q3[((size_t)e.si.pbase + port) * s.q3_cap + pt.q3_head];
+    pt.q3_head = pt.q3_head + 1 == s.q3_cap ? 0 : pt.q3_head + 1;
+    pt.q3_n--;
+    pt.bytes_total -= p.size;
+    s_start_q3(e, port, p);
+}
+
+// the egress port and queue of a data frame or ACK (-1: no route) (SwitchNode::GetOutDev)
+TR_HD int s_route(const RSim &s, const SwEv &e, const Pkt &p, int *q)
+{
+    const bool data = p.kind == K_DATA;
+    *q = (e.w->nic.ack_high_prio && !data) ? 0 : PG;
+    // (an ACK carries its data frame's hosts: it travels from dst to src)
+    const int src = p.src - e.si.hbase, dst = p.dst - e.si.hbase, to = data ? dst : src;
+    const uint32_t off = s.rt[2 * ((size_t)e.si.rt_off + to)], n = s.rt[2 * ((size_t)e.si.rt_off + to) + 1];
+    if (n == 0)
+        return -1;
+    return s.rtp[off + ecmp_choice(src, dst, p.sport, data, e.si.seed, (int)n)];
+}
+
+// SwitchNode::SendToDev: admission, PFC, then the egress port's queue (or straight on when idle)
+TR_HD void s_forward(SwEv &e, int inport, Pkt p, int out, int q)
+{
+    if (out < 0)
+        return;
+    if (q != 0)
+    {
+        PortEv &in = e.pe[inport];
+        const unsigned r = mmu_admit(e.w->buffer_size, e.sw.mmu, in.pt.mmu, in.info.hdrm_cap, in.info.shift, e.pe[out].pt.mmu, p.size, false);
+        if (r & MMU_DROP)
+        {
+            count(*e.s, EV_DROP);
+            return;
+        }
+        if (r & MMU_PAUSE)
+            s_send_pfc(e, inport, false);
+    }
+    p.inport = (uint8_t)inport;
+    Port &o = e.pe[out].pt;
+    if (q != 0 && o.tc_at < 0 && o.q0_n == 0 && o.q3_n == 0 && !(o.paused >> PG & 1))
+    {
+        s_start_q3(e, out, p);
+        return;
+    }
+    s_enqueue(e, out, q, p);
+    s_dequeue(e, out);
+}
+
+TR_HD void sw_peek(const RSim &s, PortEv &pe)
+{
+    if (pe.have_a || pe.ai >= pe.an)
+        return;
+    ld_frame(pe.af, &s.msg[pe.abase + pe.ai]);
+    pe.acode = arrival_code(pe.lin, pe.af);
+    pe.have_a = true;
+}
+
+// A switch's events of slot t in ns-3's order: every port's arrivals and TransmitCompletes.
+// pe: room for its ports. Returns whether it sent or holds frames.
+// (reference: switch_step's serial path, src/rdma/rstep.cuh:2583-3446)
+TR_HD bool switch_slot(const RSim &s, int x, int64_t t, PortEv *pe)
+{
+    SwEv e;
+    e.s = &s;
+    e.x = x;
+    e.si = s.sinfo[x];
+    e.w = &s.world[e.si.world];
+    e.sw = s.sw[x];
+    e.pe = pe;
+    const int deg = e.si.deg;
+    const int64_t t1 = (t + 1) * s.D;
+    bool any = false;
+    for (int p = 0; p < deg; p++)
+    {
+        PortEv &q = pe[p];
+        q.pt = s.port[e.si.pbase + p];
+        q.info = s.pinfo[e.si.pbase + p];
+        q.lin = s.link[q.info.link_in];
+        q.out.open(s, q.info.link_out, q.pt.ob_last);
+        q.an = bucket_of(s, q.info.link_in, t, &q.abase);
+        q.ai = 0;
+        q.nout = 0;
+        q.have_a = false;
+        any |= q.an > 0 || (q.pt.tc_at >= 0 && q.pt.tc_at < t1);
+    }
+    if (any)
+        for (;;)
+        {
+            // the earliest event: a port's next arrival or its TransmitComplete; ties by the chains
+            int best = -1, bk = 0;
+            int64_t bt = INT64_MAX;
+            for (int p = 0; p < deg; p++)
+            {
+                PortEv &q = pe[p];
+                sw_peek(s, q);
+                const int64_t ta = q.have_a ? q.af.ts : INT64_MAX, tc = q.pt.tc_at >= 0 && q.pt.tc_at < t1 ? q.pt.tc_at : INT64_MAX;
+                for (int k = 0; k < 2; k++)
+                {
+                    const int64_t tt = k ? tc : ta;
+                    if (tt == INT64_MAX || tt > bt)
+                        continue;
+                    if (tt < bt || best < 0)
+                    {
+                        best = p, bk = k, bt = tt;
+                        continue;
+                    }
+                    const Chain &ca = k ? s.p_tc[e.si.pbase + p] : q.af.c, &cb = bk ? s.p_tc[e.si.pbase + best] : pe[best].af.c;
+                    if (runs_before(s, tt, k ? 0 : q.acode, ca, bt, bk ? 0 : pe[best].acode, cb))
+                        best = p, bk = k;
+                }
+            }
+            if (best < 0)
+                break;
+            PortEv &q = pe[best];
+            e.now = bt;
+            e.ord = 0;
+            count(s, EV_SWITCH_EVENTS);
+            if (bk == 1)
+            {
+                e.cur = s.p_tc[e.si.pbase + best];
+                q.pt.tc_at = -1;
+                s_dequeue(e, best);
+                continue;
+            }
+            chain_push(s, e.cur, q.acode, q.af.c);
+            const Pkt pk = q.af.p;
+            q.have_a = false;
+            q.ai++;
+            if (pk.kind == K_PAUSE || pk.kind == K_RESUME)
+            {
+                if (e.w->qbb)
+                {
+                    if (pk.kind == K_PAUSE)
+                        q.pt.paused |= 1u << pk.q;
+                    else
+                    {
+                        q.pt.paused &= ~(1u << pk.q);
+                        s_dequeue(e, best);
+                    }
+                }
+                continue;
+            }
+            int qi = PG;
+            const int out = s_route(s, e, pk, &qi);
+            s_forward(e, best, pk, out, qi);
+        }
+    bool act = false;
+    unsigned long long sent = 0;
+    for (int p = 0; p < deg; p++)
+    {
+        PortEv &q = pe[p];
+        q.out.flush(s);
+        q.pt.ob_last = q.out.last;
+        if (q.nout > 0 || q.pt.q0_n > 0 || q.pt.q3_n > 0 || q.pt.tc_at >= 0)
+            act = true;
+        sent += q.nout;
+        s.port[e.si.pbase + p] = q.pt;
+    }
+    s.sw[x] = e.sw;
+    if (sent)
+        count(s, EV_FRAMES_SENT, sent);
+    return act;
+}
+
+// ------------------------------------------------------------------ the slot's end
+// After every entity ran slot t: the run ends when every flow is done or at the stop time; a slot
+// in which nothing was sent or held goes on at the earliest host event or frame arrival; nothing
+// left at all ends the run (quiescence). (reference: slot_end, src/rdma/rstep.cuh:3451-3577)
+TR_HD void slot_close(const RSim &s, int64_t t, unsigned activity, unsigned long long next_wake)
+{
+    RCtl &c = *s.ctl;
+    if (c.flows_done >= (unsigned)s.F || t + 1 >= s.max_slots)
+        c.finished = 1;
+    s.pend[t % s.pend_n] = 0;
+    int64_t next = t + 1;
+    if (activity == 0)
+    {
+        int64_t ws = next_wake != ~0ull ? (int64_t)(next_wake / (unsigned long long)s.D) : INT64_MAX;
+        for (int i = 1; i < s.pend_n; i++)
+            if (s.pend[(t + i) % s.pend_n])
+            {
+                ws = t + i < ws ? t + i : ws;
+                break;
+            }
+        if (ws != INT64_MAX && ws > next)
+            next = ws < s.max_slots ? ws : s.max_slots;
+        if (ws == INT64_MAX)
+            c.finished = 1;
+    }
+    c.slot = next;
+    c.slots_run++;
+}
+
+} // namespace tr

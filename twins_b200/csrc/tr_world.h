@@ -83,6 +83,7 @@ struct RdmaWorldParams
     int fast_react, sample_feedback;
     uint32_t int_multi, buffer_size, ecn_pcnt;
     double g, rate_first_cnp, u_target;
+    int clamp; // CLAMP_TARGET_RATE
 };
 
 struct RdmaPortCfg
@@ -229,6 +230,7 @@ inline bool build_rdma_world(RdmaWorld &w, const RdmaConfig &cfg, const std::str
     P.ecn = (int)u32("ENABLE_QCN", 1);
     P.g = num("EWMA_GAIN", 1.0 / 16);
     P.rate_first_cnp = 1.0;
+    P.clamp = (int)u32("CLAMP_TARGET_RATE", 0);
     // (MicroSeconds of an integer: the attributes are doubles)
     P.alpha_int = (int64_t)(uint64_t)num("ALPHA_RESUME_INTERVAL", 55) * 1000;
     P.dec_int = (int64_t)(uint64_t)num("RATE_DECREASE_INTERVAL", 4) * 1000;
