@@ -109,6 +109,26 @@ int tb_world_add_tcp(tb_ctx *ctx, const tb_topology *topo, int n_flows, const in
                      const long long *size, const long long *start_ns, const long long *conn,
                      const unsigned *hash_data, const unsigned *hash_ack, const tb_tcp_params *params, int *world);
 
+/* Adds one RDMA world (the reference's twins-rdma model of the HPCC fork of ns-3.17: NICs with
+ * queue pairs paced by rate, a window and go-back-N; switches with the PFC shared-buffer MMU and
+ * ECN at dequeue; DCQCN, HPCC or DCTCP) and returns its id in *world. config: the HPCC config
+ * file's "KEY VALUE" lines with any KEY=VALUE overrides applied (src/rdma/rmain.cu:100-143,
+ * 364-527); topology: TwiNS's "hosts H / switches S / link A B" text (src/rdma/rmain.cu:471-520),
+ * every link at link_bps with link_delay_ns; flows: rows of a flow file src,dst,flow_size,start_ns
+ * (src/rdma/rmain.cu:842-1021). A context holds TCP worlds or RDMA worlds, not both (TB_ERR_STATE);
+ * RDMA worlds of one context run side by side in one launch, as the reference's --batch
+ * (src/rdma/rmain.cu:1204-1362). Refusals the reference makes return TB_ERR_ARG with its reason. */
+int tb_world_add_rdma(tb_ctx *ctx, const char *config, const char *topology, int n_flows, const int *src, const int *dst,
+                      const long long *size, const long long *start_ns, unsigned long long link_bps, long long link_delay_ns,
+                      int *world);
+/* After tb_run of RDMA worlds: per flow (in file order) its start and completion time minus start
+ * (ns; -1: not done), as the reference's "id start_ns fct_ns" output (src/rdma/rmain.cu:2178-2200).
+ * tb_counters gives the run's 40 counters in the reference's order (src/rdma/rmain.cu:2239-2261:
+ * drops, marks, pauses, resumes, tx / queue / ackq / qps overflows, undecided ties, lost tails, ACKs
+ * for done QPs, NACKs, due overflow, late data); tb_run returns TB_WARN_INEXACT where the reference
+ * exits 3. */
+int tb_rdma_results(tb_ctx *ctx, int world, long long *start_ns, long long *fct_ns);
+
 /* Builds the batch's device state (routes, connections, rings) and uploads it. Called by
  * tb_run when needed; separate so that timing can exclude it. Replaces src/main.cu:807-1015. */
 int tb_prepare(tb_ctx *ctx);

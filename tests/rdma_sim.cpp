@@ -125,7 +125,7 @@ int rs_run(int n, const char **cfg, const char **topo, const char **flows, long 
         for (int x = 0; x < L.S; x++)
             if (switch_slot(s, x, t, pe.data()))
                 act++;
-        slot_close(s, t, act, wake);
+        slot_close(s, t, act, wake, ctl.flows_done);
     }
     for (int f = 0; f < L.F; f++)
         fct[f] = fctv[f];

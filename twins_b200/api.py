@@ -98,6 +98,10 @@ ENTRY_POINTS = [
     ("tb_world_add_tcp", ctypes.c_int, [ctypes.c_void_p, _P(_Topology), ctypes.c_int, _P(ctypes.c_int), _P(ctypes.c_int),
                                         _P(ctypes.c_longlong), _P(ctypes.c_longlong), _P(ctypes.c_longlong),
                                         _P(ctypes.c_uint), _P(ctypes.c_uint), _P(_TcpParams), _P(ctypes.c_int)]),
+    ("tb_world_add_rdma", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, _P(ctypes.c_int), _P(ctypes.c_int),
+                                         _P(ctypes.c_longlong), _P(ctypes.c_longlong), ctypes.c_ulonglong, ctypes.c_longlong,
+                                         _P(ctypes.c_int)]),
+    ("tb_rdma_results", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _P(ctypes.c_longlong), _P(ctypes.c_longlong)]),
     ("tb_prepare", ctypes.c_int, [ctypes.c_void_p]),
     ("tb_reset", ctypes.c_int, [ctypes.c_void_p]),
     ("tb_run", ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
@@ -357,6 +361,32 @@ class Simulator:
         self.sizes.append(len(flows))
         return wid.value
 
+    def add_rdma_world(self, config: str, topology: str, flows: Flows, link_bps: int = 100_000_000_000,
+                       link_delay_ns: int = 1000) -> int:
+        """An RDMA world (tb_world_add_rdma): the HPCC config's "KEY VALUE" text, a TwiNS topology
+        text (hosts / switches / link), the flows (src, dst, size, start_ns; conn unused)."""
+        wid = ctypes.c_int()
+        self._check(self.lib.tb_world_add_rdma(
+            self.ctx, config.encode(), topology.encode(), len(flows), _ptr(flows.src, ctypes.c_int), _ptr(flows.dst, ctypes.c_int),
+            _ptr(flows.size, ctypes.c_longlong), _ptr(flows.start_ns, ctypes.c_longlong), int(link_bps), int(link_delay_ns),
+            ctypes.byref(wid)))
+        self.sizes.append(len(flows))
+        return wid.value
+
+    def rdma_results(self, world: int) -> tuple[np.ndarray, np.ndarray]:
+        """(start_ns, fct_ns) per flow of an RDMA world; fct -1: not done."""
+        n = self.sizes[world]
+        start = np.empty(n, dtype=np.int64)
+        fct = np.empty(n, dtype=np.int64)
+        self._check(self.lib.tb_rdma_results(self.ctx, world, _ptr(start, ctypes.c_longlong), _ptr(fct, ctypes.c_longlong)))
+        return start, fct
+
+    def rdma_counters(self, world: int = 0) -> list[int]:
+        """The run's 40 RDMA counters in the reference's order."""
+        out = np.zeros(40, dtype=np.uint64)
+        self._check(self.lib.tb_counters(self.ctx, world, _ptr(out, ctypes.c_ulonglong), 40))
+        return [int(x) for x in out]
+
     def prepare(self) -> None:
         self._check(self.lib.tb_prepare(self.ctx))
 
@@ -407,6 +437,25 @@ class Simulator:
             self.close()
         except Exception:
             pass
+
+
+RDMA_COUNTERS_LINE = ("drops {0} marks {1} pauses {2} resumes {3} nacks {11} | undecided ties {8}, on lost tails {9} | "
+                      "overflows: tx {4} queue {5} ackq {6} qps {7} due {12} | acks for done QPs {10}")
+
+
+def rdma_counters_line(ev) -> str:
+    """The reference's counters line of twins-rdma (src/rdma/rmain.cu:2239-2261)."""
+    return RDMA_COUNTERS_LINE.format(*ev)
+
+
+def run_rdma_world(config: str, topology: str, flows: Flows, link_bps: int = 100_000_000_000, link_delay_ns: int = 1000,
+                   max_slots: int = 0, device: int = 0):
+    """One RDMA world: (start_ns, fct_ns, counters, stats, status)."""
+    with Simulator(device=device) as sim:
+        w = sim.add_rdma_world(config, topology, flows, link_bps, link_delay_ns)
+        status = sim.run(max_slots)
+        start, fct = sim.rdma_results(w)
+        return start, fct, sim.rdma_counters(w), sim.stats(), status
 
 
 def run_world(topo: Topology, flows: Flows, params: TcpParams, max_slots: int = 0, **kw):

@@ -35,7 +35,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # exactness: no floating-point contraction (fma() is written where ns-3 fuses), IEEE division
 NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "--fmad=false", "-prec-div=true", "-prec-sqrt=true",
            "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off"] + ARCH
-SOURCES = ["tb_kernel.cu", "tb_capi.cu"]
+SOURCES = ["tb_kernel.cu", "tb_capi.cu", "tr_kernel.cu", "tr_capi.cu"]
 
 
 def _nvcc() -> str:
@@ -54,8 +54,7 @@ def _stale(out: Path, deps) -> bool:
 
 def build(force: bool = False, verbose: bool = False) -> Path:
     LIB.mkdir(exist_ok=True)
-    # (the RDMA rules and set-up, tr_*, are not in the libraries yet)
-    deps = [d for d in list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) if not d.name.startswith("tr_")] + \
+    deps = [d for d in list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h"))] + \
         [ROOT / "include" / "twinsb200.h", Path(__file__)]
     nvcc = _nvcc()
     # every stale library's objects compile at once (each is one nvcc process), then link

@@ -4,6 +4,8 @@
 #include "tb_kernel.h"
 #include "tb_state.cuh"
 #include "tb_rng_host.h"
+#include "tr_capi.h"
+#include "tr_kernel.h"
 #include "../../include/twinsb200.h"
 
 #include <algorithm>
@@ -484,8 +486,15 @@ struct tb_ctx
     // tb_run_static: device state carved from a fixed area instead of allocated
     unsigned char *arena = nullptr;
     size_t arena_cap = 0, arena_used = 0;
+    // RDMA worlds (tb_world_add_rdma): a context holds TCP worlds or RDMA worlds
+    tr::RdmaRun *rdma = nullptr;
 
-    ~tb_ctx() { release(); }
+    ~tb_ctx()
+    {
+        release();
+        if (rdma)
+            tr::rdma_delete(rdma);
+    }
     void release()
     {
         for (void *p : allocs)
@@ -1029,6 +1038,8 @@ int tb_world_add_tcp(tb_ctx *ctx, const tb_topology *topo, int n_flows, const in
         return fail(TB_ERR_ARG, "tb_world_add_tcp: missing argument");
     if (ctx->prepared)
         return fail(TB_ERR_STATE, "the batch is already prepared");
+    if (ctx->rdma)
+        return fail(TB_ERR_STATE, "a context holds TCP worlds or RDMA worlds, not both");
     HostWorld w;
     int r = make_world(topo, n_flows, src, dst, size, start_ns, conn, hash_data, hash_ack, params, w);
     if (r)
@@ -1044,10 +1055,42 @@ int tb_world_add_tcp(tb_ctx *ctx, const tb_topology *topo, int n_flows, const in
     return TB_OK;
 }
 
+int tb_world_add_rdma(tb_ctx *ctx, const char *config, const char *topology, int n_flows, const int *src, const int *dst,
+                      const long long *size, const long long *start_ns, unsigned long long link_bps, long long link_delay_ns, int *world)
+{
+    if (!ctx)
+        return fail(TB_ERR_ARG, "tb_world_add_rdma: missing argument");
+    if (!ctx->worlds.empty() || ctx->prepared)
+        return fail(TB_ERR_STATE, "a context holds TCP worlds or RDMA worlds, not both");
+    if (!ctx->rdma)
+        ctx->rdma = tr::rdma_new(ctx->device < 0 ? 0 : ctx->device);
+    std::string err;
+    const int r = tr::rdma_add_world(ctx->rdma, config, topology, n_flows, src, dst, size, start_ns, link_bps, link_delay_ns, &err);
+    if (r < 0)
+        return fail(r, err);
+    if (world)
+        *world = r;
+    return TB_OK;
+}
+
+int tb_rdma_results(tb_ctx *ctx, int world, long long *start_ns, long long *fct_ns)
+{
+    if (!ctx || !ctx->rdma)
+        return fail(TB_ERR_STATE, "no RDMA worlds");
+    const int r = tr::rdma_results(ctx->rdma, world, start_ns, fct_ns);
+    return r ? fail(r, r == TB_ERR_STATE ? "not run yet" : "no such world") : TB_OK;
+}
+
 int tb_prepare(tb_ctx *ctx)
 {
     if (!ctx)
         return fail(TB_ERR_ARG, "ctx is NULL");
+    if (ctx->rdma)
+    {
+        std::string err;
+        const int r = tr::rdma_prepare(ctx->rdma, &err);
+        return r ? fail(r, err) : TB_OK;
+    }
     return prepare(ctx);
 }
 
@@ -1102,6 +1145,14 @@ int tb_run(tb_ctx *ctx, long long max_slots)
 {
     if (!ctx)
         return fail(TB_ERR_ARG, "ctx is NULL");
+    if (ctx->rdma)
+    {
+        std::string err;
+        const int r = tr::rdma_run(ctx->rdma, max_slots, &err);
+        if (r)
+            g_err = err;
+        return r;
+    }
     int r = prepare(ctx);
     if (r)
         return r;
@@ -1276,6 +1327,12 @@ int tb_results(tb_ctx *ctx, int world, long long *established_ns, long long *com
 
 int tb_counters(tb_ctx *ctx, int world, unsigned long long *out, int n)
 {
+    if (ctx && ctx->rdma && out && n >= 0)
+    {
+        if (world < 0 || world >= tr::rdma_worlds(ctx->rdma))
+            return fail(TB_ERR_ARG, "no such world");
+        return tr::rdma_counters(ctx->rdma, out, n) ? fail(TB_ERR_STATE, "no run yet") : TB_OK;
+    }
     if (!ctx || !out || n < 0 || world < 0 || world >= (int)ctx->worlds.size())
         return fail(TB_ERR_ARG, "bad arguments");
     if (!ctx->ran)
@@ -1353,6 +1410,30 @@ int tb_get_stats(tb_ctx *ctx, tb_stats *out)
 {
     if (!ctx || !out)
         return fail(TB_ERR_ARG, "bad arguments");
+    if (ctx->rdma)
+    {
+        // an RDMA run: host arrivals split by side (ACKs at senders), frames the NICs sent
+        tr::RStats r{};
+        tr::rdma_stats(ctx->rdma, &r);
+        tb_stats o{};
+        o.slots = r.slots;
+        o.slots_run = r.slots_run;
+        o.launches = r.launches;
+        o.kernel_ms = r.kernel_ms;
+        o.upload_ms = r.upload_ms;
+        o.host_events = r.host_events;
+        o.switch_events = r.switch_events;
+        o.packet_events = r.host_events + r.switch_events;
+        o.host_sender_events = r.host_ack_events;
+        o.host_frames = r.frames_sent;
+        o.bytes_h2d = r.bytes_h2d;
+        o.bytes_d2h = r.bytes_d2h;
+        o.grid = r.grid;
+        o.host_lanes = 1;
+        o.warps_per_block = tr::RDMA_WARPS;
+        *out = o;
+        return TB_OK;
+    }
     *out = ctx->stats;
     return TB_OK;
 }

@@ -1,0 +1,121 @@
+// twins-b200: the RDMA model's slot kernel. One persistent cooperative launch runs many slots: a
+// warp owns NIC hosts and switches (the same ones every slot, so their records stay in its SM's L1)
+// and runs each one's events of the slot (tr_sim.cuh: host_slot, switch_slot); a grid barrier ends
+// the slot and its last block applies the slot's end (finish, exact idle skip). Every wait is
+// bounded: a barrier that waits too long sets the run's error flag and the launch returns.
+// (reference: rdma_slot / rdma_persist / slot_end, src/rdma/rstep.cuh:3451-3577, 4020-4214)
+#include "tr_kernel.h"
+
+namespace tr
+{
+
+constexpr long long BARRIER_SPIN_LIMIT = 1ll << 22; // polls of ~64 ns: a quarter of a second or more
+
+__device__ __forceinline__ unsigned ld_volatile(const unsigned *p) { return *(const volatile unsigned *)p; }
+
+// a warp's scratch in shared memory: the DCQCN timers of a NIC's slot, a switch's ports
+__host__ __device__ inline size_t warp_scratch_bytes(int max_deg)
+{
+    return (sizeof(Due) * MAX_DUE + sizeof(PortEv) * (size_t)max_deg + 15) & ~(size_t)15;
+}
+
+__global__ void __launch_bounds__(RDMA_WARPS * 32) rdma_slot_kernel(RSim s, int slots, int max_deg)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int blk_last;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int gwarp = blockIdx.x * RDMA_WARPS + warp, nwarps = gridDim.x * RDMA_WARPS;
+    unsigned char *mine = smem + warp_scratch_bytes(max_deg) * warp;
+    Due *due = reinterpret_cast<Due *>(mine);
+    PortEv *pe = reinterpret_cast<PortEv *>(mine + sizeof(Due) * MAX_DUE);
+    RCtl *ctl = s.ctl;
+    volatile RCtl *vc = ctl;
+    const int units = s.H + s.S;
+    for (int it = 0; it < slots; it++)
+    {
+        if (vc->finished)
+            return;
+        const int64_t t = vc->slot;
+        if (lane == 0)
+            for (int u = gwarp; u < units; u += nwarps)
+            {
+                if (u < s.H)
+                {
+                    int64_t w = INT64_MAX;
+                    if (host_slot(s, u, t, &w, due))
+                        atomicAdd(&ctl->activity, 1u);
+                    if (w != INT64_MAX)
+                        atomicMin(&ctl->next_wake, (unsigned long long)w);
+                }
+                else if (switch_slot(s, u - s.H, t, pe))
+                    atomicAdd(&ctl->activity, 1u);
+            }
+        __syncthreads();
+        unsigned g = 0;
+        if (threadIdx.x == 0)
+        {
+            g = ld_volatile(&ctl->gen);
+            __threadfence();
+            blk_last = atomicAdd(&ctl->arrive, 1u) + 1 == gridDim.x;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            if (blk_last)
+            {
+                __threadfence();
+                const unsigned act = atomicExch(&ctl->activity, 0u);
+                const unsigned long long wake = atomicExch(&ctl->next_wake, ~0ull);
+                const unsigned done = atomicAdd(&ctl->flows_done, 0u);
+                slot_close(s, t, act, wake, done);
+                vc->arrive = 0;
+                __threadfence();
+                atomicAdd(&ctl->gen, 1u);
+            }
+            else
+            {
+                long long spins = 0;
+                while (ld_volatile(&ctl->gen) == g)
+                {
+                    if (++spins > BARRIER_SPIN_LIMIT)
+                    {
+                        atomicExch(&ctl->error, 1);
+                        atomicExch(&ctl->finished, 1);
+                        atomicAdd(&s.ev[EV_TIMEOUT], 1ull);
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+            }
+            __threadfence();
+        }
+        __syncthreads();
+    }
+}
+
+int rdma_launch_shape(int max_deg, int units, int *grid, size_t *smem)
+{
+    *smem = warp_scratch_bytes(max_deg) * RDMA_WARPS;
+    if (cudaFuncSetAttribute((const void *)rdma_slot_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem) != cudaSuccess)
+        return (int)cudaGetLastError();
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)rdma_slot_kernel, RDMA_WARPS * 32, *smem) != cudaSuccess)
+        return (int)cudaGetLastError();
+    if (per_sm < 1)
+        return (int)cudaErrorInvalidConfiguration;
+    // a warp per entity where they fit at once; else every resident warp takes several
+    const int want = (units + RDMA_WARPS - 1) / RDMA_WARPS;
+    *grid = want < per_sm * sms ? want : per_sm * sms;
+    return 0;
+}
+
+int rdma_launch(const RSim &s, int grid, size_t smem, int slots, int max_deg, cudaStream_t stream)
+{
+    void *args[] = {(void *)&s, (void *)&slots, (void *)&max_deg};
+    const cudaError_t e = cudaLaunchCooperativeKernel((const void *)rdma_slot_kernel, dim3(grid), dim3(RDMA_WARPS * 32), args, smem, stream);
+    return e == cudaSuccess ? 0 : (int)e;
+}
+
+} // namespace tr

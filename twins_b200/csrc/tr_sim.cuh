@@ -206,11 +206,13 @@ enum
     EV_NACK = 11,
     EV_OVF_DUE = 12,
     EV_LATE_DATA = 13,
-    EV_HOST_EVENTS = 20,
-    EV_SWITCH_EVENTS = 21,
-    EV_FRAMES_SENT = 22,
-    EV_HOST_ACK_EVENTS = 23,
-    EV_HOST_DATA_EVENTS = 24,
+    EV_HOST_ARRIVALS = 20,   // frames a NIC received (packet-events at hosts)
+    EV_SWITCH_ARRIVALS = 21, // frames a switch received (packet-events at switches)
+    EV_HOST_FRAMES = 22,     // frames NICs sent
+    EV_HOST_ACKS = 23,       // of the NICs' arrivals: ACKs and NACKs
+    EV_HOST_DATA = 24,       // of the NICs' arrivals: data
+    EV_HOST_EVENTS = 25,     // every NIC event (arrivals, transmissions done, sends, timers, starts)
+    EV_SWITCH_EVENTS = 26,   // every switch event (arrivals, transmissions done)
     EV_TIMEOUT = 36,
     EV_N = 40
 };
@@ -262,6 +264,7 @@ struct RSim
 // read from L2, never from a stale L1 line.
 #ifdef __CUDA_ARCH__
 __device__ __forceinline__ long long ld_tag(const long long *p) { return __ldcg(p); }
+__device__ __forceinline__ unsigned ld_flag(const unsigned *p) { return __ldcg(p); }
 __device__ __forceinline__ TailNode ld_tail(const TailNode *p)
 {
     TailNode n;
@@ -285,6 +288,7 @@ __device__ __forceinline__ unsigned atom_add(unsigned *p, unsigned v) { return a
 __device__ __forceinline__ void atom_min(unsigned long long *p, unsigned long long v) { atomicMin(p, v); }
 #else
 inline long long ld_tag(const long long *p) { return *p; }
+inline unsigned ld_flag(const unsigned *p) { return *p; }
 inline TailNode ld_tail(const TailNode *p) { return *p; }
 inline void ld_frame(Frame &f, const Frame *src) { f = *src; }
 inline unsigned long long atom_add(unsigned long long *p, unsigned long long v)
@@ -875,15 +879,16 @@ TR_HD bool host_slot(const RSim &s, int h, int64_t t, int64_t *wake, Due *due)
         {
             have_a = false;
             ai++;
+            count(s, EV_HOST_ARRIVALS);
             const Pkt &p = af.p;
             if (p.kind == K_DATA)
             {
-                count(s, EV_HOST_DATA_EVENTS);
+                count(s, EV_HOST_DATA);
                 h_data(e, p);
             }
             else if (p.kind == K_ACK || p.kind == K_NACK)
             {
-                count(s, EV_HOST_ACK_EVENTS);
+                count(s, EV_HOST_ACKS);
                 h_ack(e, p);
             }
             else if (e.w->qbb)
@@ -952,7 +957,7 @@ TR_HD bool host_slot(const RSim &s, int h, int64_t t, int64_t *wake, Due *due)
     ng = e.n;
     *wake = w;
     if (e.nout)
-        count(s, EV_FRAMES_SENT, (unsigned long long)e.nout);
+        count(s, EV_HOST_FRAMES, (unsigned long long)e.nout);
     return act;
 }
 
@@ -1230,6 +1235,7 @@ TR_HD bool switch_slot(const RSim &s, int x, int64_t t, PortEv *pe)
                 continue;
             }
             chain_push(s, e.cur, q.acode, q.af.c);
+            count(s, EV_SWITCH_ARRIVALS);
             const Pkt pk = q.af.p;
             q.have_a = false;
             q.ai++;
@@ -1252,7 +1258,6 @@ TR_HD bool switch_slot(const RSim &s, int x, int64_t t, PortEv *pe)
             s_forward(e, best, pk, out, qi);
         }
     bool act = false;
-    unsigned long long sent = 0;
     for (int p = 0; p < deg; p++)
     {
         PortEv &q = pe[p];
@@ -1260,12 +1265,9 @@ TR_HD bool switch_slot(const RSim &s, int x, int64_t t, PortEv *pe)
         q.pt.ob_last = q.out.last;
         if (q.nout > 0 || q.pt.q0_n > 0 || q.pt.q3_n > 0 || q.pt.tc_at >= 0)
             act = true;
-        sent += q.nout;
         s.port[e.si.pbase + p] = q.pt;
     }
     s.sw[x] = e.sw;
-    if (sent)
-        count(s, EV_FRAMES_SENT, sent);
     return act;
 }
 
@@ -1273,10 +1275,11 @@ TR_HD bool switch_slot(const RSim &s, int x, int64_t t, PortEv *pe)
 // After every entity ran slot t: the run ends when every flow is done or at the stop time; a slot
 // in which nothing was sent or held goes on at the earliest host event or frame arrival; nothing
 // left at all ends the run (quiescence). (reference: slot_end, src/rdma/rstep.cuh:3451-3577)
-TR_HD void slot_close(const RSim &s, int64_t t, unsigned activity, unsigned long long next_wake)
+// (activity, next_wake and flows_done: the entities' sums of the slot, read by the caller)
+TR_HD void slot_close(const RSim &s, int64_t t, unsigned activity, unsigned long long next_wake, unsigned flows_done)
 {
     RCtl &c = *s.ctl;
-    if (c.flows_done >= (unsigned)s.F || t + 1 >= s.max_slots)
+    if (flows_done >= (unsigned)s.F || t + 1 >= s.max_slots)
         c.finished = 1;
     s.pend[t % s.pend_n] = 0;
     int64_t next = t + 1;
@@ -1284,7 +1287,7 @@ TR_HD void slot_close(const RSim &s, int64_t t, unsigned activity, unsigned long
     {
         int64_t ws = next_wake != ~0ull ? (int64_t)(next_wake / (unsigned long long)s.D) : INT64_MAX;
         for (int i = 1; i < s.pend_n; i++)
-            if (s.pend[(t + i) % s.pend_n])
+            if (ld_flag(&s.pend[(t + i) % s.pend_n]))
             {
                 ws = t + i < ws ? t + i : ws;
                 break;

@@ -127,6 +127,8 @@ struct RdmaWorld
 // for hosts of one link). ns-3 starts them through one ScheduleFlowInputs event per start time,
 // each scheduled by the previous one (or by main), then Application::Start, then StartApplication:
 // their start chains.
+inline bool finish_rdma_flows(RdmaWorld &w);
+
 inline bool build_rdma_flows(RdmaWorld &w, const std::string &csv)
 {
     std::istringstream f(csv);
@@ -145,6 +147,27 @@ inline bool build_rdma_flows(RdmaWorld &w, const std::string &csv)
         x.src = (int)a, x.dst = (int)b, x.size = sz, x.start = (int64_t)st;
         w.flows.push_back(x);
     }
+    return finish_rdma_flows(w);
+}
+
+// the same from arrays (a flow file's columns)
+inline bool build_rdma_flows(RdmaWorld &w, int n, const int *src, const int *dst, const long long *size, const long long *start_ns)
+{
+    w.flows.clear();
+    for (int i = 0; i < n; i++)
+    {
+        if (src[i] < 0 || dst[i] < 0 || size[i] < 0 || start_ns[i] < 0)
+            return w.error = "a flow with a negative node id, size or start", false;
+        RdmaFlow x{};
+        x.src = src[i], x.dst = dst[i], x.size = (uint64_t)size[i], x.start = start_ns[i];
+        w.flows.push_back(x);
+    }
+    return finish_rdma_flows(w);
+}
+
+// the flows read: their checks, source ports, start order and chains, the hosts' start lists
+inline bool finish_rdma_flows(RdmaWorld &w)
+{
     const int F = (int)w.flows.size(), H = w.H;
     for (RdmaFlow &x : w.flows)
     {
