@@ -78,14 +78,15 @@ struct Pkt
 };
 static_assert(sizeof(Pkt) == 64, "Pkt");
 
-// a frame on a link: its arrival time, the chain of the event that sent it, its contents
-struct Frame
+// a frame on a link: its arrival time, the chain of the event that sent it, its contents (16-byte
+// aligned: frames move as 16-byte words, ld_frame)
+struct alignas(16) Frame
 {
     int64_t ts;
     Chain c;
     Pkt p;
 };
-static_assert(sizeof(Frame) == 144, "Frame");
+static_assert(sizeof(Frame) == 144 && alignof(Frame) == 16, "Frame");
 
 // a NIC (QbbNetDevice + RdmaEgressQueue of a host with one link)
 struct Nic
@@ -963,7 +964,7 @@ TR_HD bool host_slot(const RSim &s, int h, int64_t t, int64_t *wake, Due *due)
 
 // ------------------------------------------------------------------ a switch's slot
 // a switch port during the slot: its state, its out link, its arrivals' cursor
-struct PortEv
+struct alignas(16) PortEv
 {
     Port pt;
     OutLink out;
