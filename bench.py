@@ -439,6 +439,77 @@ def serve_leg(device: int, requests: int, rate: float, serve_worlds: int):
             "capacities": caps, "clocks": clocks.summary()}
 
 
+# algorithmic bytes per RDMA packet-event, from the reference's record sizes: a switch event moves a
+# 176-byte LFrame in and out; a NIC event reads its frame, writes the frames it emits, and reads and
+# writes the queue pair (208-byte SndQP for an ACK or NACK, 16-byte RcvQP for data)
+LFRAME_B, SNDQP_B, RCVQP_B = 176, 208, 16
+
+
+def rdma_algorithmic_bytes(st: dict) -> int:
+    return (2 * LFRAME_B * st["switch_events"] + LFRAME_B * st["host_events"] + LFRAME_B * st["host_frames"]
+            + 2 * SNDQP_B * st["host_sender_events"] + 2 * RCVQP_B * (st["host_events"] - st["host_sender_events"]))
+
+
+def c3_leg(device: int, warmup: int = 3, ref: bool = True):
+    """C3: the RDMA model on FatTree k=16 (1,024 hosts, 320 switches), 50,000 all-to-all flows at 40%
+    load plus 16 incasts of 64 x 256 KB, once with DCQCN and once with HPCC-INT. Device time of the
+    slot kernel (state resident), end to end through the C ABI, the roofline of the algorithmic bytes,
+    and the reference's own twins-rdma (built for sm_100a) on the same files: its time and every FCT
+    compared."""
+    import torch
+    from twins_b200 import api, workloads
+    peak, _ = hbm_peak()
+    d = Path(tempfile.mkdtemp(prefix="twins_c3_"))
+    out = {"config": "FatTree k=16 (1,024 hosts, 320 switches, 100 Gb/s, 1 us), 50,000 web-search-like all-to-all flows at 40% load "
+                     "+ 16 incasts of 64 x 256 KB; HPCC example configuration (32 MB buffers, PFC, ECN)"}
+    for w in workloads.c3():
+        cc = w.name.split("_")[-1]
+        with api.Simulator(device=device) as sim:
+            i = sim.add_rdma_world(w.config, w.topology, w.flows)
+            sim.prepare()
+            for _ in range(warmup):
+                sim.run(300)
+            torch.cuda.synchronize()
+            status = sim.run()
+            st = sim.stats()
+            _, fct = sim.rdma_results(i)
+            ev = sim.rdma_counters(i)
+        t0 = time.perf_counter()
+        with api.Simulator(device=device) as s2:
+            j = s2.add_rdma_world(w.config, w.topology, w.flows)
+            s2.run()
+            s2.rdma_results(j)
+            st2 = s2.stats()
+        e2e_s = time.perf_counter() - t0
+        sec = st["kernel_ms"] / 1000.0
+        alg = rdma_algorithmic_bytes(st)
+        leg = {"packet_events_per_s": st["packet_events"] / sec, "seconds": sec, "packet_events": st["packet_events"],
+               "slots": st["slots"], "slots_run": st["slots_run"], "launches": st["launches"], "grid": st["grid"],
+               "flows": len(w.flows), "flows_done": int((fct >= 0).sum()), "status": status, "counters": api.rdma_counters_line(ev),
+               "e2e": {"packet_events_per_s": st["packet_events"] / e2e_s, "seconds": e2e_s, "h2d_bytes": st2["bytes_h2d"],
+                       "d2h_bytes": st2["bytes_d2h"]},
+               "roofline": {"bound": "hbm", "achieved": alg / sec / 1e9, "peak": peak, "unit": "GB/s", "frac": alg / sec / 1e9 / peak,
+                            "algorithmic_bytes": alg}}
+        exe = ROOT / "oracle" / "_ref" / "twins-rdma"
+        if ref and exe.exists():
+            cfg, topo, fl = workloads.write_rdma(w, d)
+            r = subprocess.run([str(exe), cfg.name, f"--topo={topo.name}", f"--flows={fl.name}", f"--out={w.name}.ref.fct"], cwd=d,
+                               capture_output=True, text=True, timeout=1200)
+            line = next((x for x in r.stdout.splitlines() if x.startswith("flows done")), "")
+            ref_wall = float(line.split(" in ")[1].split(" s wall")[0]) if line else None
+            want = np.full(len(w.flows), -1, dtype=np.int64)
+            for x in (d / f"{w.name}.ref.fct").read_text().splitlines() if (d / f"{w.name}.ref.fct").exists() else []:
+                a, _, f = (int(v) for v in x.split())
+                want[a] = f
+            leg["reference_gpu"] = {"rc": r.returncode, "seconds": ref_wall,
+                                    "packet_events_per_s": st["packet_events"] / ref_wall if ref_wall else None,
+                                    "counters": next((x for x in r.stdout.splitlines() if x.startswith("drops ")), ""),
+                                    "flows_equal": f"{int((want == fct).sum())}/{len(fct)}",
+                                    "binary": "oracle/_ref/twins-rdma (reference src/rdma/rmain.cu, nvcc sm_100a)"}
+        out[cc] = leg
+    return out
+
+
 def reference_arm(args, worlds, config):
     """The reference arm: the reference's CPU path for this model on the host cores, which is the
     oracle port (the reference has no CPU build of its TCP model): every world of the workload
@@ -470,7 +541,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c2s", "c4", "c5"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c2s", "c3", "c4", "c5"])
     ap.add_argument("--requests", type=int, default=200, help="C5: requests in the served stream")
     ap.add_argument("--rate", type=float, default=100.0, help="C5: request arrivals per second (Poisson)")
     ap.add_argument("--serve-worlds", type=int, default=256, help="C5: requests the server holds at once")
@@ -493,6 +564,12 @@ def main():
     rank = int(os.environ.get("RANK", 0))
     world_size = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.workload == "c3" and args.impl == "ours":
+        if rank == 0:
+            import torch
+            torch.cuda.set_device(local_rank)
+            print(json.dumps({"workload": "c3", **c3_leg(local_rank)}))
+        return
     if args.workload == "c5" and args.impl == "ours":
         if rank == 0:  # (one server on one GPU; other ranks have nothing to add)
             import torch
@@ -614,6 +691,7 @@ def main():
         extras["c4"] = c4_leg(local_rank, args.plain_sample, 3, 200)
         extras["c5"] = serve_leg(local_rank, args.requests, args.rate, args.serve_worlds)
         extras["sweep_k8"] = sweep_leg(local_rank)
+        extras["c3"] = c3_leg(local_rank)
     elif args.workload == "c4":
         extras["plain"] = plain_sample(worlds, args.plain_sample, local_rank, len(worlds) / (ms_max / 1000.0),
                                        batched=dict(enumerate(ours[w.name] for w in worlds)))

@@ -10,6 +10,7 @@ Outputs (git-ignored, they travel with the repository to the GPU machine):
     twins_b200/lib/twins128               reference's twins128 build (-DTWINS_CHAIN_RUNS=25)
     twins_b200/lib/libtwinsb200_trace.so  the same recording every enqueue (the reference's
     twins_b200/lib/twins-trace            --qtrace); twins runs twins-trace when given --qtrace
+    twins_b200/lib/twins-rdma             the reference's RDMA command line over libtwinsb200.so
 """
 from __future__ import annotations
 
@@ -28,6 +29,7 @@ SO25 = LIB / "libtwinsb200_runs25.so"
 CLI25 = LIB / "twins128"
 SO_TRACE = LIB / "libtwinsb200_trace.so"
 CLI_TRACE = LIB / "twins-trace"
+CLI_RDMA = LIB / "twins-rdma"
 # (library, front-end, extra flags): 9-run chains, 25-run chains, 9-run chains with the enqueue trace
 VARIANTS = [(SO, CLI, []), (SO25, CLI25, ["-DTB_CHAIN_RUNS=25"]), (SO_TRACE, CLI_TRACE, ["-DTB_QTRACE"])]
 
@@ -82,6 +84,9 @@ def build(force: bool = False, verbose: bool = False) -> Path:
             cmd = ["g++", "-std=c++17", "-O2", "-o", str(cli), str(CSRC / "twins_cli.cpp"),
                    f"-L{LIB}", f"-l{so.stem[3:]}", f"-Wl,-rpath,$ORIGIN"]
             subprocess.run(cmd, check=True)
+    if force or _stale(CLI_RDMA, deps + [SO]):
+        subprocess.run(["g++", "-std=c++17", "-O2", "-o", str(CLI_RDMA), str(CSRC / "twins_rdma_cli.cpp"), f"-L{LIB}", "-ltwinsb200",
+                        "-Wl,-rpath,$ORIGIN"], check=True)
     return SO
 
 

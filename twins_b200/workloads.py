@@ -244,3 +244,93 @@ def served_stream(seed: int = 1, n: int = 200, rate_per_s: float = 40.0, size_ca
                            int(rng.choice([100, 200, 400])), spray=bool(kind in ("jf", "df")))
         out.append(Request(f"c5_{i:04d}_{kind}", t, topo, flows, params))
     return out
+
+
+# ------------------------------------------------------------------ RDMA worlds (C3 shape)
+# The HPCC fork's parameters as its example configuration sets them (the reference runs its RDMA
+# validation with these: validation/hpcc/hpcc.cfg), in its "KEY VALUE" input format.
+HPCC_CONFIG = {
+    "ENABLE_QCN": "1", "USE_DYNAMIC_PFC_THRESHOLD": "1", "PACKET_PAYLOAD_SIZE": "1000", "SIMULATOR_STOP_TIME": "4.00",
+    "CC_MODE": "3", "ALPHA_RESUME_INTERVAL": "1", "RATE_DECREASE_INTERVAL": "4", "CLAMP_TARGET_RATE": "0", "RP_TIMER": "900",
+    "EWMA_GAIN": "0.00390625", "FAST_RECOVERY_TIMES": "1", "RATE_AI": "50Mb/s", "RATE_HAI": "100Mb/s", "MIN_RATE": "100Mb/s",
+    "DCTCP_RATE_AI": "1000Mb/s", "ERROR_RATE_PER_LINK": "0.0000", "L2_CHUNK_SIZE": "4000", "L2_ACK_INTERVAL": "1",
+    "L2_BACK_TO_ZERO": "0", "HAS_WIN": "1", "GLOBAL_T": "1", "VAR_WIN": "1", "FAST_REACT": "1", "U_TARGET": "0.95", "MI_THRESH": "0",
+    "INT_MULTI": "1", "MULTI_RATE": "0", "SAMPLE_FEEDBACK": "0", "PINT_LOG_BASE": "1.05", "PINT_PROB": "1.0", "RATE_BOUND": "1",
+    "ACK_HIGH_PRIO": "0", "LINK_DOWN": "0 0 0", "ENABLE_TRACE": "0",
+    "KMAX_MAP": "3 25000000000 400 50000000000 800 100000000000 1600",
+    "KMIN_MAP": "3 25000000000 100 50000000000 200 100000000000 400",
+    "PMAX_MAP": "3 25000000000 0.2 50000000000 0.2 100000000000 0.2", "BUFFER_SIZE": "32",
+}
+RDMA_CC = {"dcqcn": 1, "hpcc": 3, "dctcp": 8}
+
+
+def rdma_config(cc: str, **over) -> str:
+    cfg = {**HPCC_CONFIG, "CC_MODE": str(RDMA_CC[cc]), **{k: str(v) for k, v in over.items()}}
+    return "".join(f"{k} {v}\n" for k, v in cfg.items())
+
+
+def fattree_text(k: int) -> str:
+    """A FatTree k in TwiNS's topology format: hosts, then edge, aggregation and core switches."""
+    h, e = k ** 3 // 4, k * k // 2
+    links = [(f"h{x * (k // 2) + j}", f"s{x}") for x in range(e) for j in range(k // 2)]
+    links += [(f"s{pod * (k // 2) + b}", f"s{e + pod * (k // 2) + a}") for pod in range(k) for a in range(k // 2) for b in range(k // 2)]
+    links += [(f"s{e + pod * (k // 2) + a}", f"s{2 * e + a * (k // 2) + c}") for pod in range(k) for a in range(k // 2) for c in range(k // 2)]
+    return f"hosts {h}\nswitches {e + e + (k // 2) ** 2}\n" + "".join(f"link {a} {b}\n" for a, b in links)
+
+
+@dataclass
+class RdmaWorld:
+    name: str
+    config: str
+    topology: str
+    flows: Flows
+
+
+def c3_flows(seed: int = 1, k: int = 16, n: int = 50_000, load: float = 0.4, incasts: int = 16, fanin: int = 64,
+             incast_bytes: int = 262_144) -> Flows:
+    """All-to-all flows between seeded uniform distinct host pairs, web-search-like sizes, Poisson
+    arrivals at `load` of the hosts' 100 Gb/s; plus `incasts` bursts of `fanin` senders to one
+    seeded receiver, incast_bytes each, at seeded times within the arrivals' span."""
+    rng = np.random.default_rng(seed)
+    H = k ** 3 // 4
+    src = rng.integers(0, H, n)
+    dst = (src + rng.integers(1, H, n)) % H
+    size = web_sizes(rng, n)
+    rate = load * H * LINK_BYTES_PER_NS / web_mean()
+    start = np.cumsum(rng.exponential(1.0 / rate, n)).astype(np.int64) + 1000
+    span = int(start[-1])
+    s2, d2, z2, t2 = [src], [dst], [size], [start]
+    for _ in range(incasts):
+        r = int(rng.integers(H))
+        others = np.array([h for h in range(H) if h != r])
+        snd = rng.choice(others, fanin, replace=False)
+        t = int(rng.integers(1000, span))
+        s2.append(snd)
+        d2.append(np.full(fanin, r))
+        z2.append(np.full(fanin, incast_bytes))
+        t2.append(np.full(fanin, t))
+    src, dst, size, start = (np.concatenate(x) for x in (s2, d2, z2, t2))
+    order = np.argsort(start, kind="stable")
+    return Flows.from_arrays(src[order], dst[order], size[order], start[order])
+
+
+def c3(seed: int = 1, ccs=("dcqcn", "hpcc"), **kw) -> list[RdmaWorld]:
+    """C3: FatTree k=16 (1,024 hosts, 320 switches, 100 Gb/s, 1 us), 50,000 flows plus 16 incasts of
+    64 senders x 256 KB, once per congestion control."""
+    flows = c3_flows(seed, **kw)
+    topo = fattree_text(kw.get("k", 16))
+    return [RdmaWorld(f"c3_k16_{cc}", rdma_config(cc), topo, flows) for cc in ccs]
+
+
+def write_rdma(w: RdmaWorld, d) -> tuple:
+    """The world's files for the reference's twins-rdma: config, topology, flows."""
+    from pathlib import Path
+    d = Path(d)
+    cfg, topo, fl = d / f"{w.name}.cfg", d / f"{w.name}.topo", d / f"{w.name}.csv"
+    cfg.write_text(w.config)
+    topo.write_text(w.topology)
+    with open(fl, "w") as f:
+        f.write("src,dst,flow_size,start_ns\n")
+        for i in range(len(w.flows)):
+            f.write(f"{w.flows.src[i]},{w.flows.dst[i]},{w.flows.size[i]},{w.flows.start_ns[i]}\n")
+    return cfg, topo, fl
