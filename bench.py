@@ -450,7 +450,7 @@ def rdma_algorithmic_bytes(st: dict) -> int:
             + 2 * SNDQP_B * st["host_sender_events"] + 2 * RCVQP_B * (st["host_events"] - st["host_sender_events"]))
 
 
-def c3_leg(device: int, warmup: int = 3, ref: bool = True):
+def c3_leg(device: int, warmup: int = 3, ref: bool = True, q3cap: int = 1 << 16):
     """C3: the RDMA model on FatTree k=16 (1,024 hosts, 320 switches), 50,000 all-to-all flows at 40%
     load plus 16 incasts of 64 x 256 KB, once with DCQCN and once with HPCC-INT. Device time of the
     slot kernel (state resident), end to end through the C ABI, the roofline of the algorithmic bytes,
@@ -461,10 +461,12 @@ def c3_leg(device: int, warmup: int = 3, ref: bool = True):
     peak, _ = hbm_peak()
     d = Path(tempfile.mkdtemp(prefix="twins_c3_"))
     out = {"config": "FatTree k=16 (1,024 hosts, 320 switches, 100 Gb/s, 1 us), 50,000 web-search-like all-to-all flows at 40% load "
-                     "+ 16 incasts of 64 x 256 KB; HPCC example configuration (32 MB buffers, PFC, ECN)"}
+                     "+ 16 incasts of 64 x 256 KB; HPCC example configuration (32 MB buffers, PFC, ECN); port queues of "
+                     f"{q3cap} frames (both builds)"}
     for w in workloads.c3():
         cc = w.name.split("_")[-1]
         with api.Simulator(device=device) as sim:
+            sim.set_rdma_queue_cap(q3cap)
             i = sim.add_rdma_world(w.config, w.topology, w.flows)
             sim.prepare()
             for _ in range(warmup):
@@ -476,6 +478,7 @@ def c3_leg(device: int, warmup: int = 3, ref: bool = True):
             ev = sim.rdma_counters(i)
         t0 = time.perf_counter()
         with api.Simulator(device=device) as s2:
+            s2.set_rdma_queue_cap(q3cap)
             j = s2.add_rdma_world(w.config, w.topology, w.flows)
             s2.run()
             s2.rdma_results(j)
@@ -493,7 +496,8 @@ def c3_leg(device: int, warmup: int = 3, ref: bool = True):
         exe = ROOT / "oracle" / "_ref" / "twins-rdma"
         if ref and exe.exists():
             cfg, topo, fl = workloads.write_rdma(w, d)
-            r = subprocess.run([str(exe), cfg.name, f"--topo={topo.name}", f"--flows={fl.name}", f"--out={w.name}.ref.fct"], cwd=d,
+            r = subprocess.run([str(exe), cfg.name, f"--topo={topo.name}", f"--flows={fl.name}", f"--out={w.name}.ref.fct",
+                                f"--q3cap={q3cap}"], cwd=d,
                                capture_output=True, text=True, timeout=1200)
             line = next((x for x in r.stdout.splitlines() if x.startswith("flows done")), "")
             ref_wall = float(line.split(" in ")[1].split(" s wall")[0]) if line else None

@@ -128,6 +128,10 @@ int tb_world_add_rdma(tb_ctx *ctx, const char *config, const char *topology, int
  * for done QPs, NACKs, due overflow, late data); tb_run returns TB_WARN_INEXACT where the reference
  * exits 3. */
 int tb_rdma_results(tb_ctx *ctx, int world, long long *start_ns, long long *fct_ns);
+/* Frames a switch port's data queue holds in this context's RDMA run (default 4096, as the
+ * reference's --q3cap, src/rdma/rmain.cu:1054, 1811); a frame that finds it full is counted as an
+ * overflow (the run is then inexact). Before the first run. */
+int tb_rdma_set_queue_cap(tb_ctx *ctx, int frames);
 
 /* Builds the batch's device state (routes, connections, rings) and uploads it. Called by
  * tb_run when needed; separate so that timing can exclude it. Replaces src/main.cu:807-1015. */

@@ -33,7 +33,7 @@ const char *rs_error() { return g_err.c_str(); }
 // done) into fct (over all worlds, in world order), the counters into ev[40], the slots run into
 // *slots. Returns 0, or -1 with rs_error().
 int rs_run(int n, const char **cfg, const char **topo, const char **flows, long long *fct, unsigned long long *ev, long long *slots,
-           int tail_log2)
+           int tail_log2, int serial_only)
 {
     std::vector<RdmaWorld> worlds(n);
     std::vector<const RdmaWorld *> wp;
@@ -107,7 +107,12 @@ int rs_run(int n, const char **cfg, const char **topo, const char **flows, long 
     s.tail_mask = (1ull << tail_log2) - 1;
     s.ev = evv.data();
     s.ctl = &ctl;
-    std::vector<PortEv> pe(L.max_deg);
+    s.serial_only = serial_only;
+    std::vector<SwPort> ports(L.max_deg);
+    std::vector<SArr> arr(SW_STAGE > HOST_STAGE ? SW_STAGE : HOST_STAGE);
+    std::vector<uint16_t> ord(SW_STAGE);
+    int flags[4];
+    const SwWork work{ports.data(), arr.data(), ord.data(), flags};
     Due due[MAX_DUE];
     while (!ctl.finished)
     {
@@ -117,13 +122,13 @@ int rs_run(int n, const char **cfg, const char **topo, const char **flows, long 
         for (int h = 0; h < L.H; h++)
         {
             int64_t w = INT64_MAX;
-            if (host_slot(s, h, t, &w, due))
+            if (host_slot(s, h, t, &w, due, arr.data(), 0, 1))
                 act++;
             if (w != INT64_MAX && (unsigned long long)w < wake)
                 wake = (unsigned long long)w;
         }
         for (int x = 0; x < L.S; x++)
-            if (switch_slot(s, x, t, pe.data()))
+            if (switch_slot(s, x, t, work, 0, 1))
                 act++;
         slot_close(s, t, act, wake, ctl.flows_done);
     }

@@ -33,11 +33,11 @@ def rs(tmp_path_factory):
     lib = C.CDLL(str(so))
     lib.rs_error.restype = C.c_char_p
     lib.rs_run.argtypes = [C.c_int, C.POINTER(C.c_char_p), C.POINTER(C.c_char_p), C.POINTER(C.c_char_p), C.POINTER(C.c_longlong),
-                           C.POINTER(C.c_ulonglong), C.POINTER(C.c_longlong), C.c_int]
+                           C.POINTER(C.c_ulonglong), C.POINTER(C.c_longlong), C.c_int, C.c_int]
     return lib
 
 
-def run(rs, names, tail_log2=20):
+def run(rs, names, tail_log2=20, serial_only=0):
     n = len(names)
     arr = lambda ext: (C.c_char_p * n)(*[(RDMA / f"{x}.{ext}").read_bytes() for x in names])
     nf = sum(len((RDMA / f"{x}.csv").read_text().splitlines()) - 1 for x in names)
@@ -45,7 +45,7 @@ def run(rs, names, tail_log2=20):
     ev = np.zeros(40, dtype=np.uint64)
     slots = C.c_longlong()
     r = rs.rs_run(n, arr("cfg"), arr("topo"), arr("csv"), fct.ctypes.data_as(C.POINTER(C.c_longlong)),
-                  ev.ctypes.data_as(C.POINTER(C.c_ulonglong)), C.byref(slots), tail_log2)
+                  ev.ctypes.data_as(C.POINTER(C.c_ulonglong)), C.byref(slots), tail_log2, serial_only)
     assert r == 0, rs.rs_error().decode()
     return fct, ev
 
@@ -64,9 +64,12 @@ def counters_line(ev):
             f"overflows: tx {ev[4]} queue {ev[5]} ackq {ev[6]} qps {ev[7]} due {ev[12]} | acks for done QPs {ev[10]}")
 
 
+@pytest.mark.parametrize("serial_only", [0, 1], ids=["safe_slots", "serial"])
 @pytest.mark.parametrize("case", cases(), ids=lambda c: c["name"])
-def test_slot_code_equals_reference(rs, case):
-    fct, ev = run(rs, [case["name"]])
+def test_slot_code_equals_reference(rs, case, serial_only):
+    """Both switch paths: safe slots where they apply (egress ports apart), and every slot in one
+    order."""
+    fct, ev = run(rs, [case["name"]], serial_only=serial_only)
     w = want(case["name"])
     bad = np.nonzero(fct != w)[0]
     assert len(bad) == 0, f"{len(bad)} of {len(w)} flows differ, first {bad[0]}: {fct[bad[0]]} vs {w[bad[0]]}"

@@ -102,6 +102,7 @@ ENTRY_POINTS = [
                                          _P(ctypes.c_longlong), _P(ctypes.c_longlong), ctypes.c_ulonglong, ctypes.c_longlong,
                                          _P(ctypes.c_int)]),
     ("tb_rdma_results", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _P(ctypes.c_longlong), _P(ctypes.c_longlong)]),
+    ("tb_rdma_set_queue_cap", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("tb_prepare", ctypes.c_int, [ctypes.c_void_p]),
     ("tb_reset", ctypes.c_int, [ctypes.c_void_p]),
     ("tb_run", ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
@@ -373,6 +374,10 @@ class Simulator:
         self.sizes.append(len(flows))
         return wid.value
 
+    def set_rdma_queue_cap(self, frames: int) -> None:
+        """Frames a switch port's data queue holds (the reference's --q3cap; before the first run)."""
+        self._check(self.lib.tb_rdma_set_queue_cap(self.ctx, frames))
+
     def rdma_results(self, world: int) -> tuple[np.ndarray, np.ndarray]:
         """(start_ns, fct_ns) per flow of an RDMA world; fct -1: not done."""
         n = self.sizes[world]
@@ -449,9 +454,11 @@ def rdma_counters_line(ev) -> str:
 
 
 def run_rdma_world(config: str, topology: str, flows: Flows, link_bps: int = 100_000_000_000, link_delay_ns: int = 1000,
-                   max_slots: int = 0, device: int = 0):
+                   max_slots: int = 0, device: int = 0, queue_cap: int = 0):
     """One RDMA world: (start_ns, fct_ns, counters, stats, status)."""
     with Simulator(device=device) as sim:
+        if queue_cap:
+            sim.set_rdma_queue_cap(queue_cap)
         w = sim.add_rdma_world(config, topology, flows, link_bps, link_delay_ns)
         status = sim.run(max_slots)
         start, fct = sim.rdma_results(w)

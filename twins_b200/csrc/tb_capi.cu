@@ -1073,6 +1073,15 @@ int tb_world_add_rdma(tb_ctx *ctx, const char *config, const char *topology, int
     return TB_OK;
 }
 
+int tb_rdma_set_queue_cap(tb_ctx *ctx, int frames)
+{
+    if (!ctx || frames < 1)
+        return fail(TB_ERR_ARG, "frames >= 1");
+    if (!ctx->rdma)
+        ctx->rdma = tr::rdma_new(ctx->device < 0 ? 0 : ctx->device);
+    return tr::rdma_set_queue_cap(ctx->rdma, frames) ? fail(TB_ERR_STATE, "set before the first run") : TB_OK;
+}
+
 int tb_rdma_results(tb_ctx *ctx, int world, long long *start_ns, long long *fct_ns)
 {
     if (!ctx || !ctx->rdma)

@@ -57,6 +57,7 @@ struct RdmaRun
     RSim s{};
     bool prepared = false, ran = false;
     int tail_log2 = 0; // the tail ring's size (0: by the flows), doubled on a run that lost tails
+    int q3_cap = 4096; // frames a switch port's data queue holds
     int grid = 0;
     size_t smem = 0;
     cudaStream_t stream = nullptr;
@@ -160,7 +161,7 @@ int rdma_prepare(RdmaRun *r, std::string *err)
     std::vector<const RdmaWorld *> wp;
     for (const RdmaWorld &w : r->worlds)
         wp.push_back(&w);
-    if (!layout_rdma(r->L, wp))
+    if (!layout_rdma(r->L, wp, r->q3_cap))
         return *err = r->L.error, -1;
     if (!r->stream && cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking) != cudaSuccess)
         return *err = "cudaStreamCreate failed", -2;
@@ -172,6 +173,14 @@ int rdma_prepare(RdmaRun *r, std::string *err)
     if (int e = rdma_launch_shape(r->L.max_deg, r->L.H + r->L.S, &r->grid, &r->smem))
         return *err = std::string("the RDMA slot kernel does not fit: ") + cudaGetErrorString((cudaError_t)e), -2;
     r->prepared = true;
+    return 0;
+}
+
+int rdma_set_queue_cap(RdmaRun *r, int frames)
+{
+    if (r->prepared || frames < 1)
+        return -4;
+    r->q3_cap = frames;
     return 0;
 }
 

@@ -24,6 +24,8 @@ int rdma_world_flows(RdmaRun *r, int world);
 int rdma_add_world(RdmaRun *r, const char *config, const char *topology, int n, const int *src, const int *dst, const long long *size,
                    const long long *start_ns, unsigned long long bps, long long delay_ns, std::string *err);
 int rdma_prepare(RdmaRun *r, std::string *err);
+// frames a switch port's data queue holds (before the first run)
+int rdma_set_queue_cap(RdmaRun *r, int frames);
 // 0, 1 (inexact: a capacity overflowed or a tie was not decided exactly), or a negative status
 int rdma_run(RdmaRun *r, long long max_slots, std::string *err);
 int rdma_results(RdmaRun *r, int world, long long *start_ns, long long *fct_ns);

@@ -13,10 +13,14 @@ constexpr long long BARRIER_SPIN_LIMIT = 1ll << 22; // polls of ~64 ns: a quarte
 
 __device__ __forceinline__ unsigned ld_volatile(const unsigned *p) { return *(const volatile unsigned *)p; }
 
-// a warp's scratch in shared memory: the DCQCN timers of a NIC's slot, a switch's ports
+// a warp's scratch in shared memory: a NIC's DCQCN timers and staged arrivals, or a switch's ports,
+// staged arrivals, a safe slot's order and flags
+__host__ __device__ inline size_t sw_ports_bytes(int max_deg) { return ((size_t)max_deg * sizeof(SwPort) + 15) & ~(size_t)15; }
 __host__ __device__ inline size_t warp_scratch_bytes(int max_deg)
 {
-    return (sizeof(Due) * MAX_DUE + sizeof(PortEv) * (size_t)max_deg + 15) & ~(size_t)15;
+    const size_t host = sizeof(Due) * MAX_DUE + sizeof(SArr) * HOST_STAGE;
+    const size_t sw = sw_ports_bytes(max_deg) + sizeof(SArr) * SW_STAGE + sizeof(uint16_t) * SW_STAGE + 4 * sizeof(int);
+    return ((host > sw ? host : sw) + 15) & ~(size_t)15;
 }
 
 __global__ void __launch_bounds__(RDMA_WARPS * 32) rdma_slot_kernel(RSim s, int slots, int max_deg)
@@ -27,7 +31,12 @@ __global__ void __launch_bounds__(RDMA_WARPS * 32) rdma_slot_kernel(RSim s, int 
     const int gwarp = blockIdx.x * RDMA_WARPS + warp, nwarps = gridDim.x * RDMA_WARPS;
     unsigned char *mine = smem + warp_scratch_bytes(max_deg) * warp;
     Due *due = reinterpret_cast<Due *>(mine);
-    PortEv *pe = reinterpret_cast<PortEv *>(mine + sizeof(Due) * MAX_DUE);
+    SArr *hstage = reinterpret_cast<SArr *>(mine + sizeof(Due) * MAX_DUE);
+    SwWork work;
+    work.port = reinterpret_cast<SwPort *>(mine);
+    work.arr = reinterpret_cast<SArr *>(mine + sw_ports_bytes(max_deg));
+    work.ord = reinterpret_cast<uint16_t *>(mine + sw_ports_bytes(max_deg) + sizeof(SArr) * SW_STAGE);
+    work.flags = reinterpret_cast<int *>(mine + sw_ports_bytes(max_deg) + (sizeof(SArr) + sizeof(uint16_t)) * SW_STAGE);
     RCtl *ctl = s.ctl;
     volatile RCtl *vc = ctl;
     const int units = s.H + s.S;
@@ -36,20 +45,23 @@ __global__ void __launch_bounds__(RDMA_WARPS * 32) rdma_slot_kernel(RSim s, int 
         if (vc->finished)
             return;
         const int64_t t = vc->slot;
-        if (lane == 0)
-            for (int u = gwarp; u < units; u += nwarps)
+        for (int u = gwarp; u < units; u += nwarps)
+        {
+            if (u < s.H)
             {
-                if (u < s.H)
+                int64_t w = INT64_MAX;
+                const bool act = host_slot(s, u, t, &w, due, hstage, lane, 32);
+                if (lane == 0)
                 {
-                    int64_t w = INT64_MAX;
-                    if (host_slot(s, u, t, &w, due))
+                    if (act)
                         atomicAdd(&ctl->activity, 1u);
                     if (w != INT64_MAX)
                         atomicMin(&ctl->next_wake, (unsigned long long)w);
                 }
-                else if (switch_slot(s, u - s.H, t, pe))
-                    atomicAdd(&ctl->activity, 1u);
             }
+            else if (switch_slot(s, u - s.H, t, work, lane, 32) && lane == 0)
+                atomicAdd(&ctl->activity, 1u);
+        }
         __syncthreads();
         unsigned g = 0;
         if (threadIdx.x == 0)

@@ -210,6 +210,7 @@ inline bool layout_rdma(RLayout &o, const std::vector<const RdmaWorld *> &worlds
                 pi.pmax = c.pmax;
                 o.pinfo.push_back(pi);
                 st.mmu.total_hdrm += c.hdrm_cap;
+                st.max_shift = c.shift > st.max_shift ? c.shift : st.max_shift;
                 Port pt{};
                 pt.tc_at = -1;
                 pt.ob_last = -(1ll << 16);

@@ -20,6 +20,7 @@
 #include "tr_nic.cuh"
 
 #include <climits>
+#include <cstddef>
 
 namespace tr
 {
@@ -59,8 +60,9 @@ struct TailNode
     uint64_t next, pos;
 };
 
-// a frame's contents (the reference's wire format: INT hop words, flow, sequence, size, ...)
-struct Pkt
+// a frame's contents (the reference's wire format: INT hop words, flow, sequence, size, ...; 16-byte
+// aligned: it moves as 16-byte words, ld_pkt)
+struct alignas(16) Pkt
 {
     uint64_t hop[MAX_HOP];
     uint32_t flow;
@@ -76,7 +78,7 @@ struct Pkt
     uint16_t sport;
     uint16_t src, dst; // hosts (numbered over all worlds)
 };
-static_assert(sizeof(Pkt) == 64, "Pkt");
+static_assert(sizeof(Pkt) == 64 && alignof(Pkt) == 16, "Pkt");
 
 // a frame on a link: its arrival time, the chain of the event that sent it, its contents (16-byte
 // aligned: frames move as 16-byte words, ld_frame)
@@ -86,7 +88,7 @@ struct alignas(16) Frame
     Chain c;
     Pkt p;
 };
-static_assert(sizeof(Frame) == 144 && alignof(Frame) == 16, "Frame");
+static_assert(sizeof(Frame) == 144 && alignof(Frame) == 16 && offsetof(Frame, p) % 16 == 0, "Frame");
 
 // a NIC (QbbNetDevice + RdmaEgressQueue of a host with one link)
 struct Nic
@@ -131,6 +133,7 @@ struct Port
 struct SwState
 {
     MmuSwitch mmu;
+    uint32_t max_shift; // its ports' largest PFC threshold shift (the lowest threshold)
 };
 
 // static set-up
@@ -214,6 +217,10 @@ enum
     EV_HOST_DATA = 24,       // of the NICs' arrivals: data
     EV_HOST_EVENTS = 25,     // every NIC event (arrivals, transmissions done, sends, timers, starts)
     EV_SWITCH_EVENTS = 26,   // every switch event (arrivals, transmissions done)
+    EV_PROF_CMPS = 30,       // (TR_PROFILE builds) chain comparisons
+    EV_PROF_TAIL_LOADS = 31, // (TR_PROFILE builds) tail nodes read by them
+    EV_PROF_SAFE = 32,       // (TR_PROFILE builds) switch slots run as safe slots
+    EV_PROF_SERIAL = 33,     // (TR_PROFILE builds) switch slots with events run in one order
     EV_TIMEOUT = 36,
     EV_N = 40
 };
@@ -258,6 +265,7 @@ struct RSim
     uint64_t tail_mask;
     unsigned long long *ev;
     RCtl *ctl;
+    int serial_only; // switches run every slot's events in one order (no safe slots)
 };
 
 // ------------------------------------------------------------------ memory shared between entities
@@ -402,6 +410,9 @@ struct RunWalk
             return;
         }
         const TailNode n = ld_tail(&s.tail[(node - 1) & s.tail_mask]);
+#ifdef TR_PROFILE
+        count(s, EV_PROF_TAIL_LOADS);
+#endif
         if (n.pos != node)
         {
             lost = true;
@@ -480,6 +491,9 @@ TR_HD bool runs_before(const RSim &s, int64_t ta, uint32_t pa, const Chain &a, i
     if (ta != tb)
         return ta < tb;
     bool inexact;
+#ifdef TR_PROFILE
+    count(s, EV_PROF_CMPS);
+#endif
     const int c = chain_cmp(s, pa, a, pb, b, &inexact);
     if (inexact)
         count(s, EV_LOST_TAIL);
@@ -553,6 +567,71 @@ TR_HD int bucket_of(const RSim &s, int link, int64_t t, uint64_t *base)
 
 // the code of a frame's arrival: lead its tx time + the link's delay, its ordinal
 TR_HD uint32_t arrival_code(const LinkInfo &l, const Frame &f) { return event_code(link_tx_ns(l, f.p.size) + l.delay, f.p.ord); }
+
+// ------------------------------------------------------------------ a warp's lanes
+// (lanes = 1 on the CPU: every lane's share runs in turn)
+#ifdef __CUDA_ARCH__
+__device__ __forceinline__ void lanes_sync() { __syncwarp(); }
+__device__ __forceinline__ void sh_add(uint32_t *p, uint32_t v) { atomicAdd(p, v); }
+__device__ __forceinline__ void sh_add(int *p, int v) { atomicAdd(p, v); }
+__device__ __forceinline__ void sh_sub(uint32_t *p, uint32_t v) { atomicSub(p, v); }
+__device__ __forceinline__ void ld_pkt(Pkt &p, const Pkt *src)
+{
+    const uint4 *s = reinterpret_cast<const uint4 *>(src);
+    uint4 *d = reinterpret_cast<uint4 *>(&p);
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+        d[i] = __ldcg(s + i);
+}
+__device__ __forceinline__ void ld_chain(Chain &c, const Chain *src)
+{
+    const uint2 *s = reinterpret_cast<const uint2 *>(src);
+    uint2 *d = reinterpret_cast<uint2 *>(&c);
+#pragma unroll
+    for (int i = 0; i < (int)(sizeof(Chain) / 8); i++)
+        d[i] = __ldcg(s + i);
+}
+#else
+inline void lanes_sync() {}
+inline void sh_add(uint32_t *p, uint32_t v) { *p += v; }
+inline void sh_add(int *p, int v) { *p += v; }
+inline void sh_sub(uint32_t *p, uint32_t v) { *p -= v; }
+inline void ld_pkt(Pkt &p, const Pkt *src) { p = *src; }
+inline void ld_chain(Chain &c, const Chain *src) { c = *src; }
+#endif
+
+// an arrival of the slot staged by the lanes: what the event order and the route need (the frame
+// itself stays in its link's bucket, msg[frame])
+struct SArr
+{
+    int64_t ts;
+    uint32_t acode;
+    uint32_t frame;
+    int16_t out;      // egress port (-1: a PFC frame, or no route)
+    uint8_t q, in;    // its queue; its ingress port
+    uint16_t size;
+    uint8_t kind, pad;
+};
+static_assert(sizeof(SArr) == 24, "SArr");
+
+constexpr int HOST_STAGE = 128; // a NIC's arrivals of a slot staged; more are read one by one
+constexpr int SW_STAGE = 384;   // a switch's arrivals of a slot staged; more run unstaged, serially
+constexpr int SAFE_PORTS = 32;  // switches with more ports run every slot serially
+
+TR_HD void stage_arrival(const RSim &s, SArr &a, uint32_t frame, const LinkInfo &lin)
+{
+    const Frame *f = &s.msg[frame];
+    a.ts = (int64_t)ld_tag((const long long *)&f->ts);
+    Pkt p;
+    ld_pkt(p, &f->p);
+    a.acode = event_code(link_tx_ns(lin, p.size) + lin.delay, p.ord);
+    a.frame = frame;
+    a.size = p.size;
+    a.kind = p.kind;
+    a.out = -1;
+    a.q = PG;
+    a.in = 0;
+}
 
 // ------------------------------------------------------------------ a NIC host's slot
 struct Due
@@ -798,21 +877,46 @@ TR_HD void h_collect_due(const RSim &s, int h, Nic &n, int64_t t1, Due *due, int
 }
 
 // A NIC host's events of slot t in ns-3's order: arrivals on its in link, its TransmitComplete,
-// its next send, its DCQCN timers and its flows' starts. Returns whether it sent or holds frames;
-// *wake: its earliest event without input (INT64_MAX: none). due: room for MAX_DUE timers.
+// its next send, its DCQCN timers and its flows' starts. The lanes stage the slot's arrivals; lane 0
+// runs the events. Returns (on lane 0) whether it sent or holds frames; *wake: its earliest event
+// without input (INT64_MAX: none). due: room for MAX_DUE timers; stage: for HOST_STAGE arrivals.
 // (reference: host_step<1>, src/rdma/rstep.cuh:1649-2114)
-TR_HD bool host_slot(const RSim &s, int h, int64_t t, int64_t *wake, Due *due)
+TR_HD bool host_events(const RSim &s, int h, int64_t t, int64_t *wake, Due *due, const SArr *stage, int na, uint64_t abase);
+
+TR_HD bool host_slot(const RSim &s, int h, int64_t t, int64_t *wake, Due *due, SArr *stage, int lane, int lanes)
 {
     const HostInfo hi = s.hinfo[h];
     const int64_t t1 = (t + 1) * s.D;
     uint64_t abase;
     const int na = bucket_of(s, hi.link_in, t, &abase);
-    Nic &ng = s.nic[h];
-    if (na == 0 && ng.wake >= t1)
+    const int64_t wake0 = s.nic[h].wake;
+    if (na == 0 && wake0 >= t1)
     {
-        *wake = ng.wake;
+        *wake = wake0;
         return false;
     }
+    if (na <= HOST_STAGE)
+    {
+        const LinkInfo lin = s.link[hi.link_in];
+        for (int j = lane; j < na; j += lanes)
+            stage_arrival(s, stage[j], (uint32_t)(abase + j), lin);
+        lanes_sync();
+    }
+    bool act = false;
+    if (lane == 0)
+        act = host_events(s, h, t, wake, due, stage, na, abase);
+    lanes_sync();
+    return act;
+}
+
+// lane 0's share of host_slot: the events
+TR_HD bool host_events(const RSim &s, int h, int64_t t, int64_t *wake, Due *due, const SArr *stage, int na, uint64_t abase)
+{
+    const HostInfo hi = s.hinfo[h];
+    const int64_t t1 = (t + 1) * s.D;
+    Nic &ng = s.nic[h];
+    const LinkInfo lin = s.link[hi.link_in];
+    const bool staged = na <= HOST_STAGE;
     HostEv e;
     e.s = &s;
     e.w = &s.world[hi.world];
@@ -820,23 +924,26 @@ TR_HD bool host_slot(const RSim &s, int h, int64_t t, int64_t *wake, Due *due)
     e.n = ng;
     e.out.open(s, hi.link_out, e.n.ob_last);
     e.nout = 0;
-    const LinkInfo lin = s.link[hi.link_in];
     int ndue = 0;
     if (e.w->nic.cc == 1)
         h_collect_due(s, h, e.n, t1, due, &ndue);
     int ai = 0, di = 0;
-    Frame af;           // the next arrival
-    uint32_t acode = 0;
-    bool have_a = false;
+    SArr a{};           // the next arrival
+    Chain ac;           // its chain (read when a tie or its event needs it)
+    bool have_a = false, have_ac = false;
     int sf_at = -1, sf = -1;
     int64_t sf_t = INT64_MAX;
+    unsigned long long n_ev = 0, n_arr = 0, n_ack = 0, n_data = 0;
     for (;;)
     {
         if (!have_a && ai < na)
         {
-            ld_frame(af, &s.msg[abase + ai]);
-            acode = arrival_code(lin, af);
+            if (staged)
+                a = stage[ai];
+            else
+                stage_arrival(s, a, (uint32_t)(abase + ai), lin);
             have_a = true;
+            have_ac = false;
         }
         while (di < ndue && s.qp[due[di].flow].t[due[di].kind] != due[di].at)
             di++; // (stopped or moved)
@@ -848,7 +955,7 @@ TR_HD bool host_slot(const RSim &s, int h, int64_t t, int64_t *wake, Due *due)
         }
         // candidates in the reference's order: arrival, TransmitComplete, next send, timer, start
         int64_t ct[5];
-        ct[0] = have_a ? af.ts : INT64_MAX;
+        ct[0] = have_a ? a.ts : INT64_MAX;
         ct[1] = e.n.tc_at >= 0 && e.n.tc_at < t1 ? e.n.tc_at : INT64_MAX;
         ct[2] = e.n.ns_at >= 0 && e.n.ns_at < t1 ? e.n.ns_at : INT64_MAX;
         ct[3] = di < ndue ? due[di].at : INT64_MAX;
@@ -858,38 +965,44 @@ TR_HD bool host_slot(const RSim &s, int h, int64_t t, int64_t *wake, Due *due)
             tmin = ct[k] < tmin ? ct[k] : tmin;
         if (tmin == INT64_MAX)
             break;
+        if (ct[0] == tmin && !have_ac)
+        {
+            ld_chain(ac, &s.msg[a.frame].c);
+            have_ac = true;
+        }
         auto chain_of = [&](int k) -> const Chain & {
-            return k == 0 ? af.c : k == 1 ? s.h_tc[h] : k == 2 ? s.h_ns[h] : k == 3 ? s.qc[due[di].flow].c[due[di].kind] : s.flow[sf].start_chain;
+            return k == 0 ? ac : k == 1 ? s.h_tc[h] : k == 2 ? s.h_ns[h] : k == 3 ? s.qc[due[di].flow].c[due[di].kind] : s.flow[sf].start_chain;
         };
         int bk = -1;
         for (int k = 0; k < 5; k++)
         {
             if (ct[k] != tmin)
                 continue;
-            if (bk < 0 || runs_before(s, tmin, k == 0 ? acode : 0, chain_of(k), tmin, bk == 0 ? acode : 0, chain_of(bk)))
+            if (bk < 0 || runs_before(s, tmin, k == 0 ? a.acode : 0, chain_of(k), tmin, bk == 0 ? a.acode : 0, chain_of(bk)))
                 bk = k;
         }
         e.now = tmin;
         if (bk == 0)
-            chain_push(s, e.cur, acode, af.c);
+            chain_push(s, e.cur, a.acode, ac);
         else
             e.cur = chain_of(bk);
         e.ord = 0;
-        count(s, EV_HOST_EVENTS);
+        n_ev++;
         if (bk == 0)
         {
             have_a = false;
             ai++;
-            count(s, EV_HOST_ARRIVALS);
-            const Pkt &p = af.p;
+            n_arr++;
+            Pkt p;
+            ld_pkt(p, &s.msg[a.frame].p);
             if (p.kind == K_DATA)
             {
-                count(s, EV_HOST_DATA);
+                n_data++;
                 h_data(e, p);
             }
             else if (p.kind == K_ACK || p.kind == K_NACK)
             {
-                count(s, EV_HOST_ACKS);
+                n_ack++;
                 h_ack(e, p);
             }
             else if (e.w->qbb)
@@ -957,25 +1070,43 @@ TR_HD bool host_slot(const RSim &s, int h, int64_t t, int64_t *wake, Due *due)
     e.n.wake = w;
     ng = e.n;
     *wake = w;
+    count(s, EV_HOST_EVENTS, n_ev);
+    if (n_arr)
+    {
+        count(s, EV_HOST_ARRIVALS, n_arr);
+        count(s, EV_HOST_ACKS, n_ack);
+        count(s, EV_HOST_DATA, n_data);
+    }
     if (e.nout)
         count(s, EV_HOST_FRAMES, (unsigned long long)e.nout);
     return act;
 }
 
 // ------------------------------------------------------------------ a switch's slot
-// a switch port during the slot: its state, its out link, its arrivals' cursor
-struct alignas(16) PortEv
+// a switch port during the slot (in the warp's shared memory)
+struct alignas(16) SwPort
 {
     Port pt;
     OutLink out;
     PortInfo info;
-    LinkInfo lin;
-    uint64_t abase;
-    int an, ai;
-    int nout;
-    bool have_a;
-    uint32_t acode;
-    Frame af;
+    LinkInfo lin;          // its in link
+    uint64_t abase;        // its arrivals' bucket in msg
+    int an, first;         // its arrivals this slot; the first one's place among the staged
+    int nout;              // frames it sent this slot
+    int ai, aend;          // the serial path's cursor over its arrivals
+    uint32_t ing0, abytes; // safe slots: its ingress bytes at the slot's start; bytes arriving on it for queue PG
+    int ocnt, obase;       // safe slots: arrivals leaving by it; their place in the order array
+    SArr pa;               // the unstaged serial path's next arrival
+    bool have_pa;
+};
+
+// the warp's switch workspace (shared memory): its ports, staged arrivals, a safe lane's order
+struct SwWork
+{
+    SwPort *port;  // [deg]
+    SArr *arr;     // [SW_STAGE]
+    uint16_t *ord; // [SW_STAGE]: per egress port, its arrivals in event order
+    int *flags;    // [4]: ports with an event, arrivals, safe, (unused)
 };
 
 struct SwEv
@@ -984,19 +1115,19 @@ struct SwEv
     const RWorld *w;
     int x;
     SwInfo si;
-    SwState sw;
-    PortEv *pe; // [deg]
+    MmuSwitch mmu;
+    SwPort *pe;
+    bool safe; // no buffer decision can occur in this slot: lanes run egress ports apart
     int64_t now;
     Chain cur;
     int ord;
+    unsigned long long n_ev, n_arr;
 };
-
-TR_HD uint32_t sw_pfc_threshold(const SwEv &e, int port) { return pfc_threshold(e.w->buffer_size, e.sw.mmu, e.pe[port].info.shift); }
 
 TR_HD void s_transmit(SwEv &e, int port, Pkt p)
 {
     const RSim &s = *e.s;
-    PortEv &pe = e.pe[port];
+    SwPort &pe = e.pe[port];
     const int64_t tx = link_tx_ns(pe.out.li, p.size);
     pe.pt.tc_at = e.now + tx;
     chain_push(s, s.p_tc[e.si.pbase + port], event_code(tx, e.ord++), e.cur);
@@ -1075,15 +1206,33 @@ TR_HD void s_send_pfc(SwEv &e, int port, bool resume)
 }
 
 // a frame of queue PG leaves: the buffer gives its bytes back, ECN may mark it, a paused ingress
-// may resume, an HPCC data frame takes the port's INT word; then TransmitStart
+// may resume, an HPCC data frame takes the port's INT word; then TransmitStart. In a safe slot only
+// the ingress and egress byte counts change (no headroom is in use and no port is paused).
 TR_HD void s_start_q3(SwEv &e, int port, Pkt p)
 {
     const RWorld &w = *e.w;
-    PortEv &pe = e.pe[port];
-    PortEv &in = e.pe[p.inport];
+    SwPort &pe = e.pe[port];
+    SwPort &in = e.pe[p.inport];
     tb::Rng &rng = pe.pt.rng;
-    const unsigned r = mmu_release(w.buffer_size, e.sw.mmu, in.pt.mmu, in.info.shift, pe.pt.mmu, p.size, w.ecn != 0, pe.info.kmin,
-                                   pe.info.kmax, pe.info.pmax, false, [&]() { return tb::rand_u01(rng); });
+    unsigned r;
+    if (e.safe)
+    {
+        sh_sub(&in.pt.mmu.ing, p.size);
+        pe.pt.mmu.egr -= p.size;
+        r = 0;
+        if (w.ecn)
+        {
+            const uint32_t egr = pe.pt.mmu.egr;
+            if (egr > pe.info.kmax)
+                r = MMU_MARK;
+            else if (egr > pe.info.kmin &&
+                     tb::rand_u01(rng) < pe.info.pmax * (double)(egr - pe.info.kmin) / (double)(pe.info.kmax - pe.info.kmin))
+                r = MMU_MARK;
+        }
+    }
+    else
+        r = mmu_release(w.buffer_size, e.mmu, in.pt.mmu, in.info.shift, pe.pt.mmu, p.size, w.ecn != 0, pe.info.kmin, pe.info.kmax,
+                        pe.info.pmax, false, [&]() { return tb::rand_u01(rng); });
     if (r & MMU_MARK)
     {
         p.ecn = 3;
@@ -1119,16 +1268,16 @@ TR_HD void s_dequeue(SwEv &e, int port)
 }
 
 // the egress port and queue of a data frame or ACK (-1: no route) (SwitchNode::GetOutDev)
-TR_HD int s_route(const RSim &s, const SwEv &e, const Pkt &p, int *q)
+TR_HD int s_route(const RSim &s, const SwInfo &si, const RWorld &w, const Pkt &p, int *q)
 {
     const bool data = p.kind == K_DATA;
-    *q = (e.w->nic.ack_high_prio && !data) ? 0 : PG;
+    *q = (w.nic.ack_high_prio && !data) ? 0 : PG;
     // (an ACK carries its data frame's hosts: it travels from dst to src)
-    const int src = p.src - e.si.hbase, dst = p.dst - e.si.hbase, to = data ? dst : src;
-    const uint32_t off = s.rt[2 * ((size_t)e.si.rt_off + to)], n = s.rt[2 * ((size_t)e.si.rt_off + to) + 1];
+    const int src = p.src - si.hbase, dst = p.dst - si.hbase, to = data ? dst : src;
+    const uint32_t off = s.rt[2 * ((size_t)si.rt_off + to)], n = s.rt[2 * ((size_t)si.rt_off + to) + 1];
     if (n == 0)
         return -1;
-    return s.rtp[off + ecmp_choice(src, dst, p.sport, data, e.si.seed, (int)n)];
+    return s.rtp[off + ecmp_choice(src, dst, p.sport, data, si.seed, (int)n)];
 }
 
 // SwitchNode::SendToDev: admission, PFC, then the egress port's queue (or straight on when idle)
@@ -1138,15 +1287,24 @@ TR_HD void s_forward(SwEv &e, int inport, Pkt p, int out, int q)
         return;
     if (q != 0)
     {
-        PortEv &in = e.pe[inport];
-        const unsigned r = mmu_admit(e.w->buffer_size, e.sw.mmu, in.pt.mmu, in.info.hdrm_cap, in.info.shift, e.pe[out].pt.mmu, p.size, false);
-        if (r & MMU_DROP)
+        if (e.safe)
         {
-            count(*e.s, EV_DROP);
-            return;
+            // below every threshold for the whole slot: no drop, no headroom, no PAUSE
+            sh_add(&e.pe[inport].pt.mmu.ing, (uint32_t)p.size);
+            e.pe[out].pt.mmu.egr += p.size;
         }
-        if (r & MMU_PAUSE)
-            s_send_pfc(e, inport, false);
+        else
+        {
+            SwPort &in = e.pe[inport];
+            const unsigned r = mmu_admit(e.w->buffer_size, e.mmu, in.pt.mmu, in.info.hdrm_cap, in.info.shift, e.pe[out].pt.mmu, p.size, false);
+            if (r & MMU_DROP)
+            {
+                count(*e.s, EV_DROP);
+                return;
+            }
+            if (r & MMU_PAUSE)
+                s_send_pfc(e, inport, false);
+        }
     }
     p.inport = (uint8_t)inport;
     Port &o = e.pe[out].pt;
@@ -1159,116 +1317,369 @@ TR_HD void s_forward(SwEv &e, int inport, Pkt p, int out, int q)
     s_dequeue(e, out);
 }
 
-TR_HD void sw_peek(const RSim &s, PortEv &pe)
+// an arrival's event: PFC frames pause or resume their port's egress; the others are forwarded
+TR_HD void s_arrival(SwEv &e, const SArr &a)
 {
-    if (pe.have_a || pe.ai >= pe.an)
+    const RSim &s = *e.s;
+    Chain c;
+    ld_chain(c, &s.msg[a.frame].c);
+    chain_push(s, e.cur, a.acode, c);
+    e.ord = 0;
+    e.n_ev++;
+    e.n_arr++;
+    if (a.kind == K_PAUSE || a.kind == K_RESUME)
+    {
+        if (e.w->qbb)
+        {
+            Pkt p;
+            ld_pkt(p, &s.msg[a.frame].p);
+            if (a.kind == K_PAUSE)
+                e.pe[a.in].pt.paused |= 1u << p.q;
+            else
+            {
+                e.pe[a.in].pt.paused &= ~(1u << p.q);
+                s_dequeue(e, a.in);
+            }
+        }
         return;
-    ld_frame(pe.af, &s.msg[pe.abase + pe.ai]);
-    pe.acode = arrival_code(pe.lin, pe.af);
-    pe.have_a = true;
+    }
+    if (a.out < 0)
+        return;
+    Pkt p;
+    ld_pkt(p, &s.msg[a.frame].p);
+    s_forward(e, a.in, p, a.out, a.q);
 }
 
-// A switch's events of slot t in ns-3's order: every port's arrivals and TransmitCompletes.
-// pe: room for its ports. Returns whether it sent or holds frames.
-// (reference: switch_step's serial path, src/rdma/rstep.cuh:2583-3446)
-TR_HD bool switch_slot(const RSim &s, int x, int64_t t, PortEv *pe)
+// a port's TransmitComplete
+TR_HD void s_tc(SwEv &e, int port)
 {
-    SwEv e;
-    e.s = &s;
-    e.x = x;
-    e.si = s.sinfo[x];
-    e.w = &s.world[e.si.world];
-    e.sw = s.sw[x];
-    e.pe = pe;
-    const int deg = e.si.deg;
-    const int64_t t1 = (t + 1) * s.D;
-    bool any = false;
+    e.cur = e.s->p_tc[e.si.pbase + port];
+    e.ord = 0;
+    e.n_ev++;
+    e.pe[port].pt.tc_at = -1;
+    s_dequeue(e, port);
+}
+
+// does staged arrival a run before staged arrival b (same time: by their chains)?
+TR_HD bool arr_before(const RSim &s, const SArr &a, const SArr &b)
+{
+    if (a.ts != b.ts)
+        return a.ts < b.ts;
+    Chain ca, cb;
+    ld_chain(ca, &s.msg[a.frame].c);
+    ld_chain(cb, &s.msg[b.frame].c);
+    return runs_before(s, a.ts, a.acode, ca, b.ts, b.acode, cb);
+}
+
+// does a port's arrival a run before its TransmitComplete at the same time?
+TR_HD bool arr_before_tc(const RSim &s, const SArr &a, const Chain &tc)
+{
+    Chain ca;
+    ld_chain(ca, &s.msg[a.frame].c);
+    return runs_before(s, a.ts, a.acode, ca, a.ts, 0, tc);
+}
+
+// A safe slot's egress port o, on its own lane: the arrivals routed to it (and PFC frames arriving
+// at it) in event order, merged with its TransmitCompletes. Restricting ns-3's order to one port's
+// events keeps their order, and in a safe slot ports meet only in their ingress byte counts.
+TR_HD void safe_egress(SwEv &e, const SwWork &w, int o, int64_t t1, int total)
+{
+    const RSim &s = *e.s;
+    SwPort &me = e.pe[o];
+    uint16_t *list = w.ord + me.obase; // (this port's share of the order array)
+    int n = 0;
+    for (int j = 0; j < total; j++)
+    {
+        const SArr &a = w.arr[j];
+        const int own = a.out >= 0 ? a.out : (a.kind == K_PAUSE || a.kind == K_RESUME ? a.in : -1);
+        if (own != o)
+            continue;
+        // insertion in event order (an undecided tie keeps the earlier port's arrival first)
+        int k = n++;
+        while (k > 0 && arr_before(s, a, w.arr[list[k - 1]]))
+        {
+            list[k] = list[k - 1];
+            k--;
+        }
+        list[k] = (uint16_t)j;
+    }
+    int i = 0;
+    for (;;)
+    {
+        const int64_t ta = i < n ? w.arr[list[i]].ts : INT64_MAX, tc = me.pt.tc_at;
+        const bool htc = tc >= 0 && tc < t1;
+        if (ta == INT64_MAX && !htc)
+            break;
+        bool arr;
+        if (!htc || ta == INT64_MAX)
+            arr = !htc;
+        else if (ta != tc)
+            arr = ta < tc;
+        else
+            arr = arr_before_tc(s, w.arr[list[i]], s.p_tc[e.si.pbase + o]);
+        if (!arr)
+        {
+            e.now = tc;
+            s_tc(e, o);
+            continue;
+        }
+        const SArr &a = w.arr[list[i++]];
+        e.now = a.ts;
+        s_arrival(e, a);
+    }
+}
+
+// The switch's events in one order by lane 0: every port's next arrival and TransmitComplete,
+// ties by the chains (from the staged arrivals, or read from the links when they did not fit)
+TR_HD void serial_events(SwEv &e, const SwWork &w, int deg, int64_t t1, bool staged)
+{
+    const RSim &s = *e.s;
     for (int p = 0; p < deg; p++)
     {
-        PortEv &q = pe[p];
-        q.pt = s.port[e.si.pbase + p];
-        q.info = s.pinfo[e.si.pbase + p];
+        SwPort &q = e.pe[p];
+        q.ai = staged ? q.first : 0;
+        q.aend = staged ? q.first + q.an : q.an;
+        q.have_pa = false;
+    }
+    for (;;)
+    {
+        int best = -1, bk = 0;
+        int64_t bt = INT64_MAX;
+        const SArr *ba = nullptr;
+        for (int p = 0; p < deg; p++)
+        {
+            SwPort &q = e.pe[p];
+            const SArr *a = nullptr;
+            if (q.ai < q.aend)
+            {
+                if (staged)
+                    a = &w.arr[q.ai];
+                else
+                {
+                    if (!q.have_pa)
+                    {
+                        stage_arrival(s, q.pa, (uint32_t)(q.abase + q.ai), q.lin);
+                        q.pa.in = (uint8_t)p;
+                        Pkt pk;
+                        ld_pkt(pk, &s.msg[q.pa.frame].p);
+                        int qi = PG;
+                        q.pa.out = (int16_t)(pk.kind == K_PAUSE || pk.kind == K_RESUME ? -1 : s_route(s, e.si, *e.w, pk, &qi));
+                        q.pa.q = (uint8_t)qi;
+                        q.have_pa = true;
+                    }
+                    a = &q.pa;
+                }
+            }
+            const int64_t ta = a ? a->ts : INT64_MAX, tc = q.pt.tc_at >= 0 && q.pt.tc_at < t1 ? q.pt.tc_at : INT64_MAX;
+            for (int k = 0; k < 2; k++)
+            {
+                const int64_t tt = k ? tc : ta;
+                if (tt == INT64_MAX || tt > bt)
+                    continue;
+                if (tt < bt || best < 0)
+                {
+                    best = p, bk = k, bt = tt, ba = a;
+                    continue;
+                }
+                // a tie: the chains
+                bool b4;
+                if (k == 0 && bk == 0)
+                    b4 = arr_before(s, *a, *ba);
+                else if (k == 0)
+                    b4 = arr_before_tc(s, *a, s.p_tc[e.si.pbase + best]);
+                else if (bk == 0)
+                {
+                    Chain cb;
+                    ld_chain(cb, &s.msg[ba->frame].c);
+                    b4 = runs_before(s, tt, 0, s.p_tc[e.si.pbase + p], bt, ba->acode, cb);
+                }
+                else
+                    b4 = runs_before(s, tt, 0, s.p_tc[e.si.pbase + p], bt, 0, s.p_tc[e.si.pbase + best]);
+                if (b4)
+                    best = p, bk = k, ba = a;
+            }
+        }
+        if (best < 0)
+            break;
+        e.now = bt;
+        if (bk == 1)
+        {
+            s_tc(e, best);
+            continue;
+        }
+        const SArr a = *ba;
+        SwPort &q = e.pe[best];
+        q.ai++;
+        q.have_pa = false;
+        s_arrival(e, a);
+    }
+}
+
+// A switch's events of slot t in ns-3's order: every port's arrivals and TransmitCompletes, by the
+// warp's lanes. They load the ports and stage the slot's arrivals with their routes; then, when no
+// buffer decision (drop, headroom, PAUSE, RESUME) can occur in the slot, each lane runs egress
+// ports of its own (a safe slot), else lane 0 runs all events in one order; the lanes store the
+// ports. Returns (on every lane) whether the switch sent or holds frames.
+// (reference: switch_step, src/rdma/rstep.cuh:2583-3446)
+TR_HD bool switch_slot(const RSim &s, int x, int64_t t, const SwWork &w, int lane, int lanes)
+{
+    const SwInfo si = s.sinfo[x];
+    const RWorld &wp = s.world[si.world];
+    const int deg = si.deg;
+    const int64_t t1 = (t + 1) * s.D;
+    if (lane == 0)
+        w.flags[0] = w.flags[1] = w.flags[2] = w.flags[3] = 0;
+    lanes_sync();
+    for (int p = lane; p < deg; p += lanes)
+    {
+        SwPort &q = w.port[p];
+        q.pt = s.port[si.pbase + p];
+        q.info = s.pinfo[si.pbase + p];
         q.lin = s.link[q.info.link_in];
         q.out.open(s, q.info.link_out, q.pt.ob_last);
         q.an = bucket_of(s, q.info.link_in, t, &q.abase);
-        q.ai = 0;
         q.nout = 0;
-        q.have_a = false;
-        any |= q.an > 0 || (q.pt.tc_at >= 0 && q.pt.tc_at < t1);
+        q.abytes = 0;
+        q.ocnt = 0;
+        q.ing0 = q.pt.mmu.ing;
+        if (q.an > 0 || (q.pt.tc_at >= 0 && q.pt.tc_at < t1))
+            sh_add(&w.flags[2], 1);
     }
-    if (any)
-        for (;;)
-        {
-            // the earliest event: a port's next arrival or its TransmitComplete; ties by the chains
-            int best = -1, bk = 0;
-            int64_t bt = INT64_MAX;
-            for (int p = 0; p < deg; p++)
-            {
-                PortEv &q = pe[p];
-                sw_peek(s, q);
-                const int64_t ta = q.have_a ? q.af.ts : INT64_MAX, tc = q.pt.tc_at >= 0 && q.pt.tc_at < t1 ? q.pt.tc_at : INT64_MAX;
-                for (int k = 0; k < 2; k++)
-                {
-                    const int64_t tt = k ? tc : ta;
-                    if (tt == INT64_MAX || tt > bt)
-                        continue;
-                    if (tt < bt || best < 0)
-                    {
-                        best = p, bk = k, bt = tt;
-                        continue;
-                    }
-                    const Chain &ca = k ? s.p_tc[e.si.pbase + p] : q.af.c, &cb = bk ? s.p_tc[e.si.pbase + best] : pe[best].af.c;
-                    if (runs_before(s, tt, k ? 0 : q.acode, ca, bt, bk ? 0 : pe[best].acode, cb))
-                        best = p, bk = k;
-                }
-            }
-            if (best < 0)
-                break;
-            PortEv &q = pe[best];
-            e.now = bt;
-            e.ord = 0;
-            count(s, EV_SWITCH_EVENTS);
-            if (bk == 1)
-            {
-                e.cur = s.p_tc[e.si.pbase + best];
-                q.pt.tc_at = -1;
-                s_dequeue(e, best);
-                continue;
-            }
-            chain_push(s, e.cur, q.acode, q.af.c);
-            count(s, EV_SWITCH_ARRIVALS);
-            const Pkt pk = q.af.p;
-            q.have_a = false;
-            q.ai++;
-            if (pk.kind == K_PAUSE || pk.kind == K_RESUME)
-            {
-                if (e.w->qbb)
-                {
-                    if (pk.kind == K_PAUSE)
-                        q.pt.paused |= 1u << pk.q;
-                    else
-                    {
-                        q.pt.paused &= ~(1u << pk.q);
-                        s_dequeue(e, best);
-                    }
-                }
-                continue;
-            }
-            int qi = PG;
-            const int out = s_route(s, e, pk, &qi);
-            s_forward(e, best, pk, out, qi);
-        }
-    bool act = false;
-    for (int p = 0; p < deg; p++)
+    lanes_sync();
+    if (w.flags[2] == 0)
     {
-        PortEv &q = pe[p];
+        // no event: the ports stay as they are
+        bool act = false;
+        for (int p = 0; p < deg; p++)
+        {
+            const Port &pt = w.port[p].pt;
+            act |= pt.q0_n > 0 || pt.q3_n > 0 || pt.tc_at >= 0;
+        }
+        lanes_sync();
+        return act;
+    }
+    if (lane == 0)
+    {
+        int total = 0;
+        for (int p = 0; p < deg; p++)
+        {
+            w.port[p].first = total;
+            total += w.port[p].an;
+        }
+        w.flags[1] = total;
+    }
+    lanes_sync();
+    const int total = w.flags[1];
+    const bool staged = total <= SW_STAGE;
+    if (staged)
+    {
+        for (int j = lane; j < total; j += lanes)
+        {
+            int p = 0;
+            while (j >= w.port[p].first + w.port[p].an)
+                p++;
+            SArr &a = w.arr[j];
+            const uint32_t frame = (uint32_t)(w.port[p].abase + (j - w.port[p].first));
+            stage_arrival(s, a, frame, w.port[p].lin);
+            a.in = (uint8_t)p;
+            Pkt pk;
+            ld_pkt(pk, &s.msg[frame].p);
+            int qi = PG;
+            a.out = (int16_t)(pk.kind == K_PAUSE || pk.kind == K_RESUME ? -1 : s_route(s, si, wp, pk, &qi));
+            a.q = (uint8_t)qi;
+            if (a.out >= 0 && a.q != 0)
+                sh_add(&w.port[p].abytes, (uint32_t)a.size);
+            const int own = a.out >= 0 ? a.out : (a.kind == K_PAUSE || a.kind == K_RESUME ? p : -1);
+            if (own >= 0)
+                sh_add(&w.port[own].ocnt, 1);
+        }
+        lanes_sync();
+    }
+    SwEv e;
+    e.s = &s;
+    e.w = &wp;
+    e.x = x;
+    e.si = si;
+    e.mmu = s.sw[x].mmu;
+    e.pe = w.port;
+    e.n_ev = e.n_arr = 0;
+    // a safe slot: nothing paused, no headroom in use, and every port below the lowest PFC
+    // threshold the slot can reach even if all its arrivals stay (lane 0 decides for all)
+    if (lane == 0)
+    {
+        bool safe = staged && deg <= SAFE_PORTS && !s.serial_only;
+        int64_t amax = (int64_t)e.mmu.shared_used;
+        for (int p = 0; p < deg; p++)
+        {
+            amax += w.port[p].abytes;
+            if (w.port[p].pt.mmu.hdrm || w.port[p].pt.mmu.paused)
+                safe = false;
+        }
+        const int64_t room = (int64_t)(uint32_t)(wp.buffer_size - e.mmu.total_hdrm - e.mmu.total_rsrv) - amax;
+        const int64_t th_min = room > 0 ? room >> s.sw[x].max_shift : -1;
+        for (int p = 0; p < deg && safe; p++)
+        {
+            const int64_t su = (int64_t)w.port[p].pt.mmu.ing + w.port[p].abytes - MMU_RESERVE;
+            if ((su > 0 ? su : 0) >= th_min)
+                safe = false;
+        }
+        int at = 0;
+        for (int p = 0; p < deg; p++)
+        {
+            w.port[p].obase = at;
+            at += w.port[p].ocnt;
+        }
+        w.flags[2] = safe;
+    }
+    lanes_sync();
+    const bool safe = w.flags[2] != 0;
+    e.safe = safe;
+#ifdef TR_PROFILE
+    if (lane == 0)
+        count(s, safe ? EV_PROF_SAFE : EV_PROF_SERIAL);
+#endif
+    if (safe)
+        for (int o = lane; o < deg; o += lanes)
+            safe_egress(e, w, o, t1, total);
+    else if (lane == 0)
+        serial_events(e, w, deg, t1, staged);
+    lanes_sync();
+    bool act = false;
+    for (int p = lane; p < deg; p += lanes)
+    {
+        SwPort &q = w.port[p];
         q.out.flush(s);
         q.pt.ob_last = q.out.last;
-        if (q.nout > 0 || q.pt.q0_n > 0 || q.pt.q3_n > 0 || q.pt.tc_at >= 0)
-            act = true;
-        s.port[e.si.pbase + p] = q.pt;
+        s.port[si.pbase + p] = q.pt;
     }
-    s.sw[x] = e.sw;
+    lanes_sync();
+    for (int p = 0; p < deg; p++)
+    {
+        const SwPort &q = w.port[p];
+        act |= q.nout > 0 || q.pt.q0_n > 0 || q.pt.q3_n > 0 || q.pt.tc_at >= 0;
+    }
+    if (e.n_ev)
+    {
+        count(s, EV_SWITCH_EVENTS, e.n_ev);
+        count(s, EV_SWITCH_ARRIVALS, e.n_arr);
+    }
+    if (lane == 0)
+    {
+        if (safe)
+        {
+            // shared_used follows from the ingress counts (modulo 2^32, as the counter)
+            uint32_t d = 0;
+            for (int p = 0; p < deg; p++)
+            {
+                const uint32_t a = w.port[p].ing0 > MMU_RESERVE ? w.port[p].ing0 - MMU_RESERVE : 0;
+                const uint32_t b = w.port[p].pt.mmu.ing > MMU_RESERVE ? w.port[p].pt.mmu.ing - MMU_RESERVE : 0;
+                d += b - a;
+            }
+            e.mmu.shared_used += d;
+        }
+        s.sw[x].mmu = e.mmu;
+    }
+    lanes_sync();
     return act;
 }
 

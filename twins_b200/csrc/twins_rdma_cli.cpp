@@ -1,6 +1,6 @@
 // twins-rdma: the reference's RDMA command line (src/rdma/rmain.cu:1-42, 1023-1240) over the
 // twins-b200 C ABI.
-//   twins-rdma CONFIG --topo=F --flows=F [--out=fct.txt] [--rate=100Gbps] [--delay=1000] [--q3cap=N]
+//   twins-rdma CONFIG --topo=F --flows=F [--out=fct.txt] [--rate=100Gbps] [--delay=1000] [--q3cap=4096]
 //              [KEY=VALUE ...]
 //   twins-rdma CONFIG --batch=JOBFILE --outdir=DIR [--path=DIR:DIR...] [options] [KEY=VALUE ...]
 // CONFIG: an HPCC config file ("KEY v1 v2 ..." per line); KEY=VALUE (KEY=V1,V2,.. for several
@@ -12,8 +12,9 @@
 // and the counters line, as the reference prints them. Exit status: 0 every flow done; 2 some
 // unfinished at the stop time; 3 an error counter (an overflow: the results are not exact); 1 a
 // usage, input or device error.
-// The reference's launch-shape options (--win, --gwin, --rank*, --persist, --spread, --serial,
-// --tail, --dcap) change no result; they are accepted and have no effect here.
+// --q3cap: frames a switch port's data queue holds (an overflow is reported, exit 3). The reference's
+// launch-shape options (--win, --gwin, --rank*, --persist, --spread, --serial, --tail, --dcap) change
+// no result; they are accepted and have no effect here.
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -150,7 +151,7 @@ int main(int argc, char **argv)
     }
     std::string topo_file, flow_file, out_file = "fct.txt", batch_file, out_dir = ".", data_dirs, rate_s = "100Gbps";
     long long delay = 1000;
-    int device = 0;
+    int device = 0, q3cap = 4096;
     for (int i = 2; i < argc; i++)
     {
         const std::string a = argv[i];
@@ -174,9 +175,10 @@ int main(int argc, char **argv)
             delay = atoll(v.c_str());
         else if (k == "--device")
             device = atoi(v.c_str());
+        else if (k == "--q3cap")
+            q3cap = atoi(v.c_str());
         else if (k == "--win" || k == "--gwin" || k == "--rank" || k == "--rank-join" || k == "--rank-bs" || k == "--rank-every" ||
-                 k == "--persist" || k == "--spread" || k == "--serial" || k == "--tail" || k == "--tail-auto" || k == "--dcap" ||
-                 k == "--q3cap")
+                 k == "--persist" || k == "--spread" || k == "--serial" || k == "--tail" || k == "--tail-auto" || k == "--dcap")
             continue; // (launch shapes and capacities of the reference's kernels: no result depends on them)
         else if (k.compare(0, 2, "--") != 0 && eq != std::string::npos)
             set_override(base, k, v);
@@ -244,6 +246,11 @@ int main(int argc, char **argv)
     }
     tb_ctx *ctx = nullptr;
     if (tb_ctx_create(device, 0, &ctx))
+    {
+        fprintf(stderr, "%s\n", tb_last_error());
+        return 1;
+    }
+    if (tb_rdma_set_queue_cap(ctx, q3cap))
     {
         fprintf(stderr, "%s\n", tb_last_error());
         return 1;
