@@ -98,6 +98,7 @@ int rs_run(int n, const char **cfg, const char **topo, const char **flows, long 
     s.rx = rx.data();
     s.fct = fctv.data();
     s.link = L.link.data();
+    s.txt = L.txt.data();
     s.msg = msg.data();
     s.msg_cnt = tags.data();
     s.pend = pend.data();

@@ -32,6 +32,8 @@ CLI_TRACE = LIB / "twins-trace"
 CLI_RDMA = LIB / "twins-rdma"
 # (library, front-end, extra flags): 9-run chains, 25-run chains, 9-run chains with the enqueue trace
 VARIANTS = [(SO, CLI, []), (SO25, CLI25, ["-DTB_CHAIN_RUNS=25"]), (SO_TRACE, CLI_TRACE, ["-DTB_QTRACE"])]
+# (on request: the RDMA slot kernel's timers of the slots' longest NIC and switch, TR_PROFILE)
+SO_PROF = LIB / "libtwinsb200_prof.so"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # exactness: no floating-point contraction (fma() is written where ns-3 fuses), IEEE division
@@ -52,6 +54,21 @@ def _stale(out: Path, deps) -> bool:
         return True
     t = out.stat().st_mtime
     return any(Path(d).stat().st_mtime > t for d in deps)
+
+
+def build_profile() -> Path:
+    """The profiling build (TR_PROFILE counters in the RDMA slot kernel), for measurements only."""
+    LIB.mkdir(exist_ok=True)
+    nvcc = _nvcc()
+    objs = []
+    for src in SOURCES:
+        obj = LIB / (Path(src).stem + "_prof.o")
+        subprocess.run([nvcc, *NVFLAGS, "-DTR_PROFILE", "-c", str(CSRC / src), "-o", str(obj)], check=True)
+        objs.append(str(obj))
+    subprocess.run([nvcc, *ARCH, "-shared", "-o", str(SO_PROF), *objs, "-lcudart"], check=True)
+    for o in objs:
+        Path(o).unlink(missing_ok=True)
+    return SO_PROF
 
 
 def build(force: bool = False, verbose: bool = False) -> Path:
@@ -91,5 +108,8 @@ def build(force: bool = False, verbose: bool = False) -> Path:
 
 
 if __name__ == "__main__":
+    if "--profile" in sys.argv:
+        print(build_profile())
+        sys.exit(0)
     build(force="--force" in sys.argv, verbose="-v" in sys.argv)
     print(SO)

@@ -107,7 +107,7 @@ struct RdmaRun
                   d.zeroed(&x.q0, (size_t)l.P * l.q0_cap) && d.zeroed(&x.q3, (size_t)l.P * l.q3_cap) &&
                   d.copy((uint32_t **)&x.rt, l.rt) && d.copy((uint8_t **)&x.rtp, l.rtp) && d.copy((FlowInfo **)&x.flow, l.flow) &&
                   d.copy((int **)&x.start_list, l.start_list) && d.copy((uint32_t **)&x.root_rank, l.root_rank) && d.zeroed(&x.qp, l.F) &&
-                  d.zeroed(&x.qc, l.F) && d.zeroed(&x.rx, l.F) && d.copy(&x.fct, minus1) && d.copy((LinkInfo **)&x.link, l.link) &&
+                  d.zeroed(&x.qc, l.F) && d.zeroed(&x.rx, l.F) && d.copy(&x.fct, minus1) && d.copy((LinkInfo **)&x.link, l.link) && d.copy((int32_t **)&x.txt, l.txt) &&
                   d.zeroed(&x.msg, l.n_frames) && d.copy(&x.msg_cnt, tags) && d.zeroed(&x.pend, (size_t)l.pend_n) &&
                   d.zeroed(&x.tail, (size_t)1 << tl) && d.zeroed(&x.tail_cnt, 1) && d.zeroed(&x.ev, EV_N) && d.copy(&x.ctl, ctl);
         if (!ok)
@@ -170,7 +170,7 @@ int rdma_prepare(RdmaRun *r, std::string *err)
         cudaEventCreate(&r->e0);
         cudaEventCreate(&r->e1);
     }
-    if (int e = rdma_launch_shape(r->L.max_deg, r->L.H + r->L.S, &r->grid, &r->smem))
+    if (int e = rdma_launch_shape(r->L.max_deg, (r->L.H + RDMA_WARPS - 1) / RDMA_WARPS + r->L.S, &r->grid, &r->smem))
         return *err = std::string("the RDMA slot kernel does not fit: ") + cudaGetErrorString((cudaError_t)e), -2;
     r->prepared = true;
     return 0;

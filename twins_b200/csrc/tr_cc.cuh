@@ -93,7 +93,9 @@ TR_HD uint64_t hop_make(uint64_t time, uint64_t bytes, uint32_t qlen, uint64_t r
             code = c;
             break;
         }
-    const uint64_t b = bytes / (128ull * multi), q = qlen / (80u * multi);
+    // (multi 1, the usual: the same quotients without a division routine)
+    const uint64_t b = multi == 1 ? bytes >> 7 : bytes / (128ull * multi);
+    const uint64_t q = multi == 1 ? qlen / 80u : qlen / (80u * multi);
     return code | (time & 0xFFFFFF) << 3 | (b & 0xFFFFF) << 27 | (q & 0x1FFFF) << 47;
 }
 // the differences of two words' counters, across one wrap

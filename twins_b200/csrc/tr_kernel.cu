@@ -12,55 +12,79 @@ namespace tr
 constexpr long long BARRIER_SPIN_LIMIT = 1ll << 22; // polls of ~64 ns: a quarter of a second or more
 
 __device__ __forceinline__ unsigned ld_volatile(const unsigned *p) { return *(const volatile unsigned *)p; }
-
-// a warp's scratch in shared memory: a NIC's DCQCN timers and staged arrivals, or a switch's ports,
-// staged arrivals, a safe slot's order and flags
-__host__ __device__ inline size_t sw_ports_bytes(int max_deg) { return ((size_t)max_deg * sizeof(SwPort) + 15) & ~(size_t)15; }
-__host__ __device__ inline size_t warp_scratch_bytes(int max_deg)
+#ifdef TR_PROFILE
+__device__ __forceinline__ unsigned long long gtimer()
 {
-    const size_t host = sizeof(Due) * MAX_DUE + sizeof(SArr) * HOST_STAGE;
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+#endif
+
+// a block's scratch in shared memory: per warp a NIC's DCQCN timers and staged arrivals, or one
+// switch's ports, staged arrivals, a safe slot's order and flags
+__host__ __device__ inline size_t host_scratch_bytes() { return (sizeof(Due) * MAX_DUE + sizeof(SArr) * HOST_STAGE + 15) & ~(size_t)15; }
+__host__ __device__ inline size_t sw_ports_bytes(int max_deg) { return ((size_t)max_deg * sizeof(SwPort) + 15) & ~(size_t)15; }
+__host__ __device__ inline size_t block_scratch_bytes(int max_deg)
+{
+    const size_t host = host_scratch_bytes() * RDMA_WARPS;
     const size_t sw = sw_ports_bytes(max_deg) + sizeof(SArr) * SW_STAGE + sizeof(uint16_t) * SW_STAGE + 4 * sizeof(int);
     return ((host > sw ? host : sw) + 15) & ~(size_t)15;
 }
 
+// A block's units: a group of RDMA_WARPS NIC hosts (a warp each) or one switch (all its warps: its
+// egress ports spread over them in safe slots).
 __global__ void __launch_bounds__(RDMA_WARPS * 32) rdma_slot_kernel(RSim s, int slots, int max_deg)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int blk_last;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int gwarp = blockIdx.x * RDMA_WARPS + warp, nwarps = gridDim.x * RDMA_WARPS;
-    unsigned char *mine = smem + warp_scratch_bytes(max_deg) * warp;
-    Due *due = reinterpret_cast<Due *>(mine);
-    SArr *hstage = reinterpret_cast<SArr *>(mine + sizeof(Due) * MAX_DUE);
+    Due *due = reinterpret_cast<Due *>(smem + host_scratch_bytes() * warp);
+    SArr *hstage = reinterpret_cast<SArr *>(smem + host_scratch_bytes() * warp + sizeof(Due) * MAX_DUE);
     SwWork work;
-    work.port = reinterpret_cast<SwPort *>(mine);
-    work.arr = reinterpret_cast<SArr *>(mine + sw_ports_bytes(max_deg));
-    work.ord = reinterpret_cast<uint16_t *>(mine + sw_ports_bytes(max_deg) + sizeof(SArr) * SW_STAGE);
-    work.flags = reinterpret_cast<int *>(mine + sw_ports_bytes(max_deg) + (sizeof(SArr) + sizeof(uint16_t)) * SW_STAGE);
+    work.port = reinterpret_cast<SwPort *>(smem);
+    work.arr = reinterpret_cast<SArr *>(smem + sw_ports_bytes(max_deg));
+    work.ord = reinterpret_cast<uint16_t *>(smem + sw_ports_bytes(max_deg) + sizeof(SArr) * SW_STAGE);
+    work.flags = reinterpret_cast<int *>(smem + sw_ports_bytes(max_deg) + (sizeof(SArr) + sizeof(uint16_t)) * SW_STAGE);
     RCtl *ctl = s.ctl;
     volatile RCtl *vc = ctl;
-    const int units = s.H + s.S;
+    const int groups = (s.H + RDMA_WARPS - 1) / RDMA_WARPS, units = groups + s.S;
     for (int it = 0; it < slots; it++)
     {
         if (vc->finished)
             return;
         const int64_t t = vc->slot;
-        for (int u = gwarp; u < units; u += nwarps)
+        for (int u = blockIdx.x; u < units; u += gridDim.x)
         {
-            if (u < s.H)
+#ifdef TR_PROFILE
+            const unsigned long long p0 = gtimer();
+#endif
+            if (u < groups)
             {
-                int64_t w = INT64_MAX;
-                const bool act = host_slot(s, u, t, &w, due, hstage, lane, 32);
-                if (lane == 0)
+                const int h = u * RDMA_WARPS + warp;
+                if (h < s.H)
                 {
-                    if (act)
-                        atomicAdd(&ctl->activity, 1u);
-                    if (w != INT64_MAX)
-                        atomicMin(&ctl->next_wake, (unsigned long long)w);
+                    int64_t w = INT64_MAX;
+                    const bool act = host_slot(s, h, t, &w, due, hstage, lane, 32);
+                    if (lane == 0)
+                    {
+                        if (act)
+                            atomicAdd(&ctl->activity, 1u);
+                        if (w != INT64_MAX)
+                            atomicMin(&ctl->next_wake, (unsigned long long)w);
+                    }
                 }
             }
-            else if (switch_slot(s, u - s.H, t, work, lane, 32) && lane == 0)
-                atomicAdd(&ctl->activity, 1u);
+            else
+            {
+                if (switch_slot(s, u - groups, t, work, threadIdx.x, RDMA_WARPS * 32) && threadIdx.x == 0)
+                    atomicAdd(&ctl->activity, 1u);
+            }
+#ifdef TR_PROFILE
+            if (lane == 0)
+                atomicMax(u < groups ? &ctl->prof_host_max : &ctl->prof_sw_max, gtimer() - p0);
+#endif
+            __syncthreads(); // (the scratch is the next unit's)
         }
         __syncthreads();
         unsigned g = 0;
@@ -80,6 +104,14 @@ __global__ void __launch_bounds__(RDMA_WARPS * 32) rdma_slot_kernel(RSim s, int 
                 const unsigned long long wake = atomicExch(&ctl->next_wake, ~0ull);
                 const unsigned done = atomicAdd(&ctl->flows_done, 0u);
                 slot_close(s, t, act, wake, done);
+#ifdef TR_PROFILE
+                const unsigned long long now = gtimer();
+                if (vc->prof_release)
+                    s.ev[EV_PROF_SLOT_NS] += now - vc->prof_release;
+                vc->prof_release = now;
+                s.ev[EV_PROF_HOST_NS] += atomicExch(&ctl->prof_host_max, 0ull);
+                s.ev[EV_PROF_SW_NS] += atomicExch(&ctl->prof_sw_max, 0ull);
+#endif
                 vc->arrive = 0;
                 __threadfence();
                 atomicAdd(&ctl->gen, 1u);
@@ -107,7 +139,7 @@ __global__ void __launch_bounds__(RDMA_WARPS * 32) rdma_slot_kernel(RSim s, int 
 
 int rdma_launch_shape(int max_deg, int units, int *grid, size_t *smem)
 {
-    *smem = warp_scratch_bytes(max_deg) * RDMA_WARPS;
+    *smem = block_scratch_bytes(max_deg);
     if (cudaFuncSetAttribute((const void *)rdma_slot_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem) != cudaSuccess)
         return (int)cudaGetLastError();
     int dev = 0, sms = 0, per_sm = 0;
@@ -117,9 +149,9 @@ int rdma_launch_shape(int max_deg, int units, int *grid, size_t *smem)
         return (int)cudaGetLastError();
     if (per_sm < 1)
         return (int)cudaErrorInvalidConfiguration;
-    // a warp per entity where they fit at once; else every resident warp takes several
-    const int want = (units + RDMA_WARPS - 1) / RDMA_WARPS;
-    *grid = want < per_sm * sms ? want : per_sm * sms;
+    // a block per unit (a group of NIC hosts or a switch) where they fit at once; else every
+    // resident block takes several
+    *grid = units < per_sm * sms ? units : per_sm * sms;
     return 0;
 }
 

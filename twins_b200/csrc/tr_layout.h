@@ -36,6 +36,7 @@ struct RLayout
     std::vector<int> start_list;
     std::vector<uint32_t> root_rank;
     std::vector<LinkInfo> link;
+    std::vector<int32_t> txt; // [rate classes][TXT_N]
     std::vector<int> world_hbase, world_fbase;
     size_t n_frames = 0, n_tags = 0;
     int pend_n = 2;
@@ -135,6 +136,7 @@ inline bool layout_rdma(RLayout &o, const std::vector<const RdmaWorld *> &worlds
     std::vector<std::vector<uint32_t>> root_leads(F);
     std::vector<uint32_t> root_of(F);
     std::vector<int> per_nic(H, 0);
+    std::vector<uint64_t> rates;
     size_t sl = 0;
     for (int wi = 0; wi < W; wi++)
     {
@@ -156,6 +158,17 @@ inline bool layout_rdma(RLayout &o, const std::vector<const RdmaWorld *> &worlds
                 return o.error = "a link's delay is too long for the slot", false;
             x.nb = (uint16_t)nb;
             x.cap = (uint16_t)cap;
+            // its rate's row of tx times
+            size_t rc = 0;
+            while (rc < rates.size() && rates[rc] != x.bps)
+                rc++;
+            if (rc == rates.size())
+            {
+                rates.push_back(x.bps);
+                for (int b = 0; b < TXT_N; b++)
+                    o.txt.push_back((int32_t)tx_ns(x.bps, (uint32_t)b));
+            }
+            x.rc = (uint32_t)rc;
             x.moff = o.n_frames;
             x.coff = (uint32_t)o.n_tags;
             o.n_frames += (size_t)nb * cap;

@@ -170,7 +170,9 @@ struct LinkInfo
     uint64_t moff;   // its first frame slot in msg
     uint32_t coff;   // its first bucket tag in msg_cnt
     uint16_t nb, cap;
+    uint32_t rc;     // its rate's class: its row of tx times (RSim::txt)
 };
+constexpr int TXT_N = 9216; // frames shorter than this many bytes take their tx time from a table
 struct FlowInfo
 {
     int src, dst;       // hosts over all worlds
@@ -191,6 +193,8 @@ struct RCtl
     unsigned int activity;
     unsigned int arrive, gen;
     int finished, error;
+    // (TR_PROFILE builds) this slot's longest NIC and switch (ns), the last release of the barrier
+    unsigned long long prof_host_max, prof_sw_max, prof_release;
 };
 
 // counters (the reference's event counters, same indices)
@@ -221,6 +225,9 @@ enum
     EV_PROF_TAIL_LOADS = 31, // (TR_PROFILE builds) tail nodes read by them
     EV_PROF_SAFE = 32,       // (TR_PROFILE builds) switch slots run as safe slots
     EV_PROF_SERIAL = 33,     // (TR_PROFILE builds) switch slots with events run in one order
+    EV_PROF_HOST_NS = 34,    // (TR_PROFILE builds) the slots' longest NIC, summed (ns)
+    EV_PROF_SW_NS = 35,      // (TR_PROFILE builds) the slots' longest switch, summed (ns)
+    EV_PROF_SLOT_NS = 37,    // (TR_PROFILE builds) the slots' durations, barrier to barrier, summed (ns)
     EV_TIMEOUT = 36,
     EV_N = 40
 };
@@ -256,6 +263,7 @@ struct RSim
     RxQp *rx;
     int64_t *fct;
     const LinkInfo *link;
+    const int32_t *txt; // [rate classes][TXT_N]: tx_ns(rate, bytes)
     Frame *msg;
     long long *msg_cnt;
     unsigned int *pend;
@@ -503,7 +511,19 @@ TR_HD bool runs_before(const RSim &s, int64_t ta, uint32_t pa, const Chain &a, i
 }
 
 // ------------------------------------------------------------------ links
-TR_HD int64_t link_tx_ns(const LinkInfo &l, uint32_t bytes) { return tx_ns(l.bps, bytes); }
+// a frame's transmission time on a link (from its rate's table below TXT_N bytes: the same values)
+TR_HD int64_t link_tx_ns(const RSim &s, const LinkInfo &l, uint32_t bytes)
+{
+    if (bytes < (uint32_t)TXT_N)
+    {
+#ifdef __CUDA_ARCH__
+        return __ldg(&s.txt[(size_t)l.rc * TXT_N + bytes]);
+#else
+        return s.txt[(size_t)l.rc * TXT_N + bytes];
+#endif
+    }
+    return tx_ns(l.bps, bytes);
+}
 
 // a sender's place in its out link's ring: the bucket of the slot its frames arrive in
 struct OutLink
@@ -566,12 +586,20 @@ TR_HD int bucket_of(const RSim &s, int link, int64_t t, uint64_t *base)
 }
 
 // the code of a frame's arrival: lead its tx time + the link's delay, its ordinal
-TR_HD uint32_t arrival_code(const LinkInfo &l, const Frame &f) { return event_code(link_tx_ns(l, f.p.size) + l.delay, f.p.ord); }
+TR_HD uint32_t arrival_code(const RSim &s, const LinkInfo &l, const Frame &f) { return event_code(link_tx_ns(s, l, f.p.size) + l.delay, f.p.ord); }
 
 // ------------------------------------------------------------------ a warp's lanes
 // (lanes = 1 on the CPU: every lane's share runs in turn)
 #ifdef __CUDA_ARCH__
 __device__ __forceinline__ void lanes_sync() { __syncwarp(); }
+// the lanes of a switch: a warp (32) or the whole block
+__device__ __forceinline__ void group_sync(int lanes)
+{
+    if (lanes <= 32)
+        __syncwarp();
+    else
+        __syncthreads();
+}
 __device__ __forceinline__ void sh_add(uint32_t *p, uint32_t v) { atomicAdd(p, v); }
 __device__ __forceinline__ void sh_add(int *p, int v) { atomicAdd(p, v); }
 __device__ __forceinline__ void sh_sub(uint32_t *p, uint32_t v) { atomicSub(p, v); }
@@ -593,6 +621,7 @@ __device__ __forceinline__ void ld_chain(Chain &c, const Chain *src)
 }
 #else
 inline void lanes_sync() {}
+inline void group_sync(int) {}
 inline void sh_add(uint32_t *p, uint32_t v) { *p += v; }
 inline void sh_add(int *p, int v) { *p += v; }
 inline void sh_sub(uint32_t *p, uint32_t v) { *p -= v; }
@@ -618,13 +647,12 @@ constexpr int HOST_STAGE = 128; // a NIC's arrivals of a slot staged; more are r
 constexpr int SW_STAGE = 384;   // a switch's arrivals of a slot staged; more run unstaged, serially
 constexpr int SAFE_PORTS = 32;  // switches with more ports run every slot serially
 
-TR_HD void stage_arrival(const RSim &s, SArr &a, uint32_t frame, const LinkInfo &lin)
+TR_HD void stage_arrival(const RSim &s, SArr &a, uint32_t frame, const LinkInfo &lin, Pkt &p)
 {
     const Frame *f = &s.msg[frame];
     a.ts = (int64_t)ld_tag((const long long *)&f->ts);
-    Pkt p;
     ld_pkt(p, &f->p);
-    a.acode = event_code(link_tx_ns(lin, p.size) + lin.delay, p.ord);
+    a.acode = event_code(link_tx_ns(s, lin, p.size) + lin.delay, p.ord);
     a.frame = frame;
     a.size = p.size;
     a.kind = p.kind;
@@ -657,7 +685,7 @@ struct HostEv
 TR_HD void h_transmit(HostEv &e, Pkt p)
 {
     const RSim &s = *e.s;
-    const int64_t tx = link_tx_ns(e.out.li, p.size);
+    const int64_t tx = link_tx_ns(*e.s, e.out.li, p.size);
     e.n.tc_at = e.now + tx;
     chain_push(s, s.h_tc[e.h], event_code(tx, e.ord++), e.cur);
     p.ord = (uint8_t)(e.ord < 255 ? e.ord : 255);
@@ -899,7 +927,10 @@ TR_HD bool host_slot(const RSim &s, int h, int64_t t, int64_t *wake, Due *due, S
     {
         const LinkInfo lin = s.link[hi.link_in];
         for (int j = lane; j < na; j += lanes)
-            stage_arrival(s, stage[j], (uint32_t)(abase + j), lin);
+        {
+            Pkt p;
+            stage_arrival(s, stage[j], (uint32_t)(abase + j), lin, p);
+        }
         lanes_sync();
     }
     bool act = false;
@@ -941,7 +972,10 @@ TR_HD bool host_events(const RSim &s, int h, int64_t t, int64_t *wake, Due *due,
             if (staged)
                 a = stage[ai];
             else
-                stage_arrival(s, a, (uint32_t)(abase + ai), lin);
+            {
+                Pkt p;
+                stage_arrival(s, a, (uint32_t)(abase + ai), lin, p);
+            }
             have_a = true;
             have_ac = false;
         }
@@ -1128,7 +1162,7 @@ TR_HD void s_transmit(SwEv &e, int port, Pkt p)
 {
     const RSim &s = *e.s;
     SwPort &pe = e.pe[port];
-    const int64_t tx = link_tx_ns(pe.out.li, p.size);
+    const int64_t tx = link_tx_ns(s, pe.out.li, p.size);
     pe.pt.tc_at = e.now + tx;
     chain_push(s, s.p_tc[e.si.pbase + port], event_code(tx, e.ord++), e.cur);
     p.ord = (uint8_t)(e.ord < 255 ? e.ord : 255);
@@ -1458,10 +1492,9 @@ TR_HD void serial_events(SwEv &e, const SwWork &w, int deg, int64_t t1, bool sta
                 {
                     if (!q.have_pa)
                     {
-                        stage_arrival(s, q.pa, (uint32_t)(q.abase + q.ai), q.lin);
-                        q.pa.in = (uint8_t)p;
                         Pkt pk;
-                        ld_pkt(pk, &s.msg[q.pa.frame].p);
+                        stage_arrival(s, q.pa, (uint32_t)(q.abase + q.ai), q.lin, pk);
+                        q.pa.in = (uint8_t)p;
                         int qi = PG;
                         q.pa.out = (int16_t)(pk.kind == K_PAUSE || pk.kind == K_RESUME ? -1 : s_route(s, e.si, *e.w, pk, &qi));
                         q.pa.q = (uint8_t)qi;
@@ -1515,8 +1548,8 @@ TR_HD void serial_events(SwEv &e, const SwWork &w, int deg, int64_t t1, bool sta
     }
 }
 
-// A switch's events of slot t in ns-3's order: every port's arrivals and TransmitCompletes, by the
-// warp's lanes. They load the ports and stage the slot's arrivals with their routes; then, when no
+// A switch's events of slot t in ns-3's order: every port's arrivals and TransmitCompletes, by a
+// group of lanes (a warp, or a block's warps). They load the ports and stage the slot's arrivals with their routes; then, when no
 // buffer decision (drop, headroom, PAUSE, RESUME) can occur in the slot, each lane runs egress
 // ports of its own (a safe slot), else lane 0 runs all events in one order; the lanes store the
 // ports. Returns (on every lane) whether the switch sent or holds frames.
@@ -1529,7 +1562,7 @@ TR_HD bool switch_slot(const RSim &s, int x, int64_t t, const SwWork &w, int lan
     const int64_t t1 = (t + 1) * s.D;
     if (lane == 0)
         w.flags[0] = w.flags[1] = w.flags[2] = w.flags[3] = 0;
-    lanes_sync();
+    group_sync(lanes);
     for (int p = lane; p < deg; p += lanes)
     {
         SwPort &q = w.port[p];
@@ -1545,7 +1578,7 @@ TR_HD bool switch_slot(const RSim &s, int x, int64_t t, const SwWork &w, int lan
         if (q.an > 0 || (q.pt.tc_at >= 0 && q.pt.tc_at < t1))
             sh_add(&w.flags[2], 1);
     }
-    lanes_sync();
+    group_sync(lanes);
     if (w.flags[2] == 0)
     {
         // no event: the ports stay as they are
@@ -1555,7 +1588,7 @@ TR_HD bool switch_slot(const RSim &s, int x, int64_t t, const SwWork &w, int lan
             const Port &pt = w.port[p].pt;
             act |= pt.q0_n > 0 || pt.q3_n > 0 || pt.tc_at >= 0;
         }
-        lanes_sync();
+        group_sync(lanes);
         return act;
     }
     if (lane == 0)
@@ -1568,7 +1601,7 @@ TR_HD bool switch_slot(const RSim &s, int x, int64_t t, const SwWork &w, int lan
         }
         w.flags[1] = total;
     }
-    lanes_sync();
+    group_sync(lanes);
     const int total = w.flags[1];
     const bool staged = total <= SW_STAGE;
     if (staged)
@@ -1580,10 +1613,9 @@ TR_HD bool switch_slot(const RSim &s, int x, int64_t t, const SwWork &w, int lan
                 p++;
             SArr &a = w.arr[j];
             const uint32_t frame = (uint32_t)(w.port[p].abase + (j - w.port[p].first));
-            stage_arrival(s, a, frame, w.port[p].lin);
-            a.in = (uint8_t)p;
             Pkt pk;
-            ld_pkt(pk, &s.msg[frame].p);
+            stage_arrival(s, a, frame, w.port[p].lin, pk);
+            a.in = (uint8_t)p;
             int qi = PG;
             a.out = (int16_t)(pk.kind == K_PAUSE || pk.kind == K_RESUME ? -1 : s_route(s, si, wp, pk, &qi));
             a.q = (uint8_t)qi;
@@ -1593,7 +1625,7 @@ TR_HD bool switch_slot(const RSim &s, int x, int64_t t, const SwWork &w, int lan
             if (own >= 0)
                 sh_add(&w.port[own].ocnt, 1);
         }
-        lanes_sync();
+        group_sync(lanes);
     }
     SwEv e;
     e.s = &s;
@@ -1631,7 +1663,7 @@ TR_HD bool switch_slot(const RSim &s, int x, int64_t t, const SwWork &w, int lan
         }
         w.flags[2] = safe;
     }
-    lanes_sync();
+    group_sync(lanes);
     const bool safe = w.flags[2] != 0;
     e.safe = safe;
 #ifdef TR_PROFILE
@@ -1639,11 +1671,15 @@ TR_HD bool switch_slot(const RSim &s, int x, int64_t t, const SwWork &w, int lan
         count(s, safe ? EV_PROF_SAFE : EV_PROF_SERIAL);
 #endif
     if (safe)
-        for (int o = lane; o < deg; o += lanes)
+    {
+        // egress ports spread over the warps (a warp's lanes diverge: fewer ports each, less waiting)
+        const int wl = lanes < 32 ? lanes : 32, nw = lanes < 32 ? 1 : lanes / 32;
+        for (int o = lane / wl + nw * (lane % wl); o < deg; o += nw * wl)
             safe_egress(e, w, o, t1, total);
+    }
     else if (lane == 0)
         serial_events(e, w, deg, t1, staged);
-    lanes_sync();
+    group_sync(lanes);
     bool act = false;
     for (int p = lane; p < deg; p += lanes)
     {
@@ -1652,7 +1688,7 @@ TR_HD bool switch_slot(const RSim &s, int x, int64_t t, const SwWork &w, int lan
         q.pt.ob_last = q.out.last;
         s.port[si.pbase + p] = q.pt;
     }
-    lanes_sync();
+    group_sync(lanes);
     for (int p = 0; p < deg; p++)
     {
         const SwPort &q = w.port[p];
@@ -1679,7 +1715,7 @@ TR_HD bool switch_slot(const RSim &s, int x, int64_t t, const SwWork &w, int lan
         }
         s.sw[x].mmu = e.mmu;
     }
-    lanes_sync();
+    group_sync(lanes);
     return act;
 }
 
