@@ -112,6 +112,7 @@ int rs_run(int n, const char **cfg, const char **topo, const char **flows, long 
     std::vector<SwPort> ports(L.max_deg);
     std::vector<SArr> arr(SW_STAGE > HOST_STAGE ? SW_STAGE : HOST_STAGE);
     std::vector<uint16_t> ord(SW_STAGE);
+    std::vector<HPre> hpre(HOST_STAGE);
     int flags[4];
     const SwWork work{ports.data(), arr.data(), ord.data(), flags};
     Due due[MAX_DUE];
@@ -123,7 +124,7 @@ int rs_run(int n, const char **cfg, const char **topo, const char **flows, long 
         for (int h = 0; h < L.H; h++)
         {
             int64_t w = INT64_MAX;
-            if (host_slot(s, h, t, &w, due, arr.data(), 0, 1))
+            if (host_slot(s, h, t, &w, due, arr.data(), hpre.data(), 0, 1))
                 act++;
             if (w != INT64_MAX && (unsigned long long)w < wake)
                 wake = (unsigned long long)w;

@@ -39,6 +39,27 @@ TR_HD int64_t tx_ns(uint64_t bps, uint32_t bytes) { return ns_seconds((double)by
 TR_HD int64_t tx_ns36(uint64_t bps, uint32_t bytes) { return (int64_t)(((uint64_t)bytes * 8000000000ull) / bps); }
 TR_HD int64_t tx_time(bool ns336, uint64_t bps, uint32_t bytes) { return ns336 ? tx_ns36(bps, bytes) : tx_ns(bps, bytes); }
 
+// a queue pair's last tx time asked (PktSent and ChangeRate ask for the same rate and size in turn):
+// the value again without the division
+struct TxMemo
+{
+    uint64_t rate;
+    uint32_t size;
+    int64_t val;
+};
+TR_HD int64_t tx_time_memo(TxMemo *m, bool ns336, uint64_t bps, uint32_t bytes)
+{
+    if (!m)
+        return tx_time(ns336, bps, bytes);
+    if (m->rate != bps || m->size != bytes)
+    {
+        m->rate = bps;
+        m->size = bytes;
+        m->val = tx_time(ns336, bps, bytes);
+    }
+    return m->val;
+}
+
 // DataRate from a double: truncation (reference: src/rdma/rstep.cuh:152)
 TR_HD uint64_t rate_of(double d) { return (uint64_t)d; }
 
@@ -266,6 +287,27 @@ TR_HD double hpcc_hop_u(uint64_t now, uint64_t was, uint32_t multi, uint64_t max
     return tx_rate / lr + (double)(qa < qb ? qa : qb) * (double)max_rate / lr / (double)win;
 }
 
+// the largest hop utilisation U (the first of equal ones) and its interval of an ACK's nhop INT
+// words against the hops the queue pair holds, without SAMPLE_FEEDBACK (hpcc_ack's loop)
+TR_HD void hpcc_hops_u(const uint64_t *hops, int nhop, const uint64_t *held, uint32_t multi, uint64_t max_rate, uint32_t win, double *U_out,
+                       uint64_t *dt_out)
+{
+    double U = 0;
+    uint64_t dt = 0;
+    for (int i = 0; i < nhop; i++)
+    {
+        uint64_t tau;
+        const double u = hpcc_hop_u(hops[i], held[i], multi, max_rate, win, &tau);
+        if (u > U)
+        {
+            U = u;
+            dt = tau;
+        }
+    }
+    *U_out = U;
+    *dt_out = dt;
+}
+
 // HPCC's rate rule for an ACK carrying nhop INT words (RdmaHw::UpdateRateHp, one rate for the
 // path): the largest hop utilisation U (the first of equal ones) and its interval dt set the EWMA
 // u = (u (B - dt) + U dt) / B over the base RTT B (dt at most B); u / u_target >= 1 or mi_thresh
@@ -274,7 +316,10 @@ TR_HD double hpcc_hop_u(uint64_t now, uint64_t was, uint32_t multi, uint64_t max
 // the next send: paced_after_change); the hops are stored, and the reference rate and stage too
 // unless `fast` (fast react), and the last sequence number updated (reference:
 // src/rdma/rstep.cuh:1208-1313)
-TR_HD bool hpcc_ack(QpRate &q, const CcParams &P, const uint64_t *hops, int nhop, bool fast)
+// (pre: the hops' U and tau worked out ahead by hpcc_hops_u, when the queue pair's stored hops were
+// known then; the same values the loop below gives)
+TR_HD bool hpcc_ack(QpRate &q, const CcParams &P, const uint64_t *hops, int nhop, bool fast, const double *pre_u = nullptr,
+                    uint64_t pre_dt = 0)
 {
     const uint32_t next_seq = (uint32_t)q.snd_nxt;
     if (q.last_update_seq == 0)
@@ -290,7 +335,16 @@ TR_HD bool hpcc_ack(QpRate &q, const CcParams &P, const uint64_t *hops, int nhop
         double U = 0;
         uint64_t dt = 0;
         bool any = false;
-        for (int i = 0; i < nhop; i++)
+        if (pre_u)
+        {
+            U = *pre_u;
+            dt = pre_dt;
+            any = nhop > 0;
+            for (int i = 0; i < nhop; i++)
+                q.hop[i] = hops[i];
+        }
+        else
+            for (int i = 0; i < nhop; i++)
         {
             if (P.sample_feedback && hop_qlen(hops[i]) == 0 && fast)
                 continue;
@@ -342,9 +396,11 @@ TR_HD bool hpcc_ack(QpRate &q, const CcParams &P, const uint64_t *hops, int nhop
 
 // a rate change's effect on pacing (ChangeRate): the next send moves by the difference of the last
 // packet's tx times at the new and the old rate (reference: src/rdma/rstep.cuh:1198-1206)
-TR_HD int64_t paced_after_change(int64_t next_avail, bool ns336, uint64_t old_rate, uint64_t new_rate, uint32_t last_pkt)
+TR_HD int64_t paced_after_change(int64_t next_avail, bool ns336, uint64_t old_rate, uint64_t new_rate, uint32_t last_pkt,
+                                 TxMemo *m = nullptr)
 {
-    return next_avail + tx_time(ns336, new_rate, last_pkt) - tx_time(ns336, old_rate, last_pkt);
+    const int64_t st = tx_time_memo(m, ns336, old_rate, last_pkt);
+    return next_avail + tx_time_memo(m, ns336, new_rate, last_pkt) - st;
 }
 
 } // namespace tr

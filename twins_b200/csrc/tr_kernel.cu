@@ -23,7 +23,10 @@ __device__ __forceinline__ unsigned long long gtimer()
 
 // a block's scratch in shared memory: per warp a NIC's DCQCN timers and staged arrivals, or one
 // switch's ports, staged arrivals, a safe slot's order and flags
-__host__ __device__ inline size_t host_scratch_bytes() { return (sizeof(Due) * MAX_DUE + sizeof(SArr) * HOST_STAGE + 15) & ~(size_t)15; }
+__host__ __device__ inline size_t host_scratch_bytes()
+{
+    return (sizeof(Due) * MAX_DUE + sizeof(SArr) * HOST_STAGE + sizeof(HPre) * HOST_STAGE + 15) & ~(size_t)15;
+}
 __host__ __device__ inline size_t sw_ports_bytes(int max_deg) { return ((size_t)max_deg * sizeof(SwPort) + 15) & ~(size_t)15; }
 __host__ __device__ inline size_t block_scratch_bytes(int max_deg)
 {
@@ -41,6 +44,7 @@ __global__ void __launch_bounds__(RDMA_WARPS * 32) rdma_slot_kernel(RSim s, int 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     Due *due = reinterpret_cast<Due *>(smem + host_scratch_bytes() * warp);
     SArr *hstage = reinterpret_cast<SArr *>(smem + host_scratch_bytes() * warp + sizeof(Due) * MAX_DUE);
+    HPre *hpre = reinterpret_cast<HPre *>(smem + host_scratch_bytes() * warp + sizeof(Due) * MAX_DUE + sizeof(SArr) * HOST_STAGE);
     SwWork work;
     work.port = reinterpret_cast<SwPort *>(smem);
     work.arr = reinterpret_cast<SArr *>(smem + sw_ports_bytes(max_deg));
@@ -65,7 +69,7 @@ __global__ void __launch_bounds__(RDMA_WARPS * 32) rdma_slot_kernel(RSim s, int 
                 if (h < s.H)
                 {
                     int64_t w = INT64_MAX;
-                    const bool act = host_slot(s, h, t, &w, due, hstage, lane, 32);
+                    const bool act = host_slot(s, h, t, &w, due, hstage, hpre, lane, 32);
                     if (lane == 0)
                     {
                         if (act)

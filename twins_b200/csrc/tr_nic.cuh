@@ -60,18 +60,26 @@ TR_HD uint64_t bytes_left(const QpRate &r, const QpSend &q) { return q.size >= r
 
 // the window holds no more (RdmaQueuePair::IsWinBound): bytes in flight reach the window, scaled by
 // rate / line rate with VAR_WIN (at least 1) (reference: src/rdma/rstep.cuh:1036-1053)
+// (VAR_WIN: with n = win * rate (64 bits, wrapping as the reference's product) and m the line rate,
+// inflight >= max(1, floor(n / m)) holds exactly when inflight >= 1 and n < (inflight + 1) m, a
+// 128-bit product instead of a division routine)
 TR_HD bool win_bound(const NicParams &P, const QpRate &r, const QpSend &q)
 {
     if (r.win == 0)
         return false;
-    uint64_t w = r.win;
-    if (P.var_win)
-    {
-        w = (uint64_t)r.win * r.rate / r.max_rate;
-        if (w == 0)
-            w = 1;
-    }
-    return r.snd_nxt - q.snd_una >= w;
+    const uint64_t inflight = r.snd_nxt - q.snd_una;
+    if (!P.var_win)
+        return inflight >= r.win;
+    if (inflight == 0 || inflight == ~0ull)
+        return inflight != 0;
+    const uint64_t n = (uint64_t)r.win * r.rate, a = inflight + 1, m = r.max_rate;
+#ifdef __CUDA_ARCH__
+    const uint64_t hi = __umul64hi(a, m), lo = a * m;
+#else
+    const unsigned __int128 am = (unsigned __int128)a * m;
+    const uint64_t hi = (uint64_t)(am >> 64), lo = (uint64_t)am;
+#endif
+    return hi > 0 || n < lo;
 }
 
 // RdmaEgressQueue::GetNextQindex over a NIC's queue pairs list[0 .. *n): -1 the ACK queue (not
@@ -146,7 +154,7 @@ TR_HD void qp_start(const NicParams &P, QpRate &r, QpSend &q, uint64_t size, uin
 // the next data frame of a queue pair (RdmaHw::GetNxtPacket, PktSent, UpdateNextAvail): its
 // sequence number (*seq) and size; snd_nxt moves past its payload, and the next send waits its tx
 // time at the rate (or the line rate without RATE_BOUND) (reference: src/rdma/rstep.cuh:1162-1181)
-TR_HD uint32_t next_data(const NicParams &P, QpRate &r, QpSend &q, int64_t now, bool rate_bound, uint32_t *seq)
+TR_HD uint32_t next_data(const NicParams &P, QpRate &r, QpSend &q, int64_t now, bool rate_bound, uint32_t *seq, TxMemo *m = nullptr)
 {
     const uint64_t left = bytes_left(r, q);
     const uint32_t payload = left < P.mtu ? (uint32_t)left : P.mtu;
@@ -154,7 +162,7 @@ TR_HD uint32_t next_data(const NicParams &P, QpRate &r, QpSend &q, int64_t now, 
     *seq = (uint32_t)r.snd_nxt;
     r.snd_nxt += payload;
     q.last_pkt = size;
-    q.next_avail = now + tx_time(P.ns336 != 0, rate_bound ? r.rate : r.max_rate, size);
+    q.next_avail = now + tx_time_memo(m, P.ns336 != 0, rate_bound ? r.rate : r.max_rate, size);
     return size;
 }
 
@@ -231,7 +239,7 @@ enum : unsigned
 // the congestion control: DCQCN's CNP, HPCC's update (fast react on ACKs of old data), DCTCP's ACK
 // (reference: src/rdma/rstep.cuh:1438-1485). A queue pair already done is the caller's to skip.
 TR_HD unsigned ack_received(const NicParams &P, const CcParams &C, QpRate &r, QpSend &q, uint32_t seq, bool nack, bool cnp,
-                            const uint64_t *hops, int nhop)
+                            const uint64_t *hops, int nhop, const double *pre_u = nullptr, uint64_t pre_dt = 0, TxMemo *m = nullptr)
 {
     unsigned out = 0;
     if (seq > q.snd_una)
@@ -248,9 +256,9 @@ TR_HD unsigned ack_received(const NicParams &P, const CcParams &C, QpRate &r, Qp
     if (P.cc == 3 && (seq > r.last_update_seq || P.fast_react))
     {
         const uint64_t old = r.rate;
-        if (hpcc_ack(r, C, hops, nhop, !(seq > r.last_update_seq)))
+        if (hpcc_ack(r, C, hops, nhop, !(seq > r.last_update_seq), pre_u, pre_dt))
         {
-            q.next_avail = paced_after_change(q.next_avail, P.ns336 != 0, old, r.rate, q.last_pkt);
+            q.next_avail = paced_after_change(q.next_avail, P.ns336 != 0, old, r.rate, q.last_pkt, m);
             out |= ACK_RATE_SET;
         }
     }

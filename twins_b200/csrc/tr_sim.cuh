@@ -110,6 +110,7 @@ struct Qp
     QpRate r;
     QpSend q;
     int64_t t[3]; // alpha update, rate-decrease check, rate increase (-1: none)
+    TxMemo tx;    // its last tx time computed
 };
 struct QpChains
 {
@@ -636,12 +637,21 @@ struct SArr
     int64_t ts;
     uint32_t acode;
     uint32_t frame;
+    uint32_t flow;
     int16_t out;      // egress port (-1: a PFC frame, or no route)
     uint8_t q, in;    // its queue; its ingress port
     uint16_t size;
-    uint8_t kind, pad;
+    uint8_t kind;
+    uint8_t pre;      // a NIC's HPCC ACK: its hops' U and tau were worked out by the lanes (HPre)
 };
-static_assert(sizeof(SArr) == 24, "SArr");
+static_assert(sizeof(SArr) == 32, "SArr");
+
+// an HPCC ACK's hop utilisation U and its interval, worked out ahead (hpcc_hops_u)
+struct HPre
+{
+    double U;
+    uint64_t dt;
+};
 
 constexpr int HOST_STAGE = 128; // a NIC's arrivals of a slot staged; more are read one by one
 constexpr int SW_STAGE = 384;   // a switch's arrivals of a slot staged; more run unstaged, serially
@@ -654,8 +664,10 @@ TR_HD void stage_arrival(const RSim &s, SArr &a, uint32_t frame, const LinkInfo 
     ld_pkt(p, &f->p);
     a.acode = event_code(link_tx_ns(s, lin, p.size) + lin.delay, p.ord);
     a.frame = frame;
+    a.flow = p.flow;
     a.size = p.size;
     a.kind = p.kind;
+    a.pre = 0;
     a.out = -1;
     a.q = PG;
     a.in = 0;
@@ -743,7 +755,7 @@ TR_HD void h_dequeue(HostEv &e)
         p.size = (uint16_t)data_size(e.w->nic, payload);
         h_transmit(e, p);
         uint32_t seq;
-        next_data(e.w->nic, q.r, q.q, e.now, e.w->rate_bound != 0, &seq);
+        next_data(e.w->nic, q.r, q.q, e.now, e.w->rate_bound != 0, &seq, &q.tx);
         return;
     }
     const int64_t t = next_send_at(e.w->nic, list, e.n.qp_n, e.now, view);
@@ -763,7 +775,7 @@ TR_HD void h_timer_set(HostEv &e, int f, int kind, int64_t lead)
 }
 
 // RdmaHw::ReceiveAck
-TR_HD void h_ack(HostEv &e, const Pkt &p)
+TR_HD void h_ack(HostEv &e, const Pkt &p, const double *pre_u = nullptr, uint64_t pre_dt = 0)
 {
     const RSim &s = *e.s;
     const RWorld &w = *e.w;
@@ -774,7 +786,7 @@ TR_HD void h_ack(HostEv &e, const Pkt &p)
         count(s, EV_ACK_DONE);
         return;
     }
-    const unsigned r = ack_received(w.nic, w.cc, q.r, q.q, p.seq, p.kind == K_NACK, p.cnp != 0, p.hop, p.nhop);
+    const unsigned r = ack_received(w.nic, w.cc, q.r, q.q, p.seq, p.kind == K_NACK, p.cnp != 0, p.hop, p.nhop, pre_u, pre_dt, &q.tx);
     if (r & ACK_COMPLETED)
     {
         q.t[0] = q.t[1] = q.t[2] = -1;
@@ -909,9 +921,9 @@ TR_HD void h_collect_due(const RSim &s, int h, Nic &n, int64_t t1, Due *due, int
 // runs the events. Returns (on lane 0) whether it sent or holds frames; *wake: its earliest event
 // without input (INT64_MAX: none). due: room for MAX_DUE timers; stage: for HOST_STAGE arrivals.
 // (reference: host_step<1>, src/rdma/rstep.cuh:1649-2114)
-TR_HD bool host_events(const RSim &s, int h, int64_t t, int64_t *wake, Due *due, const SArr *stage, int na, uint64_t abase);
+TR_HD bool host_events(const RSim &s, int h, int64_t t, int64_t *wake, Due *due, const SArr *stage, const HPre *pre, int na, uint64_t abase);
 
-TR_HD bool host_slot(const RSim &s, int h, int64_t t, int64_t *wake, Due *due, SArr *stage, int lane, int lanes)
+TR_HD bool host_slot(const RSim &s, int h, int64_t t, int64_t *wake, Due *due, SArr *stage, HPre *pre, int lane, int lanes)
 {
     const HostInfo hi = s.hinfo[h];
     const int64_t t1 = (t + 1) * s.D;
@@ -932,16 +944,51 @@ TR_HD bool host_slot(const RSim &s, int h, int64_t t, int64_t *wake, Due *due, S
             stage_arrival(s, stage[j], (uint32_t)(abase + j), lin, p);
         }
         lanes_sync();
+        // HPCC with fast react and no sampled feedback: an ACK's hop utilisations depend only on its
+        // INT words and those its queue pair holds then, the previous ACK's of the slot (or the
+        // stored ones): the lanes work them out ahead (reference: src/rdma/rstep.cuh:1729-1748)
+        const RWorld &w = s.world[hi.world];
+        if (w.nic.cc == 3 && w.nic.fast_react && !w.cc.sample_feedback)
+        {
+            for (int j = lane; j < na; j += lanes)
+            {
+                SArr &a = stage[j];
+                if (a.kind != K_ACK && a.kind != K_NACK)
+                    continue;
+                Pkt p;
+                ld_pkt(p, &s.msg[a.frame].p);
+                if (p.nhop > MAX_HOP)
+                    continue;
+                int k = j - 1;
+                while (k >= 0 && !(stage[k].flow == a.flow && (stage[k].kind == K_ACK || stage[k].kind == K_NACK)))
+                    k--;
+                const QpRate &r = s.qp[a.flow].r;
+                uint64_t held[MAX_HOP];
+                if (k >= 0)
+                {
+                    Pkt pk;
+                    ld_pkt(pk, &s.msg[stage[k].frame].p);
+                    for (int i = 0; i < MAX_HOP; i++)
+                        held[i] = pk.hop[i];
+                }
+                else
+                    for (int i = 0; i < MAX_HOP; i++)
+                        held[i] = r.hop[i];
+                hpcc_hops_u(p.hop, p.nhop, held, w.cc.int_multi, r.max_rate, r.win, &pre[j].U, &pre[j].dt);
+                a.pre = 1;
+            }
+            lanes_sync();
+        }
     }
     bool act = false;
     if (lane == 0)
-        act = host_events(s, h, t, wake, due, stage, na, abase);
+        act = host_events(s, h, t, wake, due, stage, pre, na, abase);
     lanes_sync();
     return act;
 }
 
 // lane 0's share of host_slot: the events
-TR_HD bool host_events(const RSim &s, int h, int64_t t, int64_t *wake, Due *due, const SArr *stage, int na, uint64_t abase)
+TR_HD bool host_events(const RSim &s, int h, int64_t t, int64_t *wake, Due *due, const SArr *stage, const HPre *pre, int na, uint64_t abase)
 {
     const HostInfo hi = s.hinfo[h];
     const int64_t t1 = (t + 1) * s.D;
@@ -1037,7 +1084,8 @@ TR_HD bool host_events(const RSim &s, int h, int64_t t, int64_t *wake, Due *due,
             else if (p.kind == K_ACK || p.kind == K_NACK)
             {
                 n_ack++;
-                h_ack(e, p);
+                const bool pv = staged && a.pre;
+                h_ack(e, p, pv ? &pre[ai - 1].U : nullptr, pv ? pre[ai - 1].dt : 0);
             }
             else if (e.w->qbb)
             {
