@@ -115,6 +115,7 @@ __global__ void __launch_bounds__(RDMA_WARPS * 32) rdma_slot_kernel(RSim s, int 
                 vc->prof_release = now;
                 s.ev[EV_PROF_HOST_NS] += atomicExch(&ctl->prof_host_max, 0ull);
                 s.ev[EV_PROF_SW_NS] += atomicExch(&ctl->prof_sw_max, 0ull);
+                s.ev[EV_PROF_LANE_EV] += atomicExch(&s.ev[EV_PROF_LANE_EV_SLOT], 0ull);
 #endif
                 vc->arrive = 0;
                 __threadfence();

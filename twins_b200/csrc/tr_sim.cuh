@@ -60,6 +60,12 @@ struct TailNode
     uint64_t next, pos;
 };
 
+// an entity's reserved positions of the tail ring: next .. end - 1
+struct TailChunk
+{
+    uint64_t next, end;
+};
+
 // a frame's contents (the reference's wire format: INT hop words, flow, sequence, size, ...; 16-byte
 // aligned: it moves as 16-byte words, ld_pkt)
 struct alignas(16) Pkt
@@ -102,6 +108,7 @@ struct Nic
     int ackq_head, ackq_n;
     int qp_n, rr;         // its queue-pair list's length; the last one served
     int next_start, start_end; // its flows, in start order, still to start
+    TailChunk tail;       // its positions of the tail ring
 };
 
 // a sending queue pair: its rate state (tr_cc.cuh), its NIC view (tr_nic.cuh), its DCQCN timers
@@ -129,6 +136,7 @@ struct Port
     uint32_t bytes_total;
     MmuPort mmu;
     tb::Rng rng;
+    TailChunk tail; // its positions of the tail ring
 };
 
 struct SwState
@@ -222,6 +230,7 @@ enum
     EV_HOST_DATA = 24,       // of the NICs' arrivals: data
     EV_HOST_EVENTS = 25,     // every NIC event (arrivals, transmissions done, sends, timers, starts)
     EV_SWITCH_EVENTS = 26,   // every switch event (arrivals, transmissions done)
+    EV_PROF_SPILLS = 29,     // (TR_PROFILE builds) chain runs spilled into tail nodes
     EV_PROF_CMPS = 30,       // (TR_PROFILE builds) chain comparisons
     EV_PROF_TAIL_LOADS = 31, // (TR_PROFILE builds) tail nodes read by them
     EV_PROF_SAFE = 32,       // (TR_PROFILE builds) switch slots run as safe slots
@@ -229,6 +238,8 @@ enum
     EV_PROF_HOST_NS = 34,    // (TR_PROFILE builds) the slots' longest NIC, summed (ns)
     EV_PROF_SW_NS = 35,      // (TR_PROFILE builds) the slots' longest switch, summed (ns)
     EV_PROF_SLOT_NS = 37,    // (TR_PROFILE builds) the slots' durations, barrier to barrier, summed (ns)
+    EV_PROF_LANE_EV = 38,    // (TR_PROFILE builds) the slots' most events of one switch lane, summed
+    EV_PROF_LANE_EV_SLOT = 39, // (TR_PROFILE builds) this slot's most events of one switch lane
     EV_TIMEOUT = 36,
     EV_N = 40
 };
@@ -331,8 +342,11 @@ TR_HD void count(const RSim &s, int i, unsigned long long n = 1) { atom_add(&s.e
 
 // ------------------------------------------------------------------ event order
 // the chain of an event that the event with chain `par` schedules with `code`; a run pushed out of
-// the inline runs goes to a new tail node (reference: cpush, src/rdma/rstep.cuh:233-290)
-TR_HD void chain_push(const RSim &s, Chain &out, uint32_t code, const Chain &par)
+// the inline runs goes to a new tail node, at the next position of the caller's chunk of the ring
+// (an entity takes TAIL_CHUNK positions at a time: one shared counter for every spill was the slot
+// kernel's most contended address) (reference: cpush, src/rdma/rstep.cuh:233-290)
+constexpr uint64_t TAIL_CHUNK = 64;
+TR_HD void chain_push(const RSim &s, Chain &out, uint32_t code, const Chain &par, TailChunk &tc)
 {
     Chain c;
     if (par.r[0].code == code)
@@ -352,7 +366,15 @@ TR_HD void chain_push(const RSim &s, Chain &out, uint32_t code, const Chain &par
         c.pad = 0;
         if (par.r[RUNS - 1].code)
         {
-            const uint64_t pos = atom_add(s.tail_cnt, 1ull) + 1;
+#ifdef TR_PROFILE
+            count(s, EV_PROF_SPILLS);
+#endif
+            if (tc.next == tc.end)
+            {
+                tc.next = atom_add(s.tail_cnt, TAIL_CHUNK) + 1;
+                tc.end = tc.next + TAIL_CHUNK;
+            }
+            const uint64_t pos = tc.next++;
             TailNode &n = s.tail[(pos - 1) & s.tail_mask];
             n.code = par.r[RUNS - 1].code;
             n.cnt = par.r[RUNS - 1].cnt;
@@ -699,7 +721,7 @@ TR_HD void h_transmit(HostEv &e, Pkt p)
     const RSim &s = *e.s;
     const int64_t tx = link_tx_ns(*e.s, e.out.li, p.size);
     e.n.tc_at = e.now + tx;
-    chain_push(s, s.h_tc[e.h], event_code(tx, e.ord++), e.cur);
+    chain_push(s, s.h_tc[e.h], event_code(tx, e.ord++), e.cur, e.n.tail);
     p.ord = (uint8_t)(e.ord < 255 ? e.ord : 255);
     e.ord++;
     e.nout++;
@@ -715,7 +737,7 @@ TR_HD void h_transmit(HostEv &e, Pkt p)
 TR_HD void h_next_send(HostEv &e, int64_t at)
 {
     e.n.ns_at = at;
-    chain_push(*e.s, e.s->h_ns[e.h], event_code(at - e.now, e.ord++), e.cur);
+    chain_push(*e.s, e.s->h_ns[e.h], event_code(at - e.now, e.ord++), e.cur, e.n.tail);
 }
 
 // QbbNetDevice::DequeueAndTransmit of a host: the ACK queue first, then the next queue pair in
@@ -771,7 +793,7 @@ TR_HD void h_timer_set(HostEv &e, int f, int kind, int64_t lead)
     q.t[kind] = e.now + lead;
     if (q.t[kind] < e.n.due_min)
         e.n.due_min = q.t[kind];
-    chain_push(s, s.qc[f].c[kind], event_code(lead, e.ord++), e.cur);
+    chain_push(s, s.qc[f].c[kind], event_code(lead, e.ord++), e.cur, e.n.tail);
 }
 
 // RdmaHw::ReceiveAck
@@ -1064,7 +1086,7 @@ TR_HD bool host_events(const RSim &s, int h, int64_t t, int64_t *wake, Due *due,
         }
         e.now = tmin;
         if (bk == 0)
-            chain_push(s, e.cur, a.acode, ac);
+            chain_push(s, e.cur, a.acode, ac, e.n.tail);
         else
             e.cur = chain_of(bk);
         e.ord = 0;
@@ -1200,6 +1222,7 @@ struct SwEv
     MmuSwitch mmu;
     SwPort *pe;
     bool safe; // no buffer decision can occur in this slot: lanes run egress ports apart
+    TailChunk *tail; // the tail positions of the running event's port (its lane's alone)
     int64_t now;
     Chain cur;
     int ord;
@@ -1212,7 +1235,7 @@ TR_HD void s_transmit(SwEv &e, int port, Pkt p)
     SwPort &pe = e.pe[port];
     const int64_t tx = link_tx_ns(s, pe.out.li, p.size);
     pe.pt.tc_at = e.now + tx;
-    chain_push(s, s.p_tc[e.si.pbase + port], event_code(tx, e.ord++), e.cur);
+    chain_push(s, s.p_tc[e.si.pbase + port], event_code(tx, e.ord++), e.cur, *e.tail);
     p.ord = (uint8_t)(e.ord < 255 ? e.ord : 255);
     e.ord++;
     pe.nout++;
@@ -1403,9 +1426,11 @@ TR_HD void s_forward(SwEv &e, int inport, Pkt p, int out, int q)
 TR_HD void s_arrival(SwEv &e, const SArr &a)
 {
     const RSim &s = *e.s;
+    if (!e.safe)
+        e.tail = &e.pe[a.in].pt.tail;
     Chain c;
     ld_chain(c, &s.msg[a.frame].c);
-    chain_push(s, e.cur, a.acode, c);
+    chain_push(s, e.cur, a.acode, c, *e.tail);
     e.ord = 0;
     e.n_ev++;
     e.n_arr++;
@@ -1435,6 +1460,8 @@ TR_HD void s_arrival(SwEv &e, const SArr &a)
 // a port's TransmitComplete
 TR_HD void s_tc(SwEv &e, int port)
 {
+    if (!e.safe)
+        e.tail = &e.pe[port].pt.tail;
     e.cur = e.s->p_tc[e.si.pbase + port];
     e.ord = 0;
     e.n_ev++;
@@ -1468,6 +1495,7 @@ TR_HD void safe_egress(SwEv &e, const SwWork &w, int o, int64_t t1, int total)
 {
     const RSim &s = *e.s;
     SwPort &me = e.pe[o];
+    e.tail = &me.pt.tail;
     uint16_t *list = w.ord + me.obase; // (this port's share of the order array)
     int n = 0;
     for (int j = 0; j < total; j++)
@@ -1724,6 +1752,9 @@ TR_HD bool switch_slot(const RSim &s, int x, int64_t t, const SwWork &w, int lan
         const int wl = lanes < 32 ? lanes : 32, nw = lanes < 32 ? 1 : lanes / 32;
         for (int o = lane / wl + nw * (lane % wl); o < deg; o += nw * wl)
             safe_egress(e, w, o, t1, total);
+#if defined(TR_PROFILE) && defined(__CUDA_ARCH__)
+        atomicMax(&s.ev[EV_PROF_LANE_EV_SLOT], e.n_ev);
+#endif
     }
     else if (lane == 0)
         serial_events(e, w, deg, t1, staged);
