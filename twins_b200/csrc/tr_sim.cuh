@@ -230,7 +230,6 @@ enum
     EV_HOST_DATA = 24,       // of the NICs' arrivals: data
     EV_HOST_EVENTS = 25,     // every NIC event (arrivals, transmissions done, sends, timers, starts)
     EV_SWITCH_EVENTS = 26,   // every switch event (arrivals, transmissions done)
-    EV_PROF_SPILLS = 29,     // (TR_PROFILE builds) chain runs spilled into tail nodes
     EV_PROF_CMPS = 30,       // (TR_PROFILE builds) chain comparisons
     EV_PROF_TAIL_LOADS = 31, // (TR_PROFILE builds) tail nodes read by them
     EV_PROF_SAFE = 32,       // (TR_PROFILE builds) switch slots run as safe slots
@@ -366,9 +365,6 @@ TR_HD void chain_push(const RSim &s, Chain &out, uint32_t code, const Chain &par
         c.pad = 0;
         if (par.r[RUNS - 1].code)
         {
-#ifdef TR_PROFILE
-            count(s, EV_PROF_SPILLS);
-#endif
             if (tc.next == tc.end)
             {
                 tc.next = atom_add(s.tail_cnt, TAIL_CHUNK) + 1;
