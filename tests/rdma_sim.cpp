@@ -112,9 +112,10 @@ int rs_run(int n, const char **cfg, const char **topo, const char **flows, long 
     std::vector<SwPort> ports(L.max_deg);
     std::vector<SArr> arr(SW_STAGE > HOST_STAGE ? SW_STAGE : HOST_STAGE);
     std::vector<uint16_t> ord(SW_STAGE);
+    std::vector<Frame> fr(SW_FRAMES);
     std::vector<HPre> hpre(HOST_STAGE);
     int flags[4];
-    const SwWork work{ports.data(), arr.data(), ord.data(), flags};
+    const SwWork work{ports.data(), fr.data(), arr.data(), ord.data(), flags};
     Due due[MAX_DUE];
     while (!ctl.finished)
     {

@@ -28,10 +28,11 @@ __host__ __device__ inline size_t host_scratch_bytes()
     return (sizeof(Due) * MAX_DUE + sizeof(SArr) * HOST_STAGE + sizeof(HPre) * HOST_STAGE + 15) & ~(size_t)15;
 }
 __host__ __device__ inline size_t sw_ports_bytes(int max_deg) { return ((size_t)max_deg * sizeof(SwPort) + 15) & ~(size_t)15; }
+__host__ __device__ inline size_t sw_frames_bytes() { return sizeof(Frame) * SW_FRAMES; }
 __host__ __device__ inline size_t block_scratch_bytes(int max_deg)
 {
     const size_t host = host_scratch_bytes() * RDMA_WARPS;
-    const size_t sw = sw_ports_bytes(max_deg) + sizeof(SArr) * SW_STAGE + sizeof(uint16_t) * SW_STAGE + 4 * sizeof(int);
+    const size_t sw = sw_frames_bytes() + sw_ports_bytes(max_deg) + sizeof(SArr) * SW_STAGE + sizeof(uint16_t) * SW_STAGE + 4 * sizeof(int);
     return ((host > sw ? host : sw) + 15) & ~(size_t)15;
 }
 
@@ -46,10 +47,16 @@ __global__ void __launch_bounds__(RDMA_WARPS * 32) rdma_slot_kernel(RSim s, int 
     SArr *hstage = reinterpret_cast<SArr *>(smem + host_scratch_bytes() * warp + sizeof(Due) * MAX_DUE);
     HPre *hpre = reinterpret_cast<HPre *>(smem + host_scratch_bytes() * warp + sizeof(Due) * MAX_DUE + sizeof(SArr) * HOST_STAGE);
     SwWork work;
-    work.port = reinterpret_cast<SwPort *>(smem);
-    work.arr = reinterpret_cast<SArr *>(smem + sw_ports_bytes(max_deg));
-    work.ord = reinterpret_cast<uint16_t *>(smem + sw_ports_bytes(max_deg) + sizeof(SArr) * SW_STAGE);
-    work.flags = reinterpret_cast<int *>(smem + sw_ports_bytes(max_deg) + (sizeof(SArr) + sizeof(uint16_t)) * SW_STAGE);
+    unsigned char *sw = smem;
+    work.fr = reinterpret_cast<Frame *>(sw);
+    sw += sw_frames_bytes();
+    work.port = reinterpret_cast<SwPort *>(sw);
+    sw += sw_ports_bytes(max_deg);
+    work.arr = reinterpret_cast<SArr *>(sw);
+    sw += sizeof(SArr) * SW_STAGE;
+    work.ord = reinterpret_cast<uint16_t *>(sw);
+    sw += sizeof(uint16_t) * SW_STAGE;
+    work.flags = reinterpret_cast<int *>(sw);
     RCtl *ctl = s.ctl;
     volatile RCtl *vc = ctl;
     const int groups = (s.H + RDMA_WARPS - 1) / RDMA_WARPS, units = groups + s.S;

@@ -638,9 +638,12 @@ __device__ __forceinline__ void ld_chain(Chain &c, const Chain *src)
     for (int i = 0; i < (int)(sizeof(Chain) / 8); i++)
         d[i] = __ldcg(s + i);
 }
+// (own data: written only by this entity's lane, so an L1 line of it is never stale)
+__device__ __forceinline__ void prefetch_l1(const void *p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
 #else
 inline void lanes_sync() {}
 inline void group_sync(int) {}
+inline void prefetch_l1(const void *) {}
 inline void sh_add(uint32_t *p, uint32_t v) { *p += v; }
 inline void sh_add(int *p, int v) { *p += v; }
 inline void sh_sub(uint32_t *p, uint32_t v) { *p -= v; }
@@ -661,8 +664,10 @@ struct SArr
     uint16_t size;
     uint8_t kind;
     uint8_t pre;      // a NIC's HPCC ACK: its hops' U and tau were worked out by the lanes (HPre)
+    uint16_t copy;    // its frame's copy in shared memory (SwWork::fr), or NO_COPY: read from its link
 };
 static_assert(sizeof(SArr) == 32, "SArr");
+constexpr uint16_t NO_COPY = 0xFFFF;
 
 // an HPCC ACK's hop utilisation U and its interval, worked out ahead (hpcc_hops_u)
 struct HPre
@@ -672,7 +677,8 @@ struct HPre
 };
 
 constexpr int HOST_STAGE = 128; // a NIC's arrivals of a slot staged; more are read one by one
-constexpr int SW_STAGE = 384;   // a switch's arrivals of a slot staged; more run unstaged, serially
+constexpr int SW_STAGE = 512;   // a switch's arrivals of a slot staged; more run unstaged, serially
+constexpr int SW_FRAMES = 192;  // of them, those whose frames are copied into shared memory
 constexpr int SAFE_PORTS = 32;  // switches with more ports run every slot serially
 
 TR_HD void stage_arrival(const RSim &s, SArr &a, uint32_t frame, const LinkInfo &lin, Pkt &p)
@@ -686,6 +692,7 @@ TR_HD void stage_arrival(const RSim &s, SArr &a, uint32_t frame, const LinkInfo 
     a.size = p.size;
     a.kind = p.kind;
     a.pre = 0;
+    a.copy = NO_COPY;
     a.out = -1;
     a.q = PG;
     a.in = 0;
@@ -960,6 +967,19 @@ TR_HD bool host_slot(const RSim &s, int h, int64_t t, int64_t *wake, Due *due, S
         {
             Pkt p;
             stage_arrival(s, stage[j], (uint32_t)(abase + j), lin, p);
+            // the queue pair its event will read (the NIC's own records: L1 holds no stale copy)
+            if (p.kind == K_ACK || p.kind == K_NACK)
+            {
+                prefetch_l1(&s.qp[p.flow]);
+                prefetch_l1(reinterpret_cast<const char *>(&s.qp[p.flow]) + 128);
+            }
+            else if (p.kind == K_DATA)
+                prefetch_l1(&s.rx[p.flow]);
+        }
+        if (lane == 0)
+        {
+            prefetch_l1(&s.h_tc[h]);
+            prefetch_l1(&s.h_ns[h]);
         }
         lanes_sync();
         // HPCC with fast react and no sampled feedback: an ACK's hop utilisations depend only on its
@@ -1198,12 +1218,14 @@ struct alignas(16) SwPort
     int ocnt, obase;       // safe slots: arrivals leaving by it; their place in the order array
     SArr pa;               // the unstaged serial path's next arrival
     bool have_pa;
+    Chain tc;              // its TransmitComplete's chain, for the slot (p_tc)
 };
 
 // the warp's switch workspace (shared memory): its ports, staged arrivals, a safe lane's order
 struct SwWork
 {
     SwPort *port;  // [deg]
+    Frame *fr;     // [SW_FRAMES] copies of the first staged arrivals' frames
     SArr *arr;     // [SW_STAGE]
     uint16_t *ord; // [SW_STAGE]: per egress port, its arrivals in event order
     int *flags;    // [4]: ports with an event, arrivals, safe, (unused)
@@ -1231,7 +1253,7 @@ TR_HD void s_transmit(SwEv &e, int port, Pkt p)
     SwPort &pe = e.pe[port];
     const int64_t tx = link_tx_ns(s, pe.out.li, p.size);
     pe.pt.tc_at = e.now + tx;
-    chain_push(s, s.p_tc[e.si.pbase + port], event_code(tx, e.ord++), e.cur, *e.tail);
+    chain_push(s, pe.tc, event_code(tx, e.ord++), e.cur, *e.tail);
     p.ord = (uint8_t)(e.ord < 255 ? e.ord : 255);
     e.ord++;
     pe.nout++;
@@ -1418,14 +1440,30 @@ TR_HD void s_forward(SwEv &e, int inport, Pkt p, int out, int q)
     s_dequeue(e, out);
 }
 
+// a staged arrival's chain and contents: its copy in shared memory, or read from its link
+TR_HD void arr_chain(const RSim &s, const SwWork &w, const SArr &a, Chain &c)
+{
+    if (a.copy != NO_COPY)
+        c = w.fr[a.copy].c;
+    else
+        ld_chain(c, &s.msg[a.frame].c);
+}
+TR_HD void arr_pkt(const RSim &s, const SwWork &w, const SArr &a, Pkt &p)
+{
+    if (a.copy != NO_COPY)
+        p = w.fr[a.copy].p;
+    else
+        ld_pkt(p, &s.msg[a.frame].p);
+}
+
 // an arrival's event: PFC frames pause or resume their port's egress; the others are forwarded
-TR_HD void s_arrival(SwEv &e, const SArr &a)
+TR_HD void s_arrival(SwEv &e, const SwWork &w, const SArr &a)
 {
     const RSim &s = *e.s;
     if (!e.safe)
         e.tail = &e.pe[a.in].pt.tail;
     Chain c;
-    ld_chain(c, &s.msg[a.frame].c);
+    arr_chain(s, w, a, c);
     chain_push(s, e.cur, a.acode, c, *e.tail);
     e.ord = 0;
     e.n_ev++;
@@ -1435,7 +1473,7 @@ TR_HD void s_arrival(SwEv &e, const SArr &a)
         if (e.w->qbb)
         {
             Pkt p;
-            ld_pkt(p, &s.msg[a.frame].p);
+            arr_pkt(s, w, a, p);
             if (a.kind == K_PAUSE)
                 e.pe[a.in].pt.paused |= 1u << p.q;
             else
@@ -1449,7 +1487,7 @@ TR_HD void s_arrival(SwEv &e, const SArr &a)
     if (a.out < 0)
         return;
     Pkt p;
-    ld_pkt(p, &s.msg[a.frame].p);
+    arr_pkt(s, w, a, p);
     s_forward(e, a.in, p, a.out, a.q);
 }
 
@@ -1458,7 +1496,7 @@ TR_HD void s_tc(SwEv &e, int port)
 {
     if (!e.safe)
         e.tail = &e.pe[port].pt.tail;
-    e.cur = e.s->p_tc[e.si.pbase + port];
+    e.cur = e.pe[port].tc;
     e.ord = 0;
     e.n_ev++;
     e.pe[port].pt.tc_at = -1;
@@ -1466,21 +1504,21 @@ TR_HD void s_tc(SwEv &e, int port)
 }
 
 // does staged arrival a run before staged arrival b (same time: by their chains)?
-TR_HD bool arr_before(const RSim &s, const SArr &a, const SArr &b)
+TR_HD bool arr_before(const RSim &s, const SwWork &w, const SArr &a, const SArr &b)
 {
     if (a.ts != b.ts)
         return a.ts < b.ts;
     Chain ca, cb;
-    ld_chain(ca, &s.msg[a.frame].c);
-    ld_chain(cb, &s.msg[b.frame].c);
+    arr_chain(s, w, a, ca);
+    arr_chain(s, w, b, cb);
     return runs_before(s, a.ts, a.acode, ca, b.ts, b.acode, cb);
 }
 
 // does a port's arrival a run before its TransmitComplete at the same time?
-TR_HD bool arr_before_tc(const RSim &s, const SArr &a, const Chain &tc)
+TR_HD bool arr_before_tc(const RSim &s, const SwWork &w, const SArr &a, const Chain &tc)
 {
     Chain ca;
-    ld_chain(ca, &s.msg[a.frame].c);
+    arr_chain(s, w, a, ca);
     return runs_before(s, a.ts, a.acode, ca, a.ts, 0, tc);
 }
 
@@ -1502,7 +1540,7 @@ TR_HD void safe_egress(SwEv &e, const SwWork &w, int o, int64_t t1, int total)
             continue;
         // insertion in event order (an undecided tie keeps the earlier port's arrival first)
         int k = n++;
-        while (k > 0 && arr_before(s, a, w.arr[list[k - 1]]))
+        while (k > 0 && arr_before(s, w, a, w.arr[list[k - 1]]))
         {
             list[k] = list[k - 1];
             k--;
@@ -1522,7 +1560,7 @@ TR_HD void safe_egress(SwEv &e, const SwWork &w, int o, int64_t t1, int total)
         else if (ta != tc)
             arr = ta < tc;
         else
-            arr = arr_before_tc(s, w.arr[list[i]], s.p_tc[e.si.pbase + o]);
+            arr = arr_before_tc(s, w, w.arr[list[i]], me.tc);
         if (!arr)
         {
             e.now = tc;
@@ -1531,7 +1569,7 @@ TR_HD void safe_egress(SwEv &e, const SwWork &w, int o, int64_t t1, int total)
         }
         const SArr &a = w.arr[list[i++]];
         e.now = a.ts;
-        s_arrival(e, a);
+        s_arrival(e, w, a);
     }
 }
 
@@ -1589,17 +1627,17 @@ TR_HD void serial_events(SwEv &e, const SwWork &w, int deg, int64_t t1, bool sta
                 // a tie: the chains
                 bool b4;
                 if (k == 0 && bk == 0)
-                    b4 = arr_before(s, *a, *ba);
+                    b4 = arr_before(s, w, *a, *ba);
                 else if (k == 0)
-                    b4 = arr_before_tc(s, *a, s.p_tc[e.si.pbase + best]);
+                    b4 = arr_before_tc(s, w, *a, e.pe[best].tc);
                 else if (bk == 0)
                 {
                     Chain cb;
-                    ld_chain(cb, &s.msg[ba->frame].c);
-                    b4 = runs_before(s, tt, 0, s.p_tc[e.si.pbase + p], bt, ba->acode, cb);
+                    arr_chain(s, w, *ba, cb);
+                    b4 = runs_before(s, tt, 0, e.pe[p].tc, bt, ba->acode, cb);
                 }
                 else
-                    b4 = runs_before(s, tt, 0, s.p_tc[e.si.pbase + p], bt, 0, s.p_tc[e.si.pbase + best]);
+                    b4 = runs_before(s, tt, 0, e.pe[p].tc, bt, 0, e.pe[best].tc);
                 if (b4)
                     best = p, bk = k, ba = a;
             }
@@ -1616,7 +1654,7 @@ TR_HD void serial_events(SwEv &e, const SwWork &w, int deg, int64_t t1, bool sta
         SwPort &q = e.pe[best];
         q.ai++;
         q.have_pa = false;
-        s_arrival(e, a);
+        s_arrival(e, w, a);
     }
 }
 
@@ -1648,7 +1686,14 @@ TR_HD bool switch_slot(const RSim &s, int x, int64_t t, const SwWork &w, int lan
         q.ocnt = 0;
         q.ing0 = q.pt.mmu.ing;
         if (q.an > 0 || (q.pt.tc_at >= 0 && q.pt.tc_at < t1))
+        {
             sh_add(&w.flags[2], 1);
+            q.tc = s.p_tc[si.pbase + p];
+            // the queue's next frames, for the slot's dequeues
+            const Pkt *q3 = s.q3 + (size_t)(si.pbase + p) * s.q3_cap;
+            for (int i = 0; i < q.pt.q3_n && i < 8; i += 2)
+                prefetch_l1(q3 + (q.pt.q3_head + i) % s.q3_cap);
+        }
     }
     group_sync(lanes);
     if (w.flags[2] == 0)
@@ -1678,6 +1723,24 @@ TR_HD bool switch_slot(const RSim &s, int x, int64_t t, const SwWork &w, int lan
     const bool staged = total <= SW_STAGE;
     if (staged)
     {
+        // the first SW_FRAMES frames copied whole into shared memory, 16 bytes a lane at a time (a
+        // port's frames of the slot lie together in its link's bucket)
+        const int nfr = total < SW_FRAMES ? total : SW_FRAMES;
+        for (int k = lane; k < nfr * (int)(sizeof(Frame) / 16); k += lanes)
+        {
+            const int j = k / (int)(sizeof(Frame) / 16), word = k % (int)(sizeof(Frame) / 16);
+            int p = 0;
+            while (j >= w.port[p].first + w.port[p].an)
+                p++;
+            const Frame *src = &s.msg[w.port[p].abase + (j - w.port[p].first)];
+#ifdef __CUDA_ARCH__
+            reinterpret_cast<uint4 *>(&w.fr[j])[word] = __ldcg(reinterpret_cast<const uint4 *>(src) + word);
+#else
+            if (word == 0)
+                w.fr[j] = *src;
+#endif
+        }
+        group_sync(lanes);
         for (int j = lane; j < total; j += lanes)
         {
             int p = 0;
@@ -1686,7 +1749,21 @@ TR_HD bool switch_slot(const RSim &s, int x, int64_t t, const SwWork &w, int lan
             SArr &a = w.arr[j];
             const uint32_t frame = (uint32_t)(w.port[p].abase + (j - w.port[p].first));
             Pkt pk;
-            stage_arrival(s, a, frame, w.port[p].lin, pk);
+            if (j < nfr)
+            {
+                const Frame &f = w.fr[j];
+                pk = f.p;
+                a.ts = f.ts;
+                a.acode = event_code(link_tx_ns(s, w.port[p].lin, pk.size) + w.port[p].lin.delay, pk.ord);
+                a.frame = frame;
+                a.flow = pk.flow;
+                a.size = pk.size;
+                a.kind = pk.kind;
+                a.pre = 0;
+                a.copy = (uint16_t)j;
+            }
+            else
+                stage_arrival(s, a, frame, w.port[p].lin, pk);
             a.in = (uint8_t)p;
             int qi = PG;
             a.out = (int16_t)(pk.kind == K_PAUSE || pk.kind == K_RESUME ? -1 : s_route(s, si, wp, pk, &qi));
@@ -1762,6 +1839,8 @@ TR_HD bool switch_slot(const RSim &s, int x, int64_t t, const SwWork &w, int lan
         q.out.flush(s);
         q.pt.ob_last = q.out.last;
         s.port[si.pbase + p] = q.pt;
+        if (q.nout)
+            s.p_tc[si.pbase + p] = q.tc;
     }
     group_sync(lanes);
     for (int p = 0; p < deg; p++)
