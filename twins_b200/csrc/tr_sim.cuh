@@ -230,6 +230,9 @@ enum
     EV_HOST_DATA = 24,       // of the NICs' arrivals: data
     EV_HOST_EVENTS = 25,     // every NIC event (arrivals, transmissions done, sends, timers, starts)
     EV_SWITCH_EVENTS = 26,   // every switch event (arrivals, transmissions done)
+    EV_PROF_SW_PHASE = 14,   // (TR_PROFILE builds) 14..18: switch slots' phases on their lane 0, summed (cycles):
+                             // ports loaded, arrivals staged, safe or not decided, events, ports stored
+    EV_PROF_SW_BUSY = 19,    // (TR_PROFILE builds) switch slots with events
     EV_PROF_CMPS = 30,       // (TR_PROFILE builds) chain comparisons
     EV_PROF_TAIL_LOADS = 31, // (TR_PROFILE builds) tail nodes read by them
     EV_PROF_SAFE = 32,       // (TR_PROFILE builds) switch slots run as safe slots
@@ -1664,8 +1667,28 @@ TR_HD void serial_events(SwEv &e, const SwWork &w, int deg, int64_t t1, bool sta
 // ports of its own (a safe slot), else lane 0 runs all events in one order; the lanes store the
 // ports. Returns (on every lane) whether the switch sent or holds frames.
 // (reference: switch_step, src/rdma/rstep.cuh:2583-3446)
+#if defined(TR_PROFILE) && defined(__CUDA_ARCH__)
+#define SW_PHASE(i)                                                                                                             \
+    do                                                                                                                          \
+    {                                                                                                                           \
+        if (lane == 0)                                                                                                          \
+        {                                                                                                                       \
+            const long long c = clock64();                                                                                      \
+            atomicAdd(&s.ev[EV_PROF_SW_PHASE + (i)], (unsigned long long)(c - ph0));                                           \
+            ph0 = c;                                                                                                            \
+        }                                                                                                                       \
+    } while (0)
+#else
+#define SW_PHASE(i)                                                                                                             \
+    do                                                                                                                          \
+    {                                                                                                                           \
+    } while (0)
+#endif
 TR_HD bool switch_slot(const RSim &s, int x, int64_t t, const SwWork &w, int lane, int lanes)
 {
+#if defined(TR_PROFILE) && defined(__CUDA_ARCH__)
+    long long ph0 = clock64();
+#endif
     const SwInfo si = s.sinfo[x];
     const RWorld &wp = s.world[si.world];
     const int deg = si.deg;
@@ -1708,6 +1731,11 @@ TR_HD bool switch_slot(const RSim &s, int x, int64_t t, const SwWork &w, int lan
         group_sync(lanes);
         return act;
     }
+    SW_PHASE(0);
+#if defined(TR_PROFILE) && defined(__CUDA_ARCH__)
+    if (lane == 0)
+        atomicAdd(&s.ev[EV_PROF_SW_BUSY], 1ull);
+#endif
     if (lane == 0)
     {
         int total = 0;
@@ -1776,6 +1804,7 @@ TR_HD bool switch_slot(const RSim &s, int x, int64_t t, const SwWork &w, int lan
         }
         group_sync(lanes);
     }
+    SW_PHASE(1);
     SwEv e;
     e.s = &s;
     e.w = &wp;
@@ -1815,6 +1844,7 @@ TR_HD bool switch_slot(const RSim &s, int x, int64_t t, const SwWork &w, int lan
     group_sync(lanes);
     const bool safe = w.flags[2] != 0;
     e.safe = safe;
+    SW_PHASE(2);
 #ifdef TR_PROFILE
     if (lane == 0)
         count(s, safe ? EV_PROF_SAFE : EV_PROF_SERIAL);
@@ -1832,6 +1862,7 @@ TR_HD bool switch_slot(const RSim &s, int x, int64_t t, const SwWork &w, int lan
     else if (lane == 0)
         serial_events(e, w, deg, t1, staged);
     group_sync(lanes);
+    SW_PHASE(3);
     bool act = false;
     for (int p = lane; p < deg; p += lanes)
     {
@@ -1870,6 +1901,7 @@ TR_HD bool switch_slot(const RSim &s, int x, int64_t t, const SwWork &w, int lan
         s.sw[x].mmu = e.mmu;
     }
     group_sync(lanes);
+    SW_PHASE(4);
     return act;
 }
 
