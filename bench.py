@@ -514,6 +514,62 @@ def c3_leg(device: int, warmup: int = 3, ref: bool = True, q3cap: int = 1 << 16)
     return out
 
 
+def rdma_sweep_leg(device: int, ref: bool = True):
+    """The reference's RDMA k=8 sweep (validation/hpcc/sweep_k8.txt: 32 worlds of FatTree k=8, two
+    workloads x DCQCN/HPCC x two buffer sizes x four ECN thresholds) as one batch: worlds/s over
+    device time, against the reference's own twins-rdma running the same job file as its --batch,
+    every FCT compared. Published: 19.8 worlds/s on an RTX 5090 (its docs/nvidia.md:147)."""
+    import torch
+    from twins_b200 import api, workloads
+    worlds = workloads.rdma_sweep_k8(ROOT / "tests" / "golden")
+    with api.Simulator(device=device) as sim:
+        ids = [sim.add_rdma_world(w.config, w.topology, w.flows) for w in worlds]
+        sim.prepare()
+        sim.run(300)  # (warm-up: a short run)
+        torch.cuda.synchronize()
+        status = sim.run()
+        st = sim.stats()
+        res = [sim.rdma_results(i)[1] for i in ids]
+    sec = st["kernel_ms"] / 1000.0
+    out = {"config": "32 worlds of the reference's k=8 RDMA sweep (FatTree k=8, k8_a2a30 / k8_a2a50s flows, DCQCN / HPCC, 2 / 32 MB "
+                     "buffers, Kmin 20 / 50 / 100 / 400 KB) in one batch",
+           "worlds_per_s": len(worlds) / sec, "seconds": sec, "packet_events": st["packet_events"], "status": status,
+           "flows_done": int(sum((r >= 0).sum() for r in res)), "flows": int(sum(len(r) for r in res)),
+           "published": {"rtx5090_worlds_per_s": 19.8, "rx9060xt_worlds_per_s": 10.0, "source": "reference docs/nvidia.md:147, README.md:286-289"}}
+    exe = ROOT / "oracle" / "_ref" / "twins-rdma"
+    if ref and exe.exists():
+        d = Path(tempfile.mkdtemp(prefix="twins_rsweep_"))
+        jobs = []
+        for w in worlds:
+            cfg, topo, fl = workloads.write_rdma(w, d)
+            jobs.append(f"{w.name} {topo.name} {fl.name}")
+        (d / "jobs.txt").write_text("\n".join(jobs) + "\n")
+        (d / "out").mkdir()
+        base = d / f"{worlds[0].name}.cfg"
+        # (each world's own config: the job lines carry its keys as overrides of the first one's)
+        lines = []
+        for w in worlds:
+            kv = dict(line.split(" ", 1) for line in w.config.strip().splitlines())
+            over = " ".join(f"{k}={v.replace(' ', ',')}" for k, v in kv.items() if k in ("CC_MODE", "BUFFER_SIZE", "KMIN_MAP", "KMAX_MAP"))
+            lines.append(f"{w.name} {w.name}.topo {w.name}.csv {over}")
+        (d / "jobs.txt").write_text("\n".join(lines) + "\n")
+        r = subprocess.run([str(exe), base.name, "--batch=jobs.txt", "--outdir=out"], cwd=d, capture_output=True, text=True, timeout=1200)
+        line = next((x for x in r.stdout.splitlines() if x.startswith("flows done")), "")
+        ref_wall = float(line.split(" in ")[1].split(" s wall")[0]) if line else None
+        equal = 0
+        for w, fct in zip(worlds, res):
+            want = np.full(len(fct), -1, dtype=np.int64)
+            f = d / "out" / f"{w.name}.fct"
+            for x in f.read_text().splitlines() if f.exists() else []:
+                a, _, v = (int(y) for y in x.split())
+                want[a] = v
+            equal += int((want == fct).all())
+        out["reference_gpu"] = {"rc": r.returncode, "seconds": ref_wall, "worlds_per_s": len(worlds) / ref_wall if ref_wall else None,
+                                "worlds_equal": f"{equal}/{len(worlds)}",
+                                "binary": "oracle/_ref/twins-rdma --batch (reference src/rdma/rmain.cu, nvcc sm_100a)"}
+    return out
+
+
 def reference_arm(args, worlds, config):
     """The reference arm: the reference's CPU path for this model on the host cores, which is the
     oracle port (the reference has no CPU build of its TCP model): every world of the workload
@@ -572,7 +628,7 @@ def main():
         if rank == 0:
             import torch
             torch.cuda.set_device(local_rank)
-            print(json.dumps({"workload": "c3", **c3_leg(local_rank)}))
+            print(json.dumps({"workload": "c3", **c3_leg(local_rank), "rdma_sweep_k8": rdma_sweep_leg(local_rank)}))
         return
     if args.workload == "c5" and args.impl == "ours":
         if rank == 0:  # (one server on one GPU; other ranks have nothing to add)
@@ -696,6 +752,7 @@ def main():
         extras["c5"] = serve_leg(local_rank, args.requests, args.rate, args.serve_worlds)
         extras["sweep_k8"] = sweep_leg(local_rank)
         extras["c3"] = c3_leg(local_rank)
+        extras["rdma_sweep_k8"] = rdma_sweep_leg(local_rank)
     elif args.workload == "c4":
         extras["plain"] = plain_sample(worlds, args.plain_sample, local_rank, len(worlds) / (ms_max / 1000.0),
                                        batched=dict(enumerate(ours[w.name] for w in worlds)))

@@ -7,7 +7,8 @@ validation/check_sweeps.sh runs each sweep as batches of worlds (bench/sweep.py)
 columns 1-6 with those files. This script keeps what that comparison needs: the flow files
 (copied unchanged into tests/golden/flows/) and, per configuration, columns 5-6 (established_ns,
 completed_ns) in one compressed array file per sweep, after checking that columns 1-4 of every
-output equal its flow file.
+output equal its flow file. It also copies the topology of the reference's RDMA k=8 sweep
+(data/topo/fattree8.txt, for validation/hpcc/sweep_k8.txt).
 
     TWINS_REFERENCE=/path/to/reference python tests/golden/make_sweep_fixtures.py
 
@@ -58,6 +59,11 @@ def main(ref: Path) -> None:
         index[sweep] = configs
         print(f"{sweep}: {len(configs)} configurations")
     (out / "index.json").write_text(json.dumps(index, indent=1) + "\n")
+    # the RDMA k=8 sweep's topology (the reference's validation/hpcc/sweep_k8.txt runs its worlds on
+    # data/topo/fattree8.txt with the flows data/flows/k8_a2a30.csv and k8_a2a50s.csv)
+    shutil.copyfile(ref / "data" / "topo" / "fattree8.txt", HERE / "topo" / "fattree8.txt")
+    for f in ("k8_a2a30.csv", "k8_a2a50s.csv"):
+        shutil.copyfile(ref / "data" / "flows" / f, HERE / "flows" / f)
 
 
 if __name__ == "__main__":

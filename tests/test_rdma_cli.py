@@ -101,3 +101,34 @@ def test_cli_stop_time_exit_2(native_lib, tmp_path):
 
 def case_flows(name):
     return next(c["flows"] for c in CASES if c["name"] == name)
+
+
+@pytest.mark.skipif(not REF_GPU.exists(), reason="the reference's GPU build (make -C oracle ref-rdma) is not here")
+def test_rdma_sweep_batch_equals_reference_batch(native_lib, tmp_path):
+    """The reference's RDMA k=8 sweep (32 worlds: two workloads x DCQCN/HPCC x two buffer sizes x four
+    ECN thresholds on its fattree8 topology) in one batch equals, world for world, the reference's
+    own twins-rdma running the same worlds as its --batch."""
+    from twins_b200 import api, workloads
+    worlds = workloads.rdma_sweep_k8(GOLDEN)
+    with api.Simulator() as sim:
+        ids = [sim.add_rdma_world(w.config, w.topology, w.flows) for w in worlds]
+        assert sim.run() == api.TB_OK
+        got = [sim.rdma_results(i)[1] for i in ids]
+    lines = []
+    for w in worlds:
+        workloads.write_rdma(w, tmp_path)
+        kv = dict(line.split(" ", 1) for line in w.config.strip().splitlines())
+        over = " ".join(f"{k}={v.replace(' ', ',')}" for k, v in kv.items() if k in ("CC_MODE", "BUFFER_SIZE", "KMIN_MAP", "KMAX_MAP"))
+        lines.append(f"{w.name} {w.name}.topo {w.name}.csv {over}")
+    (tmp_path / "jobs.txt").write_text("\n".join(lines) + "\n")
+    (tmp_path / "out").mkdir()
+    r = subprocess.run([str(REF_GPU), f"{worlds[0].name}.cfg", "--batch=jobs.txt", "--outdir=out"], cwd=tmp_path, capture_output=True,
+                       text=True, timeout=1200)
+    assert r.returncode == 0, r.stderr[-500:]
+    for w, fct in zip(worlds, got):
+        want = {i: f for i, _, f in fct_rows(tmp_path / "out" / f"{w.name}.fct")}
+        assert len(want) == len(fct) and all(want[i] == fct[i] for i in range(len(fct))), w.name
+
+
+def fct_rows(path):
+    return [tuple(int(x) for x in l.split()) for l in path.read_text().splitlines() if l.strip()]

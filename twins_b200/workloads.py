@@ -334,3 +334,22 @@ def write_rdma(w: RdmaWorld, d) -> tuple:
         for i in range(len(w.flows)):
             f.write(f"{w.flows.src[i]},{w.flows.dst[i]},{w.flows.size[i]},{w.flows.start_ns[i]}\n")
     return cfg, topo, fl
+
+
+def rdma_sweep_k8(golden_dir) -> list[RdmaWorld]:
+    """The reference's RDMA k=8 parameter sweep (its validation/hpcc/sweep_k8.txt): FatTree k=8
+    (its data/topo/fattree8.txt), flows k8_a2a30 and k8_a2a50s, DCQCN and HPCC, buffers of 2 and
+    32 MB, and ECN thresholds Kmin/Kmax of 20/80, 50/200, 100/400 and 400/1600 KB at 100 Gb/s:
+    32 worlds."""
+    from pathlib import Path
+    g = Path(golden_dir)
+    topo = (g / "topo" / "fattree8.txt").read_text()
+    out = []
+    for wl in ("k8_a2a30", "k8_a2a50s"):
+        flows = Flows.load(g / "flows" / f"{wl}.csv", 128)
+        for cc in ("dcqcn", "hpcc"):
+            for buf in (2, 32):
+                for kmin in (20, 50, 100, 400):
+                    cfg = rdma_config(cc, BUFFER_SIZE=buf, KMIN_MAP=f"1 100000000000 {kmin}", KMAX_MAP=f"1 100000000000 {4 * kmin}")
+                    out.append(RdmaWorld(f"sw_{wl}_cc{RDMA_CC[cc]}_b{buf}_k{kmin}", cfg, topo, flows))
+    return out
