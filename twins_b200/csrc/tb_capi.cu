@@ -671,7 +671,7 @@ void build_image(const HostWorld &w, const Place &pl, WorldImage &img)
         S_.m_cnt = (int)cr.size();
         S_.fin_on = R.fin_on = (uint8_t)(w.p.fin != 0);
         uint64_t segs = (w.conn_bytes[cc] + MSS - 1) / MSS + cr.size() + 1;
-        S_.it_cap = (uint32_t)std::min<uint64_t>(segs, 65536);
+        S_.it_cap = sent_list_cap(segs);
         S_.it_off = pl.it0 + it_n;
         it_n += S_.it_cap;
         R.oo_cap = (uint32_t)std::min<uint64_t>(segs / 2 + 2, 4096);
@@ -863,7 +863,7 @@ int prepare(tb_ctx *c)
         pl.port0 = w.port0;
         pl.conn0 = w.conn0;
         pl.msg0 = w.msg0;
-        pl.it0 = it_total;
+        pl.it0 = it_total; // (a multiple of 8: every capacity is)
         pl.oo0 = oo_total;
         pl.port_links = H;
         WorldImage img;
@@ -903,7 +903,7 @@ int prepare(tb_ctx *c)
     if ((r = c->alloc(&s.host_ring, (size_t)H * ring, false)) || (r = c->alloc(&s.port_ring, (size_t)P * ring, false)) ||
         (r = c->alloc(&s.act_snd, (size_t)H * s.act_cap, false)) || (r = c->alloc(&s.act_rcv, (size_t)H * s.act_cap, false)) ||
         (r = c->alloc(&s.it_start, it_total, false)) || (r = c->alloc(&s.it_fl, it_total, false)) ||
-        (r = c->alloc(&s.h_seq, it_total, false)) || (r = c->alloc(&s.h_cnt, it_total, false)) || (r = c->alloc(&s.h_t, it_total, false)) ||
+        (r = c->alloc(&s.h_seq, it_total, false)) || (r = c->alloc(&s.h_end, it_total, false)) || (r = c->alloc(&s.h_t, it_total, false)) ||
         (r = c->alloc(&s.oo_s, oo_total, false)) || (r = c->alloc(&s.oo_e, oo_total, false)) ||
         (r = c->alloc(&s.msg, (size_t)NB * s.L * MAX_TX, false)))
         return r;

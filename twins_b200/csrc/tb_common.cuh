@@ -38,7 +38,6 @@ constexpr int DATA_RETRIES = 6;
 constexpr double DCTCP_G = 0.0625;
 
 constexpr uint8_t F_ACK = 1, F_SYN = 2, F_ECE = 4, F_ECT = 8, F_CE = 16, F_DATA = 32, F_CWR = 64, F_FIN = 128;
-constexpr uint8_t IT_SACKED = 1, IT_LOST = 2, IT_RETX = 4;
 constexpr uint8_t FIN_CLOSE = 1, FIN_SENT = 2, FIN_ACKED = 4, FIN_TW = 8;
 enum : uint8_t { S_IDLE = 0, S_SYN_SENT, S_EST, S_DONE };
 enum : uint8_t { C_OPEN = 0, C_DISORDER, C_CWR, C_RECOVERY, C_LOSS };

@@ -92,242 +92,172 @@ TB_D int msg_count(const Sim &s, int64_t slot, int link)
 }
 TB_D const Frame *msg_frames(const Sim &s, int64_t slot, int link) { return s.msg + msg_index(s, slot, link) * MAX_TX; }
 
-// The egress port's working copy for one slot (reference: src/step.cuh:163-317, Fifo).
-struct Egress
+// The sending end of a point-to-point link for one slot: ns-3's RED queue disc over a one-packet
+// device queue over the wire (reference: src/step.cuh:163-317). `ring` holds the frames that have
+// not started, each stamped with its enqueue time; the wire is busy until `busy_until` with the
+// frame that began at `began`, whose chain is *tx_chain. A frame begins at max(its enqueue time,
+// busy_until); its transmission's copy, stamped with its arrival at the far end, goes to this
+// slot's link message `msg` (at most MAX_TX; more is counted as an overflow).
+// SHADOW: the frame enqueued last is also kept at *shadow (shared memory) with its ring index, so
+// that a frame queued and started in the same slot is not read back from global memory.
+template <bool SHADOW>
+struct Transmitter
 {
     Frame *ring;
     int cap, head, size;
-    int64_t link_free, last_start;
-    Chain *last; // persistent: the chain of the transmission in progress
+    int64_t busy_until, began;
+    Chain *tx_chain;
     int red_k, qcap;
-    int64_t woke, idle_start, slot_end;
-    Frame *out; // this slot's link message
-    int sent;
-    unsigned drops, marks, ovf, emitted;
+    int64_t horizon;    // the slot's end: nothing begins at or after it
+    int64_t kicked;     // the instant of a ScheduleNow'd event being handled (-1: none)
+    int64_t idle_began; // the last start this slot on an idle wire (-1: none)
+    Frame *msg;
+    int n_out;
+    unsigned drops, marks, ovf, offered;
+    Frame *shadow;
+    int shadow_at;
 #ifdef TB_QTRACE
     const Sim *qs; // the trace's sink; the queue's ns-3 node and device
     int qnode, qdev;
 #endif
 
-    // start every frame whose transmission begins by `until` and within this slot
+    TB_D void open(Frame *ring_, int cap_, int head_, int size_, int64_t busy_until_, int64_t began_, Chain *tx_chain_, int red_k_,
+                   int qcap_, int64_t horizon_, Frame *msg_)
+    {
+        ring = ring_;
+        cap = cap_;
+        head = head_;
+        size = size_;
+        busy_until = busy_until_;
+        began = began_;
+        tx_chain = tx_chain_;
+        red_k = red_k_;
+        qcap = qcap_;
+        horizon = horizon_;
+        kicked = idle_began = -1;
+        msg = msg_;
+        n_out = 0;
+        drops = marks = ovf = offered = 0;
+        shadow = nullptr;
+        shadow_at = -1;
+    }
+    TB_D const Frame &at_head() const { return SHADOW && head == shadow_at ? *shadow : ring[head]; }
+
+    // every waiting frame that begins by `until` (and before the horizon) goes on the wire; a frame
+    // that found the wire busy begins at the previous one's TransmitComplete, whose chain is its
+    // parent's; one that found it idle begins at its own enqueue, its chain unchanged
     TB_D void advance(int64_t until)
     {
-        while (size > 0)
+        for (; size; size--)
         {
-            Frame *f = &ring[head];
-            int64_t start = f->ts > link_free ? f->ts : link_free;
-            if (start > until || start >= slot_end)
+            const Frame &f = at_head();
+            const int64_t t0 = f.ts > busy_until ? f.ts : busy_until;
+            if (t0 > until || t0 >= horizon)
                 return;
-            if (sent >= MAX_TX)
+            if (n_out == MAX_TX)
             {
                 ovf++;
                 return;
             }
-            int64_t end = start + (int64_t)f->len * PS_PER_BYTE;
             Frame o;
-            frame_copy(&o, f);
-            // its parent event: the previous frame's TransmitComplete, unless the link was idle
-            if (f->ts <= link_free && link_free > last_start)
-                chain_child(o.ch, *last, code_tc((int)((link_free - last_start) / PS_PER_BYTE)));
+            frame_copy(&o, &f);
+            const bool behind = busy_until >= f.ts && busy_until > began;
+            if (behind)
+                chain_child(o.ch, *tx_chain, code_tc((int)((busy_until - began) / PS_PER_BYTE)));
             else
-                idle_start = start;
-            *last = o.ch;
-            last_start = start;
-            o.ts = end + PROP_PS;
-            frame_store_link(&out[sent], o);
-            sent++;
-            link_free = end;
+                idle_began = t0;
+            *tx_chain = o.ch;
+            began = t0;
+            busy_until = t0 + (int64_t)f.len * PS_PER_BYTE;
+            o.ts = busy_until + PROP_PS;
+            frame_store_link(&msg[n_out++], o);
             head = head + 1 == cap ? 0 : head + 1;
-            size--;
         }
     }
 
-    // RED with MinTh = MaxTh = K and QW = 1 on the queue disc's length, which excludes the
-    // device queue's packet once ns-3's Wake (ScheduleNow) has refilled it; then the limit
+    // the frames RED counts at `now`: the waiting ones, less the one the device queue holds while
+    // the wire is busy, once the Wake that refills it has run. The Wake is ScheduleNow'd when a
+    // transmission begins, so it has run for one that began earlier; for one that began at this
+    // instant only a ScheduleNow'd event sees it, after a start on an idle wire (a start at a
+    // TransmitComplete comes after the arrivals that scheduled such events).
+    TB_D int disc_backlog(int64_t now) const
+    {
+        if (!size || busy_until <= now)
+            return size;
+        const bool woken = began < now || (kicked == now && idle_began == now);
+        return size - (woken ? 1 : 0);
+    }
+
+#ifdef TB_QTRACE
+    TB_D void trace(const Frame &g, int backlog, int64_t now) const
+    {
+        if (!qs->qtrace || now >= qs->qtrace_until || now < qs->qtrace_from)
+            return;
+#if defined(__CUDA_ARCH__)
+        const unsigned long long i = atomicAdd(qs->qtrace_cnt, 1ull);
+#else
+        const unsigned long long i = (*qs->qtrace_cnt)++;
+#endif
+        if (i >= qs->qtrace_n)
+            return;
+        QRec &r = qs->qtrace[i];
+        const SndRec &S = qs->snd[g.flow];
+        r.ts = now;
+        r.node = qnode;
+        r.dev = qdev;
+        r.src = g.to_sender ? S.dst_local : S.src_local;
+        r.dst = g.to_sender ? S.src_local : S.dst_local;
+        r.sa = g.sa;
+        r.len = g.len;
+        r.qlen = (uint16_t)(backlog + 1);
+        r.flags = g.flags;
+    }
+#endif
+
+    // a frame offered at `now` (its ts becomes now): the wire first takes what begins by now; RED
+    // with MinTh = MaxTh = K and weight 1 (no averaging) marks an ECT frame or drops another when
+    // the backlog is at least K (and above 1); then the disc's limit drops. False: dropped.
     TB_D bool enqueue(Frame &g, int64_t now)
     {
-        emitted++;
+        offered++;
         advance(now);
-        bool refilled = last_start < now || (woke == now && idle_start == now);
-        int nq = (size > 0 && link_free > now && refilled) ? size - 1 : size;
+        const int backlog = disc_backlog(now);
         g.ts = now;
-        if (nq >= red_k && nq > 1)
+        if (backlog >= red_k && backlog > 1)
         {
-            if (g.flags & F_ECT)
-            {
-                g.flags |= F_CE;
-                marks++;
-            }
-            else
+            if (!(g.flags & F_ECT))
             {
                 drops++;
                 return false;
             }
+            g.flags |= F_CE;
+            marks++;
         }
-        if (nq >= qcap)
+        if (backlog >= qcap)
         {
             drops++;
             return false;
         }
 #ifdef TB_QTRACE
-        if (qs->qtrace && now < qs->qtrace_until && now >= qs->qtrace_from)
-        {
-#if defined(__CUDA_ARCH__)
-            const unsigned long long i = atomicAdd(qs->qtrace_cnt, 1ull);
-#else
-            const unsigned long long i = (*qs->qtrace_cnt)++;
+        trace(g, backlog, now);
 #endif
-            if (i < qs->qtrace_n)
-            {
-                QRec &r = qs->qtrace[i];
-                const SndRec &S = qs->snd[g.flow];
-                r.ts = now;
-                r.node = qnode;
-                r.dev = qdev;
-                r.src = g.to_sender ? S.dst_local : S.src_local;
-                r.dst = g.to_sender ? S.src_local : S.dst_local;
-                r.sa = g.sa;
-                r.len = g.len;
-                r.qlen = (uint16_t)(nq + 1);
-                r.flags = g.flags;
-            }
-        }
-#endif
-        if (size >= cap)
+        if (size == cap)
         {
             ovf++;
             return false;
         }
-        int at = head + size;
-        if (at >= cap)
-            at -= cap;
+        const int at = head + size < cap ? head + size : head + size - cap;
         frame_copy(&ring[at], &g);
+        if (SHADOW)
+        {
+            *shadow = g;
+            shadow_at = at;
+        }
         size++;
         return true;
     }
 };
-
-// A switch port's working copy for one slot, as Egress, with the chain of the transmission in
-// progress and the frame last enqueued kept in the warp's shared scratch for the slot (the caller
-// loads the chain and stores it back), so that a started frame does not read back from L2 what
-// the step before had just written. (A separate kernel instantiation uses it: the plain Egress
-// keeps the other one's code as it is.)
-struct PortEgress
-{
-    Frame *ring;
-    int cap, head, size;
-    int64_t link_free, last_start;
-    Chain *last; // the chain of the transmission in progress: the slot's copy in shared memory
-    Frame *tailp; // the frame last enqueued (ring index tail_at; -1: none), in shared memory
-    int tail_at;
-    int red_k, qcap;
-    int64_t woke, idle_start, slot_end;
-    Frame *out; // this slot's link message
-    int sent;
-    unsigned drops, marks, ovf, emitted;
-#ifdef TB_QTRACE
-    const Sim *qs; // the trace's sink; the queue's ns-3 node and device
-    int qnode, qdev;
-#endif
-
-    // start every frame whose transmission begins by `until` and within this slot
-    TB_D void advance(int64_t until)
-    {
-        while (size > 0)
-        {
-            const Frame *f = head == tail_at ? tailp : &ring[head];
-            int64_t start = f->ts > link_free ? f->ts : link_free;
-            if (start > until || start >= slot_end)
-                return;
-            if (sent >= MAX_TX)
-            {
-                ovf++;
-                return;
-            }
-            int64_t end = start + (int64_t)f->len * PS_PER_BYTE;
-            Frame o;
-            frame_copy(&o, f);
-            // its parent event: the previous frame's TransmitComplete, unless the link was idle
-            if (f->ts <= link_free && link_free > last_start)
-                chain_child(o.ch, *last, code_tc((int)((link_free - last_start) / PS_PER_BYTE)));
-            else
-                idle_start = start;
-            *last = o.ch;
-            last_start = start;
-            o.ts = end + PROP_PS;
-            frame_store_link(&out[sent], o);
-            sent++;
-            link_free = end;
-            head = head + 1 == cap ? 0 : head + 1;
-            size--;
-        }
-    }
-
-    // RED with MinTh = MaxTh = K and QW = 1 on the queue disc's length, which excludes the
-    // device queue's packet once ns-3's Wake (ScheduleNow) has refilled it; then the limit
-    TB_D bool enqueue(Frame &g, int64_t now)
-    {
-        emitted++;
-        advance(now);
-        bool refilled = last_start < now || (woke == now && idle_start == now);
-        int nq = (size > 0 && link_free > now && refilled) ? size - 1 : size;
-        g.ts = now;
-        if (nq >= red_k && nq > 1)
-        {
-            if (g.flags & F_ECT)
-            {
-                g.flags |= F_CE;
-                marks++;
-            }
-            else
-            {
-                drops++;
-                return false;
-            }
-        }
-        if (nq >= qcap)
-        {
-            drops++;
-            return false;
-        }
-#ifdef TB_QTRACE
-        if (qs->qtrace && now < qs->qtrace_until && now >= qs->qtrace_from)
-        {
-#if defined(__CUDA_ARCH__)
-            const unsigned long long i = atomicAdd(qs->qtrace_cnt, 1ull);
-#else
-            const unsigned long long i = (*qs->qtrace_cnt)++;
-#endif
-            if (i < qs->qtrace_n)
-            {
-                QRec &r = qs->qtrace[i];
-                const SndRec &S = qs->snd[g.flow];
-                r.ts = now;
-                r.node = qnode;
-                r.dev = qdev;
-                r.src = g.to_sender ? S.dst_local : S.src_local;
-                r.dst = g.to_sender ? S.src_local : S.dst_local;
-                r.sa = g.sa;
-                r.len = g.len;
-                r.qlen = (uint16_t)(nq + 1);
-                r.flags = g.flags;
-            }
-        }
-#endif
-        if (size >= cap)
-        {
-            ovf++;
-            return false;
-        }
-        int at = head + size;
-        if (at >= cap)
-            at -= cap;
-        frame_copy(&ring[at], &g);
-        *tailp = g;
-        tail_at = at;
-        size++;
-        return true;
-    }
-};
+using Egress = Transmitter<false>;
+using PortEgress = Transmitter<true>;
 
 } // namespace tb

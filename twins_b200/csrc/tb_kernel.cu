@@ -195,10 +195,10 @@ __device__ __forceinline__ void host_unit(const Sim &s, int u, int host_lanes, i
                         prefetch_l1((const char *)S + b);
                     const uint64_t off = S->it_off;
                     prefetch_l1(&s.it_start[off + S->it_head]);
-                    prefetch_l1(&s.it_fl[off + S->it_head]);
+                    prefetch_l1(&s.it_fl[off + 4 * (S->it_head >> 3)]); // (the flag word of the head's eight)
                     const uint32_t hh = S->h_head;
                     prefetch_l1(&s.h_seq[off + hh]);
-                    prefetch_l1(&s.h_cnt[off + hh]);
+                    prefetch_l1(&s.h_end[off + hh]);
                     prefetch_l1(&s.h_t[off + hh]);
                 }
                 else

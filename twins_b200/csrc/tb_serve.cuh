@@ -109,7 +109,7 @@ void ring_needs(const HostWorld &w, uint64_t &it_n, uint64_t &oo_n)
     for (size_t cc = 0; cc < w.conn_rows.size(); cc++)
     {
         uint64_t segs = (w.conn_bytes[cc] + MSS - 1) / MSS + w.conn_rows[cc].size() + 1;
-        it_n += std::min<uint64_t>(segs, 65536);
+        it_n += sent_list_cap(segs);
         oo_n += std::min<uint64_t>(segs / 2 + 2, 4096);
     }
 }
@@ -186,6 +186,12 @@ int admit(tb_server *v, tb_server::Req &q, long long gslot)
         if (o0 >= 0)
             v->a_oo.give(o0, q.oo_n);
         return 0;
+    }
+    if (i0 & 7)
+    {
+        // (sent-list ranges are multiples of 8 entries from 0, so that their flag words are aligned)
+        g_err = "internal: a sent-list range off the 8-entry grid";
+        return -1;
     }
     Place &pl = q.pl;
     pl.world = (int)wi;
@@ -467,7 +473,7 @@ int server_alloc(tb_server *v)
         (r = c.alloc(&s.host_ring, (size_t)s.H * s.ring, false)) || (r = c.alloc(&s.port_ring, (size_t)s.P * s.ring, false)) ||
         (r = c.alloc(&s.act_snd, (size_t)s.H * s.act_cap, false)) || (r = c.alloc(&s.act_rcv, (size_t)s.H * s.act_cap, false)) ||
         (r = c.alloc(&s.it_start, k.sent_list_entries, false)) || (r = c.alloc(&s.it_fl, k.sent_list_entries, false)) ||
-        (r = c.alloc(&s.h_seq, k.sent_list_entries, false)) || (r = c.alloc(&s.h_cnt, k.sent_list_entries, false)) ||
+        (r = c.alloc(&s.h_seq, k.sent_list_entries, false)) || (r = c.alloc(&s.h_end, k.sent_list_entries, false)) ||
         (r = c.alloc(&s.h_t, k.sent_list_entries, false)) || (r = c.alloc(&s.oo_s, k.ooo_blocks, false)) ||
         (r = c.alloc(&s.oo_e, k.ooo_blocks, false)) || (r = c.alloc(&s.msg, (size_t)NB * s.L * MAX_TX, false)) ||
         (r = c.alloc(&s.msg_tag, (size_t)NB * s.L, false)) || (r = c.alloc(&s.sw_rng, s.S, false)))

@@ -90,21 +90,8 @@ TB_D bool host_step(const Sim &s, int h, int64_t t, int64_t gt, int64_t *wake, u
     c.retx = c.rtos = c.ovf = c.done = 0;
     c.pkts = c.snd_pkts = 0;
     Egress &nic = c.nic;
-    nic.ring = s.host_ring + (size_t)h * s.ring;
-    nic.cap = s.ring;
-    nic.head = hr.q_head;
-    nic.size = hr.q_size;
-    nic.link_free = hr.link_free;
-    nic.last_start = hr.last_start;
-    nic.last = &hr.last;
-    nic.red_k = wd.red_k;
-    nic.qcap = wd.qcap;
-    nic.woke = -1;
-    nic.idle_start = -1;
-    nic.slot_end = E0;
-    nic.out = s.msg + msg_index(s, gt, h) * MAX_TX;
-    nic.sent = 0;
-    nic.drops = nic.marks = nic.ovf = nic.emitted = 0;
+    nic.open(s.host_ring + (size_t)h * s.ring, s.ring, hr.q_head, hr.q_size, hr.link_free, hr.last_start, &hr.last, wd.red_k, wd.qcap, E0,
+             s.msg + msg_index(s, gt, h) * MAX_TX);
 #ifdef TB_QTRACE
     nic.qs = &s;
     nic.qnode = hr.local;
@@ -114,7 +101,7 @@ TB_D bool host_step(const Sim &s, int h, int64_t t, int64_t gt, int64_t *wake, u
 
     TB_PHASE(0)
     // timers due in this slot (new timers lie >= 10 us ahead, except the 1 ps Send deferral,
-    // which due_insert adds), by time
+    // which timer_in_slot adds), by time
     int *act_snd = s.act_snd + (size_t)h * s.act_cap, *act_rcv = s.act_rcv + (size_t)h * s.act_cap;
     const int ns = hr.n_snd, nr = hr.n_rcv;
     c.nd = 0;
@@ -209,32 +196,8 @@ TB_D bool host_step(const Sim &s, int h, int64_t t, int64_t gt, int64_t *wake, u
         TB_PHASE(8)
         if (now == tp)
         {
-            int f = s.msgs[pm].conn;
-            SndRec &S = s.snd[f];
             pn++;
-            if (S.m_first != pm)
-            {
-                // a later message of a connection: FlowSender::SendMessage
-                chain_msg_root(c.ech, pm - wd.msg0);
-                S.m_due++;
-                if (S.st == S_EST)
-                    app_write(c, f, S, now);
-            }
-            else
-            {
-                // the connection's application starts: SYN (SendEmptyPacket)
-                chain_app_root(c.ech, hr.local, f - wd.conn0);
-                S.m_due = 1;
-                add_active(s, act_snd, hr.n_snd, f, c.ovf);
-                S.st = S_SYN_SENT;
-                if (c.cubic)
-                    cub_hystart_reset(S, now);
-                S.rto = CONN_TO_PS;
-                S.syn_at = now + CONN_TO_PS;
-                chain_child(S.rchain, c.ech, code_lead(CONN_TO_PS));
-                S.timing_time = now;
-                emit_snd(c, f, S, F_SYN, 0, 0, SYN_LEN, now);
-            }
+            app_event(c, hr, act_snd, pm, now);
             TB_PHASE(10)
             continue;
         }
@@ -251,59 +214,9 @@ TB_D bool host_step(const Sim &s, int h, int64_t t, int64_t gt, int64_t *wake, u
         }
         if (timer)
         {
-            Due d = c.due[c.di++];
+            const Due d = c.due[c.di++];
             c.ech = due_chain(s, d);
-            const int f = d.flow;
-            if (d.kind == 0 || d.kind == 2)
-            {
-                SndRec &S = s.snd[f];
-                if (d.kind == 0 && S.rto_at == d.at)
-                    on_rto(c, f, S, now);
-                else if (d.kind == 2 && S.syn_at == d.at && S.st == S_EST)
-                {
-                    S.syn_at = -1; // SendPendingData, deferred by Socket::Send
-                    send_pending(c, f, S, now);
-                }
-                else if (d.kind == 2 && S.syn_at == d.at && S.st == S_SYN_SENT)
-                {
-                    // SYN retransmission, backing off the connection timeout
-                    int tries = ++S.syn_tries;
-                    S.rto = CONN_TO_PS << tries;
-                    S.syn_at = now + S.rto;
-                    chain_child(S.rchain, c.ech, code_lead(S.rto));
-                    emit_snd(c, f, S, F_SYN, 0, 0, SYN_LEN, now);
-                }
-            }
-            else
-            {
-                RcvRec &R = s.rcv[f];
-                if (d.kind == 1 && R.delack_at == d.at)
-                    on_delack(c, f, R, now);
-                else if (d.kind == 4 && R.last_at == d.at && R.st == R_LAST_ACK)
-                {
-                    // LastAckTimeout: resend the FIN+ACK a limited number of times
-                    if (R.last_n == 0)
-                        rcv_closed(R);
-                    else
-                    {
-                        R.last_n--;
-                        send_fin_ack(c, f, R, now);
-                        int64_t lr = last_rto(R);
-                        R.last_at = now + lr;
-                        chain_child(R.dchain, c.ech, code_lead(lr));
-                    }
-                }
-                else if (d.kind == 5 && R.frx_at == d.at && R.st == R_LAST_ACK)
-                {
-                    R.frx_at = -1;
-                    send_fin_ack(c, f, R, now);
-                }
-                else if (d.kind == 3 && R.syn_at == d.at && !R.est)
-                {
-                    R.syn_at = -1;
-                    send_synack(c, f, R, now);
-                }
-            }
+            timer_event(c, d, now);
             TB_PHASE(10)
             continue;
         }
@@ -321,11 +234,11 @@ TB_D bool host_step(const Sim &s, int h, int64_t t, int64_t gt, int64_t *wake, u
     }
     TB_PHASE(2)
     nic.advance(E0 - 1);
-    tag_store(&s.msg_tag[msg_index(s, gt, h)], (int64_t)gt << 16 | nic.sent);
+    tag_store(&s.msg_tag[msg_index(s, gt, h)], (int64_t)gt << 16 | nic.n_out);
     hr.q_head = nic.head;
     hr.q_size = nic.size;
-    hr.link_free = nic.link_free;
-    hr.last_start = nic.last_start;
+    hr.link_free = nic.busy_until;
+    hr.last_start = nic.began;
     hr.pend_next = pn;
 
     TB_PHASE(3)
@@ -379,14 +292,14 @@ TB_D bool host_step(const Sim &s, int h, int64_t t, int64_t gt, int64_t *wake, u
     ev_add(s, hr.world, EV_RTO, c.rtos);
     ev_add(s, hr.world, EV_HOST_PKT, c.pkts);
     ev_add(s, hr.world, EV_HOST_SND, c.snd_pkts);
-    ev_add(s, hr.world, EV_HOST_FRAMES, nic.emitted);
+    ev_add(s, hr.world, EV_HOST_FRAMES, nic.offered);
     ev_add(s, hr.world, EV_OVF_RING, c.ovf);
     ev_add(s, hr.world, EV_OVF_TX, nic.ovf);
     ev_add(s, hr.world, EV_TIES, ties);
     *ties_out += ties;
     *done_out += c.done;
     TB_PHASE(5)
-    return nic.sent > 0 || nic.size > 0;
+    return nic.n_out > 0 || nic.size > 0;
 }
 
 // ------------------------------------------------------------------ switches

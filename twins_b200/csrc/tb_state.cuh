@@ -37,6 +37,16 @@ struct WorldDesc
     int n_fail;
 };
 
+// a connection's sent-list ring (and RTT history): an item per segment, message and FIN at most,
+// capped at 65536, rounded up to a multiple of 8: the ring's flags are 32-bit words of eight
+// positions (cap / 2 of the cap flag bytes the connection owns), and with every capacity a
+// multiple of 8 every connection's offset, and so its words, are aligned
+TB_HD uint32_t sent_list_cap(uint64_t segs)
+{
+    const uint64_t n = segs < 8 ? 8 : segs > 65536 ? 65536 : segs;
+    return (uint32_t)((n + 7) & ~7ull);
+}
+
 // the sending side of a connection (TcpSocketBase, TcpTxBuffer, the congestion control)
 struct SndRec
 {
@@ -52,8 +62,7 @@ struct SndRec
     uint32_t tail, una, nxt, high;
     uint32_t cwnd, ssthresh, dupacks;
     uint32_t it_head, it_n, h_head, h_n;
-    uint32_t sack_b, lost_b, rtx_b, sacked_n, hisack;
-    uint32_t cand, cand_n;      // NextSeg: no candidate item below cand; candidates counted
+    uint32_t sack_b, lost_b, rtx_b, cand_b, sack_n, hisack; // the sent list's byte counters, sacked items, highest sack
     uint8_t sack_seen, recover_active, first_partial, cwnd_limited;
     uint32_t recover, cwnd_cnt, ack_rem;
     // TcpCubic
@@ -236,7 +245,7 @@ struct Sim
     MsgRec *msgs;
     uint32_t *it_start;
     uint8_t *it_fl;
-    uint32_t *h_seq, *h_cnt;
+    uint32_t *h_seq, *h_end;
     int64_t *h_t;
     uint32_t *oo_s, *oo_e;
     Frame *msg;          // [NB][L][MAX_TX]

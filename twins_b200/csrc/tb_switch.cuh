@@ -348,30 +348,17 @@ TB_D bool sw_phase_egress(const SwCtx &x, SwShared &sh, int e, unsigned &ties, u
     PortRec &pr = x.ports[e];
     const int port = x.sr->port0 + e;
     typename std::conditional<PORT_LOCAL, PortEgress, Egress>::type eg;
-    eg.ring = s.port_ring + (size_t)port * s.ring;
-    eg.cap = s.ring;
-    eg.head = pr.q_head;
-    eg.size = pr.q_size;
-    eg.link_free = pr.link_free;
-    eg.last_start = pr.last_start;
+    Chain *tx_chain = &pr.last;
     if constexpr (PORT_LOCAL)
     {
         sh.eg_last()[e] = pr.last;
-        eg.last = &sh.eg_last()[e];
-        eg.tailp = &sh.eg_tail()[e];
-        eg.tail_at = -1;
+        tx_chain = &sh.eg_last()[e];
     }
-    else
-        eg.last = &pr.last;
-    eg.red_k = pr.red_k;
-    eg.qcap = pr.qcap;
-    eg.woke = -1;
-    eg.idle_start = -1;
-    eg.slot_end = (x.t + 1) * SLOT_PS;
     const int out_link = s.H + port;
-    eg.out = s.msg + msg_index(s, x.gt, out_link) * MAX_TX;
-    eg.sent = 0;
-    eg.drops = eg.marks = eg.ovf = eg.emitted = 0;
+    eg.open(s.port_ring + (size_t)port * s.ring, s.ring, pr.q_head, pr.q_size, pr.link_free, pr.last_start, tx_chain, pr.red_k, pr.qcap,
+            (x.t + 1) * SLOT_PS, s.msg + msg_index(s, x.gt, out_link) * MAX_TX);
+    if constexpr (PORT_LOCAL)
+        eg.shadow = &sh.eg_tail()[e];
 #ifdef TB_QTRACE
     eg.qs = &s;
     eg.qnode = x.wd->H1 + x.sr->local;
@@ -384,18 +371,18 @@ TB_D bool sw_phase_egress(const SwCtx &x, SwShared &sh, int e, unsigned &ties, u
         chain_child(p.ch, p.ch, code_arrival(p.len)); // queued: the arrival event's chain
         eg.enqueue(p, p.ts);
     }
-    eg.advance(eg.slot_end - 1);
-    tag_store(&s.msg_tag[msg_index(s, x.gt, out_link)], (int64_t)x.gt << 16 | eg.sent);
+    eg.advance(eg.horizon - 1);
+    tag_store(&s.msg_tag[msg_index(s, x.gt, out_link)], (int64_t)x.gt << 16 | eg.n_out);
     pr.q_head = eg.head;
     pr.q_size = eg.size;
-    pr.link_free = eg.link_free;
-    pr.last_start = eg.last_start;
+    pr.link_free = eg.busy_until;
+    pr.last_start = eg.began;
     if constexpr (PORT_LOCAL)
-        pr.last = *eg.last;
+        pr.last = *eg.tx_chain;
     drops += eg.drops;
     marks += eg.marks;
     ovf += eg.ovf;
-    return eg.sent > 0 || eg.size > 0;
+    return eg.n_out > 0 || eg.size > 0;
 }
 
 } // namespace tb

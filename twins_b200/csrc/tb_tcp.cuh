@@ -1,6 +1,8 @@
-// twins-b200: the host's TCP (ns-3 TcpSocketBase with NewReno / DCTCP / Cubic, TcpTxBuffer
-// without SACK, TcpRxBuffer, delayed ACKs, FIN) as device functions over one host's records.
-// Reference: src/step.cuh:319-2236 (function-by-function citations below).
+// twins-b200: a host's TCP sockets for one slot, as ns-3.46's TcpSocketBase runs them (NewReno, DCTCP
+// over TcpLinuxReno, Cubic; TcpTxBuffer without the SACK option, so SACK is emulated from duplicate
+// ACKs; TcpRxBuffer; delayed ACKs; FIN and the closing states), over one host's connection records.
+// Each function cites the reference code of the same ns-3 behaviour (src/step.cuh), which fixes what
+// a simultaneous event sees; the data structures and the order of the checks are this file's own.
 #pragma once
 #include "tb_egress.cuh"
 
@@ -9,320 +11,354 @@ namespace tb
 
 constexpr int DUE_CAP = 64;
 
+// a timer of the host due in the slot: the connection and which one
 struct Due
 {
     int64_t at;
     int flow;
-    int kind; // 0 RTO, 1 delayed ACK, 2 SYN / deferred SendPendingData, 3 SYN-ACK retx, 4 LastAck, 5 FIN+ACK retx
+    int kind; // 0 retransmission, 1 delayed ACK, 2 SYN or deferred send, 3 SYN-ACK, 4 LAST_ACK, 5 FIN+ACK
 };
 
-// one host's context for one slot
+// one host's slot: its egress, the running event's chain, the timers due, counters
 struct HostCtx
 {
     const Sim *s;
     const WorldDesc *wd;
-    int h;       // global host id
+    int h;
     bool dctcp, cubic;
     Egress nic;
-    Chain ech;   // the chain of the event being handled
+    Chain ech;
     Due due[DUE_CAP];
-    int nd, di;  // timers collected / handled
+    int nd, di;
     int64_t slot_end;
     unsigned retx, rtos, ovf, done;
     unsigned long long pkts, snd_pkts;
 };
 
-// a timer set during the slot and due within it (due_insert, step.cuh:342-360)
-TB_D void due_insert(HostCtx &c, int64_t at, int f, int kind)
+// a timer armed during the slot that falls due before its end joins the slot's timers, after the
+// ones of its time already there (reference: due_insert, src/step.cuh:342-360)
+TB_D void timer_in_slot(HostCtx &c, int64_t at, int f, int kind)
 {
     if (at >= c.slot_end)
         return;
-    if (c.nd >= DUE_CAP)
+    if (c.nd == DUE_CAP)
     {
         c.ovf++;
         return;
     }
-    int j = c.nd;
-    while (j > c.di && c.due[j - 1].at > at)
-    {
+    int j = c.nd++;
+    for (; j > c.di && c.due[j - 1].at > at; j--)
         c.due[j] = c.due[j - 1];
-        j--;
-    }
-    c.due[j] = {at, f, kind};
-    c.nd++;
+    c.due[j] = Due{at, f, kind};
 }
 
-// a frame into the host's egress (emit, step.cuh:368-384)
-TB_D void emit(HostCtx &c, int f, uint8_t flags, uint32_t seq, uint32_t ack, uint16_t len, bool to_sender, int64_t now,
-               uint32_t hash, int dst_local)
+// ------------------------------------------------------------------ frames out
+// a segment leaves the socket for the host's device queue: data carry their sequence number, the
+// others their acknowledgement; the ECMP uplink is the direction's flow hash (reference: emit,
+// src/step.cuh:368-384)
+TB_D void to_device(HostCtx &c, int f, uint8_t flags, uint32_t num, uint16_t wire_len, bool toward_sender, uint32_t hash, int dst,
+                    int64_t now)
 {
     Frame fr;
     fr.ts = now;
     fr.flow = (uint32_t)f;
-    fr.sa = (flags & F_DATA) ? seq : ack;
-    fr.len = len;
-    fr.dst = (uint16_t)dst_local;
-    fr.flags = flags | (c.dctcp ? F_ECT : 0);
-    fr.to_sender = to_sender ? 1 : 0;
+    fr.sa = num;
+    fr.len = wire_len;
+    fr.dst = (uint16_t)dst;
+    fr.flags = (uint8_t)(flags | (c.dctcp ? F_ECT : 0));
+    fr.to_sender = toward_sender ? 1 : 0;
     fr.up = (uint16_t)(hash % (uint32_t)c.wd->ecmp_n);
     fr.ch = c.ech;
     c.nic.enqueue(fr, now);
 }
-TB_D void emit_snd(HostCtx &c, int f, const SndRec &S, uint8_t flags, uint32_t seq, uint32_t ack, uint16_t len, int64_t now)
+TB_D void emit_snd(HostCtx &c, int f, const SndRec &S, uint8_t flags, uint32_t num, uint16_t wire_len, int64_t now)
 {
-    emit(c, f, flags, seq, ack, len, false, now, S.hash_data, S.dst_local);
+    to_device(c, f, flags, num, wire_len, false, S.hash_data, S.dst_local, now);
 }
 TB_D void emit_rcv(HostCtx &c, int f, const RcvRec &R, uint8_t flags, uint32_t ack, uint16_t len, int64_t now)
 {
-    emit(c, f, flags, 0, ack, len, true, now, R.hash_ack, R.src_local);
+    to_device(c, f, flags, ack, len, true, R.hash_ack, R.src_local, now);
 }
 
-// SendEmptyPacket(ACK) at the receiver (send_ack, step.cuh:387-407)
-TB_D void send_ack(HostCtx &c, int f, RcvRec &R, uint32_t ack, bool force_ece, bool no_ece, int64_t now)
+// the receiver's pure ACK (SendEmptyPacket): ECE while it owes the sender an echo of CE, unless this
+// ACK is the one that must not carry it; it cancels a pending delayed ACK (reference: send_ack,
+// src/step.cuh:387-407)
+enum AckEcho
 {
-    bool ece = false;
-    if (force_ece)
-        ece = true;
-    else if (!no_ece && (R.ecn_r == E_CE_RCVD || R.ecn_r == E_SENDING_ECE))
+    ECHO_AS_STATE,
+    ECHO_FORCE,
+    ECHO_NEVER
+};
+TB_D void rcv_ack(HostCtx &c, int f, RcvRec &R, uint32_t ack, AckEcho echo, int64_t now)
+{
+    bool ece = echo == ECHO_FORCE;
+    if (echo == ECHO_AS_STATE && (R.ecn_r == E_CE_RCVD || R.ecn_r == E_SENDING_ECE))
     {
-        ece = true;
         R.ecn_r = E_SENDING_ECE;
+        ece = true;
     }
-    R.delack_at = -1;
     R.delack_count = 0;
-    emit_rcv(c, f, R, F_ACK | (ece ? F_ECE : 0), ack, CTRL_LEN, now);
+    R.delack_at = -1;
+    emit_rcv(c, f, R, (uint8_t)(F_ACK | (ece ? F_ECE : 0)), ack, CTRL_LEN, now);
 }
 
-// ------------------------------------------------------------------ the sent list (TcpTxBuffer)
-// A ring of items (start sequence number, TcpTxItem flags) at it_off; an item ends where the
-// next starts, the last at `high`; byte counters sack_b / lost_b / rtx_b as ns-3 keeps them.
-struct Tx
+// ------------------------------------------------------------------ the sent list
+// ns-3's TcpTxBuffer keeps the transmitted items in order (start, size; lost, retransmitted, sacked)
+// with byte counters of the three flags and its highest sacked item. Here the items' starts form a
+// ring (an item ends where the next begins, the last at `high`), and the flags of each eight ring
+// positions share one 32-bit word of the connection's flag bytes: bits 0-7 lost, 8-15
+// retransmitted, 16-23 sacked, bit b of a byte for position 8g + b. One load answers eight items,
+// so the first retransmission candidate is a scan of a few words, and an item's three flags are one
+// word's read and write. Stale bits outside the live items are never read: every item written
+// writes its three bits. (The ring's capacity is a multiple of 8 and its offset too, so the words
+// are aligned.) Beside ns-3's three byte counters the list counts the candidates' bytes (lost,
+// neither retransmitted nor sacked), which tells in O(1) that there is none, and the sacked items,
+// where the Reno emulation's next SACK starts looking.
+enum : uint8_t
 {
-    SndRec &S;
-    uint32_t *st;
-    uint8_t *fl;
-    uint32_t cap;
-    TB_D Tx(const Sim &s, SndRec &S_) : S(S_)
-    {
-        st = s.it_start + S.it_off;
-        fl = s.it_fl + S.it_off;
-        cap = S.it_cap;
-    }
-    TB_D uint32_t at(uint32_t i) const
-    {
-        uint32_t x = S.it_head + i;
-        return x >= cap ? x - cap : x;
-    }
-    TB_D uint32_t beg(uint32_t i) const { return st[at(i)]; }
-    TB_D uint32_t end(uint32_t i) const { return i + 1 < S.it_n ? st[at(i + 1)] : S.high; }
-    TB_D uint8_t flags(uint32_t i) const { return fl[at(i)]; }
+    FL_LOST = 1,
+    FL_RETX = 2,
+    FL_SACK = 4
 };
 
-TB_D bool it_cand(uint8_t fl) { return (fl & (IT_LOST | IT_RETX | IT_SACKED)) == IT_LOST; }
-
-// new flags for item i, keeping the byte counters, the sacked count and the NextSeg cursor
-// (it_set, step.cuh:453-483)
-TB_D void it_set(Tx &t, uint32_t i, uint8_t nf)
+struct SentList
 {
-    SndRec &S = t.S;
-    uint32_t k = t.at(i);
-    uint8_t of = t.fl[k];
-    if (of == nf)
-        return;
-    uint32_t len = t.end(i) - t.st[k];
-    uint8_t d = of ^ nf;
-    if (d & IT_SACKED)
+    SndRec &S;
+    uint32_t *start;
+    uint32_t *fw; // flag words
+    uint32_t cap;
+
+    TB_D SentList(const Sim &s, SndRec &S_) : S(S_)
     {
-        S.sack_b += (nf & IT_SACKED) ? len : 0u - len;
-        S.sacked_n += (nf & IT_SACKED) ? 1u : 0u - 1u;
+        start = s.it_start + S.it_off;
+        fw = reinterpret_cast<uint32_t *>(s.it_fl + S.it_off);
+        cap = S.it_cap;
     }
-    if (d & IT_LOST)
-        S.lost_b += (nf & IT_LOST) ? len : 0u - len;
-    if (d & IT_RETX)
-        S.rtx_b += (nf & IT_RETX) ? len : 0u - len;
-    if (it_cand(of) != it_cand(nf))
+    TB_D uint32_t pos(uint32_t i) const
     {
-        if (it_cand(nf))
+        const uint32_t p = S.it_head + i;
+        return p >= cap ? p - cap : p;
+    }
+    TB_D uint32_t n() const { return S.it_n; }
+    TB_D uint32_t beg(uint32_t i) const { return start[pos(i)]; }
+    TB_D uint32_t end(uint32_t i) const { return i + 1 < S.it_n ? start[pos(i + 1)] : S.high; }
+    TB_D static uint32_t spread(uint8_t f) { return (f & 1u) | (f & 2u) << 7 | (f & 4u) << 14; } // (flag bits -> plane bits)
+    TB_D uint8_t flags_at(uint32_t p) const
+    {
+        const uint32_t w = fw[p >> 3] >> (p & 7);
+        return (uint8_t)((w & 1u) | (w >> 7 & 2u) | (w >> 14 & 4u));
+    }
+    TB_D void write_at(uint32_t p, uint8_t f)
+    {
+        const uint32_t b = p & 7;
+        fw[p >> 3] = (fw[p >> 3] & ~(0x010101u << b)) | spread(f) << b;
+    }
+    TB_D uint8_t flags(uint32_t i) const { return flags_at(pos(i)); }
+    TB_D static bool candidate(uint8_t f) { return (f & (FL_LOST | FL_RETX | FL_SACK)) == FL_LOST; }
+    TB_D static uint32_t lowest(uint32_t m) // (m != 0)
+    {
+#if defined(__CUDA_ARCH__)
+        return (uint32_t)__ffs((int)m) - 1;
+#else
+        return (uint32_t)__builtin_ctz(m);
+#endif
+    }
+
+    // item i's flags become f; the byte counters follow its length (TcpTxItem's flags with
+    // m_lostOut, m_retrans, m_sackedOut, and the candidates' bytes), the sacked items their count
+    TB_D void mark(uint32_t i, uint8_t f)
+    {
+        const uint32_t p = pos(i);
+        const uint8_t was = flags_at(p);
+        if (was == f)
+            return;
+        const uint32_t len = end(i) - start[p];
+        auto adjust = [&](uint32_t &ctr, bool before, bool after) {
+            if (before != after)
+                ctr = after ? ctr + len : ctr - len;
+        };
+        adjust(S.sack_b, was & FL_SACK, f & FL_SACK);
+        adjust(S.lost_b, was & FL_LOST, f & FL_LOST);
+        adjust(S.rtx_b, was & FL_RETX, f & FL_RETX);
+        adjust(S.cand_b, candidate(was), candidate(f));
+        if ((was ^ f) & FL_SACK)
+            S.sack_n += (f & FL_SACK) ? 1u : ~0u;
+        write_at(p, f);
+    }
+
+    // a new item at index i, the ones from i moving up a place (new data at the end, or the second
+    // half of a split); false when the ring is full (counted)
+    TB_D bool open(uint32_t i, uint32_t seq, uint8_t f, unsigned &ovf)
+    {
+        if (S.it_n >= cap)
         {
-            S.cand_n++;
-            if (i < S.cand)
-                S.cand = i;
+            ovf++;
+            return false;
         }
-        else
-            S.cand_n--;
+        for (uint32_t j = S.it_n; j > i; j--)
+        {
+            const uint32_t to = pos(j), from = pos(j - 1);
+            start[to] = start[from];
+            write_at(to, flags_at(from));
+        }
+        start[pos(i)] = seq;
+        write_at(pos(i), f);
+        S.sack_n += (f & FL_SACK) ? 1u : 0u;
+        S.it_n++;
+        return true;
     }
-    t.fl[k] = nf;
-}
+    // item i joins item i - 1, which keeps its flags (its start is removed; the ones after it move
+    // down a place); the candidates' bytes and the sacked count follow the joined item's flags
+    TB_D void join_previous(uint32_t i)
+    {
+        const uint8_t a = flags(i - 1), b = flags(i);
+        const uint32_t lb = end(i) - beg(i);
+        S.cand_b += (candidate(a) ? lb : 0u) - (candidate(b) ? lb : 0u);
+        S.sack_n -= (b & FL_SACK) ? 1u : 0u;
+        for (uint32_t j = i; j + 1 < S.it_n; j++)
+        {
+            const uint32_t to = pos(j), from = pos(j + 1);
+            start[to] = start[from];
+            write_at(to, flags_at(from));
+        }
+        S.it_n--;
+    }
+    // the first item at or after index from whose planes satisfy want(lost, retx, sack) (eight
+    // positions a word; a set bit b: position 8g + b qualifies); n() if none
+    template <class Want>
+    TB_D uint32_t find(uint32_t from, Want want) const
+    {
+        for (uint32_t i = from; i < S.it_n;)
+        {
+            const uint32_t p = pos(i), b = p & 7;
+            uint32_t run = 8 - b; // (items of this word from p, within the ring and the list)
+            if (run > cap - p)
+                run = cap - p;
+            if (run > S.it_n - i)
+                run = S.it_n - i;
+            const uint32_t w = fw[p >> 3];
+            const uint32_t m = (want(w & 0xFFu, w >> 8 & 0xFFu, w >> 16 & 0xFFu) >> b) & ((1u << run) - 1);
+            if (m)
+                return i + lowest(m);
+            i += run;
+        }
+        return S.it_n;
+    }
+    // the first item starting at or after seq (binary search over the starts)
+    TB_D uint32_t first_from(uint32_t seq) const
+    {
+        uint32_t lo = 0, hi = S.it_n;
+        while (lo < hi)
+        {
+            const uint32_t m = (lo + hi) >> 1;
+            if (beg(m) < seq)
+                lo = m + 1;
+            else
+                hi = m;
+        }
+        return lo;
+    }
+};
 
-// insert an item at index i (a split, or new data at the end) (it_insert, step.cuh:486-512)
-TB_D bool it_insert(Tx &t, uint32_t i, uint32_t start, uint8_t fl, unsigned &ovf)
-{
-    SndRec &S = t.S;
-    if (S.it_n >= t.cap)
-    {
-        ovf++;
-        return false;
-    }
-    for (uint32_t j = S.it_n; j > i; j--)
-    {
-        uint32_t a = t.at(j), b = t.at(j - 1);
-        t.st[a] = t.st[b];
-        t.fl[a] = t.fl[b];
-    }
-    uint32_t k = t.at(i);
-    t.st[k] = start;
-    t.fl[k] = fl;
-    S.it_n++;
-    if (S.cand >= i && S.cand > 0)
-        S.cand++;
-    if (it_cand(fl))
-    {
-        S.cand_n++;
-        if (i < S.cand)
-            S.cand = i;
-    }
-    return true;
-}
+// bytes sent and not acknowledged; BytesInFlight = sent - (sacked + lost) + retransmitted, in
+// unsigned arithmetic as ns-3 computes it (reference: src/step.cuh:594-607)
+TB_D uint32_t sent_bytes(const SndRec &S) { return S.it_n ? S.high - S.una : 0u; }
+TB_D uint32_t inflight(const SndRec &S) { return sent_bytes(S) - (S.sack_b + S.lost_b) + S.rtx_b; }
 
-// remove item i's start, merging it into item i - 1 (it_remove_start, step.cuh:515-529)
-TB_D void it_remove_start(Tx &t, uint32_t i)
-{
-    SndRec &S = t.S;
-    for (uint32_t j = i; j + 1 < S.it_n; j++)
-    {
-        uint32_t a = t.at(j), b = t.at(j + 1);
-        t.st[a] = t.st[b];
-        t.fl[a] = t.fl[b];
-    }
-    S.it_n--;
-    if (S.cand > i)
-        S.cand--;
-}
+// a retransmission candidate: lost, neither retransmitted nor sacked
+TB_D uint32_t candidates(uint32_t l, uint32_t r, uint32_t k) { return l & ~r & ~k; }
 
-TB_D uint32_t it_lower(const Tx &t, uint32_t seq)
+// AddRenoSack: a duplicate ACK counts the first item after the sacked ones (from the second) as
+// sacked; the highest sack moves there (reference: src/step.cuh:649-662)
+TB_D void reno_sack_one(SentList &L)
 {
-    uint32_t lo = 0, hi = t.S.it_n;
-    while (lo < hi)
-    {
-        uint32_t m = (lo + hi) / 2;
-        if (t.beg(m) < seq)
-            lo = m + 1;
-        else
-            hi = m;
-    }
-    return lo;
-}
-
-TB_D uint32_t tb_sent(const SndRec &S) { return S.it_n ? S.high - S.una : 0u; }
-// BytesInFlight = sent - (sacked + lost) + retransmitted, unsigned as in ns-3
-TB_D uint32_t inflight(const SndRec &S) { return tb_sent(S) - (S.sack_b + S.lost_b) + S.rtx_b; }
-
-// AddRenoSack (step.cuh:649-662)
-TB_D void add_reno_sack(Tx &t)
-{
-    SndRec &S = t.S;
-    uint32_t i = 1 + S.sacked_n;
-    while (i < S.it_n && (t.flags(i) & IT_SACKED))
-        i++;
-    if (i < S.it_n)
-    {
-        it_set(t, i, t.flags(i) | IT_SACKED);
-        S.sack_seen = 1;
-        S.hisack = t.beg(i);
-    }
-}
-// MarkHeadAsLost (step.cuh:672-677)
-TB_D void mark_head_lost(Tx &t)
-{
-    if (t.S.it_n == 0)
+    SndRec &S = L.S;
+    const uint32_t i = L.find(1 + S.sack_n, [](uint32_t, uint32_t, uint32_t k) { return ~k; });
+    if (i >= L.n())
         return;
-    it_set(t, 0, (uint8_t)((t.flags(0) & ~(IT_SACKED | IT_RETX)) | IT_LOST));
+    L.mark(i, (uint8_t)(L.flags(i) | FL_SACK));
+    S.sack_seen = 1;
+    S.hisack = L.beg(i);
 }
-// ResetRenoSack + SetSentListLost (step.cuh:687-712)
-TB_D void all_lost(Tx &t)
+// MarkHeadAsLost: the first item is lost, neither sacked nor retransmitted any more (reference:
+// src/step.cuh:672-677)
+TB_D void head_to_lost(SentList &L)
 {
-    SndRec &S = t.S;
+    if (L.n())
+        L.mark(0, (uint8_t)((L.flags(0) & ~(FL_SACK | FL_RETX)) | FL_LOST));
+}
+// an RTO: ResetRenoSack and SetSentListLost, every item lost and nothing else (reference:
+// src/step.cuh:687-712)
+TB_D void everything_lost(SentList &L)
+{
+    SndRec &S = L.S;
     for (uint32_t i = 0; i < S.it_n; i++)
-        t.fl[t.at(i)] = IT_LOST;
-    S.sack_b = 0;
-    S.sacked_n = 0;
-    S.rtx_b = 0;
-    S.lost_b = tb_sent(S);
-    S.cand_n = S.it_n;
-    S.cand = 0;
+        L.write_at(L.pos(i), FL_LOST);
+    S.lost_b = S.cand_b = sent_bytes(S);
+    S.sack_b = S.rtx_b = S.sack_n = 0;
     S.sack_seen = 0;
     S.hisack = 0;
 }
-// DiscardUpTo(ack): the bytes of the items removed whole (step.cuh:716-780)
-TB_D uint32_t discard(Tx &t, uint32_t ack)
+
+// DiscardUpTo: the items acknowledged whole leave the list (their bytes are returned), a partly
+// acknowledged first item is cut at the ACK; a sacked first item is unsacked and the Reno emulation
+// moves on (the next item sacked, the first marked lost); a highest sack at or below the ACK is
+// forgotten (reference: src/step.cuh:716-780)
+TB_D uint32_t ack_drop(SentList &L, uint32_t ack)
 {
-    SndRec &S = t.S;
-    uint32_t delivered = 0, removed = 0;
-    while (S.it_n > 0)
+    SndRec &S = L.S;
+    uint32_t gone = 0;
+    while (S.it_n)
     {
-        uint32_t k = t.at(0), b = t.st[k], e = t.end(0);
-        if (ack >= e)
-        {
-            if (t.fl[k])
-                it_set(t, 0, 0);
-            S.it_head = t.at(1);
-            S.it_n--;
-            removed++;
-            delivered += e - b;
-        }
-        else
+        const uint32_t b = L.beg(0), e = L.end(0);
+        if (ack < e)
         {
             if (ack > b)
             {
-                uint8_t fl = t.fl[k];
-                uint32_t off = ack - b;
-                if (fl & IT_SACKED)
-                    S.sack_b -= off;
-                if (fl & IT_LOST)
-                    S.lost_b -= off;
-                if (fl & IT_RETX)
-                    S.rtx_b -= off;
-                t.st[k] = ack;
+                const uint8_t f = L.flags(0);
+                const uint32_t cut = ack - b;
+                if (f & FL_SACK)
+                    S.sack_b -= cut;
+                if (f & FL_LOST)
+                    S.lost_b -= cut;
+                if (f & FL_RETX)
+                    S.rtx_b -= cut;
+                if (SentList::candidate(f))
+                    S.cand_b -= cut;
+                L.start[L.pos(0)] = ack;
             }
             break;
         }
+        L.mark(0, 0);
+        gone += e - b;
+        S.it_head = L.pos(1);
+        S.it_n--;
     }
-    if (removed)
-        S.cand = S.cand > removed ? S.cand - removed : 0;
     S.una = ack;
-    if (S.it_n > 0 && (t.flags(0) & IT_SACKED))
+    if (S.it_n && (L.flags(0) & FL_SACK))
     {
-        it_set(t, 0, (uint8_t)(t.flags(0) & ~IT_SACKED));
-        add_reno_sack(t);
-        mark_head_lost(t);
+        L.mark(0, (uint8_t)(L.flags(0) & ~FL_SACK));
+        reno_sack_one(L);
+        head_to_lost(L);
     }
     if (S.hisack <= ack)
     {
         S.sack_seen = 0;
         S.hisack = 0;
     }
-    return delivered;
+    return gone;
 }
-// NextSeg without SACK: the first lost item neither retransmitted nor sacked, below the highest
-// sack; else new data (step.cuh:784-834)
-TB_D bool next_seg(Tx &t, uint32_t *seq)
+
+// NextSeg without SACK: the first retransmission candidate, if it lies below the highest sack; else
+// new data beyond `high` (reference: src/step.cuh:784-834)
+TB_D bool next_to_send(const SentList &L, uint32_t *seq)
 {
-    SndRec &S = t.S;
-    if (S.cand_n > 0)
+    const SndRec &S = L.S;
+    const uint32_t i = S.cand_b ? L.find(0, candidates) : L.n();
+    if (i < L.n() && (!S.sack_seen || L.beg(i) < S.hisack))
     {
-        for (uint32_t i = S.cand; i < S.it_n; i++)
-        {
-            if (!it_cand(t.flags(i)))
-                continue;
-            S.cand = i;
-            uint32_t b = t.beg(i);
-            if (!S.sack_seen || b < S.hisack)
-            {
-                *seq = b;
-                return true;
-            }
-            break;
-        }
+        *seq = L.beg(i);
+        return true;
     }
     if (S.tail > S.high)
     {
@@ -331,311 +367,323 @@ TB_D bool next_seg(Tx &t, uint32_t *seq)
     }
     return false;
 }
-// IsLost(SND.UNA) (step.cuh:838-846)
-TB_D bool head_lost(const Tx &t)
+// IsLost(SND.UNA) (reference: src/step.cuh:838-846)
+TB_D bool first_is_lost(const SentList &L)
 {
-    const SndRec &S = t.S;
-    if (!S.sack_seen || S.una >= S.hisack || S.it_n == 0)
-        return false;
-    return t.flags(0) & IT_LOST;
+    const SndRec &S = L.S;
+    return S.sack_seen && S.una < S.hisack && L.n() && (L.flags(0) & FL_LOST);
 }
-// IsRetransmittedDataAcked(x) (step.cuh:849-869)
-TB_D bool retx_ends_at(const Tx &t, uint32_t x)
+// IsRetransmittedDataAcked(x): an item ends exactly at x, retransmitted and not sacked (reference:
+// src/step.cuh:849-869)
+TB_D bool retransmission_ends_at(const SentList &L, uint32_t x)
 {
-    const SndRec &S = t.S;
-    if (S.it_n == 0 || x <= S.una || x > S.high)
+    const SndRec &S = L.S;
+    if (!L.n() || x <= S.una || x > S.high)
         return false;
-    uint32_t i = it_lower(t, x) - 1;
-    if (t.end(i) != x)
+    const uint32_t i = L.first_from(x) - 1; // (the item holding byte x - 1)
+    if (L.end(i) != x)
         return false;
-    uint8_t fl = t.flags(i);
-    return !(fl & IT_SACKED) && (fl & IT_RETX);
+    const uint8_t f = L.flags(i);
+    return (f & FL_RETX) && !(f & FL_SACK);
 }
-// GetTransmittedSegment (step.cuh:874-916)
-TB_D uint32_t retransmit(Tx &t, uint32_t i, uint32_t num, unsigned &ovf)
+
+// GetTransmittedSegment: a retransmission of up to `want` bytes from item i. It may take in the
+// next item when that one is not sacked and agrees on being lost (the joined item keeps item i's
+// flags, a retransmission mark of either side dropped first), or it may take part of item i (the
+// rest becomes an item of its own, same flags); the item sent is marked retransmitted (reference:
+// src/step.cuh:874-916)
+TB_D uint32_t resend_item(SentList &L, uint32_t i, uint32_t want, unsigned &ovf)
 {
-    SndRec &S = t.S;
-    uint32_t len = t.end(i) - t.beg(i);
-    uint32_t sz = num;
+    SndRec &S = L.S;
+    uint32_t len = L.end(i) - L.beg(i);
+    uint32_t limit = len;
     if (i + 1 < S.it_n)
     {
-        uint8_t a = t.flags(i), b = t.flags(i + 1);
-        uint32_t nlen = t.end(i + 1) - t.beg(i + 1);
-        if (!(b & IT_SACKED) && (a & IT_LOST) == (b & IT_LOST))
-            sz = sz < len + nlen ? sz : len + nlen;
-        else
-            sz = sz < len ? sz : len;
+        const uint8_t a = L.flags(i), b = L.flags(i + 1);
+        if (!(b & FL_SACK) && (a & FL_LOST) == (b & FL_LOST))
+            limit = len + (L.end(i + 1) - L.beg(i + 1));
     }
-    else
-        sz = sz < len ? sz : len;
-    if (sz > len)
+    const uint32_t take = want < limit ? want : limit;
+    if (take > len)
     {
-        uint8_t a = t.flags(i), b = t.flags(i + 1);
-        if ((a ^ b) & IT_RETX)
-        {
-            if (a & IT_RETX)
-                it_set(t, i, a &= (uint8_t)~IT_RETX);
-            else
-                it_set(t, i + 1, b &= (uint8_t)~IT_RETX);
-        }
-        if (it_cand(b))
-            S.cand_n--;
-        it_remove_start(t, i + 1);
-        len = t.end(i) - t.beg(i);
+        const uint8_t a = L.flags(i), b = L.flags(i + 1);
+        if ((a & FL_RETX) && !(b & FL_RETX))
+            L.mark(i, (uint8_t)(a & ~FL_RETX));
+        else if ((b & FL_RETX) && !(a & FL_RETX))
+            L.mark(i + 1, (uint8_t)(b & ~FL_RETX));
+        L.join_previous(i + 1);
+        len = L.end(i) - L.beg(i);
     }
-    if (sz < len)
-        it_insert(t, i + 1, t.beg(i) + sz, t.flags(i), ovf);
-    uint8_t fl = t.flags(i);
-    if (!(fl & IT_RETX))
-        it_set(t, i, fl | IT_RETX);
-    return sz;
+    if (take < len)
+        L.open(i + 1, L.beg(i) + take, L.flags(i), ovf);
+    if (!(L.flags(i) & FL_RETX))
+        L.mark(i, (uint8_t)(L.flags(i) | FL_RETX));
+    return take;
 }
-// CopyFromSequence (step.cuh:920-975)
-TB_D uint32_t tb_copy(Tx &t, uint32_t num, uint32_t seq, bool *retx, unsigned &ovf)
+
+// CopyFromSequence: what a send of up to `want` bytes at seq takes: a retransmission of the item
+// starting there (when all of it was sent before), or new data appended as an item (when none of it
+// was); a send straddling `high` is cut at `high` (reference: src/step.cuh:920-975)
+TB_D uint32_t take_segment(SentList &L, uint32_t want, uint32_t seq, bool *again, unsigned &ovf)
 {
-    SndRec &S = t.S;
+    SndRec &S = L.S;
     for (;;)
     {
-        uint32_t avail = S.tail > seq ? S.tail - seq : 0;
-        uint32_t sz = num < avail ? num : avail;
-        if (sz == 0)
+        const uint32_t avail = S.tail > seq ? S.tail - seq : 0;
+        const uint32_t sz = want < avail ? want : avail;
+        if (!sz)
             return 0;
-        if (S.high >= seq + sz)
+        if (seq + sz <= S.high)
         {
-            uint32_t i = it_lower(t, seq);
-            if (i >= S.it_n || t.beg(i) != seq)
+            const uint32_t i = L.first_from(seq);
+            if (i >= L.n() || L.beg(i) != seq)
             {
-                ovf++; // (not an item start: cannot happen)
+                ovf++; // (a send always starts at an item: counted, never seen)
                 return 0;
             }
-            *retx = true;
-            return retransmit(t, i, sz, ovf);
+            *again = true;
+            return resend_item(L, i, sz, ovf);
         }
-        if (S.high <= seq)
+        if (seq >= S.high)
         {
-            if (!it_insert(t, S.it_n, seq, 0, ovf))
+            if (!L.open(L.n(), seq, 0, ovf))
                 return 0;
             S.high = seq + sz;
-            *retx = false;
+            *again = false;
             return sz;
         }
-        num = S.high - seq;
+        want = S.high - seq;
     }
 }
 
-// ------------------------------------------------------------------ RTT history and estimator
-// m_history: first transmissions in order, a ring sharing the sent list's capacity; bit 31 of
-// the count marks a retransmitted entry (step.cuh:977-1126)
-TB_D uint32_t h_at(const SndRec &S, uint32_t j)
+// ------------------------------------------------------------------ RTT samples and the RTO
+// RttMeanDeviation's RTO: srtt + max(4 rttvar, granularity) (the initial RTT while there is no
+// sample), at least the minimum RTO unless the caller takes it raw (reference: src/step.cuh:1066-1086)
+TB_D int64_t rto_raw(int64_t srtt, int64_t rttvar)
 {
-    uint32_t x = S.h_head + j;
-    return x >= S.it_cap ? x - S.it_cap : x;
+    const int64_t v = 4 * rttvar;
+    return (srtt >= 0 ? srtt : INIT_RTT_PS) + (v > GRAN_PS ? v : GRAN_PS);
 }
-TB_D void rtt_history(const Sim &s, SndRec &S, uint32_t seq, uint32_t sz, bool retx, int64_t now, unsigned &ovf)
+TB_D int64_t rto_of(int64_t srtt, int64_t rttvar)
 {
-    uint32_t *hs = s.h_seq + S.it_off, *hc = s.h_cnt + S.it_off;
-    if (!retx)
+    const int64_t r = rto_raw(srtt, rttvar);
+    return r > MIN_RTO_PS ? r : MIN_RTO_PS;
+}
+// a measurement m: the first sets srtt = m, rttvar = m / 2; later ones move srtt by an eighth and
+// rttvar by a quarter of the difference, rounded down as ns-3's shifts round
+TB_D void rtt_update(SndRec &S, int64_t m)
+{
+    if (S.srtt < 0)
     {
-        if (S.h_n >= S.it_cap)
+        S.srtt = m;
+        S.rttvar = m / 2;
+    }
+    else
+    {
+        const int64_t d = m - S.srtt;
+        S.srtt += d >> 3;
+        S.rttvar = (3 * S.rttvar + (d < 0 ? -d : d)) >> 2;
+    }
+    S.rto = rto_of(S.srtt, S.rttvar);
+}
+
+// ns-3's RTT history (m_history): an entry per first transmission, oldest first, in a ring of the
+// sent list's capacity: its first byte, one past its last, and when it left. A retransmission
+// starting inside an entry stretches it to the retransmission's end and keeps its time complemented
+// (negative), so that the entry gives no sample (Karn) (reference: src/step.cuh:977-1126)
+struct RttLog
+{
+    SndRec &S;
+    uint32_t *lo, *hi;
+    int64_t *at;
+    TB_D RttLog(const Sim &s, SndRec &S_) : S(S_), lo(s.h_seq + S_.it_off), hi(s.h_end + S_.it_off), at(s.h_t + S_.it_off) {}
+    TB_D uint32_t slot(uint32_t j) const
+    {
+        const uint32_t x = S.h_head + j;
+        return x >= S.it_cap ? x - S.it_cap : x;
+    }
+    TB_D void first_send(uint32_t seq, uint32_t len, int64_t now, unsigned &ovf)
+    {
+        if (S.h_n == S.it_cap)
         {
             ovf++;
             return;
         }
-        uint32_t k = h_at(S, S.h_n);
-        hs[k] = seq;
-        hc[k] = sz;
-        s.h_t[S.it_off + k] = now;
-        S.h_n++;
-        return;
+        const uint32_t k = slot(S.h_n++);
+        lo[k] = seq;
+        hi[k] = seq + len;
+        at[k] = now;
     }
-    for (uint32_t j = 0; j < S.h_n; j++)
+    TB_D void resend(uint32_t seq, uint32_t len)
     {
-        uint32_t k = h_at(S, j);
-        uint32_t cnt = hc[k] & 0x7FFFFFFFu;
-        if (seq >= hs[k] && seq < hs[k] + cnt)
+        for (uint32_t j = 0; j < S.h_n; j++)
         {
-            hc[k] = 0x80000000u | (seq + sz - hs[k]);
-            return;
+            const uint32_t k = slot(j);
+            if (seq >= lo[k] && seq < hi[k])
+            {
+                hi[k] = seq + len;
+                if (at[k] >= 0)
+                    at[k] = ~at[k];
+                return;
+            }
         }
     }
-}
-// RttMeanDeviation::Measurement and the RTO (step.cuh:1066-1086)
-TB_D void rtt_sample(SndRec &S, int64_t m)
-{
-    int64_t est = S.srtt, var = S.rttvar;
-    if (est < 0)
+    // an ACK: the oldest entry, covered whole and never resent, is a measurement; every entry it
+    // covers whole is dropped
+    TB_D void acked(uint32_t ack, int64_t now)
     {
-        est = m;
-        var = m / 2;
+        if (!S.h_n)
+            return;
+        const uint32_t k = slot(0);
+        if (at[k] >= 0 && ack >= hi[k])
+            rtt_update(S, now - at[k]);
+        while (S.h_n && hi[slot(0)] <= ack)
+        {
+            S.h_head = slot(1);
+            S.h_n--;
+        }
     }
-    else
-    {
-        int64_t delta = m - est;
-        est = ((est << 3) + delta) >> 3;
-        if (delta < 0)
-            delta = -delta;
-        var = ((var << 2) + delta - var) >> 2;
-    }
-    S.srtt = est;
-    S.rttvar = var;
-    int64_t v = 4 * var;
-    int64_t rto = est + (v > GRAN_PS ? v : GRAN_PS);
-    S.rto = rto > MIN_RTO_PS ? rto : MIN_RTO_PS;
-}
-// EstimateRtt (step.cuh:1088-1126)
-TB_D void rtt_ack(const Sim &s, SndRec &S, uint32_t ack, int64_t now)
-{
-    if (S.h_n == 0)
-        return;
-    uint32_t *hs = s.h_seq + S.it_off, *hc = s.h_cnt + S.it_off;
-    uint32_t k = h_at(S, 0);
-    if (!(hc[k] & 0x80000000u) && ack >= hs[k] + hc[k])
-        rtt_sample(S, now - s.h_t[S.it_off + k]);
-    while (S.h_n > 0)
-    {
-        k = h_at(S, 0);
-        if (hs[k] + (hc[k] & 0x7FFFFFFFu) > ack)
-            break;
-        S.h_head = h_at(S, 1);
-        S.h_n--;
-    }
-}
+};
 
-// ------------------------------------------------------------------ TcpCubic (step.cuh:1201-1345)
-constexpr double CUB_C = 0.4, CUB_BETA = 0.7;
-constexpr int64_t CUB_ACK_DELTA = 2000000000, CUB_DELAY_MIN = 4000000000, CUB_DELAY_MAX = 1000000000000,
-                  CUB_DELTA = 10000000000;
-
-// double -> uint32_t as GCC/x86-64 converts it (cvttsd2si to 64 bits, the low half; out of
-// range: the "integer indefinite" 2^63)
-TB_D uint32_t cub_u32(double d)
+// ------------------------------------------------------------------ TcpCubic
+// ns-3's TcpCubic with fast convergence, TCP friendliness and HyStart's delay exit, over the
+// connection's cub_* fields; windows in segments (reference: src/step.cuh:1201-1345)
+namespace cubic
 {
-    int64_t v = (d >= -9223372036854775808.0 && d < 9223372036854775808.0) ? (int64_t)d : INT64_MIN;
-    return (uint32_t)(uint64_t)v;
+constexpr double C = 0.4, BETA = 0.7;
+constexpr int64_t ACK_DELTA = 2000000000, DELAY_MIN = 4000000000, DELAY_MAX = 1000000000000, EPOCH_GUARD = 10000000000;
+// Reno's growth per cubic ACK count in TCP-friendly mode, 8 (1 + beta) / (3 (1 - beta)) in ns-3's
+// 1024-scaled terms, truncated
+constexpr uint32_t FRIENDLY = 15;
+static_assert((uint32_t)(8 * (1024 + BETA * 1024) / 3 / (1024 - BETA * 1024)) == FRIENDLY, "Cubic's friendliness factor");
+
+// double -> uint32_t as ns-3's x86-64 build converts it: to a 64-bit integer (out of range: the
+// "integer indefinite" INT64_MIN), then its low half
+TB_D uint32_t x86_u32(double d)
+{
+    const bool fits = d >= -9223372036854775808.0 && d < 9223372036854775808.0;
+    return (uint32_t)(uint64_t)(fits ? (int64_t)d : INT64_MIN);
 }
-TB_D void cub_hystart_reset(SndRec &S, int64_t now)
+// HyStart's round: starts now, ends when the byte after the highest sent is acknowledged
+TB_D void new_round(SndRec &S, int64_t now)
 {
     S.cub_roundstart = S.cub_lastack = now;
     S.cub_endseq = S.st == S_EST ? S.high + 1 : 0;
     S.cub_currrtt = INT64_MIN;
     S.cub_samples = 0;
 }
-TB_D double cub_root(const Sim &s, uint32_t n)
+// K = cbrt(n / C) as the host's libm pow(n / C, 1/3) gives it (a host-made table), else the device pow
+TB_D double k_of(const Sim &s, uint32_t n)
 {
-    // pow(n / 0.4, 1/3) as the host's libm computes it (a table), else the device pow
-    if (n < (uint32_t)s.cub_k_n)
-        return s.cub_k_tab[n];
-    return tb_pow((double)n / CUB_C, 1 / 3.);
+    return n < (uint32_t)s.cub_k_n ? s.cub_k_tab[n] : tb_pow((double)n / C, 1 / 3.);
 }
-TB_D uint32_t cub_update(const Sim &s, SndRec &S, uint32_t segs, int64_t now)
+// the ACKs that one more segment of window takes (ns-3's Update)
+TB_D uint32_t acks_per_segment(const Sim &s, SndRec &S, uint32_t segs, int64_t now)
 {
-    uint32_t seg_cwnd = S.cwnd / MSS;
+    const uint32_t w = S.cwnd / MSS;
     S.cub_ackcnt += segs;
     if (S.cub_epoch == INT64_MIN)
     {
+        // a new epoch: the curve's plateau is the window before the last loss, K away
+        const bool below = S.cub_lastmax > w;
         S.cub_epoch = now;
         S.cub_ackcnt = segs;
-        S.cub_tcpcwnd = seg_cwnd;
-        if (S.cub_lastmax <= seg_cwnd)
-        {
-            S.cub_k = 0.0;
-            S.cub_origin = seg_cwnd;
-        }
-        else
-        {
-            S.cub_k = cub_root(s, S.cub_lastmax - seg_cwnd);
-            S.cub_origin = S.cub_lastmax;
-        }
+        S.cub_tcpcwnd = w;
+        S.cub_k = below ? k_of(s, S.cub_lastmax - w) : 0.0;
+        S.cub_origin = below ? S.cub_lastmax : w;
     }
-    int64_t t = (int64_t)((uint64_t)now + (uint64_t)S.cub_delaymin - (uint64_t)S.cub_epoch);
-    double ts = get_seconds(t), kk = S.cub_k;
-    double offs = ts < kk ? kk - ts : ts - kk;
-    uint32_t delta = cub_u32(CUB_C * tb_pow(offs, 3));
-    uint32_t target = ts < kk ? S.cub_origin - delta : S.cub_origin + delta;
-    uint32_t cnt = target > seg_cwnd ? seg_cwnd / (target - seg_cwnd) : 100 * seg_cwnd;
+    // the curve one minimum RTT ahead: origin -/+ C |t - K|^3
+    const int64_t t = (int64_t)((uint64_t)now + (uint64_t)S.cub_delaymin - (uint64_t)S.cub_epoch);
+    const double ts = get_seconds(t), K = S.cub_k;
+    const bool rising = ts < K;
+    const uint32_t d = x86_u32(C * tb_pow(rising ? K - ts : ts - K, 3));
+    const uint32_t target = rising ? S.cub_origin - d : S.cub_origin + d;
+    uint32_t cnt = target > w ? w / (target - w) : 100 * w;
     if (S.cub_lastmax == 0 && cnt > 20)
         cnt = 20;
-    uint32_t scale = cub_u32(8 * (1024 + CUB_BETA * 1024) / 3 / (1024 - CUB_BETA * 1024));
-    delta = (seg_cwnd * scale) >> 3;
-    while (S.cub_ackcnt > delta)
+    // TCP friendliness: the window Reno would have reached on the same ACKs bounds cnt
+    const uint32_t per = (w * FRIENDLY) >> 3;
+    if (S.cub_ackcnt > per)
     {
-        S.cub_ackcnt -= delta;
-        S.cub_tcpcwnd++;
+        const uint32_t k = (S.cub_ackcnt - 1) / per;
+        S.cub_ackcnt -= k * per;
+        S.cub_tcpcwnd += k;
     }
-    if (S.cub_tcpcwnd > seg_cwnd)
+    if (S.cub_tcpcwnd > w)
     {
-        uint32_t max_cnt = seg_cwnd / (S.cub_tcpcwnd - seg_cwnd);
-        if (cnt > max_cnt)
-            cnt = max_cnt;
+        const uint32_t bound = w / (S.cub_tcpcwnd - w);
+        cnt = cnt < bound ? cnt : bound;
     }
     return cnt > 2 ? cnt : 2;
 }
-TB_D void cub_pkts_acked(SndRec &S, int64_t now)
+// PktsAcked: the minimum delay and HyStart's exit from slow start (an ACK train as long as the
+// minimum delay, or an RTT rise over it in a round's first eight samples)
+TB_D void on_acked(SndRec &S, int64_t now)
 {
-    if (S.cub_epoch != INT64_MIN && now - S.cub_epoch < CUB_DELTA)
+    if (S.cub_epoch != INT64_MIN && now - S.cub_epoch < EPOCH_GUARD)
         return;
-    int64_t rtt = S.srtt;
+    const int64_t rtt = S.srtt;
     if (S.cub_delaymin == INT64_MIN || S.cub_delaymin > rtt)
         S.cub_delaymin = rtt;
-    uint32_t cwnd = S.cwnd;
-    if (!(cwnd <= S.ssthresh && cwnd >= 16 * MSS) || S.cub_found)
+    const uint32_t w = S.cwnd;
+    if (S.cub_found || w > S.ssthresh || w < 16 * MSS)
         return;
-    if (now - S.cub_lastack <= CUB_ACK_DELTA)
+    if (now - S.cub_lastack <= ACK_DELTA)
     {
         S.cub_lastack = now;
         if (now - S.cub_roundstart > S.cub_delaymin)
             S.cub_found = 1;
     }
-    if (S.cub_samples < 8)
+    if (S.cub_samples >= 8)
+    {
+        const int64_t dm = S.cub_delaymin;
+        const int64_t slack = dm < DELAY_MIN ? DELAY_MIN : dm > DELAY_MAX ? DELAY_MAX : dm;
+        if (S.cub_currrtt > dm + slack)
+            S.cub_found = 1;
+    }
+    else
     {
         if (S.cub_currrtt == INT64_MIN || S.cub_currrtt > rtt)
             S.cub_currrtt = rtt;
         S.cub_samples++;
     }
-    else
-    {
-        int64_t dm = S.cub_delaymin;
-        int64_t thresh = dm > CUB_DELAY_MAX ? CUB_DELAY_MAX : (dm < CUB_DELAY_MIN ? CUB_DELAY_MIN : dm);
-        if (S.cub_currrtt > dm + thresh)
-            S.cub_found = 1;
-    }
     if (S.cub_found)
-        S.ssthresh = cwnd;
+        S.ssthresh = w;
 }
-TB_D void cub_increase(const Sim &s, SndRec &S, uint32_t segs, uint32_t ack, int64_t now)
+// IncreaseWindow: slow start by whole segments, else one segment per acks_per_segment ACKs
+TB_D void grow(const Sim &s, SndRec &S, uint32_t segs, uint32_t ack, int64_t now)
 {
     if (!S.cwnd_limited)
         return;
     if (S.cwnd < S.ssthresh)
     {
         if (ack + 1 > S.cub_endseq)
-            cub_hystart_reset(S, now);
+            new_round(S, now);
         S.cwnd += segs * MSS;
-        segs = 0;
+        return;
     }
-    if (S.cwnd >= S.ssthresh && segs > 0)
+    if (!segs)
+        return;
+    S.cub_cnt += segs;
+    const uint32_t cnt = acks_per_segment(s, S, segs, now);
+    if (S.cub_cnt >= cnt)
     {
-        S.cub_cnt += segs;
-        uint32_t cnt = cub_update(s, S, segs, now);
-        if (S.cub_cnt >= cnt)
-        {
-            S.cwnd += MSS;
-            S.cub_cnt -= cnt;
-        }
+        S.cwnd += MSS;
+        S.cub_cnt -= cnt;
     }
 }
-TB_D uint32_t cub_ssthresh(SndRec &S)
+// GetSsThresh: beta of the window; the plateau remembered (lowered further when the window did
+// not regain the last one: fast convergence); a new epoch begins at the next increase
+TB_D uint32_t ssthresh(SndRec &S)
 {
-    uint32_t seg_cwnd = S.cwnd / MSS;
-    if (seg_cwnd < S.cub_lastmax)
-        S.cub_lastmax = cub_u32((seg_cwnd * (1 + CUB_BETA)) / 2);
-    else
-        S.cub_lastmax = seg_cwnd;
+    const uint32_t w = S.cwnd / MSS;
+    S.cub_lastmax = w < S.cub_lastmax ? x86_u32((w * (1 + BETA)) / 2) : w;
     S.cub_epoch = INT64_MIN;
-    uint32_t th = cub_u32(seg_cwnd * CUB_BETA);
+    const uint32_t th = x86_u32(w * BETA);
     return (th > 2 ? th : 2) * MSS;
 }
-TB_D void cub_loss(SndRec &S, int64_t now)
+// CongestionStateSet(CA_LOSS): the curve and HyStart start over
+TB_D void on_loss(SndRec &S, int64_t now)
 {
     S.cub_origin = 0;
     S.cub_k = 0;
@@ -643,218 +691,218 @@ TB_D void cub_loss(SndRec &S, int64_t now)
     S.cub_tcpcwnd = 0;
     S.cub_delaymin = INT64_MIN;
     S.cub_found = 0;
-    cub_hystart_reset(S, now);
+    new_round(S, now);
 }
+} // namespace cubic
 
-// ------------------------------------------------------------------ congestion control
-// GetSsThresh (step.cuh:1055-1063)
-TB_D uint32_t ssthresh_for(HostCtx &c, SndRec &S, uint32_t bif)
+// ------------------------------------------------------------------ NewReno, DCTCP (over Linux Reno)
+// GetSsThresh of the three (reference: src/step.cuh:1055-1063)
+TB_D uint32_t ssthresh_after(HostCtx &c, SndRec &S, uint32_t flight)
 {
     if (c.cubic)
-        return cub_ssthresh(S);
+        return cubic::ssthresh(S);
     if (c.dctcp)
         return (uint32_t)((1.0 - S.alpha / 2.0) * S.cwnd);
-    uint32_t half = bif / 2;
-    return half > 2 * MSS ? half : 2 * MSS;
+    return flight / 2 > 2 * MSS ? flight / 2 : 2 * MSS;
 }
-// PktsAcked (step.cuh:1348-1381)
-TB_D void pkts_acked(HostCtx &c, SndRec &S, uint32_t segs, uint32_t ack, int64_t now)
+// DCTCP's alpha: once per window of data (up to the byte next after the highest sent when the
+// window began), alpha <- (1 - g) alpha + g F, F the window's ECE-acknowledged fraction, in the fused
+// multiply-add ns-3's -march=native build makes of it
+TB_D void dctcp_acked(SndRec &S, uint32_t segs, uint32_t ack)
 {
-    if (c.cubic)
-    {
-        cub_pkts_acked(S, now);
-        return;
-    }
-    if (!c.dctcp)
-        return;
-    S.acked_total += segs * MSS;
+    const uint32_t bytes = segs * MSS;
+    S.acked_total += bytes;
     if (S.ecn_s == E_ECE_RCVD)
-        S.acked_ecn += segs * MSS;
+        S.acked_ecn += bytes;
     if (!S.next_seq_flag)
     {
-        S.next_seq = S.nxt;
         S.next_seq_flag = 1;
-    }
-    if (ack >= S.next_seq)
-    {
-        double m = S.acked_total > 0 ? (double)S.acked_ecn / S.acked_total : 0.0;
-        S.alpha = tb_fma(1.0 - DCTCP_G, S.alpha, DCTCP_G * m); // as ns-3's -march=native build fuses it
         S.next_seq = S.nxt;
-        S.acked_total = 0;
-        S.acked_ecn = 0;
     }
+    if (ack < S.next_seq)
+        return;
+    const double frac = S.acked_total ? (double)S.acked_ecn / S.acked_total : 0.0;
+    S.alpha = tb_fma(1.0 - DCTCP_G, S.alpha, DCTCP_G * frac);
+    S.next_seq = S.nxt;
+    S.acked_total = S.acked_ecn = 0;
 }
-// IncreaseWindow: TcpLinuxReno (DCTCP), TcpNewReno, TcpCubic (step.cuh:1383-1440)
-TB_D void increase_window(HostCtx &c, SndRec &S, uint32_t segs, uint32_t ack, int64_t now)
+// PktsAcked (reference: src/step.cuh:1348-1381)
+TB_D void acked_segments(HostCtx &c, SndRec &S, uint32_t segs, uint32_t ack, int64_t now)
 {
     if (c.cubic)
+        cubic::on_acked(S, now);
+    else if (c.dctcp)
+        dctcp_acked(S, segs, ack);
+}
+// TcpLinuxReno (DCTCP's window): slow start up to ssthresh; then a segment per window of ACKs,
+// counted in cwnd_cnt
+TB_D void linux_reno_grow(SndRec &S, uint32_t segs)
+{
+    if (S.cwnd < S.ssthresh)
     {
-        cub_increase(*c.s, S, segs, ack, now);
-        return;
-    }
-    uint32_t cwnd = S.cwnd, ssth = S.ssthresh;
-    if (c.dctcp)
-    {
-        if (cwnd < ssth)
+        if (segs)
         {
-            if (segs >= 1)
-            {
-                uint64_t n = (uint64_t)cwnd + (uint64_t)segs * MSS;
-                S.cwnd = (uint32_t)(n < ssth ? n : ssth);
-            }
-        }
-        else
-        {
-            uint32_t w = cwnd / MSS;
-            if (w == 0)
-                w = 1;
-            uint32_t cnt = S.cwnd_cnt;
-            if (cnt >= w)
-            {
-                cnt = 0;
-                cwnd += MSS;
-            }
-            cnt += segs;
-            if (cnt >= w)
-            {
-                uint32_t delta = cnt / w;
-                cnt -= delta * w;
-                cwnd += delta * MSS;
-            }
-            S.cwnd = cwnd;
-            S.cwnd_cnt = cnt;
+            const uint64_t w = (uint64_t)S.cwnd + (uint64_t)segs * MSS;
+            S.cwnd = (uint32_t)(w < S.ssthresh ? w : S.ssthresh);
         }
         return;
     }
-    if (cwnd < ssth && segs >= 1)
+    const uint32_t per = S.cwnd / MSS ? S.cwnd / MSS : 1;
+    if (S.cwnd_cnt >= per)
     {
-        cwnd += MSS;
-        segs -= 1;
+        S.cwnd_cnt = 0;
+        S.cwnd += MSS;
     }
-    if (cwnd >= ssth && segs > 0)
+    S.cwnd_cnt += segs;
+    if (S.cwnd_cnt >= per)
     {
-        double adder = (double)MSS * MSS / cwnd;
-        if (adder < 1.0)
-            adder = 1.0;
-        cwnd += (uint32_t)adder;
+        const uint32_t whole = S.cwnd_cnt / per;
+        S.cwnd_cnt -= whole * per;
+        S.cwnd += whole * MSS;
     }
-    S.cwnd = cwnd;
+}
+// TcpNewReno: one segment of slow start per ACK, then MSS^2 / cwnd (at least a byte)
+TB_D void newreno_grow(SndRec &S, uint32_t segs)
+{
+    if (S.cwnd < S.ssthresh && segs)
+    {
+        S.cwnd += MSS;
+        segs--;
+    }
+    if (S.cwnd >= S.ssthresh && segs)
+    {
+        const double step = (double)MSS * MSS / S.cwnd;
+        S.cwnd += (uint32_t)(step > 1.0 ? step : 1.0);
+    }
+}
+// IncreaseWindow (reference: src/step.cuh:1383-1440)
+TB_D void grow_window(HostCtx &c, SndRec &S, uint32_t segs, uint32_t ack, int64_t now)
+{
+    if (c.cubic)
+        cubic::grow(*c.s, S, segs, ack, now);
+    else if (c.dctcp)
+        linux_reno_grow(S, segs);
+    else
+        newreno_grow(S, segs);
 }
 
 // ------------------------------------------------------------------ sending
-// SendDataPacket (step.cuh:1129-1172)
-TB_D uint32_t send_segment(HostCtx &c, int f, SndRec &S, uint32_t seq, uint32_t max_size, int64_t now)
+TB_D void arm_retx_timer(HostCtx &c, SndRec &S, int64_t now)
 {
-    Tx t(*c.s, S);
-    bool retx = false;
-    uint32_t len = tb_copy(t, max_size, seq, &retx, c.ovf);
-    if (len == 0)
+    S.rto_at = now + S.rto;
+    chain_child(S.rchain, c.ech, code_lead(S.rto));
+}
+// SendDataPacket: a segment of up to max_len bytes at seq (CWR on the first new one after an echo,
+// FIN on the one reaching the end of a closing stream); the retransmission timer starts if idle;
+// the RTT history notes it (reference: src/step.cuh:1129-1172)
+TB_D uint32_t transmit(HostCtx &c, int f, SndRec &S, uint32_t seq, uint32_t max_len, int64_t now)
+{
+    SentList L(*c.s, S);
+    bool again = false;
+    const uint32_t len = take_segment(L, max_len, seq, &again, c.ovf);
+    if (!len)
         return 0;
     uint8_t flags = F_DATA;
-    if (!retx && S.ecn_s == E_ECE_RCVD && S.ecn_echo_seq > S.ecn_cwr_seq)
+    if (!again && S.ecn_s == E_ECE_RCVD && S.ecn_echo_seq > S.ecn_cwr_seq)
     {
+        flags |= F_CWR;
         S.ecn_s = E_CWR_SENT;
         S.ecn_cwr_seq = seq;
-        flags |= F_CWR;
     }
     if ((S.fin & FIN_CLOSE) && seq + len == S.tail)
     {
         flags |= F_FIN;
         S.fin |= FIN_SENT;
     }
-    emit_snd(c, f, S, flags, seq, 0, (uint16_t)(len + HDR_BYTES), now);
-    if (retx)
-        c.retx++;
+    emit_snd(c, f, S, flags, seq, (uint16_t)(len + HDR_BYTES), now);
+    c.retx += again;
     if (S.rto_at < 0)
-    {
-        S.rto_at = now + S.rto;
-        chain_child(S.rchain, c.ech, code_lead(S.rto));
-    }
+        arm_retx_timer(c, S, now);
     S.cwnd_limited = S.cwnd < inflight(S) + MSS;
-    rtt_history(*c.s, S, seq, len, retx, now, c.ovf);
+    RttLog log(*c.s, S);
+    if (again)
+        log.resend(seq, len);
+    else
+        log.first_send(seq, len, now, c.ovf);
     if (seq + len > S.high)
         S.high = seq + len;
     return len;
 }
-// SendPendingData (step.cuh:1175-1199)
+// SendPendingData: segments while the window has room (a part of a segment only when it ends the
+// data), retransmissions first; nothing more in Open once the FIN is out (reference:
+// src/step.cuh:1175-1199)
 TB_D void send_pending(HostCtx &c, int f, SndRec &S, int64_t now)
 {
     if (S.st != S_EST)
         return;
-    for (int guard = 0; guard < 4096; guard++)
+    for (int n = 0; n < 4096; n++)
     {
         if (S.cong == C_OPEN && (S.fin & (FIN_SENT | FIN_ACKED)) == FIN_SENT)
             return;
-        uint32_t pipe = inflight(S);
-        uint32_t avail = S.cwnd > pipe ? S.cwnd - pipe : 0;
-        if (avail == 0)
-            return;
+        const uint32_t flight = inflight(S);
+        const uint32_t room = S.cwnd > flight ? S.cwnd - flight : 0;
         uint32_t seq;
-        Tx t(*c.s, S);
-        if (!next_seg(t, &seq))
+        if (!room || !next_to_send(SentList(*c.s, S), &seq))
             return;
-        uint32_t remaining = S.tail - seq;
-        if (avail < MSS && remaining > avail)
+        if (room < MSS && S.tail - seq > room)
             return;
         S.nxt = seq;
-        uint32_t len = send_segment(c, f, S, seq, avail < MSS ? avail : MSS, now);
-        if (len == 0)
+        const uint32_t len = transmit(c, f, S, seq, room < MSS ? room : MSS, now);
+        if (!len)
             return;
         S.nxt = seq + len;
     }
 }
-// DoRetransmit (step.cuh:1202-1212)
-TB_D void do_retransmit(HostCtx &c, int f, SndRec &S, int64_t now)
+// DoRetransmit: the first retransmission candidate, else the first unacknowledged byte (reference:
+// src/step.cuh:1202-1212)
+TB_D void retransmit_one(HostCtx &c, int f, SndRec &S, int64_t now)
 {
-    uint32_t seq;
-    Tx t(*c.s, S);
-    if (!next_seg(t, &seq))
-        seq = S.una;
     if (S.una >= S.tail)
         return;
+    uint32_t seq;
+    if (!next_to_send(SentList(*c.s, S), &seq))
+        seq = S.una;
     S.nxt = seq;
-    send_segment(c, f, S, seq, MSS, now);
+    transmit(c, f, S, seq, MSS, now);
 }
-// NewAck: the RTO from the estimator (clearing backoff); no timer once the buffer is empty
-// outside FIN_WAIT_1 (step.cuh:1445-1464)
-TB_D void new_ack(HostCtx &c, SndRec &S, uint32_t ack, bool reset_rto, int64_t now)
+// NewAck: the retransmission timer restarts from the estimator (optionally), stops once everything
+// is acknowledged unless a FIN is out; nxt never trails the ACK (reference: src/step.cuh:1445-1464)
+TB_D void new_ack(HostCtx &c, SndRec &S, uint32_t ack, bool restart, int64_t now)
 {
-    if (reset_rto)
+    if (restart)
     {
-        int64_t est = S.srtt >= 0 ? S.srtt : INIT_RTT_PS, v = 4 * S.rttvar;
-        int64_t rto = est + (v > GRAN_PS ? v : GRAN_PS);
-        S.rto = rto > MIN_RTO_PS ? rto : MIN_RTO_PS;
-        S.rto_at = now + S.rto;
-        chain_child(S.rchain, c.ech, code_lead(S.rto));
+        S.rto = rto_of(S.srtt, S.rttvar);
+        arm_retx_timer(c, S, now);
     }
     if (ack >= S.tail && !(S.fin & FIN_SENT))
         S.rto_at = -1;
     if (ack > S.nxt)
         S.nxt = ack;
 }
-// EnterRecovery (step.cuh:1467-1481)
+// EnterRecovery: a third duplicate (or a lost head) starts fast recovery: the Reno SACK of this
+// duplicate, the head lost, recover = the highest sent, the window to ssthresh and the head resent
+// (reference: src/step.cuh:1467-1481)
 TB_D void enter_recovery(HostCtx &c, int f, SndRec &S, int64_t now)
 {
-    Tx t(*c.s, S);
-    add_reno_sack(t);
-    mark_head_lost(t);
+    {
+        SentList L(*c.s, S);
+        reno_sack_one(L);
+        head_to_lost(L);
+    }
+    S.cong = C_RECOVERY;
     S.recover = S.high;
     S.recover_active = 1;
-    S.cong = C_RECOVERY;
-    S.ssthresh = ssthresh_for(c, S, inflight(S) + MSS);
+    S.ssthresh = ssthresh_after(c, S, inflight(S) + MSS);
     S.cwnd = S.ssthresh;
-    send_segment(c, f, S, S.una, MSS, now);
+    transmit(c, f, S, S.una, MSS, now);
 }
-// every message whose last byte is acknowledged is complete (step.cuh:1484-1499)
+// messages whose last byte is acknowledged are complete; the connection is done with the last
+// (and its FIN's ACK, with FIN) (reference: src/step.cuh:1484-1499)
 TB_D void messages_acked(HostCtx &c, SndRec &S, int64_t now)
 {
-    MsgRec *M = c.s->msgs;
-    while (S.m_dn < S.m_wr && S.una >= M[S.m_first + S.m_dn].end)
-    {
-        M[S.m_first + S.m_dn].done = now;
-        S.m_dn++;
-        c.done++;
-    }
+    MsgRec *M = c.s->msgs + S.m_first;
+    for (; S.m_dn < S.m_wr && S.una >= M[S.m_dn].end; S.m_dn++, c.done++)
+        M[S.m_dn].done = now;
     if (S.m_dn == S.m_cnt && (!S.fin_on || (S.fin & FIN_ACKED)))
     {
         S.st = S_DONE;
@@ -862,157 +910,152 @@ TB_D void messages_acked(HostCtx &c, SndRec &S, int64_t now)
     }
 }
 
-// ReceivedAck + ProcessAck (step.cuh:1502-1693)
+// ------------------------------------------------------------------ ACKs at the sender
+// a duplicate ACK by congestion state: counted (Recovery counts Reno SACKs instead), Open turns
+// Disorder, and in Disorder the third duplicate (past any earlier recovery point) or a lost head
+// enters recovery; Loss ignores it
+TB_D void duplicate_ack(HostCtx &c, int f, SndRec &S, uint32_t una_before, int64_t now)
+{
+    switch (S.cong)
+    {
+    case C_LOSS:
+        return;
+    case C_RECOVERY: {
+        SentList L(*c.s, S);
+        reno_sack_one(L);
+        return;
+    }
+    case C_CWR:
+        S.dupacks++;
+        return;
+    default: // Open, Disorder
+        S.dupacks++;
+        S.cong = C_DISORDER;
+        if ((S.dupacks == DUPTHRESH && (una_before >= S.recover || !S.recover_active)) || first_is_lost(SentList(*c.s, S)))
+            enter_recovery(c, f, S, now);
+    }
+}
+// an ACK that moves una: `bytes` left the sent list; segments acknowledged with the remainder
+// carried over. Partial ACKs of a recovery retransmit; otherwise the state returns to Open and the
+// window grows (reference: src/step.cuh:1580-1680)
+TB_D void advancing_ack(HostCtx &c, int f, SndRec &S, uint32_t ack, uint32_t una_before, uint32_t bytes, int64_t now)
+{
+    uint32_t segs = bytes / MSS;
+    S.ack_rem += bytes % MSS;
+    if (S.ack_rem >= MSS)
+    {
+        S.ack_rem -= MSS;
+        segs++;
+    }
+    const uint32_t dups = S.dupacks;
+    S.dupacks = 0;
+    const bool partial = ack < S.recover;
+    if (partial && S.cong == C_RECOVERY)
+    {
+        // NewReno's partial ACK: the new head is lost and resent unless it just was
+        bool resend;
+        {
+            SentList L(*c.s, S);
+            head_to_lost(L);
+            resend = !retransmission_ends_at(L, ack + MSS);
+        }
+        if (resend)
+            retransmit_one(c, f, S, now);
+        acked_segments(c, S, 1, ack, now);
+        new_ack(c, S, ack, S.first_partial, now);
+        S.first_partial = 0;
+        return;
+    }
+    if (partial && S.cong == C_LOSS)
+    {
+        acked_segments(c, S, segs, ack, now);
+        grow_window(c, S, segs, ack, now);
+        new_ack(c, S, ack, true, now);
+        return;
+    }
+    if (S.cong == C_CWR)
+    {
+        acked_segments(c, S, segs, ack, now);
+        new_ack(c, S, ack, true, now);
+        return;
+    }
+    switch (S.cong)
+    {
+    case C_OPEN:
+        acked_segments(c, S, segs, ack, now);
+        break;
+    case C_DISORDER:
+        if (segs >= dups)
+            acked_segments(c, S, segs - dups, ack, now);
+        break;
+    case C_RECOVERY: // the recovery point reached: the window deflates to ssthresh
+        S.first_partial = 1;
+        segs = (ack - una_before) / MSS;
+        acked_segments(c, S, segs, ack, now);
+        S.cwnd = S.ssthresh;
+        break;
+    default: // Loss, the recovery point reached
+        S.first_partial = 1;
+        segs = (ack - S.recover) / MSS;
+        acked_segments(c, S, segs, ack, now);
+    }
+    S.cong = C_OPEN;
+    if (!partial)
+        S.recover_active = 0;
+    grow_window(c, S, segs, ack, now);
+    new_ack(c, S, ack, true, now);
+}
+// ReceivedAck and ProcessAck, for an ACK with or without ECE (reference: src/step.cuh:1502-1693)
 TB_D void on_ack(HostCtx &c, int f, SndRec &S, uint32_t ack, bool ece, int64_t now)
 {
-    if (S.st != S_EST)
+    if (S.st != S_EST || ack < S.una)
         return;
-    uint32_t old = S.una;
-    if (ack < old)
-        return;
-    rtt_ack(*c.s, S, ack, now);
-    bool advancing = ack > old;
-    uint32_t delivered = 0;
-    if (advancing)
+    const uint32_t una_before = S.una;
+    const bool moves = ack > una_before;
+    RttLog(*c.s, S).acked(ack, now);
+    uint32_t bytes = 0;
+    if (moves)
     {
-        Tx t(*c.s, S);
-        delivered = discard(t, ack);
+        SentList L(*c.s, S);
+        bytes = ack_drop(L, ack);
     }
     if (S.cong == C_CWR && ack > S.recover)
     {
         S.cong = C_OPEN;
         S.cwnd = S.ssthresh;
     }
-    if (advancing && c.dctcp && ece)
+    // ECN: an ECE on new data (once per echo sequence) cuts the window and enters CWR; an ACK
+    // without ECE ends the echo
+    if (!ece)
     {
-        if (S.ecn_echo_seq < (int64_t)ack)
+        if (S.ecn_s == E_ECE_RCVD)
+            S.ecn_s = E_IDLE;
+    }
+    else if (moves && c.dctcp && S.ecn_echo_seq < (int64_t)ack)
+    {
+        S.ecn_echo_seq = ack;
+        S.ecn_s = E_ECE_RCVD;
+        if (S.cong != C_CWR)
         {
-            S.ecn_echo_seq = ack;
-            S.ecn_s = E_ECE_RCVD;
-            if (S.cong != C_CWR)
-            {
-                S.ssthresh = ssthresh_for(c, S, inflight(S));
-                S.cwnd = S.ssthresh;
-                S.cong = C_CWR;
-                S.recover = S.high;
-            }
+            S.ssthresh = ssthresh_after(c, S, inflight(S));
+            S.cwnd = S.ssthresh;
+            S.cong = C_CWR;
+            S.recover = S.high;
         }
     }
-    else if (S.ecn_s == E_ECE_RCVD && !ece)
-        S.ecn_s = E_IDLE;
-
-    bool dupack = ack == old && ack < S.high;
-    uint32_t old_dup = S.dupacks;
-    if (dupack)
+    if (moves)
+        advancing_ack(c, f, S, ack, una_before, bytes, now);
+    else if (ack < S.high)
     {
-        uint8_t cg = S.cong;
-        if (cg != C_LOSS)
-        {
-            if (cg != C_RECOVERY)
-            {
-                S.dupacks++;
-                old_dup = S.dupacks - 1;
-            }
-            if (cg == C_OPEN)
-                S.cong = cg = C_DISORDER;
-            Tx t(*c.s, S);
-            if (cg == C_RECOVERY)
-                add_reno_sack(t);
-            else if (cg == C_DISORDER)
-            {
-                if (S.dupacks == DUPTHRESH && (old >= S.recover || !S.recover_active))
-                    enter_recovery(c, f, S, now);
-                else if (head_lost(t))
-                    enter_recovery(c, f, S, now);
-            }
-        }
+        duplicate_ack(c, f, S, una_before, now);
+        acked_segments(c, S, 1, ack, now);
     }
-    if (ack == old && ack == S.high)
-    {
-    }
-    else if (ack == old && ack > S.high)
+    else if (ack > S.high)
         S.nxt = ack;
-    else if (ack == old)
-        pkts_acked(c, S, 1, ack, now);
-    else if (advancing)
-    {
-        uint32_t segs = delivered / MSS;
-        S.ack_rem += delivered % MSS;
-        if (S.ack_rem >= MSS)
-        {
-            segs++;
-            S.ack_rem -= MSS;
-        }
-        if (!dupack)
-            S.dupacks = 0;
-        uint8_t cg = S.cong;
-        if (ack < S.recover && cg == C_RECOVERY)
-        {
-            Tx t(*c.s, S);
-            mark_head_lost(t);
-            if (!retx_ends_at(t, ack + MSS))
-                do_retransmit(c, f, S, now);
-            pkts_acked(c, S, 1, ack, now);
-            new_ack(c, S, ack, S.first_partial, now);
-            S.first_partial = 0;
-        }
-        else if (ack < S.recover && cg == C_LOSS)
-        {
-            pkts_acked(c, S, segs, ack, now);
-            increase_window(c, S, segs, ack, now);
-            new_ack(c, S, ack, true, now);
-        }
-        else if (cg == C_CWR)
-        {
-            pkts_acked(c, S, segs, ack, now);
-            new_ack(c, S, ack, true, now);
-        }
-        else
-        {
-            bool exited = false;
-            if (cg == C_OPEN)
-                pkts_acked(c, S, segs, ack, now);
-            else if (cg == C_DISORDER)
-            {
-                if (segs >= old_dup)
-                    pkts_acked(c, S, segs - old_dup, ack, now);
-                if (!dupack)
-                    S.cong = C_OPEN;
-            }
-            else if (cg == C_RECOVERY)
-            {
-                S.first_partial = 1;
-                segs = (ack - old) / MSS;
-                pkts_acked(c, S, segs, ack, now);
-                S.cong = C_OPEN;
-                exited = true;
-                S.dupacks = 0;
-            }
-            else if (cg == C_LOSS)
-            {
-                S.first_partial = 1;
-                segs = (ack - S.recover) / MSS;
-                pkts_acked(c, S, segs, ack, now);
-                S.cong = C_OPEN;
-            }
-            if (ack >= S.recover)
-                S.recover_active = 0;
-            if (exited)
-            {
-                new_ack(c, S, ack, true, now);
-                S.cwnd = S.ssthresh;
-            }
-            if (S.cong == C_OPEN)
-            {
-                increase_window(c, S, segs, ack, now);
-                new_ack(c, S, ack, true, now);
-            }
-        }
-    }
-    // ProcessWait: the ACK of the FIN moves FIN_WAIT_1 to FIN_WAIT_2
-    if ((S.fin & FIN_SENT) && S.it_n == 0 && ack == S.high + 1)
+    // FIN_WAIT_1 -> FIN_WAIT_2 on the FIN's ACK
+    if ((S.fin & FIN_SENT) && !S.it_n && ack == S.high + 1)
         S.fin |= FIN_ACKED;
-    if (advancing)
+    if (moves)
     {
         messages_acked(c, S, now);
         if (S.st == S_DONE)
@@ -1020,94 +1063,84 @@ TB_D void on_ack(HostCtx &c, int f, SndRec &S, uint32_t ack, bool ece, int64_t n
     }
     send_pending(c, f, S, now);
 }
-// the retransmission timeout (step.cuh:1695-1725)
+// the retransmission timeout: everything sent is lost, the timer backs off (at most 60 s), the
+// history is dropped, the window falls to a segment in Loss and sending resumes from the head
+// (reference: src/step.cuh:1695-1725)
 TB_D void on_rto(HostCtx &c, int f, SndRec &S, int64_t now)
 {
     S.rto_at = -1;
-    if (S.st != S_EST)
-        return;
-    if (S.una >= S.tail)
+    if (S.st != S_EST || S.una >= S.tail)
         return;
     c.rtos++;
-    uint32_t before = inflight(S);
-    S.dupacks = 0;
+    const uint32_t flight = inflight(S);
     {
-        Tx t(*c.s, S);
-        all_lost(t);
+        SentList L(*c.s, S);
+        everything_lost(L);
     }
+    S.dupacks = 0;
     S.recover = S.high;
     S.recover_active = 1;
-    int64_t r = 2 * S.rto;
-    S.rto = r < 60000000000000ll ? r : 60000000000000ll;
+    S.rto = 2 * S.rto < 60000000000000ll ? 2 * S.rto : 60000000000000ll;
     S.h_n = 0;
-    S.ssthresh = ssthresh_for(c, S, before);
+    S.ssthresh = ssthresh_after(c, S, flight);
     if (c.cubic)
-        cub_loss(S, now);
+        cubic::on_loss(S, now);
     S.cong = C_LOSS;
     S.cwnd = MSS;
     send_pending(c, f, S, now);
 }
 
-// ------------------------------------------------------------------ receiving
-// SYN-ACK (step.cuh:1729-1743)
+// ------------------------------------------------------------------ the receiving socket
+// SYN-ACK, its timer backing off from the connection timeout (reference: src/step.cuh:1729-1743)
 TB_D void send_synack(HostCtx &c, int f, RcvRec &R, int64_t now)
 {
-    int64_t rto = CONN_TO_PS << R.syn_n;
-    R.syn_n++;
+    const int64_t to = CONN_TO_PS << R.syn_n++;
     if (R.synack_t < 0)
         R.synack_t = now;
     emit_rcv(c, f, R, F_SYN | F_ACK, 0, SYN_LEN, now);
-    if (R.syn_at < 0)
-    {
-        R.syn_at = now + rto;
-        chain_child(R.dchain, c.ech, code_lead(rto));
-    }
+    if (R.syn_at >= 0)
+        return;
+    R.syn_at = now + to;
+    chain_child(R.dchain, c.ech, code_lead(to));
 }
 TB_D void rcv_established(RcvRec &R)
 {
-    if (!R.est)
-    {
-        R.est = 1;
-        R.syn_at = -1;
-    }
+    if (R.est)
+        return;
+    R.est = 1;
+    R.syn_at = -1;
 }
-// DCTCP's CE state machine (step.cuh:1756-1779)
-TB_D void ce_state(HostCtx &c, int f, RcvRec &R, bool ce_now, int64_t now)
+// DCTCP's receiver: when the CE state flips while an ACK is withheld by the delayed-ACK count, that
+// ACK goes out now with the old state's echo; the state and the sequence it covers are kept
+// (reference: src/step.cuh:1756-1779)
+TB_D void ce_flip(HostCtx &c, int f, RcvRec &R, bool ce, int64_t now)
 {
-    if (ce_now)
-    {
-        if (!R.ce_state && R.reserved && R.prior_flag)
-            send_ack(c, f, R, R.prior_rcv_nxt, false, true, now);
-        R.ce_state = 1;
+    if (R.reserved && R.prior_flag && (R.ce_state != 0) != ce)
+        rcv_ack(c, f, R, R.prior_rcv_nxt, ce ? ECHO_NEVER : ECHO_FORCE, now);
+    R.ce_state = ce;
+    if (ce)
         R.ecn_r = E_CE_RCVD;
-    }
-    else
-    {
-        if (R.ce_state && R.reserved && R.prior_flag)
-            send_ack(c, f, R, R.prior_rcv_nxt, true, false, now);
-        R.ce_state = 0;
-        if (R.ecn_r == E_CE_RCVD || R.ecn_r == E_SENDING_ECE)
-            R.ecn_r = E_IDLE;
-    }
+    else if (R.ecn_r == E_CE_RCVD || R.ecn_r == E_SENDING_ECE)
+        R.ecn_r = E_IDLE;
     R.prior_flag = 1;
     R.prior_rcv_nxt = R.rcv_nxt;
 }
-// ECN at the receiving socket (step.cuh:1785-1800)
-TB_D void rx_ecn(HostCtx &c, int f, RcvRec &R, const Frame &p, int64_t now)
+// ECN at the receiving socket: a CE mark beyond the last one seen flips the state to CE; any other
+// ECT frame flips it back (reference: src/step.cuh:1785-1800)
+TB_D void rcv_ecn(HostCtx &c, int f, RcvRec &R, const Frame &p, int64_t now)
 {
     if (!c.dctcp)
         return;
-    bool ce = p.flags & F_CE;
-    if (ce && R.ecn_ce_seq < (int64_t)p.sa)
+    if ((p.flags & F_CE) && R.ecn_ce_seq < (int64_t)p.sa)
     {
         R.ecn_ce_seq = p.sa;
         R.ecn_r = E_CE_RCVD;
-        ce_state(c, f, R, true, now);
+        ce_flip(c, f, R, true, now);
     }
     else if (p.flags & F_ECT)
-        ce_state(c, f, R, false, now);
+        ce_flip(c, f, R, false, now);
 }
-// ECN of ACKs at the sending socket (step.cuh:1806-1822)
+// ECN of the ACKs at the sending socket (reference: src/step.cuh:1806-1822)
 TB_D void snd_ecn(HostCtx &c, SndRec &S, const Frame &p)
 {
     if (!c.dctcp)
@@ -1116,140 +1149,136 @@ TB_D void snd_ecn(HostCtx &c, SndRec &S, const Frame &p)
     {
         S.s_ce = 3;
         S.ecn_s = E_CE_RCVD;
+        return;
     }
-    else if (p.flags & F_ECT)
-    {
-        S.s_ce &= ~2;
-        if (S.ecn_s == E_CE_RCVD || S.ecn_s == E_SENDING_ECE)
-            S.ecn_s = E_IDLE;
-    }
+    if (!(p.flags & F_ECT))
+        return;
+    S.s_ce &= ~2;
+    if (S.ecn_s == E_CE_RCVD || S.ecn_s == E_SENDING_ECE)
+        S.ecn_s = E_IDLE;
 }
-// TcpRxBuffer::Add: out-of-order blocks, sorted and disjoint beyond rcv_nxt, in a ring
-// (step.cuh:1827-1902)
+
+// TcpRxBuffer::Add: the bytes [seq, end) beyond rcv_nxt join the out-of-order blocks (sorted,
+// disjoint, never touching; a ring at oo_off). The blocks the new bytes overlap or touch fold into
+// one with them; in-order bytes move rcv_nxt to the end of that block, which never enters the ring.
+// False when nothing is new (reference: src/step.cuh:1827-1902)
 TB_D bool rx_add(const Sim &s, RcvRec &R, uint32_t seq, uint32_t end, unsigned &ovf)
 {
-    uint32_t head = seq > R.rcv_nxt ? seq : R.rcv_nxt;
-    if (head >= end)
+    const uint32_t from = seq > R.rcv_nxt ? seq : R.rcv_nxt;
+    if (from >= end)
         return false;
     uint32_t *bs = s.oo_s + R.oo_off, *be = s.oo_e + R.oo_off;
-    const uint32_t cap = R.oo_cap, h0 = R.ooo_h;
-    uint32_t n = R.ooo_n;
+    const uint32_t cap = R.oo_cap, n = R.ooo_n;
     auto at = [&](uint32_t i) {
-        uint32_t x = h0 + i;
+        const uint32_t x = R.ooo_h + i;
         return x >= cap ? x - cap : x;
     };
-    uint32_t i;
-    if (n == 0 || be[at(n - 1)] < head)
-        i = n;
-    else
+    // blocks [lo, hi) overlap or touch [from, end): lo = the first ending at or after `from`,
+    // hi = the first starting after `end`
+    uint32_t lo = 0;
+    for (uint32_t b = n; lo < b;)
     {
-        uint32_t lo = 0, hi = n - 1;
-        while (lo < hi)
-        {
-            uint32_t m = (lo + hi) / 2;
-            if (be[at(m)] < head)
-                lo = m + 1;
-            else
-                hi = m;
-        }
-        i = lo;
+        const uint32_t m = (lo + b) >> 1;
+        if (be[at(m)] < from)
+            lo = m + 1;
+        else
+            b = m;
     }
-    if (i < n && bs[at(i)] <= head && be[at(i)] >= end)
-        return false;
-    uint32_t us = head, ue = end, j = i;
-    while (j < n && bs[at(j)] <= ue)
+    uint32_t hi = lo;
+    for (uint32_t b = n; hi < b;)
     {
-        if (bs[at(j)] < us)
-            us = bs[at(j)];
-        if (be[at(j)] > ue)
-            ue = be[at(j)];
-        j++;
+        const uint32_t m = (hi + b) >> 1;
+        if (bs[at(m)] <= end)
+            hi = m + 1;
+        else
+            b = m;
     }
-    if (j == i)
+    if (lo < n && bs[at(lo)] <= from && be[at(lo)] >= end)
+        return false; // (held already)
+    const uint32_t us = lo < hi && bs[at(lo)] < from ? bs[at(lo)] : from;
+    const uint32_t ue = lo < hi && be[at(hi - 1)] > end ? be[at(hi - 1)] : end;
+    if (from == R.rcv_nxt)
     {
-        if (n >= cap)
+        // in order (then lo = 0): the folded block is delivered, the blocks it swallowed leave
+        R.rcv_nxt = ue;
+        R.ooo_h = at(hi);
+        R.ooo_n = n - hi;
+    }
+    else if (lo == hi)
+    {
+        if (n == cap)
         {
             ovf++;
             return false;
         }
-        for (uint32_t q = n; q > i; q--)
+        for (uint32_t i = n; i > lo; i--)
         {
-            bs[at(q)] = bs[at(q - 1)];
-            be[at(q)] = be[at(q - 1)];
+            bs[at(i)] = bs[at(i - 1)];
+            be[at(i)] = be[at(i - 1)];
         }
-        n++;
+        bs[at(lo)] = us;
+        be[at(lo)] = ue;
+        R.ooo_n = n + 1;
     }
     else
     {
-        uint32_t gone = j - i - 1;
-        if (gone)
-            for (uint32_t q = j; q < n; q++)
-            {
-                bs[at(q - gone)] = bs[at(q)];
-                be[at(q - gone)] = be[at(q)];
-            }
-        n -= gone;
+        const uint32_t gone = hi - lo - 1;
+        bs[at(lo)] = us;
+        be[at(lo)] = ue;
+        for (uint32_t i = hi; gone && i < n; i++)
+        {
+            bs[at(i - gone)] = bs[at(i)];
+            be[at(i - gone)] = be[at(i)];
+        }
+        R.ooo_n = n - gone;
     }
-    bs[at(i)] = us;
-    be[at(i)] = ue;
-    uint32_t h = h0;
-    if (head == R.rcv_nxt)
-    {
-        R.rcv_nxt = be[at(0)];
-        h = at(1);
-        n--;
-    }
-    R.ooo_h = n ? h : 0;
-    R.ooo_n = n;
     if (R.fin_seq >= 0 && R.rcv_nxt == (uint32_t)R.fin_seq)
         R.rcv_nxt++;
     return true;
 }
 TB_D bool rx_finished(const RcvRec &R) { return R.fin_seq >= 0 && (uint32_t)R.fin_seq < R.rcv_nxt; }
-// the receiver's FIN+ACK (step.cuh:1948-1963)
+
+// the receiver's FIN+ACK; its own retransmission timer from the receiver's estimator (reference:
+// src/step.cuh:1948-1963)
 TB_D void send_fin_ack(HostCtx &c, int f, RcvRec &R, int64_t now)
 {
     R.delack_at = -1;
     R.delack_count = 0;
     emit_rcv(c, f, R, F_ACK | F_FIN, R.rcv_nxt, CTRL_LEN, now);
-    if (R.frx_at < 0)
-    {
-        int64_t est = R.srtt >= 0 ? R.srtt : INIT_RTT_PS, v = 4 * R.rttvar;
-        int64_t rto = est + (v > GRAN_PS ? v : GRAN_PS);
-        rto = rto > MIN_RTO_PS ? rto : MIN_RTO_PS;
-        R.frx_at = now + rto;
-        chain_child(R.fchain, c.ech, code_lead(rto));
-    }
+    if (R.frx_at >= 0)
+        return;
+    const int64_t to = rto_of(R.srtt, R.rttvar);
+    R.frx_at = now + to;
+    chain_child(R.fchain, c.ech, code_lead(to));
 }
-TB_D int64_t last_rto(const RcvRec &R)
+TB_D void arm_last_ack(HostCtx &c, RcvRec &R, int64_t now)
 {
-    int64_t est = R.srtt >= 0 ? R.srtt : INIT_RTT_PS, v = 4 * R.rttvar;
-    return est + (v > GRAN_PS ? v : GRAN_PS);
+    const int64_t to = rto_raw(R.srtt, R.rttvar); // (LastAckTimeout takes the RTO unclamped)
+    R.last_at = now + to;
+    chain_child(R.dchain, c.ech, code_lead(to));
 }
-// DoPeerClose, then Close at once: FIN+ACK, LAST_ACK (step.cuh:1974-1984)
+// DoPeerClose and the application's Close right after: FIN+ACK, LAST_ACK (reference:
+// src/step.cuh:1974-1984)
 TB_D void do_peer_close(HostCtx &c, int f, RcvRec &R, int64_t now)
 {
     R.st = R_LAST_ACK;
     send_fin_ack(c, f, R, now);
     R.last_n = DATA_RETRIES;
-    int64_t lr = last_rto(R);
-    R.last_at = now + lr;
-    chain_child(R.dchain, c.ech, code_lead(lr));
+    arm_last_ack(c, R, now);
 }
 TB_D void rcv_closed(RcvRec &R)
 {
     R.st = R_CLOSED;
-    R.last_at = -1;
-    R.frx_at = -1;
-    R.delack_at = -1;
+    R.last_at = R.frx_at = R.delack_at = -1;
 }
-// ReceivedData (step.cuh:1994-2036)
+// ReceivedData: new bytes into the buffer; an ACK at once for a gap (or a filled one) or every
+// second segment, else the delayed-ACK timer (reference: src/step.cuh:1994-2036)
 TB_D void received_data(HostCtx &c, int f, RcvRec &R, uint32_t seq, uint32_t len, bool fin, int64_t now)
 {
-    uint32_t expected = R.rcv_nxt;
+    const uint32_t expected = R.rcv_nxt;
     if (!rx_add(*c.s, R, seq, seq + len, c.ovf))
     {
-        send_ack(c, f, R, R.rcv_nxt, false, false, now);
+        rcv_ack(c, f, R, R.rcv_nxt, ECHO_AS_STATE, now);
         return;
     }
     if (expected < R.rcv_nxt && rx_finished(R) && !fin)
@@ -1257,44 +1286,33 @@ TB_D void received_data(HostCtx &c, int f, RcvRec &R, uint32_t seq, uint32_t len
         do_peer_close(c, f, R, now);
         return;
     }
-    bool gap = R.ooo_n > 0;
-    bool filled = R.rcv_nxt > expected + len;
-    if (gap || filled)
+    if (R.ooo_n || R.rcv_nxt > expected + len || R.delack_count + 1u >= DELACK_COUNT)
     {
         R.reserved = 0;
-        send_ack(c, f, R, R.rcv_nxt, false, false, now);
+        rcv_ack(c, f, R, R.rcv_nxt, ECHO_AS_STATE, now);
         return;
     }
-    uint32_t cnt = R.delack_count + 1u;
-    if (cnt >= DELACK_COUNT)
-    {
-        R.reserved = 0;
-        send_ack(c, f, R, R.rcv_nxt, false, false, now);
-    }
-    else
-    {
-        R.delack_count = (uint8_t)cnt;
-        R.reserved = 1;
-        if (R.delack_at < 0)
-        {
-            R.delack_at = now + DELACK_PS;
-            chain_child(R.dchain, c.ech, code_lead(DELACK_PS));
-        }
-    }
+    R.delack_count++;
+    R.reserved = 1;
+    if (R.delack_at >= 0)
+        return;
+    R.delack_at = now + DELACK_PS;
+    chain_child(R.dchain, c.ech, code_lead(DELACK_PS));
 }
-// a data segment (or FIN) at the receiving socket (step.cuh:2040-2101)
+// a data segment or FIN at the receiving socket: old data get a duplicate ACK without ECE; a FIN
+// is taken in order only; LAST_ACK closes on the FIN's ACK (reference: src/step.cuh:2040-2101)
 TB_D void on_data(HostCtx &c, int f, RcvRec &R, const Frame &p, int64_t now)
 {
     if (!R.up || R.st == R_CLOSED)
         return;
-    uint32_t seq = p.sa, len = payload_of(p), end = seq + len;
-    bool fin = p.flags & F_FIN;
-    if (len > 0 && R.est && (R.st == R_LAST_ACK ? seq != R.rcv_nxt : end < R.rcv_nxt))
+    const uint32_t seq = p.sa, len = payload_of(p), end = seq + len;
+    const bool fin = p.flags & F_FIN;
+    if (len && R.est && (R.st == R_LAST_ACK ? seq != R.rcv_nxt : end < R.rcv_nxt))
     {
-        send_ack(c, f, R, R.rcv_nxt, false, true, now);
+        rcv_ack(c, f, R, R.rcv_nxt, ECHO_NEVER, now);
         return;
     }
-    rx_ecn(c, f, R, p, now);
+    rcv_ecn(c, f, R, p, now);
     if ((p.flags & F_CWR) && R.est && R.st == R_OPEN && R.ecn_r != E_CE_RCVD)
         R.ecn_r = E_IDLE;
     if (!R.est)
@@ -1321,39 +1339,30 @@ TB_D void on_data(HostCtx &c, int f, RcvRec &R, const Frame &p, int64_t now)
         R.rcv_nxt++;
     if (len)
         received_data(c, f, R, seq, len, true, now);
-    if (!rx_finished(R))
-        return;
-    do_peer_close(c, f, R, now);
+    if (rx_finished(R))
+        do_peer_close(c, f, R, now);
 }
-TB_D void on_delack(HostCtx &c, int f, RcvRec &R, int64_t now)
-{
-    R.delack_at = -1;
-    R.delack_count = 0;
-    R.reserved = 1;
-    send_ack(c, f, R, R.rcv_nxt, false, false, now);
-}
-// FlowSender::Write and Socket::Send's one-step deferral of SendPendingData (step.cuh:2118-2144)
+
+// ------------------------------------------------------------------ the application
+// FlowSender::Write: the messages due join the stream (the last one closes it, with FIN); the send
+// is deferred a step as Socket::Send defers SendPendingData (reference: src/step.cuh:2118-2144)
 TB_D void app_write(HostCtx &c, int f, SndRec &S, int64_t now)
 {
     if (S.m_wr >= S.m_due)
         return;
-    MsgRec *M = c.s->msgs;
-    while (S.m_wr < S.m_due)
+    MsgRec *M = c.s->msgs + S.m_first;
+    for (; S.m_wr < S.m_due; S.m_wr++)
     {
-        int m = S.m_first + S.m_wr;
-        M[m].est = now;
-        S.tail = M[m].end;
-        S.m_wr++;
+        M[S.m_wr].est = now;
+        S.tail = M[S.m_wr].end;
     }
     if (S.fin_on && S.m_wr == S.m_cnt)
         S.fin |= FIN_CLOSE;
-    uint32_t pipe = inflight(S);
-    if (S.cwnd > pipe && S.syn_at < 0)
-    {
-        S.syn_at = now + 1;
-        chain_child(S.schain, c.ech, CODE_STEP);
-        due_insert(c, now + 1, f, 2);
-    }
+    if (S.cwnd <= inflight(S) || S.syn_at >= 0)
+        return;
+    S.syn_at = now + 1;
+    chain_child(S.schain, c.ech, CODE_STEP);
+    timer_in_slot(c, now + 1, f, 2);
 }
 TB_D bool add_active(const Sim &s, int *list, int &n, int f, unsigned &ovf)
 {
@@ -1365,52 +1374,136 @@ TB_D bool add_active(const Sim &s, int *list, int &n, int f, unsigned &ovf)
     list[n++] = f;
     return true;
 }
+// a message's start time: the connection's first message opens it (SYN, the connection timeout
+// armed), a later one is written to the stream if the connection is up
+TB_D void app_event(HostCtx &c, HostRec &hr, int *act_snd, int m, int64_t now)
+{
+    const WorldDesc &wd = *c.wd;
+    const int f = c.s->msgs[m].conn;
+    SndRec &S = c.s->snd[f];
+    if (S.m_first != m)
+    {
+        chain_msg_root(c.ech, m - wd.msg0);
+        S.m_due++;
+        if (S.st == S_EST)
+            app_write(c, f, S, now);
+        return;
+    }
+    chain_app_root(c.ech, hr.local, f - wd.conn0);
+    S.m_due = 1;
+    add_active(*c.s, act_snd, hr.n_snd, f, c.ovf);
+    S.st = S_SYN_SENT;
+    if (c.cubic)
+        cubic::new_round(S, now);
+    S.rto = CONN_TO_PS;
+    S.syn_at = now + CONN_TO_PS;
+    chain_child(S.rchain, c.ech, code_lead(CONN_TO_PS));
+    S.timing_time = now;
+    emit_snd(c, f, S, F_SYN, 0, SYN_LEN, now);
+}
 
-// a frame at its destination host (on_frame, step.cuh:2147-2236)
+// ------------------------------------------------------------------ timers and frames
+// a timer of the slot fires if it is still the one armed (reference: src/step.cuh:2380-2440)
+TB_D void timer_event(HostCtx &c, const Due &d, int64_t now)
+{
+    const Sim &s = *c.s;
+    const int f = d.flow;
+    if (d.kind == 0 || d.kind == 2)
+    {
+        SndRec &S = s.snd[f];
+        if (d.kind == 0)
+        {
+            if (S.rto_at == d.at)
+                on_rto(c, f, S, now);
+            return;
+        }
+        if (S.syn_at != d.at)
+            return;
+        if (S.st == S_EST)
+        {
+            S.syn_at = -1; // the deferred SendPendingData
+            send_pending(c, f, S, now);
+        }
+        else if (S.st == S_SYN_SENT)
+        {
+            // the SYN again, the connection timeout doubled
+            S.rto = CONN_TO_PS << ++S.syn_tries;
+            S.syn_at = now + S.rto;
+            chain_child(S.rchain, c.ech, code_lead(S.rto));
+            emit_snd(c, f, S, F_SYN, 0, SYN_LEN, now);
+        }
+        return;
+    }
+    RcvRec &R = s.rcv[f];
+    switch (d.kind)
+    {
+    case 1: // delayed ACK
+        if (R.delack_at != d.at)
+            return;
+        R.delack_at = -1;
+        R.reserved = 1;
+        rcv_ack(c, f, R, R.rcv_nxt, ECHO_AS_STATE, now);
+        return;
+    case 3: // SYN-ACK again
+        if (R.syn_at != d.at || R.est)
+            return;
+        R.syn_at = -1;
+        send_synack(c, f, R, now);
+        return;
+    case 4: // LastAckTimeout: the FIN+ACK again, a limited number of times
+        if (R.last_at != d.at || R.st != R_LAST_ACK)
+            return;
+        if (!R.last_n)
+        {
+            rcv_closed(R);
+            return;
+        }
+        R.last_n--;
+        send_fin_ack(c, f, R, now);
+        arm_last_ack(c, R, now);
+        return;
+    default: // the FIN+ACK's own retransmission
+        if (R.frx_at != d.at || R.st != R_LAST_ACK)
+            return;
+        R.frx_at = -1;
+        send_fin_ack(c, f, R, now);
+    }
+}
+
+// a frame at its destination host: at the sender a SYN-ACK (connected: ACK, then the application's
+// write), an ACK, or the receiver's FIN+ACK (TIME_WAIT after its ACK); at the receiver a SYN (the
+// SYN-ACK, the fork's ScheduleNow), data or FIN, or the handshake's ACK (reference: src/step.cuh:2147-2236)
 TB_D void on_frame(HostCtx &c, HostRec &hr, const Frame &p, int64_t now)
 {
     const Sim &s = *c.s;
-    int f = (int)p.flow;
+    const int f = (int)p.flow;
     if (p.to_sender)
     {
         SndRec &S = s.snd[f];
         if (p.flags & F_SYN)
         {
-            if (S.st == S_SYN_SENT)
-            {
-                S.st = S_EST;
-                S.syn_at = -1;
-                rtt_sample(S, now - S.timing_time);
-                emit_snd(c, f, S, F_ACK, 0, 0, CTRL_LEN, now);
-                chain_child(c.ech, c.ech, CODE_NOW); // ConnectionSucceeded (ScheduleNow)
-                app_write(c, f, S, now);
-            }
-        }
-        else if (p.flags & F_FIN)
-        {
-            if (S.fin & FIN_TW)
+            if (S.st != S_SYN_SENT)
                 return;
-            snd_ecn(c, S, p);
-            on_ack(c, f, S, p.sa, p.flags & F_ECE, now);
+            S.st = S_EST;
+            S.syn_at = -1;
+            rtt_update(S, now - S.timing_time);
+            emit_snd(c, f, S, F_ACK, 0, CTRL_LEN, now);
+            chain_child(c.ech, c.ech, CODE_NOW); // (ConnectionSucceeded is ScheduleNow'd)
+            app_write(c, f, S, now);
+            return;
+        }
+        if (S.fin & FIN_TW)
+            return;
+        snd_ecn(c, S, p);
+        on_ack(c, f, S, p.sa, p.flags & F_ECE, now);
+        if (p.flags & F_FIN)
+        {
             S.fin |= FIN_TW;
-            emit_snd(c, f, S, F_ACK, 0, 1, CTRL_LEN, now);
-        }
-        else
-        {
-            if (S.fin & FIN_TW)
-                return;
-            snd_ecn(c, S, p);
-            on_ack(c, f, S, p.sa, p.flags & F_ECE, now);
+            emit_snd(c, f, S, F_ACK, 1, CTRL_LEN, now);
         }
         return;
     }
     RcvRec &R = s.rcv[f];
-    if (!(p.flags & F_SYN) && R.up && R.srtt < 0 && R.synack_t >= 0)
-    {
-        int64_t m = now - R.synack_t;
-        R.srtt = m;
-        R.rttvar = m / 2;
-    }
     if (p.flags & F_SYN)
     {
         if (!R.up)
@@ -1421,15 +1514,22 @@ TB_D void on_frame(HostCtx &c, HostRec &hr, const Frame &p, int64_t now)
         }
         if (R.est)
             return;
-        c.nic.woke = now; // CompleteFork is ScheduleNow'd by the SYN's arrival
+        c.nic.kicked = now; // (the SYN's arrival ScheduleNow's CompleteFork)
         chain_child(c.ech, c.ech, CODE_NOW);
         send_synack(c, f, R, now);
+        return;
     }
-    else if (p.flags & (F_DATA | F_FIN))
+    if (R.up && R.srtt < 0 && R.synack_t >= 0)
+    {
+        // the receiver's first sample: from its SYN-ACK to the next frame of the connection
+        R.srtt = now - R.synack_t;
+        R.rttvar = R.srtt / 2;
+    }
+    if (p.flags & (F_DATA | F_FIN))
         on_data(c, f, R, p, now);
     else if (R.up && R.st != R_CLOSED)
     {
-        rx_ecn(c, f, R, p, now);
+        rcv_ecn(c, f, R, p, now);
         rcv_established(R);
         if (R.st == R_LAST_ACK)
             rcv_closed(R);
