@@ -177,6 +177,11 @@ int tb_set_port_local(tb_ctx *ctx, int on);
  * among a fixed set by the packet-events per ms that short probe launches of each achieve. The
  * results never depend on the shape (no counterpart in the reference). */
 int tb_set_autotune(tb_ctx *ctx, int on);
+/* Batches (on by default): 1 runs each world of a batch on a barrier of its own, so that a world's
+ * slot waits only for that world's units (the reference's batch launch, src/main.cu:267-325, keeps
+ * every world of the batch in the same slot); 0 keeps one grid-wide barrier per slot. The results
+ * never depend on it (no counterpart in the reference). */
+int tb_set_free_batches(tb_ctx *ctx, int on);
 
 /* sizeof(tb_topology), sizeof(tb_tcp_params), sizeof(tb_stats), sizeof(tb_serve_caps),
  * sizeof(tb_request_info), sizeof(tb_serve_stats), sizeof(tb_qrec) in out[0..n-1], so that

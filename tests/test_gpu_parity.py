@@ -163,6 +163,36 @@ def test_batch_worlds_finish_apart(native_lib):
             assert sim.counters(i) == ctr
 
 
+@pytest.mark.parametrize("lanes,port_local", [(None, False), (1, False), (1, True), (32, False)])
+def test_free_batches_equal_lockstep(native_lib, lanes, port_local):
+    """A batch whose worlds each run on a barrier of their own (the default) gives what one
+    grid-wide barrier per slot gives: every world's results and counters, the batch's last slot;
+    autotuned and for each fixed launch shape; and a run cut at 2,000 slots cuts every world
+    there."""
+    rng = np.random.default_rng(11)
+    worlds = []
+    for i, (leaves, tcp, n) in enumerate([(4, "cubic", 200), (8, "dctcp", 120), (4, "newreno", 500), (6, "dctcp", 40), (4, "dctcp", 0)]):
+        topo = api.Topology.leafspine(leaves, leaves // 2, 16)
+        flows = workloads.leafspine_flows(rng, topo.hosts, n, 0.5) if n else api.Flows.from_arrays([], [], [], [])
+        if n:
+            flows.size = np.minimum(flows.size, 200_000)
+        worlds.append((topo, flows, api.TcpParams(tcp, [20, 40, 10, 80, 20][i], [200, 100, 400, 200, 100][i])))
+    for max_slots in (0, 2000):
+        got = {}
+        for free in (True, False):
+            kw = {} if lanes is None else {"host_lanes": lanes, "port_local": port_local}
+            with api.Simulator(free_batches=free, **kw) as sim:
+                ids = [sim.add_world(*w) for w in worlds]
+                sim.run(max_slots)
+                got[free] = ([sim.results(i) for i in ids], [sim.counters(i) for i in ids], sim.stats()["slots"])
+        (ra, ca, sa), (rb, cb, sb) = got[True], got[False]
+        assert all((x[0] == y[0]).all() and (x[1] == y[1]).all() for x, y in zip(ra, rb))
+        assert ca == cb
+        assert sa == sb
+        if max_slots:
+            assert sa == max_slots and any((x[1] < 0).any() for x in ra)
+
+
 @pytest.mark.parametrize("name", ["k8_a2a30_cubic_spray", "k8_r30_dctcp_sprayfin", "df4x9_a2a30_newreno_spray"])
 def test_chain_runs_25(native_lib, name):
     """The 25-run event-chain build (the reference's twins128, 128-byte frames) gives the same

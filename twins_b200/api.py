@@ -114,6 +114,7 @@ ENTRY_POINTS = [
     ("tb_set_launch_shape", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("tb_set_autotune", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("tb_set_port_local", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    ("tb_set_free_batches", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("tb_abi_sizes", ctypes.c_int, [_P(ctypes.c_ulonglong), ctypes.c_int]),
     ("tb_has_qtrace", ctypes.c_int, []),
     ("tb_set_qtrace", ctypes.c_int, [ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_longlong, ctypes.c_longlong]),
@@ -325,9 +326,10 @@ class Simulator:
     """A batch of worlds on one GPU: add worlds, run, read results (tb_* of the C ABI)."""
 
     def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, host_lanes: Optional[int] = None, grid: int = 0,
-                 stage_frames: int = 192, chain_runs: int = 9, port_local: bool = False):
+                 stage_frames: int = 192, chain_runs: int = 9, port_local: bool = False, free_batches: bool = True):
         """host_lanes None: the launch shape is autotuned per launch; else that fixed shape.
-        chain_runs 25: the 25-run event-chain build (the reference's twins128)."""
+        chain_runs 25: the 25-run event-chain build (the reference's twins128).
+        free_batches False: a batch's worlds share one barrier per slot (else each has its own)."""
         if chain_runs not in (9, 25):
             raise ValueError("chain_runs is 9 or 25")
         self.lib = load_library(LIB25_PATH if chain_runs == 25 else None)
@@ -336,6 +338,8 @@ class Simulator:
         if host_lanes is not None:
             self._check(self.lib.tb_set_launch_shape(self.ctx, host_lanes, stage_frames, grid))
             self._check(self.lib.tb_set_port_local(self.ctx, int(port_local)))
+        if not free_batches:
+            self._check(self.lib.tb_set_free_batches(self.ctx, 0))
         self.sizes: list[int] = []
         self.last_status = TB_OK
 

@@ -462,6 +462,9 @@ struct tb_ctx
     int host_lanes = 1, grid_req = 0, grid = 0;
     int stage_cap = SW_STAGE;     // frames staged per warp
     int *d_units = nullptr;       // the running units' list (tb_run)
+    int64_t *d_unit_done = nullptr; // batches without a grid barrier: per list entry its last slot
+    unsigned *d_wunits = nullptr;   // and per world its units in the list
+    bool free_batches = true;       // batches run each world on its own barrier
     unsigned long long qtrace_cap = 0; // the enqueue trace (trace build): records kept, window (ps)
     long long qtrace_from = 0, qtrace_until = 0;
     bool autotune = true;         // pick the launch shape per launch by measured throughput
@@ -785,11 +788,11 @@ int make_world(const tb_topology *topo, int n_flows, const int *src, const int *
 }
 
 // the grid of a launch shape: a warp per unit, at most what is co-resident (0: does not fit)
-int grid_for(const tb_ctx *c, int host_lanes, int stage, int units = -1, bool port_local = false)
+int grid_for(const tb_ctx *c, int host_lanes, int stage, int units = -1, bool port_local = false, bool free = false)
 {
     if (units < 0)
         units = (c->sim.H + host_lanes - 1) / host_lanes + c->sim.S;
-    return grid_of(units, TB_WARPS_PER_BLOCK, tb::slot_kernel_blocks_per_sm(stage, port_local, host_lanes), c->dev_sms, c->grid_req);
+    return grid_of(units, TB_WARPS_PER_BLOCK, tb::slot_kernel_blocks_per_sm(stage, port_local, host_lanes, free), c->dev_sms, c->grid_req);
 }
 
 // the launch-shape tuner's start, on this context's device: the candidates that fit, and the warps
@@ -955,7 +958,8 @@ int prepare(tb_ctx *c)
         if ((r = c->upload(&s.wctl, wctl, true)))
             return r;
     }
-    if (!c->arena && (r = c->alloc(&c->d_units, (size_t)H + S, false)))
+    if (!c->arena && ((r = c->alloc(&c->d_units, (size_t)H + S, false)) || (r = c->alloc(&c->d_unit_done, (size_t)H + S, false)) ||
+                      (r = c->alloc(&c->d_wunits, (size_t)W, false))))
         return r;
     if (c->qtrace_cap)
     {
@@ -1142,6 +1146,14 @@ int tb_set_port_local(tb_ctx *ctx, int on)
     return TB_OK;
 }
 
+int tb_set_free_batches(tb_ctx *ctx, int on)
+{
+    if (!ctx)
+        return fail(TB_ERR_ARG, "ctx is NULL");
+    ctx->free_batches = on != 0;
+    return TB_OK;
+}
+
 int tb_set_autotune(tb_ctx *ctx, int on)
 {
     if (!ctx)
@@ -1183,9 +1195,19 @@ int tb_run(tb_ctx *ctx, long long max_slots)
         wr[i] = {ctx->worlds[i].host0, ctx->worlds[i].H1, ctx->worlds[i].sw0, ctx->worlds[i].S1};
     std::vector<WorldCtl> wc(s.W);
     std::vector<int> ulist;
+    std::vector<unsigned> wunits;
     int alive = s.W, list_alive = s.W, list_lanes = 0, tuned_alive = s.W;
     s.unit_list = nullptr;
     s.n_list = 0;
+    // a batch runs each world on its own barrier (free_kernel), over a world-aligned unit list
+    const bool free = ctx->free_batches && s.W > 1 && ctx->d_units && ctx->d_unit_done && ctx->d_wunits;
+    if (free)
+    {
+        s.unit_done = ctx->d_unit_done;
+        s.w_units = ctx->d_wunits;
+        list_alive = -1;
+    }
+    bool finished = false;
     tb::SlotGraph graph;
     struct GraphRelease
     {
@@ -1203,7 +1225,25 @@ int tb_run(tb_ctx *ctx, long long max_slots)
                 continue;
             ShapeTuner::Shape &sh = tu.shapes[k];
             int grid = ctx->grid_req > 0 && !ctx->autotune ? ctx->grid : grid_for(ctx, sh.lanes, sh.stage, -1, sh.port_local);
-            if (ctx->d_units && alive < s.W)
+            if (free)
+            {
+                if (alive != list_alive || sh.lanes != list_lanes)
+                {
+                    world_units([&wc](size_t w) { return wc[w].next != INT64_MAX; }, wr, sh.lanes, s.H, ulist, wunits);
+                    if ((!ulist.empty() &&
+                         cudaMemcpyAsync(ctx->d_units, ulist.data(), sizeof(int) * ulist.size(), cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) ||
+                        cudaMemcpyAsync(ctx->d_wunits, wunits.data(), sizeof(unsigned) * s.W, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
+                        return fail(TB_ERR_CUDA, "cudaMemcpyAsync failed");
+                    list_alive = alive;
+                    list_lanes = sh.lanes;
+                }
+                s.unit_list = ctx->d_units;
+                s.n_list = (int)ulist.size();
+                grid = grid_for(ctx, sh.lanes, sh.stage, s.n_list, sh.port_local, true);
+                if (ctx->grid_req > 0 && !ctx->autotune)
+                    grid = std::min(grid, ctx->grid);
+            }
+            else if (ctx->d_units && alive < s.W)
             {
                 if (alive != list_alive || sh.lanes != list_lanes)
                 {
@@ -1221,8 +1261,9 @@ int tb_run(tb_ctx *ctx, long long max_slots)
             const long long slots_before = ctl.slots_run;
             cudaEventRecord(ctx->la, ctx->stream);
             // (the steady launches replay a captured graph; the short probes launch directly)
-            int e = explore ? tb::launch_slots(s, grid, tu.probe, sh.lanes, sh.stage, sh.port_local, ctx->stream)
-                            : tb::launch_slots_graph(graph, s, grid, run_slots, sh.lanes, sh.stage, sh.port_local, ctx->stream);
+            int e = explore ? (free ? tb::launch_free(s, grid, tu.probe, sh.lanes, sh.stage, sh.port_local, ctx->stream)
+                                    : tb::launch_slots(s, grid, tu.probe, sh.lanes, sh.stage, sh.port_local, ctx->stream))
+                            : tb::launch_slots_graph(graph, s, grid, run_slots, sh.lanes, sh.stage, sh.port_local, ctx->stream, free);
             if (e)
                 return fail(TB_ERR_CUDA, std::string("slot kernel launch: ") + cudaGetErrorString((cudaError_t)e));
             cudaEventRecord(ctx->lb, ctx->stream);
@@ -1237,20 +1278,21 @@ int tb_run(tb_ctx *ctx, long long max_slots)
                 for (const WorldCtl &x : wc)
                     alive += x.next != INT64_MAX;
             }
+            finished = ctl.error || (free ? alive == 0 : ctl.finished != 0);
             const long long ran = ctl.slots_run - slots_before;
             sh.slots += ran;
             float lms = 0;
             cudaEventElapsedTime(&lms, ctx->la, ctx->lb);
             if (ran >= tu.probe / 2)
                 per_slot[k] = lms / (double)ran;
-            if (ctl.finished || ctl.error)
+            if (finished)
                 break;
         }
         if (explore)
             tu.decide(per_slot);
         else
             tu.since++;
-        if (ctl.finished || ctl.error)
+        if (finished)
             break;
         if (4 * (tuned_alive - alive) > tuned_alive)
         {
@@ -1285,6 +1327,13 @@ int tb_run(tb_ctx *ctx, long long max_slots)
     cudaMemcpy(ctx->ev_w.data(), s.ev_w, 8 * ctx->ev_w.size(), cudaMemcpyDeviceToHost);
     tb_stats &st = ctx->stats;
     st.slots = ctl.slot;
+    if (free)
+    {
+        // (each world's own last slot; the batch's is the latest)
+        st.slots = 0;
+        for (const WorldCtl &x : wc)
+            st.slots = std::max<long long>(st.slots, x.last + 1);
+    }
     st.slots_run = ctl.slots_run;
     st.launches = launches;
     st.kernel_ms = ms;

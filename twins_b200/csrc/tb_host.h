@@ -58,6 +58,28 @@ void running_units(Alive alive, const std::vector<std::array<int, 4>> &worlds, i
                 out.push_back(host_units + worlds[w][2] + x);
 }
 
+// The units of a batch's running worlds for a launch without a grid barrier: per running world
+// its host units (the first host of up to `lanes` consecutive hosts of that world, never of two)
+// and its switches (H + switch); counts[w] the units of world w (0: it does not run).
+template <class Alive>
+void world_units(Alive alive, const std::vector<std::array<int, 4>> &worlds, int lanes, int H, std::vector<int> &out,
+                 std::vector<unsigned> &counts)
+{
+    out.clear();
+    counts.assign(worlds.size(), 0);
+    for (size_t w = 0; w < worlds.size(); w++)
+    {
+        if (!alive(w))
+            continue;
+        const size_t first = out.size();
+        for (int h = worlds[w][0]; h < worlds[w][0] + worlds[w][1]; h += lanes)
+            out.push_back(h);
+        for (int x = 0; x < worlds[w][3]; x++)
+            out.push_back(H + worlds[w][2] + x);
+        counts[w] = (unsigned)(out.size() - first);
+    }
+}
+
 // Launch-shape autotuning, for tb_run and the server. A shape is the hosts per warp, the frames a
 // warp stages per slot and the switch egress variant; no shape changes a result. It starts from
 // one host per warp while the entities fit the resident warps about twice (latency-bound: each

@@ -151,10 +151,11 @@ __device__ __forceinline__ void host_report(const Sim &s, int w, int64_t t0, boo
 // will read: the records of the frames' connections with the heads of their sent lists and RTT
 // histories, the head frames of the host's egress queue, and the timers of its active
 // connections; then lane 0 runs the host's slot (host_step) on the staged frames, or in place
-// when they do not fit. With several hosts per warp each lane runs its own host in place.
+// when they do not fit. With several hosts per warp each lane runs its own host in place: the
+// unit's hosts are h0 .. h0 + nh - 1. Flows completed are added to *done_sink.
 template <bool MANY>
-__device__ __forceinline__ void host_unit(const Sim &s, int u, int host_lanes, int64_t t, int lane, SwShared &sh, unsigned &ties,
-                                          unsigned &blk_done)
+__device__ __forceinline__ void host_unit(const Sim &s, int h0, int nh, int64_t t, int lane, SwShared &sh, unsigned &ties,
+                                          unsigned *done_sink)
 {
     int h, w = 0, n2 = -1, n1 = -1;
     int64_t t0 = 0;
@@ -162,7 +163,7 @@ __device__ __forceinline__ void host_unit(const Sim &s, int u, int host_lanes, i
     const Frame *stage = nullptr;
     if constexpr (!MANY)
     {
-        h = u;
+        h = h0;
         const HostRec &hr = s.hosts[h];
         w = hr.world;
         const int link = hr.in_link;
@@ -226,8 +227,8 @@ __device__ __forceinline__ void host_unit(const Sim &s, int u, int host_lanes, i
     }
     else
     {
-        h = u * host_lanes + lane;
-        if (lane < host_lanes && h < s.H)
+        h = h0 + lane;
+        if (lane < nh)
         {
             const HostRec &hr = s.hosts[h];
             w = hr.world;
@@ -261,7 +262,7 @@ __device__ __forceinline__ void host_unit(const Sim &s, int u, int host_lanes, i
         const bool act = host_step(s, h, t - t0, t, &wake, &ties, &done, stage, n2, n1);
         host_report(s, w, t0, act, wake, done);
         if (done)
-            atomicAdd(&blk_done, done);
+            atomicAdd(done_sink, done);
     }
     __syncwarp(); // (the staging area is reused by the warp's next unit)
 }
@@ -396,7 +397,10 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, MIN_BLOCKS) slot_kernel(
             unsigned long long p0 = globaltimer();
 #endif
             if (u < host_units)
-                host_unit<MIN_BLOCKS == MIN_BLOCKS_MANY>(s, u, host_lanes, t, lane, sh, ties, blk_done);
+            {
+                const int h0 = u * host_lanes;
+                host_unit<MIN_BLOCKS == MIN_BLOCKS_MANY>(s, h0, min(host_lanes, s.H - h0), t, lane, sh, ties, &blk_done);
+            }
             else
             {
                 const int sw = u - host_units;
@@ -499,49 +503,202 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, MIN_BLOCKS) slot_kernel(
     }
 }
 
+
+// ------------------------------------------------------------------ batches without a grid barrier
+// A batch's worlds are independent: each runs its own slots on a barrier of its own, so that a
+// slot of one world waits only for that world's units, not for the slowest unit of the batch.
+// The launch's unit list holds host units (first host h < H; up to host_lanes hosts of one world)
+// and switches (H + switch). A warp cycles over its units and runs every one whose world runs a
+// slot the unit has not done; the unit's lane 0, after the warp, counts it in its world's
+// `arrive`, and the world's last unit closes the slot: the world's slot rule (finish, the exact
+// idle skip), then the next slot is published (or the world parks: its slot budget for this
+// launch is spent, or it is done). A warp whose units are all parked leaves; one that finds
+// nothing to run waits (bounded) for its worlds to move.
+
+// the world's slot t is done by all its units: its next slot, or parked (by the unit's lane 0)
+__device__ void world_close(const Sim &s, int w, int64_t t)
+{
+    WorldCtl *wc = &s.wctl[w];
+    volatile WorldCtl *vw = wc;
+    __threadfence();
+    const unsigned cur = atomicExch(&wc->act, 0u), prev = vw->prev;
+    const unsigned long long wake = atomicExch(&wc->wake, (unsigned long long)INT64_MAX);
+    vw->prev = cur;
+    vw->last = t;
+    int64_t nx;
+    if (atomicAdd(&wc->fdone, 0u) >= (unsigned)s.worlds[w].n_msgs)
+        nx = INT64_MAX;
+    else
+    {
+        nx = (cur == 0 && prev == 0 && (int64_t)wake > t + 1) ? (int64_t)wake : t + 1;
+        if (nx >= s.max_slots)
+        {
+            nx = INT64_MAX; // (the run ends at max_slots with flows unfinished, as the batch's does)
+            vw->last = s.max_slots - 1;
+        }
+    }
+    atomicAdd((unsigned long long *)&s.ctl->slots_run, 1ull);
+    const unsigned budget = vw->budget - 1;
+    vw->budget = budget;
+    vw->next = nx;
+    vw->arrive = 0;
+    __threadfence();
+    vw->run = (nx == INT64_MAX || budget == 0) ? RUN_PARKED : nx;
+}
+
+// before a launch: every world runs from its next slot with a budget; every unit has done nothing
+__global__ void free_open(Sim s, unsigned budget)
+{
+    const int stride = gridDim.x * blockDim.x;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < s.n_list; i += stride)
+        s.unit_done[i] = RUN_PARKED;
+    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < s.W; w += stride)
+    {
+        WorldCtl &c = s.wctl[w];
+        c.arrive = 0;
+        c.units = s.w_units[w];
+        c.budget = budget;
+        c.run = c.next == INT64_MAX || c.units == 0 ? RUN_PARKED : c.next;
+    }
+}
+
+template <bool PORT_LOCAL, int MIN_BLOCKS>
+__global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, MIN_BLOCKS) free_kernel(Sim s, int host_lanes, int stage_cap)
+{
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int gwarp = blockIdx.x * WARPS_PER_BLOCK + warp, nwarps = gridDim.x * WARPS_PER_BLOCK;
+    SwShared &sh = *sw_shared_at(dyn_smem + (size_t)warp * sw_shared_bytes(stage_cap, PORT_LOCAL), stage_cap); // the warp's scratch
+    __syncwarp();
+    const unsigned FULL = 0xffffffffu;
+    long long idle = 0;
+    for (;;)
+    {
+        bool live = false, ran = false;
+        for (int i = gwarp; i < s.n_list; i += nwarps)
+        {
+            const int v = __ldg(&s.unit_list[i]);
+            const bool host = v < s.H;
+            const int w = host ? s.hosts[v].world : s.sws[v - s.H].world;
+            int64_t t = 0, done = 0;
+            if (lane == 0)
+            {
+                t = __ldcg(&s.wctl[w].run);
+                done = s.unit_done[i];
+            }
+            t = __shfl_sync(FULL, t, 0);
+            done = __shfl_sync(FULL, done, 0);
+            if (t == RUN_PARKED)
+                continue;
+            live = true;
+            if (done == t)
+                continue; // (done; its world's other units are not)
+            ran = true;
+            __threadfence(); // (what the world's units wrote in its last slot, before `run` moved)
+            unsigned ties = 0;
+            if (host)
+            {
+                const WorldDesc &wd = s.worlds[w];
+                host_unit<MIN_BLOCKS == MIN_BLOCKS_MANY>(s, v, min(host_lanes, wd.host0 + wd.H1 - v), t, lane, sh, ties,
+                                                         &s.ctl->flows_done);
+            }
+            else if (switch_step<PORT_LOCAL>(s, v - s.H, t, lane, sh, ties) && lane == 0)
+                atomicOr(&s.wctl[w].act, 1u);
+            __syncwarp();
+            if (lane == 0)
+            {
+                s.unit_done[i] = t;
+                __threadfence();
+                if (atomicAdd(&s.wctl[w].arrive, 1u) + 1 == __ldcg(&s.wctl[w].units))
+                    world_close(s, w, t);
+            }
+            __syncwarp();
+        }
+        if (!live)
+            return;
+        if (ran)
+        {
+            idle = 0;
+            continue;
+        }
+        if (++idle > BARRIER_SPIN_LIMIT || __ldcg(&s.ctl->error))
+        {
+            if (lane == 0 && idle > BARRIER_SPIN_LIMIT)
+            {
+                atomicExch(&s.ctl->error, 1);
+                atomicAdd(&s.ev[EV_BARRIER_TIMEOUT], 1ull);
+            }
+            return;
+        }
+        __nanosleep(64);
+    }
+}
+
 // dynamic shared memory of a block: one switch scratch (with its staging area) per warp
 static size_t smem_bytes(int stage_cap, bool port_local) { return sw_shared_bytes(stage_cap, port_local) * WARPS_PER_BLOCK; }
 
 // the instantiation of a launch shape: several hosts per warp, one host per warp, one host per
-// warp with port-local switch egress
+// warp with port-local switch egress; each with the grid barrier or without (F_*: batches)
 enum
 {
     K_MANY,
     K_ONE,
     K_ONE_PL,
+    F_MANY,
+    F_ONE,
+    F_ONE_PL,
     K_N
 };
-static int kind_of(int host_lanes, bool port_local) { return host_lanes > 1 ? K_MANY : port_local ? K_ONE_PL : K_ONE; }
+static int kind_of(int host_lanes, bool port_local, bool free = false)
+{
+    return (host_lanes > 1 ? K_MANY : port_local ? K_ONE_PL : K_ONE) + (free ? F_MANY : 0);
+}
 static const void *kernel_of(int k)
 {
-    return k == K_MANY ? (const void *)slot_kernel<false, MIN_BLOCKS_MANY>
-                       : k == K_ONE ? (const void *)slot_kernel<false, MIN_BLOCKS_ONE> : (const void *)slot_kernel<true, MIN_BLOCKS_ONE>;
+    switch (k)
+    {
+    case K_MANY:
+        return (const void *)slot_kernel<false, MIN_BLOCKS_MANY>;
+    case K_ONE:
+        return (const void *)slot_kernel<false, MIN_BLOCKS_ONE>;
+    case K_ONE_PL:
+        return (const void *)slot_kernel<true, MIN_BLOCKS_ONE>;
+    case F_MANY:
+        return (const void *)free_kernel<false, MIN_BLOCKS_MANY>;
+    case F_ONE:
+        return (const void *)free_kernel<false, MIN_BLOCKS_ONE>;
+    default:
+        return (const void *)free_kernel<true, MIN_BLOCKS_ONE>;
+    }
 }
 
 static bool smem_attr(int k)
 {
-    static const bool ok[K_N] = {
-        cudaFuncSetAttribute(kernel_of(K_MANY), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes(SW_STAGE_MAX, false)) == cudaSuccess,
-        cudaFuncSetAttribute(kernel_of(K_ONE), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes(SW_STAGE_MAX, false)) == cudaSuccess,
-        cudaFuncSetAttribute(kernel_of(K_ONE_PL), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes(SW_STAGE_MAX, true)) == cudaSuccess};
+    static bool ok[K_N], tried[K_N];
+    if (!tried[k])
+    {
+        tried[k] = true;
+        const bool pl = k == K_ONE_PL || k == F_ONE_PL;
+        ok[k] = cudaFuncSetAttribute(kernel_of(k), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes(SW_STAGE_MAX, pl)) == cudaSuccess;
+    }
     return ok[k];
 }
 
 // The preferred shared-memory carveout, in percent of the SM's maximum: the shared memory of the
 // blocks a launch puts on one SM and no more, so that the rest of the SM's unified L1 / shared
 // memory is L1, where the units' records, ring heads and prefetched lines stay between slots.
-static int carveout[K_N] = {-1, -1, -1}; // the last ones set (-1: none)
+static int carveout[K_N] = {-1, -1, -1, -1, -1, -1}; // the last ones set (-1: none)
 static void set_carveout(int k, int pct)
 {
     if (pct != carveout[k] && cudaFuncSetAttribute(kernel_of(k), cudaFuncAttributePreferredSharedMemoryCarveout, pct) == cudaSuccess)
         carveout[k] = pct;
 }
 
-int slot_kernel_blocks_per_sm(int stage_cap, bool port_local, int host_lanes)
+int slot_kernel_blocks_per_sm(int stage_cap, bool port_local, int host_lanes, bool free)
 {
     int n = 0;
     port_local = port_local && host_lanes == 1;
-    const int k = kind_of(host_lanes, port_local);
+    const int k = kind_of(host_lanes, port_local, free);
     if (stage_cap < 1 || stage_cap > SW_STAGE_MAX || !smem_attr(k))
         return 0;
     set_carveout(k, 100); // (occupancy with all of the shared memory)
@@ -550,12 +707,9 @@ int slot_kernel_blocks_per_sm(int stage_cap, bool port_local, int host_lanes)
     return n;
 }
 
-int launch_slots(const Sim &s, int grid, int max_slots_per_launch, int host_lanes, int stage_cap, bool port_local, cudaStream_t stream)
+// a cooperative launch of kernel kind k (all its blocks resident: the waits need it)
+static int launch_kind(int k, void **args, int grid, int stage_cap, bool port_local, cudaStream_t stream)
 {
-    port_local = port_local && host_lanes == 1; // (several hosts per warp: the plain egress)
-    const int k = kind_of(host_lanes, port_local);
-    if (!smem_attr(k) || stage_cap < 1 || stage_cap > SW_STAGE_MAX)
-        return (int)cudaErrorInvalidValue;
     int dev = 0, sms = 1, max_smem = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -564,7 +718,6 @@ int launch_slots(const Sim &s, int grid, int max_slots_per_launch, int host_lane
     const size_t bytes = smem_bytes(stage_cap, port_local);
     const long long need = per_sm * (long long)(bytes + 2048); // (+ the block's reserved and static shared memory)
     set_carveout(k, (int)std::min<long long>(100, (need * 100 + max_smem - 1) / max_smem));
-    void *args[] = {(void *)&s, (void *)&max_slots_per_launch, (void *)&host_lanes, (void *)&stage_cap};
     cudaError_t e = cudaLaunchCooperativeKernel(kernel_of(k), dim3(grid), dim3(WARPS_PER_BLOCK * 32), args, bytes, stream);
     if (e == cudaErrorCooperativeLaunchTooLarge)
     {
@@ -576,16 +729,46 @@ int launch_slots(const Sim &s, int grid, int max_slots_per_launch, int host_lane
     return e == cudaSuccess ? 0 : (int)e;
 }
 
+int launch_slots(const Sim &s, int grid, int max_slots_per_launch, int host_lanes, int stage_cap, bool port_local, cudaStream_t stream)
+{
+    port_local = port_local && host_lanes == 1; // (several hosts per warp: the plain egress)
+    const int k = kind_of(host_lanes, port_local);
+    if (!smem_attr(k) || stage_cap < 1 || stage_cap > SW_STAGE_MAX)
+        return (int)cudaErrorInvalidValue;
+    void *args[] = {(void *)&s, (void *)&max_slots_per_launch, (void *)&host_lanes, (void *)&stage_cap};
+    return launch_kind(k, args, grid, stage_cap, port_local, stream);
+}
+
+int launch_free(const Sim &s, int grid, int slots_per_world, int host_lanes, int stage_cap, bool port_local, cudaStream_t stream)
+{
+    port_local = port_local && host_lanes == 1;
+    const int k = kind_of(host_lanes, port_local, true);
+    if (!smem_attr(k) || stage_cap < 1 || stage_cap > SW_STAGE_MAX || !s.unit_list || !s.unit_done || !s.w_units || slots_per_world < 1)
+        return (int)cudaErrorInvalidValue;
+    const int n = std::max(s.n_list, s.W);
+    free_open<<<(n + 255) / 256, 256, 0, stream>>>(s, (unsigned)slots_per_world);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return (int)e;
+    void *args[] = {(void *)&s, (void *)&host_lanes, (void *)&stage_cap};
+    return launch_kind(k, args, grid, stage_cap, port_local, stream);
+}
+
 // A launch as a CUDA graph: the launch is captured once per shape, slot count and unit list and
 // replayed as a graph; where capturing or instantiating fails, plain launches follow for good.
+// free: the batch kernel without a grid barrier (launch_free), with its opening kernel.
 int launch_slots_graph(SlotGraph &g, const Sim &s, int grid, int max_slots_per_launch, int host_lanes, int stage_cap, bool port_local,
-                       cudaStream_t stream)
+                       cudaStream_t stream, bool free)
 {
-    const unsigned long long key[8] = {(unsigned long long)grid, (unsigned long long)max_slots_per_launch, (unsigned long long)host_lanes,
+    const unsigned long long key[9] = {(unsigned long long)grid, (unsigned long long)max_slots_per_launch, (unsigned long long)host_lanes,
                                        (unsigned long long)stage_cap, (unsigned long long)port_local, (unsigned long long)(uintptr_t)s.unit_list,
-                                       (unsigned long long)s.n_list, (unsigned long long)s.max_slots};
+                                       (unsigned long long)s.n_list, (unsigned long long)s.max_slots, (unsigned long long)free};
+    auto go = [&]() {
+        return free ? launch_free(s, grid, max_slots_per_launch, host_lanes, stage_cap, port_local, stream)
+                    : launch_slots(s, grid, max_slots_per_launch, host_lanes, stage_cap, port_local, stream);
+    };
     if (g.broken)
-        return launch_slots(s, grid, max_slots_per_launch, host_lanes, stage_cap, port_local, stream);
+        return go();
     if (!g.exec || memcmp(key, g.key, sizeof key) != 0)
     {
         if (g.exec)
@@ -596,7 +779,7 @@ int launch_slots_graph(SlotGraph &g, const Sim &s, int grid, int max_slots_per_l
         int e = 1;
         if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess)
         {
-            e = launch_slots(s, grid, max_slots_per_launch, host_lanes, stage_cap, port_local, stream);
+            e = go();
             if (cudaStreamEndCapture(stream, &graph) != cudaSuccess)
                 e = 1;
         }
@@ -611,7 +794,7 @@ int launch_slots_graph(SlotGraph &g, const Sim &s, int grid, int max_slots_per_l
         {
             cudaGetLastError(); // (the failed capture's error)
             g.broken = true;
-            return launch_slots(s, grid, max_slots_per_launch, host_lanes, stage_cap, port_local, stream);
+            return go();
         }
     }
     g.replays++;

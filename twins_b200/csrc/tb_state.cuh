@@ -182,6 +182,11 @@ struct SlotCtl
 // entities run (INT64_MAX: all its messages are done); `act` / `prev` whether any of its entities
 // sent or held frames in this and the previous slot; `wake` the earliest global wake-up its hosts
 // reported in this slot.
+// A batch launch without a grid-wide barrier (free_kernel) keeps each world on a barrier of its
+// own: `run` is the slot its units run now (RUN_PARKED between launches), `arrive` how many of its
+// `units` (in the launch's unit list) have done it, `budget` the slots it may still run in this
+// launch, `last` the last slot it ran.
+constexpr int64_t RUN_PARKED = -1;
 struct WorldCtl
 {
     int64_t next;
@@ -190,6 +195,8 @@ struct WorldCtl
     unsigned fdone; // messages done
     unsigned pad;
     int64_t t0;
+    int64_t run, last;
+    unsigned arrive, units, budget, pad2;
 };
 
 // one enqueue at an egress queue, as the reference's --qtrace records it (src/model.h:313-320):
@@ -265,6 +272,10 @@ struct Sim
     // running, then host_units + switch; rebuilt between launches
     const int *unit_list;
     int n_list;
+    // the free-running batch kernel: per list entry the last slot its unit ran (reset each launch),
+    // per world its units in the list
+    int64_t *unit_done;
+    const unsigned *w_units;
     // the enqueue trace (trace build; null: off): records of enqueues with from <= time < until
     QRec *qtrace;
     unsigned long long *qtrace_cnt;
