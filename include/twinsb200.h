@@ -132,6 +132,27 @@ int tb_rdma_results(tb_ctx *ctx, int world, long long *start_ns, long long *fct_
  * reference's --q3cap, src/rdma/rmain.cu:1054, 1811); a frame that finds it full is counted as an
  * overflow (the run is then inexact). Before the first run. */
 int tb_rdma_set_queue_cap(tb_ctx *ctx, int frames);
+/* A transmission of an RDMA run as the reference's --txtrace records it (src/rdma/rdma.h TxRec,
+ * written by src/rdma/rmain.cu:2262-2282): its start (ns), the ns-3 node (hosts, then switches)
+ * and device (a host's NIC 1, switch port p + 1), the kind (0 data, 1 ACK, 2 NACK, 3 PAUSE, 4
+ * RESUME; "DANPR"), a / b the flow's hosts as the sender sees them (data: source, destination;
+ * ACK / NACK: destination, source; PFC: the queue, 0), the source port, sequence, bytes and ECN. */
+typedef struct tb_tx_record
+{
+    long long ts_ns;
+    int node, dev;
+    unsigned a, b, sport, seq;
+    unsigned short size;
+    unsigned char kind, ecn;
+} tb_tx_record;
+/* Before the first run of a context with ONE RDMA world: keep up to `cap` transmission records of
+ * frames that start in [from_ns, until_ns] (the reference's --txtrace=F --from=ns --until=ns; it
+ * refuses a batch too). cap 0 turns the trace off. */
+int tb_rdma_set_txtrace(tb_ctx *ctx, long long cap, long long from_ns, long long until_ns);
+/* After the run: the records sorted by (start, node, device), up to `cap` of them into `out`;
+ * *n the records written, *total the transmissions in the window (more than kept when the trace's
+ * cap was reached, as the reference's "txtrace: N records, M kept"). */
+int tb_rdma_txtrace(tb_ctx *ctx, tb_tx_record *out, long long cap, long long *n, long long *total);
 
 /* Builds the batch's device state (routes, connections, rings) and uploads it. Called by
  * tb_run when needed; separate so that timing can exclude it. Replaces src/main.cu:807-1015. */
@@ -184,7 +205,8 @@ int tb_set_autotune(tb_ctx *ctx, int on);
 int tb_set_free_batches(tb_ctx *ctx, int on);
 
 /* sizeof(tb_topology), sizeof(tb_tcp_params), sizeof(tb_stats), sizeof(tb_serve_caps),
- * sizeof(tb_request_info), sizeof(tb_serve_stats), sizeof(tb_qrec) in out[0..n-1], so that
+ * sizeof(tb_request_info), sizeof(tb_serve_stats), sizeof(tb_qrec), sizeof(tb_tx_record) in
+ * out[0..n-1], so that
  * bindings in other languages can check their struct layouts (no counterpart in the reference). */
 int tb_abi_sizes(unsigned long long *out, int n);
 

@@ -99,6 +99,40 @@ def test_cli_stop_time_exit_2(native_lib, tmp_path):
     assert all(full[i] == (s, f) and s + f < 100_000 for i, s, f in got)
 
 
+@pytest.mark.skipif(not REF_GPU.exists(), reason="the reference's GPU build (make -C oracle ref-rdma) is not here")
+@pytest.mark.parametrize("name,window", [("ft4_incast15_dcqcn_pfc", ""), ("ft4_uniform80_hpcc", ""), ("ls4x8_uniform120_dctcp", "200000:900000")])
+def test_txtrace_equals_reference(native_lib, name, window, tmp_path):
+    """--txtrace (with --from / --until) writes, line for line, the transmission trace the
+    reference's twins-rdma writes for the same world: every frame put on a link with its start,
+    node, device, kind, hosts, port, sequence, bytes and ECN bits (PFC frames included)."""
+    stage(tmp_path, name)
+    extra = []
+    if window:
+        a, b = window.split(":")
+        extra = [f"--from={a}", f"--until={b}"]
+    for binary, out in ((REF_GPU, "ref.tx"), (CLI, "ours.tx")):
+        r = subprocess.run([str(binary), f"{name}.cfg", f"--topo={name}.topo", f"--flows={name}.csv", f"--out={out}.fct", f"--txtrace={out}"]
+                           + extra, cwd=tmp_path, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-500:]
+    ref = (tmp_path / "ref.tx").read_text().splitlines()
+    ours = (tmp_path / "ours.tx").read_text().splitlines()
+    assert len(ref) > 100 and ours == ref
+    if window:
+        assert all(200000 <= int(l.split()[0]) <= 900000 for l in ours)
+    if name.endswith("_pfc"):
+        assert any(l.split()[3] in "PR" for l in ours)
+
+
+def test_txtrace_refuses_batch(native_lib, tmp_path):
+    """As the reference: --txtrace traces one world, so a --batch run with it is refused."""
+    name = "ft4_incast15_dcqcn"
+    stage(tmp_path, name)
+    (tmp_path / "jobs.txt").write_text(f"a {name}.topo {name}.csv\nb {name}.topo {name}.csv\n")
+    r = subprocess.run([str(CLI), f"{name}.cfg", "--batch=jobs.txt", "--outdir=.", "--txtrace=t.tx"], cwd=tmp_path, capture_output=True,
+                       text=True, timeout=600)
+    assert r.returncode == 1 and "one world" in r.stderr
+
+
 def case_flows(name):
     return next(c["flows"] for c in CASES if c["name"] == name)
 

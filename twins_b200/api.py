@@ -29,6 +29,10 @@ TB_ERR = {-1: "bad argument", -2: "CUDA error", -3: "HBM budget exceeded", -4: "
           -5: "device-side wait ran out"}
 TOPO_FATTREE, TOPO_LEAFSPINE, TOPO_GRAPH = 0, 1, 2
 TCP = {"newreno": 0, "dctcp": 1, "cubic": 2}
+# tb_tx_record (the reference's RDMA TxRec layout)
+TX_RECORD = np.dtype([("ts", "<i8"), ("node", "<i4"), ("dev", "<i4"), ("a", "<u4"), ("b", "<u4"), ("sport", "<u4"), ("seq", "<u4"),
+                      ("size", "<u2"), ("kind", "u1"), ("ecn", "u1")], align=True)
+assert TX_RECORD.itemsize == 40
 COUNTERS = ["drops", "marks", "retx", "rto", "undecided_ties", "host_events", "switch_events",
             "ovf_active", "ovf_due", "ovf_ring", "ovf_ooo", "ovf_tx", "barrier_timeouts"]
 
@@ -103,6 +107,8 @@ ENTRY_POINTS = [
                                          _P(ctypes.c_int)]),
     ("tb_rdma_results", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _P(ctypes.c_longlong), _P(ctypes.c_longlong)]),
     ("tb_rdma_set_queue_cap", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    ("tb_rdma_set_txtrace", ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong]),
+    ("tb_rdma_txtrace", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_longlong, _P(ctypes.c_longlong), _P(ctypes.c_longlong)]),
     ("tb_prepare", ctypes.c_int, [ctypes.c_void_p]),
     ("tb_reset", ctypes.c_int, [ctypes.c_void_p]),
     ("tb_run", ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
@@ -152,10 +158,10 @@ def load_library(path: Optional[os.PathLike] = None) -> ctypes.CDLL:
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    sizes = (ctypes.c_ulonglong * 7)()
-    lib.tb_abi_sizes(sizes, 7)
+    sizes = (ctypes.c_ulonglong * 8)()
+    lib.tb_abi_sizes(sizes, 8)
     want = [ctypes.sizeof(_Topology), ctypes.sizeof(_TcpParams), ctypes.sizeof(_Stats), ctypes.sizeof(_ServeCaps),
-            ctypes.sizeof(_RequestInfo), ctypes.sizeof(_ServeStats), ctypes.sizeof(_QRec)]
+            ctypes.sizeof(_RequestInfo), ctypes.sizeof(_ServeStats), ctypes.sizeof(_QRec), TX_RECORD.itemsize]
     if list(sizes) != want:
         raise RuntimeError(f"{p}: struct sizes {list(sizes)} differ from these bindings' {want}: rebuild")
     if path is None:
@@ -381,6 +387,21 @@ class Simulator:
     def set_rdma_queue_cap(self, frames: int) -> None:
         """Frames a switch port's data queue holds (the reference's --q3cap; before the first run)."""
         self._check(self.lib.tb_rdma_set_queue_cap(self.ctx, frames))
+
+    def set_rdma_txtrace(self, cap: int, from_ns: int = 0, until_ns: int = 1 << 62) -> None:
+        """Keep up to `cap` transmission records (the reference's --txtrace; one world, before the run)."""
+        self._check(self.lib.tb_rdma_set_txtrace(self.ctx, cap, from_ns, until_ns))
+
+    def rdma_txtrace(self) -> tuple[list[str], int]:
+        """The run's transmissions as the reference's --txtrace lines ("ns node dev kind src dst sport
+        seq bytes ecn", sorted by ns, node, dev), and how many there were in the window."""
+        n, total = ctypes.c_longlong(), ctypes.c_longlong()
+        self._check(self.lib.tb_rdma_txtrace(self.ctx, None, 0, ctypes.byref(n), ctypes.byref(total)))
+        rec = np.zeros(total.value, dtype=TX_RECORD)
+        self._check(self.lib.tb_rdma_txtrace(self.ctx, rec.ctypes.data_as(ctypes.c_void_p), len(rec), ctypes.byref(n), ctypes.byref(total)))
+        lines = [f"{r['ts']} {r['node']} {r['dev']} {'DANPR'[r['kind']]} {r['a']} {r['b']} {r['sport']} {r['seq']} {r['size']} {r['ecn']}"
+                 for r in rec[:n.value]]
+        return lines, total.value
 
     def rdma_results(self, world: int) -> tuple[np.ndarray, np.ndarray]:
         """(start_ns, fct_ns) per flow of an RDMA world; fct -1: not done."""

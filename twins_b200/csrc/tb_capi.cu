@@ -1086,6 +1086,28 @@ int tb_rdma_set_queue_cap(tb_ctx *ctx, int frames)
     return tr::rdma_set_queue_cap(ctx->rdma, frames) ? fail(TB_ERR_STATE, "set before the first run") : TB_OK;
 }
 
+static_assert(sizeof(tb_tx_record) == sizeof(tr::TxRec) && offsetof(tb_tx_record, seq) == offsetof(tr::TxRec, seq) &&
+                  offsetof(tb_tx_record, size) == offsetof(tr::TxRec, size) && offsetof(tb_tx_record, ecn) == offsetof(tr::TxRec, ecn),
+              "tb_tx_record is the device's TxRec");
+
+int tb_rdma_set_txtrace(tb_ctx *ctx, long long cap, long long from_ns, long long until_ns)
+{
+    if (!ctx || cap < 0 || until_ns < from_ns)
+        return fail(TB_ERR_ARG, "cap >= 0, from_ns <= until_ns");
+    if (!ctx->rdma)
+        ctx->rdma = tr::rdma_new(ctx->device < 0 ? 0 : ctx->device);
+    return tr::rdma_set_txtrace(ctx->rdma, cap, from_ns, until_ns) ? fail(TB_ERR_STATE, "set before the first run") : TB_OK;
+}
+
+int tb_rdma_txtrace(tb_ctx *ctx, tb_tx_record *out, long long cap, long long *n, long long *total)
+{
+    if (!ctx || !ctx->rdma)
+        return fail(TB_ERR_STATE, "no RDMA worlds");
+    if (cap < 0)
+        return fail(TB_ERR_ARG, "cap >= 0");
+    return tr::rdma_txtrace(ctx->rdma, out, cap, n, total) ? fail(TB_ERR_STATE, "not run yet") : TB_OK;
+}
+
 int tb_rdma_results(tb_ctx *ctx, int world, long long *start_ns, long long *fct_ns)
 {
     if (!ctx || !ctx->rdma)
@@ -1417,9 +1439,9 @@ int tb_hashes(tb_ctx *ctx, int world, unsigned *hash_data, unsigned *hash_ack)
 
 int tb_abi_sizes(unsigned long long *out, int n)
 {
-    const unsigned long long v[7] = {sizeof(tb_topology),     sizeof(tb_tcp_params),  sizeof(tb_stats), sizeof(tb_serve_caps),
-                                     sizeof(tb_request_info), sizeof(tb_serve_stats), sizeof(tb_qrec)};
-    for (int i = 0; i < n && i < 7; i++)
+    const unsigned long long v[8] = {sizeof(tb_topology),     sizeof(tb_tcp_params),  sizeof(tb_stats), sizeof(tb_serve_caps),
+                                     sizeof(tb_request_info), sizeof(tb_serve_stats), sizeof(tb_qrec),  sizeof(tb_tx_record)};
+    for (int i = 0; i < n && i < 8; i++)
         out[i] = v[i];
     return TB_OK;
 }

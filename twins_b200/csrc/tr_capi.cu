@@ -7,6 +7,7 @@
 #include "tr_kernel.h"
 #include "tr_layout.h"
 
+#include <algorithm>
 #include <chrono>
 #include <cstring>
 
@@ -58,6 +59,9 @@ struct RdmaRun
     bool prepared = false, ran = false;
     int tail_log2 = 0; // the tail ring's size (0: by the flows), doubled on a run that lost tails
     int q3_cap = 4096; // frames a switch port's data queue holds
+    long long tx_cap = 0, tx_from = 0, tx_until = 0; // the transmission trace (0: none)
+    std::vector<TxRec> tx;
+    unsigned long long tx_total = 0;
     int grid = 0;
     size_t smem = 0;
     cudaStream_t stream = nullptr;
@@ -109,13 +113,17 @@ struct RdmaRun
                   d.copy((int **)&x.start_list, l.start_list) && d.copy((uint32_t **)&x.root_rank, l.root_rank) && d.zeroed(&x.qp, l.F) &&
                   d.zeroed(&x.qc, l.F) && d.zeroed(&x.rx, l.F) && d.copy(&x.fct, minus1) && d.copy((LinkInfo **)&x.link, l.link) && d.copy((int32_t **)&x.txt, l.txt) &&
                   d.zeroed(&x.msg, l.n_frames) && d.copy(&x.msg_cnt, tags) && d.zeroed(&x.pend, (size_t)l.pend_n) &&
-                  d.zeroed(&x.tail, (size_t)1 << tl) && d.zeroed(&x.tail_cnt, 1) && d.zeroed(&x.ev, EV_N) && d.copy(&x.ctl, ctl);
+                  d.zeroed(&x.tail, (size_t)1 << tl) && d.zeroed(&x.tail_cnt, 1) && d.zeroed(&x.ev, EV_N) && d.copy(&x.ctl, ctl) &&
+                  (!tx_cap || (d.zeroed(&x.tx, (size_t)tx_cap) && d.zeroed(&x.tx_cnt, 1)));
         if (!ok)
         {
             *err = std::string("device memory for the RDMA run: ") + cudaGetErrorString(cudaGetLastError());
             d.release();
             return false;
         }
+        x.tx_cap = tx_cap;
+        x.tx_from = tx_from;
+        x.tx_until = tx_until;
         s = x;
         h2d = sizeof(RWorld) * l.world.size() + sizeof(HostInfo) * l.hinfo.size() + sizeof(Nic) * l.nic.size() +
               sizeof(SwInfo) * l.sinfo.size() + sizeof(SwState) * l.sw.size() + sizeof(PortInfo) * l.pinfo.size() +
@@ -156,6 +164,8 @@ int rdma_prepare(RdmaRun *r, std::string *err)
         return 0;
     if (r->worlds.empty())
         return *err = "no worlds", -4;
+    if (r->tx_cap && r->worlds.size() > 1)
+        return *err = "--txtrace traces one world (no --batch)", -1;
     if (cudaSetDevice(r->device) != cudaSuccess)
         return *err = "cudaSetDevice failed", -2;
     std::vector<const RdmaWorld *> wp;
@@ -235,6 +245,20 @@ int rdma_run(RdmaRun *r, long long max_slots, std::string *err)
         r->st.bytes_h2d = r->h2d;
         r->st.bytes_d2h = 8 * (size_t)r->L.F + 8 * EV_N + sizeof(RCtl) * r->st.launches;
         r->st.device_bytes = r->d.bytes;
+        r->tx.clear();
+        r->tx_total = 0;
+        if (s.tx)
+        {
+            if (cudaMemcpy(&r->tx_total, s.tx_cnt, sizeof r->tx_total, cudaMemcpyDeviceToHost) != cudaSuccess)
+                return *err = "cudaMemcpy failed", -2;
+            r->tx.resize((size_t)std::min<unsigned long long>(r->tx_total, (unsigned long long)r->tx_cap));
+            if (!r->tx.empty() && cudaMemcpy(r->tx.data(), s.tx, sizeof(TxRec) * r->tx.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
+                return *err = "cudaMemcpy failed", -2;
+            std::sort(r->tx.begin(), r->tx.end(), [](const TxRec &a, const TxRec &b) {
+                return a.ts != b.ts ? a.ts < b.ts : a.node != b.node ? a.node < b.node : a.dev < b.dev;
+            });
+            r->st.bytes_d2h += sizeof(TxRec) * r->tx.size();
+        }
         r->ran = true;
         if (ctl.error)
             return *err = "a device-side barrier wait ran out; the run was abandoned", -5;
@@ -284,6 +308,30 @@ int rdma_stats(RdmaRun *r, RStats *out)
 {
     *out = r->st;
     return r->ran ? 0 : -4;
+}
+
+int rdma_set_txtrace(RdmaRun *r, long long cap, long long from_ns, long long until_ns)
+{
+    if (r->prepared || cap < 0 || until_ns < from_ns)
+        return -1;
+    r->tx_cap = cap;
+    r->tx_from = from_ns;
+    r->tx_until = until_ns;
+    return 0;
+}
+
+int rdma_txtrace(RdmaRun *r, void *out, long long cap, long long *n, long long *total)
+{
+    if (!r->ran)
+        return -4;
+    const size_t k = (size_t)std::max(0LL, std::min<long long>(cap, (long long)r->tx.size()));
+    if (k && out)
+        memcpy(out, r->tx.data(), sizeof(TxRec) * k);
+    if (n)
+        *n = (long long)k;
+    if (total)
+        *total = (long long)r->tx_total;
+    return 0;
 }
 
 int rdma_world_flows(RdmaRun *r, int world) { return world >= 0 && world < (int)r->worlds.size() ? (int)r->worlds[world].flows.size() : -1; }

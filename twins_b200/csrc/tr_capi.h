@@ -31,5 +31,9 @@ int rdma_run(RdmaRun *r, long long max_slots, std::string *err);
 int rdma_results(RdmaRun *r, int world, long long *start_ns, long long *fct_ns);
 int rdma_counters(RdmaRun *r, unsigned long long *out, int n);
 int rdma_stats(RdmaRun *r, RStats *out);
+// the transmission trace: set before the first run (one world); read after it (records of the
+// reference's TxRec layout, sorted by start, node, device)
+int rdma_set_txtrace(RdmaRun *r, long long cap, long long from_ns, long long until_ns);
+int rdma_txtrace(RdmaRun *r, void *out, long long cap, long long *n, long long *total);
 
 } // namespace tr

@@ -288,7 +288,49 @@ struct RSim
     unsigned long long *ev;
     RCtl *ctl;
     int serial_only; // switches run every slot's events in one order (no safe slots)
+    // the transmission trace (one world): a record per frame put on a link in [tx_from, tx_until]
+    struct TxRec *tx;
+    unsigned long long *tx_cnt, tx_cap;
+    int64_t tx_from, tx_until;
 };
+
+// a transmission as the reference's --txtrace records it (src/rdma/rdma.h TxRec): its start (ns),
+// the ns-3 node (hosts, then switches) and device (port + 1), the kind, the flow's source and
+// destination hosts as the frame's sender sees them (data: src, dst; ACK / NACK: dst, src; PFC:
+// the queue, 0), its port, sequence, bytes and ECN bits
+struct TxRec
+{
+    int64_t ts;
+    int32_t node, dev;
+    uint32_t a, b, sport, seq;
+    uint16_t size;
+    uint8_t kind, ecn;
+};
+
+TR_HD void trace_tx(const RSim &s, int64_t now, int node, int port, const Pkt &p)
+{
+    if (!s.tx || now < s.tx_from || now > s.tx_until)
+        return;
+#ifdef __CUDA_ARCH__
+    const unsigned long long i = atomicAdd(s.tx_cnt, 1ull);
+#else
+    const unsigned long long i = (*s.tx_cnt)++;
+#endif
+    if (i >= s.tx_cap)
+        return;
+    TxRec &r = s.tx[i];
+    r.ts = now;
+    r.node = node;
+    r.dev = port + 1;
+    r.kind = p.kind;
+    r.size = p.size;
+    r.ecn = p.ecn;
+    const bool pfc = p.kind == K_PAUSE || p.kind == K_RESUME, data = p.kind == K_DATA;
+    r.a = pfc ? p.q : data ? p.src : p.dst;
+    r.b = pfc ? 0 : data ? p.dst : p.src;
+    r.sport = pfc ? 0 : p.sport;
+    r.seq = pfc ? 0 : p.seq;
+}
 
 // ------------------------------------------------------------------ memory shared between entities
 // Frames, bucket tags and tail nodes are written by other entities (other SMs) in earlier slots:
@@ -738,6 +780,7 @@ TR_HD void h_transmit(HostEv &e, Pkt p)
     f->ts = ts;
     f->c = e.cur;
     f->p = p;
+    trace_tx(s, e.now, e.h, 0, p);
 }
 
 TR_HD void h_next_send(HostEv &e, int64_t at)
@@ -1267,6 +1310,7 @@ TR_HD void s_transmit(SwEv &e, int port, Pkt p)
     f->ts = ts;
     f->c = e.cur;
     f->p = p;
+    trace_tx(s, e.now, s.H + e.x, port, p);
 }
 
 TR_HD void s_enqueue(SwEv &e, int port, int q, const Pkt &p)

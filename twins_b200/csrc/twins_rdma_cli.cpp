@@ -1,7 +1,7 @@
 // twins-rdma: the reference's RDMA command line (src/rdma/rmain.cu:1-42, 1023-1240) over the
 // twins-b200 C ABI.
 //   twins-rdma CONFIG --topo=F --flows=F [--out=fct.txt] [--rate=100Gbps] [--delay=1000] [--q3cap=4096]
-//              [KEY=VALUE ...]
+//              [--txtrace=F [--from=ns] [--until=ns] [--txcap=N]] [KEY=VALUE ...]
 //   twins-rdma CONFIG --batch=JOBFILE --outdir=DIR [--path=DIR:DIR...] [options] [KEY=VALUE ...]
 // CONFIG: an HPCC config file ("KEY v1 v2 ..." per line); KEY=VALUE (KEY=V1,V2,.. for several
 // values) overrides it. A job file's lines "name topo flows [KEY=VALUE ...]" are worlds of one batch
@@ -12,10 +12,16 @@
 // and the counters line, as the reference prints them. Exit status: 0 every flow done; 2 some
 // unfinished at the stop time; 3 an error counter (an overflow: the results are not exact); 1 a
 // usage, input or device error.
+// --txtrace: every transmission starting in [--from, --until] (ns), one per line "ns node dev kind
+// src dst sport seq bytes ecn" sorted by (ns, node, dev), kind one of D A N P R (the reference's
+// format, src/rdma/rmain.cu:2262-2282; one world only). --txcap: records kept (default 64 Mi, as
+// the reference keeps).
 // --q3cap: frames a switch port's data queue holds (an overflow is reported, exit 3). The reference's
 // launch-shape options (--win, --gwin, --rank*, --persist, --spread, --serial, --tail, --dcap) change
 // no result; they are accepted and have no effect here.
+#include <algorithm>
 #include <chrono>
+#include <climits>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -149,8 +155,8 @@ int main(int argc, char **argv)
         fprintf(stderr, "cannot open %s\n", argv[1]);
         return 1;
     }
-    std::string topo_file, flow_file, out_file = "fct.txt", batch_file, out_dir = ".", data_dirs, rate_s = "100Gbps";
-    long long delay = 1000;
+    std::string topo_file, flow_file, out_file = "fct.txt", batch_file, out_dir = ".", data_dirs, rate_s = "100Gbps", tx_file;
+    long long delay = 1000, tx_from = 0, tx_until = LLONG_MAX, tx_cap = 64ll << 20;
     int device = 0, q3cap = 4096;
     for (int i = 2; i < argc; i++)
     {
@@ -177,6 +183,14 @@ int main(int argc, char **argv)
             device = atoi(v.c_str());
         else if (k == "--q3cap")
             q3cap = atoi(v.c_str());
+        else if (k == "--txtrace")
+            tx_file = v;
+        else if (k == "--from")
+            tx_from = atoll(v.c_str());
+        else if (k == "--until")
+            tx_until = atoll(v.c_str());
+        else if (k == "--txcap")
+            tx_cap = atoll(v.c_str());
         else if (k == "--win" || k == "--gwin" || k == "--rank" || k == "--rank-join" || k == "--rank-bs" || k == "--rank-every" ||
                  k == "--persist" || k == "--spread" || k == "--serial" || k == "--tail" || k == "--tail-auto" || k == "--dcap")
             continue; // (launch shapes and capacities of the reference's kernels: no result depends on them)
@@ -255,6 +269,19 @@ int main(int argc, char **argv)
         fprintf(stderr, "%s\n", tb_last_error());
         return 1;
     }
+    if (!tx_file.empty())
+    {
+        if (!batch_file.empty())
+        {
+            fprintf(stderr, "--txtrace traces one world (no --batch)\n");
+            return 1;
+        }
+        if (tb_rdma_set_txtrace(ctx, tx_cap, tx_from, tx_until))
+        {
+            fprintf(stderr, "%s\n", tb_last_error());
+            return 1;
+        }
+    }
     std::vector<Flows> flows(jobs.size());
     int F = 0;
     for (size_t i = 0; i < jobs.size(); i++)
@@ -319,6 +346,29 @@ int main(int argc, char **argv)
     printf("drops %llu marks %llu pauses %llu resumes %llu nacks %llu | undecided ties %llu, on lost tails %llu | overflows: tx %llu queue "
            "%llu ackq %llu qps %llu due %llu | acks for done QPs %llu\n",
            ev[0], ev[1], ev[2], ev[3], ev[11], ev[8], ev[9], ev[4], ev[5], ev[6], ev[7], ev[12], ev[10]);
+    if (!tx_file.empty())
+    {
+        long long n = 0, total = 0;
+        tb_rdma_txtrace(ctx, nullptr, 0, &n, &total);
+        std::vector<tb_tx_record> rec((size_t)std::min(total, tx_cap));
+        tb_rdma_txtrace(ctx, rec.data(), (long long)rec.size(), &n, &total);
+        if (total > (long long)rec.size())
+            fprintf(stderr, "txtrace: %lld records, %zu kept\n", total, rec.size());
+        FILE *ft = fopen(tx_file.c_str(), "w");
+        if (!ft)
+        {
+            fprintf(stderr, "cannot write %s\n", tx_file.c_str());
+            return 1;
+        }
+        const char kinds[] = "DANPR";
+        for (long long i = 0; i < n; i++)
+        {
+            const tb_tx_record &x = rec[(size_t)i];
+            fprintf(ft, "%lld %d %d %c %u %u %u %u %u %u\n", x.ts_ns, x.node, x.dev, x.kind < 5 ? kinds[x.kind] : '?', x.a, x.b, x.sport, x.seq,
+                    (unsigned)x.size, (unsigned)x.ecn);
+        }
+        fclose(ft);
+    }
     const bool bad = ev[4] || ev[5] || ev[6] || ev[7] || ev[12];
     if (bad)
         fprintf(stderr, "warning: capacity overflow, results are not exact\n");
