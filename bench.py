@@ -30,6 +30,8 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import re
+import shutil
 import statistics
 import subprocess
 import tempfile
@@ -330,7 +332,7 @@ def c4_leg(device: int, plain_n: int, warmup: int, warmup_slots: int):
             "batched_over_plain": plain["batched_over_plain_worlds_per_s"]}
 
 
-def sweep_leg(device: int):
+def sweep_leg(device: int, ref_gpu: bool = True):
     """The reference's k=8 parameter sweep (138 ecnK x queue x TCP configurations of FatTree k=8,
     its data/ns3/sweep_k8 golden set, fixtures under tests/golden/sweep) as one batch of worlds, as
     its bench/sweep.py runs it (worlds with undecided ties again on the 25-run chain build, time
@@ -365,11 +367,55 @@ def sweep_leg(device: int):
         n = c["rows"]
         equal += int((est == z["est"][at:at + n]).all() and (done == z["done"][at:at + n]).all())
         at += n
+    ref = None
+    if ref_gpu:
+        try:
+            ref = sweep_reference_gpu(index, z, g)
+        except Exception as e:
+            ref = {"error": str(e)[:200]}
     return {"config": "FatTree k=8 sweep: 138 configurations (k8_a2a30, k8_a2a50w flows) in one batch",
             "worlds_per_s": len(index) / (ms / 1000.0), "seconds": ms / 1000.0, "rerun_25_runs": len(redo),
-            "identical_to_ns3": f"{equal}/{len(index)}",
+            "identical_to_ns3": f"{equal}/{len(index)}", "reference_gpu": ref,
             "published": {"rtx5090_1x138_worlds_per_s": 52.3, "rx9060xt_2x69_worlds_per_s": 22.3,
                           "source": "reference docs/nvidia.md:126, README.md:257"}}
+
+
+def sweep_reference_gpu(index, z, g: Path):
+    """The reference's CUDA build on the same 138 configurations as one --worlds batch, as its
+    bench/sweep.py runs a batch (worlds with undecided ties again on its twins128 build, time
+    included), timed by its "Simulation Duration" lines; every configuration compared with ns-3."""
+    binary, long_binary = ROOT / "oracle" / "_ref" / "twins", ROOT / "oracle" / "_ref" / "twins128"
+    if not binary.exists():
+        return None
+    d = Path(tempfile.mkdtemp(prefix="sweep_ref_"))
+    lines = [f"flows={g / c['flows']},tcp={c['tcp']},queue={c['queue']},ecnK={c['ecn_k']},out={d / (c['name'] + '.csv')}" for c in index]
+
+    def run(b, ls, name):
+        wf = d / name
+        wf.write_text("\n".join(ls) + "\n")
+        r = subprocess.run([str(b), "--k=8", f"--worlds={wf}"], capture_output=True, text=True, timeout=1800)
+        if r.returncode != 0:
+            raise RuntimeError(r.stderr.strip()[-200:])
+        secs = sum(float(l.split(":")[1].strip().rstrip("s")) for l in r.stdout.splitlines() if l.startswith("Simulation Duration:"))
+        return r, secs
+
+    r, secs = run(binary, lines, "worlds.txt")
+    reruns = 0
+    if "undecided" in r.stderr and long_binary.exists():
+        m = re.search(r"undecided-ties by world:([ 0-9]*)", r.stdout)
+        redo = [lines[int(w)] for w in m.group(1).split()] if m else lines
+        reruns = len(redo)
+        _, s2 = run(long_binary, redo, "worlds_long.txt")
+        secs += s2
+    equal, at = 0, 0
+    for c in index:
+        n = c["rows"]
+        est, done = read_fct(d / (c["name"] + ".csv"))
+        equal += int((est == z["est"][at:at + n]).all() and (done == z["done"][at:at + n]).all())
+        at += n
+    shutil.rmtree(d, ignore_errors=True)
+    return {"seconds": secs, "worlds_per_s": len(index) / secs, "rerun_twins128": reruns, "identical_to_ns3": f"{equal}/{len(index)}",
+            "binary": "oracle/_ref/twins --k=8 --worlds (reference src/main.cu, nvcc sm_100a), one batch of 138"}
 
 
 def serve_leg(device: int, requests: int, rate: float, serve_worlds: int):
@@ -601,7 +647,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c2s", "c3", "c4", "c5"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c2s", "c3", "c4", "c4s", "c5"])
     ap.add_argument("--requests", type=int, default=200, help="C5: requests in the served stream")
     ap.add_argument("--rate", type=float, default=100.0, help="C5: request arrivals per second (Poisson)")
     ap.add_argument("--serve-worlds", type=int, default=256, help="C5: requests the server holds at once")
@@ -645,6 +691,7 @@ def main():
                            "c2": "FatTree k=8, 10,000 flows x {NewReno, DCTCP, Cubic}, FIN, spraying (C2)",
                            "c2s": "FatTree k=8, 1,500 flows x {NewReno, DCTCP, Cubic}, FIN, spraying (C2 shape, small)",
                            "c4": "256 leaf-spine worlds, 1k-20k flows each (C4)",
+                           "c4s": "32 leaf-spine worlds, 500-3,000 flows each (C4 shape, small)",
                            "c5": "200 served-stream requests (C5 shape, TCP) as worlds"}[args.workload],
               "worlds": len(worlds), "flows_per_step": int(sum(len(w.flows) for w in worlds)),
               "l2": "flushed between steps (256 MiB write); state restored device-to-device before each step",
@@ -750,7 +797,7 @@ def main():
     if args.workload == "c2" and not args.no_extras and world_size == 1:
         extras["c4"] = c4_leg(local_rank, args.plain_sample, 3, 200)
         extras["c5"] = serve_leg(local_rank, args.requests, args.rate, args.serve_worlds)
-        extras["sweep_k8"] = sweep_leg(local_rank)
+        extras["sweep_k8"] = sweep_leg(local_rank, not args.no_ref_gpu)
         extras["c3"] = c3_leg(local_rank)
         extras["rdma_sweep_k8"] = rdma_sweep_leg(local_rank)
     elif args.workload == "c4":

@@ -138,7 +138,12 @@ def c2_small(seed: int = 1, tcps=("newreno", "dctcp", "cubic")) -> list[World]:
     return [World(f"c2s_k8_{t}", topo, flows, TcpParams(t, 30, 200, fin=True, spray=True, rng_seed=1, rng_run=1)) for t in tcps]
 
 
-WORKLOADS = {"c1": c1, "c2": c2, "c2s": c2_small, "c4": c4}
+def c4_small(seed: int = 1) -> list[World]:
+    """C4's shape at a profiler's size: 32 leaf-spine worlds of 500-3,000 flows."""
+    return c4(seed, n_worlds=32, min_flows=500, max_flows=3000)
+
+
+WORKLOADS = {"c1": c1, "c2": c2, "c2s": c2_small, "c4": c4, "c4s": c4_small}
 
 
 # ------------------------------------------------------------------ served stream (C5 shape)
