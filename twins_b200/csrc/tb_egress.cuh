@@ -159,17 +159,18 @@ struct Transmitter
                 ovf++;
                 return;
             }
+            const int64_t t1 = t0 + (int64_t)f.len * PS_PER_BYTE; // (its end, read before the stores below)
+            const bool behind = busy_until >= f.ts && busy_until > began;
             Frame o;
             frame_copy(&o, &f);
-            const bool behind = busy_until >= f.ts && busy_until > began;
             if (behind)
                 chain_child(o.ch, *tx_chain, code_tc((int)((busy_until - began) / PS_PER_BYTE)));
             else
                 idle_began = t0;
             *tx_chain = o.ch;
             began = t0;
-            busy_until = t0 + (int64_t)f.len * PS_PER_BYTE;
-            o.ts = busy_until + PROP_PS;
+            busy_until = t1;
+            o.ts = t1 + PROP_PS;
             frame_store_link(&msg[n_out++], o);
             head = head + 1 == cap ? 0 : head + 1;
         }

@@ -62,7 +62,7 @@ struct SndRec
     uint32_t tail, una, nxt, high;
     uint32_t cwnd, ssthresh, dupacks;
     uint32_t it_head, it_n, h_head, h_n;
-    uint32_t sack_b, lost_b, rtx_b, cand_b, sack_n, hisack; // the sent list's byte counters, sacked items, highest sack
+    uint32_t sack_b, lost_b, rtx_b, cand_b, sack_n, cand_lo, hisack; // the sent list's byte counters, sacked items, first-candidate bound, highest sack
     uint8_t sack_seen, recover_active, first_partial, cwnd_limited;
     uint32_t recover, cwnd_cnt, ack_rem;
     // TcpCubic

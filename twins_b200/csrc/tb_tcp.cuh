@@ -113,7 +113,9 @@ TB_D void rcv_ack(HostCtx &c, int f, RcvRec &R, uint32_t ack, AckEcho echo, int6
 // writes its three bits. (The ring's capacity is a multiple of 8 and its offset too, so the words
 // are aligned.) Beside ns-3's three byte counters the list counts the candidates' bytes (lost,
 // neither retransmitted nor sacked), which tells in O(1) that there is none, and the sacked items,
-// where the Reno emulation's next SACK starts looking.
+// where the Reno emulation's next SACK starts looking. `cand_lo` is a lower bound on the first
+// candidate's index (where the search for it starts): lowered where an item becomes a candidate,
+// moved with the items when some leave the front or two join, raised to what a search finds.
 enum : uint8_t
 {
     FL_LOST = 1,
@@ -183,7 +185,66 @@ struct SentList
         adjust(S.cand_b, candidate(was), candidate(f));
         if ((was ^ f) & FL_SACK)
             S.sack_n += (f & FL_SACK) ? 1u : ~0u;
+        if (candidate(f) && i < S.cand_lo)
+            S.cand_lo = i;
         write_at(p, f);
+    }
+
+    TB_D uint32_t next_word(uint32_t w) const { return w + 1 == cap >> 3 ? 0 : w + 1; }
+    // the flags of positions pos(i) .. pos(n - 1) move up a place (to pos(n)), word by word: each
+    // plane byte shifts left, its top bit carried into the next word's bottom; positions below
+    // pos(i) in its word and above pos(n) in its word keep theirs (the head of a nearly full ring)
+    TB_D void flags_up(uint32_t i)
+    {
+        const uint32_t p0 = pos(i), pe = pos(S.it_n);
+        uint32_t words = ((p0 & 7) + (S.it_n - i)) / 8 + 1; // (the words spanned by pos(i) .. pos(n))
+        uint32_t w = p0 >> 3, carry = 0;
+        for (bool first = true;; first = false)
+        {
+            const uint32_t x = fw[w];
+            uint32_t y = ((x << 1) & 0xFEFEFEu) | carry;
+            carry = (x >> 7) & 0x010101u;
+            if (first)
+            {
+                const uint32_t keep = ((1u << (p0 & 7)) - 1) * 0x010101u;
+                y = (x & keep) | (y & ~keep);
+            }
+            if (--words == 0)
+            {
+                const uint32_t mine = ((2u << (pe & 7)) - 1) * 0x010101u;
+                fw[w] = (y & mine) | (x & ~mine);
+                return;
+            }
+            fw[w] = y;
+            w = next_word(w);
+        }
+    }
+    // the flags of positions pos(i + 1) .. pos(n - 1) move down a place (to pos(i)), word by word
+    // (the reverse of flags_up; pos(n - 1) is left with a stale copy)
+    TB_D void flags_down(uint32_t i)
+    {
+        const uint32_t p0 = pos(i), pe = pos(S.it_n - 1);
+        uint32_t words = ((p0 & 7) + (S.it_n - 1 - i)) / 8 + 1; // (the words spanned by pos(i) .. pos(n - 1))
+        uint32_t w = p0 >> 3;
+        for (bool first = true;; first = false)
+        {
+            const uint32_t x = fw[w];
+            const uint32_t nx = words == 1 ? 0u : fw[next_word(w)];
+            uint32_t y = ((x >> 1) & 0x7F7F7Fu) | ((nx & 0x010101u) << 7);
+            if (first)
+            {
+                const uint32_t keep = ((1u << (p0 & 7)) - 1) * 0x010101u;
+                y = (x & keep) | (y & ~keep);
+            }
+            if (--words == 0)
+            {
+                const uint32_t mine = ((2u << (pe & 7)) - 1) * 0x010101u;
+                fw[w] = (y & mine) | (x & ~mine);
+                return;
+            }
+            fw[w] = y;
+            w = next_word(w);
+        }
     }
 
     // a new item at index i, the ones from i moving up a place (new data at the end, or the second
@@ -195,15 +256,21 @@ struct SentList
             ovf++;
             return false;
         }
-        for (uint32_t j = S.it_n; j > i; j--)
+        if (i < S.it_n)
         {
-            const uint32_t to = pos(j), from = pos(j - 1);
-            start[to] = start[from];
-            write_at(to, flags_at(from));
+            for (uint32_t j = S.it_n; j > i; j--)
+                start[pos(j)] = start[pos(j - 1)];
+            flags_up(i);
         }
-        start[pos(i)] = seq;
-        write_at(pos(i), f);
+        const uint32_t p = pos(i);
+        start[p] = seq;
+        if (i == S.it_n && !(p & 7) && S.it_n + 8 <= cap)
+            fw[p >> 3] = spread(f); // (an append opening a word whose other positions are all free: no read)
+        else
+            write_at(p, f);
         S.sack_n += (f & FL_SACK) ? 1u : 0u;
+        if (candidate(f) && i < S.cand_lo)
+            S.cand_lo = i;
         S.it_n++;
         return true;
     }
@@ -215,11 +282,13 @@ struct SentList
         const uint32_t lb = end(i) - beg(i);
         S.cand_b += (candidate(a) ? lb : 0u) - (candidate(b) ? lb : 0u);
         S.sack_n -= (b & FL_SACK) ? 1u : 0u;
-        for (uint32_t j = i; j + 1 < S.it_n; j++)
+        if (S.cand_lo >= i)
+            S.cand_lo--; // (the items from i move down a place)
+        if (i + 1 < S.it_n)
         {
-            const uint32_t to = pos(j), from = pos(j + 1);
-            start[to] = start[from];
-            write_at(to, flags_at(from));
+            for (uint32_t j = i; j + 1 < S.it_n; j++)
+                start[pos(j)] = start[pos(j + 1)];
+            flags_down(i);
         }
         S.it_n--;
     }
@@ -292,10 +361,16 @@ TB_D void head_to_lost(SentList &L)
 TB_D void everything_lost(SentList &L)
 {
     SndRec &S = L.S;
-    for (uint32_t i = 0; i < S.it_n; i++)
-        L.write_at(L.pos(i), FL_LOST);
+    // whole words: every position of a word holding a live item reads lost, neither retransmitted
+    // nor sacked (its free positions too, which no read reaches before they are written)
+    for (uint32_t i = 0; i < S.it_n;)
+    {
+        const uint32_t p = L.pos(i);
+        L.fw[p >> 3] = 0xFFu;
+        i += 8 - (p & 7);
+    }
     S.lost_b = S.cand_b = sent_bytes(S);
-    S.sack_b = S.rtx_b = S.sack_n = 0;
+    S.sack_b = S.rtx_b = S.sack_n = S.cand_lo = 0;
     S.sack_seen = 0;
     S.hisack = 0;
 }
@@ -307,7 +382,7 @@ TB_D void everything_lost(SentList &L)
 TB_D uint32_t ack_drop(SentList &L, uint32_t ack)
 {
     SndRec &S = L.S;
-    uint32_t gone = 0;
+    uint32_t gone = 0, left = 0;
     while (S.it_n)
     {
         const uint32_t b = L.beg(0), e = L.end(0);
@@ -331,9 +406,11 @@ TB_D uint32_t ack_drop(SentList &L, uint32_t ack)
         }
         L.mark(0, 0);
         gone += e - b;
+        left++;
         S.it_head = L.pos(1);
         S.it_n--;
     }
+    S.cand_lo = S.cand_lo > left ? S.cand_lo - left : 0;
     S.una = ack;
     if (S.it_n && (L.flags(0) & FL_SACK))
     {
@@ -354,7 +431,9 @@ TB_D uint32_t ack_drop(SentList &L, uint32_t ack)
 TB_D bool next_to_send(const SentList &L, uint32_t *seq)
 {
     const SndRec &S = L.S;
-    const uint32_t i = S.cand_b ? L.find(0, candidates) : L.n();
+    const uint32_t i = S.cand_b ? L.find(S.cand_lo, candidates) : L.n();
+    if (i < L.n())
+        L.S.cand_lo = i;
     if (i < L.n() && (!S.sack_seen || L.beg(i) < S.hisack))
     {
         *seq = L.beg(i);
@@ -1174,24 +1253,39 @@ TB_D bool rx_add(const Sim &s, RcvRec &R, uint32_t seq, uint32_t end, unsigned &
         return x >= cap ? x - cap : x;
     };
     // blocks [lo, hi) overlap or touch [from, end): lo = the first ending at or after `from`,
-    // hi = the first starting after `end`
-    uint32_t lo = 0;
-    for (uint32_t b = n; lo < b;)
+    // hi = the first starting after `end`; the common cases in O(1): bytes beyond every block (an
+    // out-of-order arrival after the last), or short of the first block (in order, a gap ahead)
+    uint32_t lo = n, hi = n;
+    if (n && be[at(n - 1)] >= from)
     {
-        const uint32_t m = (lo + b) >> 1;
-        if (be[at(m)] < from)
-            lo = m + 1;
-        else
-            b = m;
-    }
-    uint32_t hi = lo;
-    for (uint32_t b = n; hi < b;)
-    {
-        const uint32_t m = (hi + b) >> 1;
-        if (bs[at(m)] <= end)
-            hi = m + 1;
-        else
-            b = m;
+        lo = 0;
+        if (be[at(0)] < from)
+        {
+            uint32_t a = 1, b = n - 1; // (the answer lies in [1, n - 1]: the last block qualifies)
+            while (a < b)
+            {
+                const uint32_t m = (a + b) >> 1;
+                if (be[at(m)] < from)
+                    a = m + 1;
+                else
+                    b = m;
+            }
+            lo = a;
+        }
+        hi = lo;
+        if (bs[at(lo)] <= end)
+        {
+            uint32_t a = lo + 1, b = n;
+            while (a < b)
+            {
+                const uint32_t m = (a + b) >> 1;
+                if (bs[at(m)] <= end)
+                    a = m + 1;
+                else
+                    b = m;
+            }
+            hi = a;
+        }
     }
     if (lo < n && bs[at(lo)] <= from && be[at(lo)] >= end)
         return false; // (held already)
