@@ -124,6 +124,14 @@ struct RdmaRun
         x.tx_cap = tx_cap;
         x.tx_from = tx_from;
         x.tx_until = tx_until;
+        // (the zeroing and copies above run on the legacy default stream, which the run's own
+        // non-blocking stream does not wait for: all of it must be done before the first launch)
+        if (cudaDeviceSynchronize() != cudaSuccess)
+        {
+            *err = std::string("device memory for the RDMA run: ") + cudaGetErrorString(cudaGetLastError());
+            d.release();
+            return false;
+        }
         s = x;
         h2d = sizeof(RWorld) * l.world.size() + sizeof(HostInfo) * l.hinfo.size() + sizeof(Nic) * l.nic.size() +
               sizeof(SwInfo) * l.sinfo.size() + sizeof(SwState) * l.sw.size() + sizeof(PortInfo) * l.pinfo.size() +
