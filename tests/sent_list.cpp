@@ -1,8 +1,8 @@
 // A randomized check of the TCP sent list (twins_b200/csrc/tb_tcp.cuh: SentList, its flag words
 // of eight positions and the word-wise shifts of open / join_previous), built with g++ for the host
 // by tests/test_sent_list.py. Random opens, joins, flag changes and whole-list losses on rings of
-// every capacity class, with the head anywhere (so that shifts wrap), are mirrored on a plain
-// per-item model; after every step each item's flags, the byte counters (lost, retransmitted,
+// every capacity class, with the head anywhere (so that shifts wrap), and ACKs that drop and cut
+// items are mirrored on a plain per-item model; after every step each item's flags, the byte counters (lost, retransmitted,
 // sacked, candidates), the sacked-item count and the candidate search bound must agree with it.
 // Exit status 0: all agree.
 #include <cstdint>
@@ -123,6 +123,26 @@ int main()
                 const uint8_t f = (uint8_t)(g() % 8);
                 L.mark(i, f);
                 m[i].f = f;
+            }
+            else if (k == 9 && S.it_n && (g() & 1))
+            {
+                // an ACK: the items below it leave, an item it falls inside is cut there (an ACK
+                // leaving a sacked item first is left out: the Reno emulation's follow-up is not modelled)
+                const uint32_t ack = m[0].start + g() % (high - m[0].start + 1);
+                size_t j = 0;
+                while (j < m.size() && (j + 1 < m.size() ? m[j + 1].start : high) <= ack)
+                    j++;
+                if (j < m.size() && (m[j].f & FL_SACK))
+                    continue;
+                const uint32_t gone = j < m.size() ? (m[j].start < ack ? m[j].start : ack) - m[0].start : high - m[0].start;
+                m.erase(m.begin(), m.begin() + j);
+                if (!m.empty() && m[0].start < ack)
+                    m[0].start = ack;
+                if (ack_drop(L, ack) != gone)
+                {
+                    printf("trial %d op %d: ack %u returned bytes differ from %u\n", trial, op, ack, gone);
+                    return 1;
+                }
             }
             else if (S.it_n)
             {

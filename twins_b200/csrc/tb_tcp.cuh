@@ -382,34 +382,40 @@ TB_D void everything_lost(SentList &L)
 TB_D uint32_t ack_drop(SentList &L, uint32_t ack)
 {
     SndRec &S = L.S;
-    uint32_t gone = 0, left = 0;
-    while (S.it_n)
+    // (the walk keeps the head, the count and the flags' byte sums in registers and settles the
+    // record once; an item leaving keeps its stale flag bits, which no read reaches)
+    const uint32_t n = S.it_n, high = S.high;
+    uint32_t head = S.it_head, left = 0, gone = 0, sack = 0, lost = 0, retx = 0, cand = 0, nsack = 0;
+    uint32_t b = n ? L.start[head] : 0;
+    while (left < n)
     {
-        const uint32_t b = L.beg(0), e = L.end(0);
+        const uint32_t nx = head + 1 == L.cap ? 0 : head + 1;
+        const uint32_t e = left + 1 < n ? L.start[nx] : high;
+        const uint8_t f = L.flags_at(head);
+        const uint32_t len = ack < e ? (ack > b ? ack - b : 0) : e - b; // (whole, or the acknowledged part)
+        sack += (f & FL_SACK) ? len : 0;
+        lost += (f & FL_LOST) ? len : 0;
+        retx += (f & FL_RETX) ? len : 0;
+        cand += SentList::candidate(f) ? len : 0;
         if (ack < e)
         {
             if (ack > b)
-            {
-                const uint8_t f = L.flags(0);
-                const uint32_t cut = ack - b;
-                if (f & FL_SACK)
-                    S.sack_b -= cut;
-                if (f & FL_LOST)
-                    S.lost_b -= cut;
-                if (f & FL_RETX)
-                    S.rtx_b -= cut;
-                if (SentList::candidate(f))
-                    S.cand_b -= cut;
-                L.start[L.pos(0)] = ack;
-            }
+                L.start[head] = ack;
             break;
         }
-        L.mark(0, 0);
-        gone += e - b;
+        nsack += (f & FL_SACK) ? 1 : 0;
+        gone += len;
         left++;
-        S.it_head = L.pos(1);
-        S.it_n--;
+        head = nx;
+        b = e;
     }
+    S.sack_b -= sack;
+    S.lost_b -= lost;
+    S.rtx_b -= retx;
+    S.cand_b -= cand;
+    S.sack_n -= nsack;
+    S.it_head = head;
+    S.it_n = n - left;
     S.cand_lo = S.cand_lo > left ? S.cand_lo - left : 0;
     S.una = ack;
     if (S.it_n && (L.flags(0) & FL_SACK))
