@@ -1341,6 +1341,9 @@ int tb_run(tb_ctx *ctx, long long max_slots)
                 ctl.prof_phase[4] / 1e3 / n, ctl.prof_phase[5] / 1e3 / n, ctl.prof_phase[6] / 1e3 / n, ctl.prof_phase[7] / 1e3 / n);
         fprintf(stderr, "profile: host events split (us per slot, summed): egress advance %.2f arrivals %.2f timers+starts %.2f\n",
                 ctl.prof_phase[8] / 1e3 / n, ctl.prof_phase[9] / 1e3 / n, ctl.prof_phase[10] / 1e3 / n);
+        fprintf(stderr, "profile: switch ingress split (us per slot, summed): staging %.2f spraying draws %.2f; "
+                        "switch slots merged by keys %.0f, by the argmin %.0f\n",
+                ctl.prof_phase[11] / 1e3 / n, ctl.prof_phase[12] / 1e3 / n, ctl.prof_phase[13] / 1e3, ctl.prof_phase[14] / 1e3);
     }
 #endif
     std::vector<unsigned long long> ev(EV_N);

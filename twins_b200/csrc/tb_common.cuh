@@ -242,11 +242,60 @@ TB_HDI double rand_u01(Rng &r)
     r.s[5] = p2;
     return p1 > p2 ? (p1 - p2) * norm : (p1 - p2 + m1) * norm;
 }
-// UniformRandomVariable::GetInteger(0, n - 1)
-TB_HDI uint32_t rand_int(Rng &r, uint32_t n)
+// UniformRandomVariable::GetInteger(0, n - 1) of an output u
+TB_HDI uint32_t int_of_u01(double u, uint32_t n) { return (uint32_t)(0.0 + u * ((double)(n - 1) + 1.0 - 0.0)); }
+TB_HDI uint32_t rand_int(Rng &r, uint32_t n) { return int_of_u01(rand_u01(r), n); }
+
+// Look-ahead of the stream. Each component is a linear recurrence modulo its m
+// (x_n = 1403580 x_{n-2} - 810728 x_{n-3} mod m1; y_n = 527612 y_{n-1} - 1370589 y_{n-3} mod m2) over the
+// state (x_{-2}, x_{-1}, x_0, y_{-2}, y_{-1}, y_0), so the value the m-th draw from a state computes
+// is a fixed combination of the three state values of its component: x_m = R_m . (x_{-2}, x_{-1}, x_0)
+// mod m1, R_m = -810728 R_{m-3} + 1403580 R_{m-2} from R_{-2,-1,0} = the unit rows (likewise y).
+// The table holds R_m of both components for m = 1..RNG_AHEAD; with them the draws of a slot are
+// computed independently of one another, each from its place in the draw order.
+constexpr int RNG_AHEAD = 384; // (a switch slot's staged arrivals at most)
+constexpr uint64_t RNG_M1 = 4294967087ull, RNG_M2 = 4294944443ull;
+struct RngAhead
 {
-    double u = rand_u01(r);
-    return (uint32_t)(0.0 + u * ((double)(n - 1) + 1.0 - 0.0));
+    uint32_t r[RNG_AHEAD + 1][6]; // [m][x: 0..2, y: 3..5]; m = 0 unused
+};
+constexpr RngAhead make_rng_ahead()
+{
+    RngAhead t{};
+    // a[c][d]: component c's coefficient of the value d steps back (d = 1, 2, 3), reduced into [0, m)
+    const uint64_t mod[2] = {RNG_M1, RNG_M2};
+    const uint64_t a[2][3] = {{0, 1403580, RNG_M1 - 810728}, {527612, 0, RNG_M2 - 1370589}};
+    for (int c = 0; c < 2; c++)
+    {
+        uint64_t w[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}}; // R_{m-3}, R_{m-2}, R_{m-1}
+        for (int m = 1; m <= RNG_AHEAD; m++)
+        {
+            uint64_t nr[3] = {0, 0, 0};
+            for (int e = 0; e < 3; e++)
+                nr[e] = (a[c][2] * w[0][e] % mod[c] + a[c][1] * w[1][e] % mod[c] + a[c][0] * w[2][e] % mod[c]) % mod[c];
+            for (int e = 0; e < 3; e++)
+            {
+                w[0][e] = w[1][e];
+                w[1][e] = w[2][e];
+                w[2][e] = nr[e];
+                t.r[m][3 * c + e] = (uint32_t)nr[e];
+            }
+        }
+    }
+    return t;
+}
+// one component's value m draws ahead (row: R_m of that component; s: its three state values)
+template <uint64_t M>
+TB_HDI double rng_ahead_value(const uint32_t *row, const double *s)
+{
+    const uint64_t v = (uint64_t)row[0] * (uint64_t)s[0] % M + (uint64_t)row[1] * (uint64_t)s[1] % M + (uint64_t)row[2] * (uint64_t)s[2] % M;
+    return (double)(v % M);
+}
+// the output of RandU01 from the two components' new values (its last line)
+TB_HDI double u01_of(double p1, double p2)
+{
+    const double m1 = 4294967087.0, norm = 1.0 / (4294967087.0 + 1.0);
+    return p1 > p2 ? (p1 - p2) * norm : (p1 - p2 + m1) * norm;
 }
 
 // ------------------------------------------------------------------ Time::GetSeconds()

@@ -47,7 +47,140 @@ __device__ __forceinline__ unsigned ld_gen(const unsigned *p)
 
 __device__ __forceinline__ void prefetch_l1(const void *p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
 
-// Per-packet spraying's draws with staged frames: the merged arrival order by a warp-wide argmin.
+// the stream's look-ahead rows (tb_common.cuh), in global memory, read through the read-only path
+__device__ const RngAhead g_rng_ahead = make_rng_ahead();
+
+// Per-packet spraying's draws with staged frames: the merged arrival order, then the draws. Each
+// frame's (time, longer first) is one 32-bit key (its offset in the slot, 21 bits; 2047 - its
+// length, 11 bits), so a merge step is one warp-wide minimum of the ports' head keys; frames that tie
+// on the key are ordered by lane 0 exactly as the serial merge (sw_phase_spray) orders them, scanning
+// the tied ports in port order. The merge only records the order: a prefix over it gives each
+// drawing frame its place among the slot's draws, and every draw is then computed at once, from the
+// stream's state and the look-ahead rows. Returns false, having written nothing but the warp's
+// scratch, when a frame's key does not fit (the argmin merge below then runs). The scratch: the
+// windows' flat starts in base (phase 5 writes it afterwards); keys, then places, in the egress
+// sources region; the merge order and each frame's draw kind in the egress times region.
+__device__ bool sw_spray_keyed(const SwCtx &x, SwShared &sh, int lane, unsigned &ties)
+{
+    const unsigned FULL = 0xffffffffu;
+    const int k = x.sr->k;
+    const WorldDesc &wd = *x.wd;
+    const int64_t S0 = x.t * SLOT_PS;
+    const Input in = input_of(x, sh, lane < k ? lane : 0);
+    const int c = lane < k ? in.count() : 0;
+    int incl = c;
+    for (int o = 1; o < 32; o <<= 1)
+    {
+        const int v = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o)
+            incl += v;
+    }
+    const int total = __shfl_sync(FULL, incl, 31), base = incl - c;
+    if (total == 0)
+        return true;
+    if (total > RNG_AHEAD)
+        return false;
+    uint32_t *key = sh.eref();                            // [total]: keys, then places
+    int *ord = reinterpret_cast<int *>(sh.ets());         // [total]: flat frames in merge order
+    int *kind = reinterpret_cast<int *>(sh.ets()) + sh.cap; // [total]: 0 port down, 1 no routes (0 written), nr + 1
+    if (lane < k)
+        sh.base[lane] = base;
+    bool bad = false;
+    for (int j = 0; j < c; j++)
+    {
+        const Frame &f = *in.at(j);
+        const int64_t off = f.ts - S0;
+        bad |= off < 0 || off >= (1 << 21) || f.len > 2047;
+        key[base + j] = (uint32_t)off << 11 | (uint32_t)(2047 - f.len);
+        const int ep = wd.n_fail ? epoch_of(wd, f.ts) : 0;
+        kind[base + j] = port_down(wd, x.sr->local, lane, ep) ? 0 : 1 + routes_to(wd, x.sr->local, f.dst, ep);
+    }
+    if (__any_sync(FULL, bad))
+        return false;
+    __syncwarp();
+    int pos = 0;
+    uint32_t head = c ? key[base] : 0xFFFFFFFFu;
+    for (int r = 0; r < total; r++)
+    {
+        const uint32_t m = __reduce_min_sync(FULL, head);
+        const unsigned cand = __ballot_sync(FULL, head == m);
+        int best = __ffs(cand) - 1;
+        if (cand & (cand - 1))
+        {
+            // equal times and lengths: the upstream chains, then the connection id
+            const Frame *bf = nullptr;
+            for (unsigned cc = cand; cc; cc &= cc - 1)
+            {
+                const int q = __ffs(cc) - 1;
+                const int pq = __shfl_sync(FULL, pos, q);
+                if (lane == 0)
+                {
+                    const Frame *f = input_of(x, sh, q).at(pq);
+                    if (!bf || frame_before(*f, *bf, ties))
+                    {
+                        best = q;
+                        bf = f;
+                    }
+                }
+            }
+            best = __shfl_sync(FULL, best, 0);
+        }
+        if (lane == best)
+        {
+            ord[r] = base + pos;
+            pos++;
+            head = pos < c ? key[base + pos] : 0xFFFFFFFFu;
+        }
+    }
+    __syncwarp();
+    // places among the draws: an exclusive prefix of the drawing frames in merge order
+    int run = 0;
+    for (int r0 = 0; r0 < total; r0 += 32)
+    {
+        const int r = r0 + lane, i = r < total ? ord[r] : 0, v = r < total && kind[i] >= 2;
+        int sc = v;
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            const int u = __shfl_up_sync(FULL, sc, o);
+            if (lane >= o)
+                sc += u;
+        }
+        if (r < total)
+            key[i] = run + sc - v;
+        run += __shfl_sync(FULL, sc, 31);
+    }
+    __syncwarp();
+    const Rng st = x.s->sw_rng[x.sw];
+    for (int i = lane; i < total; i += 32)
+    {
+        const int v = kind[i];
+        if (v == 0)
+            continue;
+        int q = 0;
+        while (q + 1 < k && sh.base[q + 1] <= i)
+            q++;
+        uint8_t u = 0;
+        if (v >= 2)
+        {
+            const uint32_t *row = g_rng_ahead.r[key[i] + 1];
+            u = (uint8_t)int_of_u01(u01_of(rng_ahead_value<RNG_M1>(row, st.s), rng_ahead_value<RNG_M2>(row + 3, st.s + 3)), (uint32_t)(v - 1));
+        }
+        x.s->sw_up[x.scratch + (size_t)q * 2 * MAX_TX + (i - sh.base[q])] = u;
+    }
+    // the stream after the slot's draws: each component's last three values
+    __syncwarp(); // (every lane has read the stream)
+    if (lane < 6)
+    {
+        const int cmp = lane / 3, m = run - 2 + lane % 3;
+        const uint32_t *row = g_rng_ahead.r[m > 0 ? m : 1] + 3 * cmp;
+        x.s->sw_rng[x.sw].s[lane] = m <= 0 ? st.s[3 * cmp + m + 2]
+                                           : (cmp ? rng_ahead_value<RNG_M2>(row, st.s + 3) : rng_ahead_value<RNG_M1>(row, st.s));
+    }
+    return true;
+}
+
+// Per-packet spraying's draws with staged frames whose keys do not fit (sw_spray_keyed): the merged
+// arrival order by a warp-wide argmin of (time, length), one draw after another.
 // Lane q holds port q's next frame; the minimum (time, longer first) wins; frames that tie on
 // both are ordered by lane 0 exactly as the serial merge (sw_phase_spray) orders them, scanning
 // the tied ports in port order. Lane 0 keeps the switch's random stream and draws.
@@ -306,14 +439,32 @@ __device__ bool switch_step(const Sim &s, int sw, int64_t gt, int lane, SwShared
     if (on)
         pk = sw_phase_window(x, sh, lane);
     __syncwarp();
+#ifdef TB_PROFILE
+    unsigned long long sp2 = globaltimer();
+    if (lane == 0)
+        atomicAdd(&s.ctl->prof_phase[11], sp2 - sp0);
+#endif
     if (x.spray)
     {
         if (sh.staged)
-            sw_phase_spray_warp(x, sh, lane, my_ties);
+        {
+            const bool keyed = sw_spray_keyed(x, sh, lane, my_ties);
+#ifdef TB_PROFILE
+            if (lane == 0)
+                atomicAdd(&s.ctl->prof_phase[keyed ? 13 : 14], 1000ull);
+#endif
+            if (!keyed)
+                sw_phase_spray_warp(x, sh, lane, my_ties);
+        }
         else if (lane == 0)
             sw_phase_spray(x, sh, my_ties);
         __syncwarp();
     }
+#ifdef TB_PROFILE
+    unsigned long long sp3 = globaltimer();
+    if (lane == 0)
+        atomicAdd(&s.ctl->prof_phase[12], sp3 - sp2);
+#endif
     if (on)
         drops += sw_phase_count(x, sh, lane);
     __syncwarp();

@@ -171,7 +171,7 @@ struct SlotCtl
     // TB_PROFILE builds: per-slot maxima of a host unit's and a switch unit's time, summed over
     // slots, the slots' own time, and host / switch phase times (ns, the GPU's global timer)
     unsigned long long prof_host_max, prof_sw_max, prof_host_sum, prof_sw_sum, prof_slot_sum, prof_release;
-    unsigned long long prof_phase[12];
+    unsigned long long prof_phase[16];
 };
 
 // Per world: the slot rule of the reference's ticket block (src/kernel.cuh:79-112) applied to each

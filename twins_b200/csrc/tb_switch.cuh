@@ -205,8 +205,8 @@ TB_D uint32_t *sw_ref_of(const SwCtx &x, SwShared &sh) { return sh.staged ? sh.e
 
 // phase 2 (one lane): per-packet ECMP draws, one per forwarded packet in the order the packets
 // arrive at the node (all ports merged), from the switch's MRG32k3a stream. (With staged frames
-// the warp does this with a warp-wide argmin, sw_phase_spray_warp in tb_kernel.cu, in the same
-// order.)
+// the warp merges 32-bit keys and computes the draws at once from the stream's look-ahead,
+// sw_spray_keyed in tb_kernel.cu, in the same order and with the same values.)
 TB_D void sw_phase_spray(const SwCtx &x, const SwShared &sh, unsigned &ties)
 {
     const int k = x.sr->k;
