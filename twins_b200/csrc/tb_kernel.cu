@@ -276,6 +276,153 @@ __device__ __forceinline__ void host_report(const Sim &s, int w, int64_t t0, boo
         atomicAdd(&wc->fdone, done);
 }
 
+// host_step's timer scan on the whole warp: the timers of the host's active connections due before
+// E0, in host_step's order (senders' retransmission then SYN timers, then receivers' delayed-ACK,
+// SYN, last-ACK and FIN timers, each list in its order), the first DUE_CAP of them into `due`; the
+// count kept is returned (every lane), the count left out goes to *ovf.
+__device__ int collect_due_warp(const Sim &s, const HostRec &hr, int h, int64_t E0, int lane, Due *due, int *ovf)
+{
+    const unsigned FULL = 0xffffffffu;
+    const int *as = s.act_snd + (size_t)h * s.act_cap, *ar = s.act_rcv + (size_t)h * s.act_cap;
+    const int ns = hr.n_snd, nr = hr.n_rcv;
+    int n = 0;
+    auto place = [&](int cnt) {
+        int incl = cnt;
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            const int v = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o)
+                incl += v;
+        }
+        const int at = n + incl - cnt;
+        n += __shfl_sync(FULL, incl, 31);
+        return at;
+    };
+    for (int i0 = 0; i0 < ns; i0 += 32)
+    {
+        const int i = i0 + lane;
+        int f = 0;
+        int64_t v[2] = {-1, -1};
+        if (i < ns)
+        {
+            f = as[i];
+            v[0] = s.snd[f].rto_at;
+            v[1] = s.snd[f].syn_at;
+        }
+        const int kinds[2] = {0, 2};
+        int at = place((v[0] >= 0 && v[0] < E0) + (v[1] >= 0 && v[1] < E0));
+        for (int j = 0; j < 2; j++)
+            if (v[j] >= 0 && v[j] < E0)
+            {
+                if (at < DUE_CAP)
+                    due[at] = {v[j], f, kinds[j]};
+                at++;
+            }
+    }
+    for (int i0 = 0; i0 < nr; i0 += 32)
+    {
+        const int i = i0 + lane;
+        int f = 0;
+        int64_t v[4] = {-1, -1, -1, -1};
+        if (i < nr)
+        {
+            f = ar[i];
+            const RcvRec &R = s.rcv[f];
+            v[0] = R.delack_at;
+            v[1] = R.syn_at;
+            v[2] = R.last_at;
+            v[3] = R.frx_at;
+        }
+        const int kinds[4] = {1, 3, 4, 5};
+        int cnt = 0;
+        for (int j = 0; j < 4; j++)
+            cnt += v[j] >= 0 && v[j] < E0;
+        int at = place(cnt);
+        for (int j = 0; j < 4; j++)
+            if (v[j] >= 0 && v[j] < E0)
+            {
+                if (at < DUE_CAP)
+                    due[at] = {v[j], f, kinds[j]};
+                at++;
+            }
+    }
+    *ovf = n > DUE_CAP ? n - DUE_CAP : 0;
+    return n < DUE_CAP ? n : DUE_CAP;
+}
+
+// host_step's last phase on the whole warp: the host's finished connections leave its active
+// lists (the others keep their order; lanes read a chunk of 32 entries, then write the kept ones
+// back at or below it) and the earliest timer of the connections that stay is returned (every
+// lane). The host's lists and counts are those its lane 0 has just written.
+__device__ int64_t prune_lists_warp(const Sim &s, int h, int lane)
+{
+    const unsigned FULL = 0xffffffffu, below = (1u << lane) - 1;
+    HostRec &hr = s.hosts[h];
+    int *as = s.act_snd + (size_t)h * s.act_cap, *ar = s.act_rcv + (size_t)h * s.act_cap;
+    int64_t next = INT64_MAX;
+    const int ns = hr.n_snd, nr = hr.n_rcv;
+    int k = 0;
+    for (int i0 = 0; i0 < ns; i0 += 32)
+    {
+        const int i = i0 + lane;
+        int f = 0;
+        bool keep = false;
+        if (i < ns)
+        {
+            f = as[i];
+            const SndRec &S = s.snd[f];
+            keep = S.st != S_DONE;
+            if (keep && S.rto_at >= 0 && S.rto_at < next)
+                next = S.rto_at;
+            if (keep && S.syn_at >= 0 && S.syn_at < next)
+                next = S.syn_at;
+        }
+        const unsigned m = __ballot_sync(FULL, keep);
+        __syncwarp(); // (every lane has read its entry)
+        if (keep)
+            as[k + __popc(m & below)] = f;
+        k += __popc(m);
+    }
+    const int ks = k;
+    k = 0;
+    for (int i0 = 0; i0 < nr; i0 += 32)
+    {
+        const int i = i0 + lane;
+        int f = 0;
+        bool keep = false;
+        if (i < nr)
+        {
+            f = ar[i];
+            const RcvRec &R = s.rcv[f];
+            keep = !rcv_idle_for_good(R);
+            if (keep)
+            {
+                const int64_t v[4] = {R.delack_at, R.syn_at, R.last_at, R.frx_at};
+                for (int j = 0; j < 4; j++)
+                    if (v[j] >= 0 && v[j] < next)
+                        next = v[j];
+            }
+        }
+        const unsigned m = __ballot_sync(FULL, keep);
+        __syncwarp();
+        if (keep)
+            ar[k + __popc(m & below)] = f;
+        k += __popc(m);
+    }
+    for (int o = 16; o > 0; o >>= 1)
+    {
+        const int64_t v = __shfl_xor_sync(FULL, next, o);
+        next = v < next ? v : next;
+    }
+    __syncwarp(); // (every lane has read the counts)
+    if (lane == 0)
+    {
+        hr.n_snd = ks;
+        hr.n_rcv = k;
+    }
+    return next;
+}
+
 // A host unit at launch slot t: one host per warp (host_lanes 1) or one per lane. With one host
 // per warp, the warp reads the host's link-message tags (by launch slot) together with its world's
 // rule; a host whose world does not run this slot, or that has no frame arriving, no timer due and
@@ -290,10 +437,11 @@ template <bool MANY>
 __device__ __forceinline__ void host_unit(const Sim &s, int h0, int nh, int64_t t, int lane, SwShared &sh, unsigned &ties,
                                           unsigned *done_sink)
 {
-    int h, w = 0, n2 = -1, n1 = -1;
+    int h, w = 0, n2 = -1, n1 = -1, due_n = 0, due_ovf = 0;
     int64_t t0 = 0;
     bool run = false;
     const Frame *stage = nullptr;
+    Due *due = nullptr;
     if constexpr (!MANY)
     {
         h = h0;
@@ -349,11 +497,19 @@ __device__ __forceinline__ void host_unit(const Sim &s, int h0, int nh, int64_t 
                 at -= s.ring;
             prefetch_l1(&s.host_ring[(size_t)h * s.ring + at]);
         }
-        const int *as = s.act_snd + (size_t)h * s.act_cap, *ar = s.act_rcv + (size_t)h * s.act_cap;
-        for (int i = lane; i < hr.n_snd; i += 32)
-            prefetch_l1(&s.snd[as[i]].rto_at);
-        for (int i = lane; i < hr.n_rcv; i += 32)
-            prefetch_l1(&s.rcv[ar[i]].delack_at);
+        if (sh.cap * (int)(sizeof(int64_t) + sizeof(uint32_t)) >= DUE_CAP * (int)sizeof(Due))
+        {
+            due = reinterpret_cast<Due *>(sh.ets()); // (the egress regions, unused by a host)
+            due_n = collect_due_warp(s, hr, h, (t - t0 + 1) * SLOT_PS, lane, due, &due_ovf);
+        }
+        else
+        {
+            const int *as = s.act_snd + (size_t)h * s.act_cap, *ar = s.act_rcv + (size_t)h * s.act_cap;
+            for (int i = lane; i < hr.n_snd; i += 32)
+                prefetch_l1(&s.snd[as[i]].rto_at);
+            for (int i = lane; i < hr.n_rcv; i += 32)
+                prefetch_l1(&s.rcv[ar[i]].delack_at);
+        }
         __syncwarp();
         stage = staged ? sh.fr() : nullptr;
         run = lane == 0;
@@ -388,15 +544,30 @@ __device__ __forceinline__ void host_unit(const Sim &s, int h0, int nh, int64_t 
             }
         }
     }
+    int64_t wake = INT64_MAX;
+    unsigned done = 0;
+    bool act = false;
     if (run)
     {
-        int64_t wake = INT64_MAX;
-        unsigned done = 0;
-        const bool act = host_step(s, h, t - t0, t, &wake, &ties, &done, stage, n2, n1);
-        host_report(s, w, t0, act, wake, done);
-        if (done)
-            atomicAdd(done_sink, done);
+        act = host_step(s, h, t - t0, t, &wake, &ties, &done, stage, n2, n1, !MANY, due, due_n, due_ovf);
+        if constexpr (MANY)
+            host_report(s, w, t0, act, wake, done);
     }
+    if constexpr (!MANY)
+    {
+        // the whole warp prunes the host's active lists; the earliest timer left bounds the wake-up
+        __syncwarp();
+        const int64_t nt = prune_lists_warp(s, h, lane);
+        if (lane == 0)
+        {
+            HostRec &hr = s.hosts[h];
+            if (hr.q_size == 0 && nt != INT64_MAX && nt / SLOT_PS < hr.wake)
+                hr.wake = nt / SLOT_PS;
+            host_report(s, w, t0, act, hr.wake, done);
+        }
+    }
+    if (run && done)
+        atomicAdd(done_sink, done);
     __syncwarp(); // (the staging area is reused by the warp's next unit)
 }
 

@@ -45,8 +45,14 @@ TB_D bool rcv_idle_for_good(const RcvRec &R)
 // `stage`: the host's link messages of slots gt-2 and gt-1 copied to shared memory by its warp
 // (msg[gt-2] then msg[gt-1], n2 and n1 frames as their tags count), or null to read them in place
 // (n2, n1 < 0: read the tags).
+// prune_later: the active lists are left unpruned and *wake counts only the host's queue and its
+// next application start; the caller prunes them (prune_lists_warp) and lowers the wake-up to the
+// earliest timer of the connections that stay. `due`: the timers due in the slot, already collected
+// in this function's scan order (the first DUE_CAP of them; due_ovf more were left out), or null
+// to scan the active lists here.
 TB_D bool host_step(const Sim &s, int h, int64_t t, int64_t gt, int64_t *wake, unsigned *ties_out, unsigned *done_out,
-                    const Frame *stage = nullptr, int n2 = -1, int n1 = -1)
+                    const Frame *stage = nullptr, int n2 = -1, int n1 = -1, bool prune_later = false, const Due *due = nullptr,
+                    int due_n = 0, int due_ovf = 0)
 {
     const int64_t S0 = t * SLOT_PS, E0 = S0 + SLOT_PS;
     TB_PHASE_START
@@ -106,7 +112,14 @@ TB_D bool host_step(const Sim &s, int h, int64_t t, int64_t gt, int64_t *wake, u
     const int ns = hr.n_snd, nr = hr.n_rcv;
     c.nd = 0;
     c.di = 0;
-    for (int i = 0; i < ns; i++)
+    if (due)
+    {
+        for (int i = 0; i < due_n; i++)
+            c.due[i] = due[i];
+        c.nd = due_n;
+        c.ovf += due_ovf;
+    }
+    for (int i = 0; i < (due ? 0 : ns); i++)
     {
         int f = act_snd[i];
         const SndRec &S = s.snd[f];
@@ -126,7 +139,7 @@ TB_D bool host_step(const Sim &s, int h, int64_t t, int64_t gt, int64_t *wake, u
                 c.ovf++;
         }
     }
-    for (int i = 0; i < nr; i++)
+    for (int i = 0; i < (due ? 0 : nr); i++)
     {
         int f = act_rcv[i];
         const RcvRec &R = s.rcv[f];
@@ -244,6 +257,7 @@ TB_D bool host_step(const Sim &s, int h, int64_t t, int64_t gt, int64_t *wake, u
     TB_PHASE(3)
     // drop finished connections from the active lists; the next wake-up
     int64_t next = INT64_MAX;
+    if (!prune_later)
     {
         int k = 0, n = hr.n_snd;
         for (int i = 0; i < n; i++)
@@ -260,6 +274,7 @@ TB_D bool host_step(const Sim &s, int h, int64_t t, int64_t gt, int64_t *wake, u
         }
         hr.n_snd = k;
     }
+    if (!prune_later)
     {
         int k = 0, n = hr.n_rcv;
         for (int i = 0; i < n; i++)
