@@ -776,7 +776,7 @@ def main():
     alg = algorithmic_bytes(stats)
     achieved = alg / (ms / 1000.0) / 1e9
     traffic = None
-    tfile = ROOT / "profiles" / "slot_kernel_traffic.json"
+    tfile = ROOT / "profiles" / "free_kernel_traffic.json"
     if tfile.exists():
         try:
             tj = json.loads(tfile.read_text())
