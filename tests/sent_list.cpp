@@ -156,5 +156,77 @@ int main()
         }
     }
     puts("sent list: all agree");
+    // the RTT history: first sends, retransmissions (some reaching past the next entry), ACKs,
+    // against a list scanned from the oldest entry every time
+    for (int trial = 0; trial < 3000; trial++)
+    {
+        const uint32_t cap = 8 * (1 + g() % 6);
+        std::vector<uint32_t> lo(cap), hi(cap);
+        std::vector<int64_t> at(cap);
+        Sim s{};
+        s.h_seq = lo.data();
+        s.h_end = hi.data();
+        s.h_t = at.data();
+        SndRec S{};
+        S.it_cap = cap;
+        S.h_head = g() % cap;
+        S.srtt = 0;
+        struct E
+        {
+            uint32_t lo, hi;
+            int64_t at;
+        };
+        std::vector<E> m;
+        uint32_t high = 1000, una = 1000;
+        unsigned ovf = 0;
+        for (int op = 0; op < 200; op++)
+        {
+            RttLog log(s, S);
+            const int k = (int)(g() % 10);
+            if (k < 4)
+            {
+                const uint32_t len = 1 + g() % 1500;
+                log.first_send(high, len, op, ovf);
+                if (m.size() < cap)
+                    m.push_back(E{high, high + len, op});
+                high += len;
+            }
+            else if (k < 8 && high > una)
+            {
+                const uint32_t seq = una + g() % (high - una), len = 1 + g() % (g() % 4 ? 1500 : 6000);
+                log.resend(seq, len);
+                for (auto &e : m)
+                    if (seq >= e.lo && seq < e.hi)
+                    {
+                        e.hi = seq + len;
+                        if (e.at >= 0)
+                            e.at = ~e.at;
+                        break;
+                    }
+            }
+            else if (high > una)
+            {
+                una += g() % (high - una + 1);
+                log.acked(una, op);
+                while (!m.empty() && m[0].hi <= una)
+                    m.erase(m.begin());
+            }
+            if (S.h_n != m.size())
+            {
+                printf("rtt history trial %d op %d: %u entries, model %zu\n", trial, op, S.h_n, m.size());
+                return 1;
+            }
+            for (uint32_t j = 0; j < S.h_n; j++)
+            {
+                const uint32_t x = (S.h_head + j) % cap;
+                if (lo[x] != m[j].lo || hi[x] != m[j].hi || at[x] != m[j].at)
+                {
+                    printf("rtt history trial %d op %d: entry %u differs\n", trial, op, j);
+                    return 1;
+                }
+            }
+        }
+    }
+    puts("rtt history: all agree");
     return 0;
 }

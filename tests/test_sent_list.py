@@ -2,7 +2,8 @@
 mirrors random opens (appends and splits), joins, flag changes and whole-list losses on a plain
 per-item model and checks every item's flags, the byte counters, the sacked-item count and the
 candidate search bound after each step, on rings whose head lies anywhere (shifts that wrap); ACKs
-that drop and cut items too. tests/rng_ahead.cpp, over twins_b200/csrc/tb_common.cuh, checks the
+that drop and cut items too; then the RTT history's first sends, retransmissions and ACKs against
+a list scanned from its oldest entry. tests/rng_ahead.cpp, over twins_b200/csrc/tb_common.cuh, checks the
 random stream's look-ahead table (the spraying draws of a switch slot computed out of order) against
 the stream drawn one value at a time."""
 import shutil
